@@ -1,0 +1,626 @@
+// fs_fcm.cu -- Force Coupling Method mobility solve on sm_100a.
+//
+// Replaces Fcm::mobility_solve (FCMfunctions.cpp:175-464):
+//   1. k_fcm_bin_keys + counting sort: beads binned by the 16-point tile that
+//      holds the start of their Gaussian stencil (gaussian_setup's index rule,
+//      FCMfunctions.cpp:565-589).
+//   2. k_spread: one CTA per 16^3 grid tile gathers the monopole + rotlet
+//      Gaussians of every bead whose stencil reaches the tile
+//      (mono_and_dipole_force_distribution, :596-646). Each warp owns one
+//      x-plane of the tile in shared memory, so every grid point is written by
+//      one warp in bead order: no atomics, bit-reproducible.
+//   3. cuFFT R2C (batched x3), 4. k_project / k_project_planes: the Stokes
+//      projection of flow_solve (:648-736), 5. cuFFT C2R (batched x3).
+//   6. k_interp: one warp per bead (in spread-bin order for L2 locality)
+//      reduces U and Omega over the stencil (particle_velocities :740-770,
+//      particle_rotations :774-808) with warp shuffles.
+// FP64 mode follows the reference arithmetic; FP32 mode keeps grids, FFTs and
+// weights in float with Kahan-compensated tile and warp sums.
+#include "fs_internal.cuh"
+
+namespace {
+
+struct FcmConsts {
+  int N[3];
+  int ngd, ngdh;
+  int nbin[3];
+  double dx;
+  double anorm, anorm2, anormdip, anormdip2, sigmadipsq;
+};
+
+__host__ __device__ inline int wrap_int(int x, int n) {
+  int r = x % n;
+  return r < 0 ? r + n : r;
+}
+
+// ---- 1. binning -------------------------------------------------------------
+__global__ void k_fcm_bin_keys(const double *__restrict__ Y, int np, FcmConsts c, int *__restrict__ key) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= np) return;
+  int bi[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    int xc = (int)(Y[3 * b + d] / c.dx);
+    int sw = wrap_int(xc - c.ngdh + 1, c.N[d]);
+    bi[d] = sw / FS_TILE;
+  }
+  key[b] = (bi[0] * c.nbin[1] + bi[1]) * c.nbin[2] + bi[2];
+}
+
+// ---- 2. spread ----------------------------------------------------------------
+template <typename R>
+struct SpreadChunk {
+  R gx[FS_SPREAD_CHUNK][16], dgx[FS_SPREAD_CHUNK][16], rx[FS_SPREAD_CHUNK][16];  // x by stencil index i
+  R gy[FS_SPREAD_CHUNK][16], dgy[FS_SPREAD_CHUNK][16], ry[FS_SPREAD_CHUNK][16];  // y compacted to the tile
+  R gz[FS_SPREAD_CHUNK][16], dgz[FS_SPREAD_CHUNK][16], rz[FS_SPREAD_CHUNK][16];  // z compacted to the tile
+  R f[FS_SPREAD_CHUNK][3];   // force
+  R th[FS_SPREAD_CHUNK][3];  // half torque (0.5 T)
+  unsigned char ly[FS_SPREAD_CHUNK][16], lz[FS_SPREAD_CHUNK][16];
+  int ax[FS_SPREAD_CHUNK];   // (X0 - stencil start) mod N
+  int cy[FS_SPREAD_CHUNK], cz[FS_SPREAD_CHUNK];
+  int bead[FS_SPREAD_CHUNK];
+};
+
+template <typename R>
+struct SpreadAcc;
+template <>
+struct SpreadAcc<double> {
+  double v[3][FS_TILE][FS_TILE][FS_TILE];
+  __device__ void add(int c, int x, int y, int z, double val) { v[c][x][y][z] += val; }
+  __device__ double result(int c, int x, int y, int z) const { return v[c][x][y][z]; }
+  __device__ void zero(int t, int nt) {
+    double *p = &v[0][0][0][0];
+    for (int i = t; i < 3 * FS_TILE * FS_TILE * FS_TILE; i += nt) p[i] = 0.0;
+  }
+};
+template <>
+struct SpreadAcc<float> {
+  float v[3][FS_TILE][FS_TILE][FS_TILE];
+  float cmp[3][FS_TILE][FS_TILE][FS_TILE];  // Kahan compensation
+  __device__ void add(int c, int x, int y, int z, float val) {
+    float s = v[c][x][y][z];
+    float yv = val - cmp[c][x][y][z];
+    float t = s + yv;
+    cmp[c][x][y][z] = (t - s) - yv;
+    v[c][x][y][z] = t;
+  }
+  __device__ float result(int c, int x, int y, int z) const { return v[c][x][y][z] - cmp[c][x][y][z]; }
+  __device__ void zero(int t, int nt) {
+    float *p = &v[0][0][0][0];
+    float *q = &cmp[0][0][0][0];
+    for (int i = t; i < 3 * FS_TILE * FS_TILE * FS_TILE; i += nt) {
+      p[i] = 0.f;
+      q[i] = 0.f;
+    }
+  }
+};
+
+template <typename R>
+struct SpreadSmem {
+  SpreadAcc<R> acc;
+  SpreadChunk<R> ch;
+};
+
+template <typename R>
+__device__ inline R fs_exp(R x);
+template <>
+__device__ inline double fs_exp<double>(double x) { return exp(x); }
+template <>
+__device__ inline float fs_exp<float>(float x) { return expf(x); }
+
+template <typename R>
+__global__ void __launch_bounds__(FS_TILE * 32, 2)
+    k_spread(const double *__restrict__ Y, const double *__restrict__ F, const double *__restrict__ T,
+             const int *__restrict__ bin_start, const int *__restrict__ sorted, FcmConsts c, R *__restrict__ fgrid) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SpreadSmem<R> &sm = *reinterpret_cast<SpreadSmem<R> *>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nthr = blockDim.x;
+  const int tile = blockIdx.x;
+  const int tz = tile % c.nbin[2], ty = (tile / c.nbin[2]) % c.nbin[1], tx = tile / (c.nbin[2] * c.nbin[1]);
+  const int X0[3] = {tx * FS_TILE, ty * FS_TILE, tz * FS_TILE};
+
+  sm.acc.zero(tid, nthr);
+
+  // candidate bins per axis: the tile's own bin and the one before it
+  int cb[3][2], ncb[3];
+  const int tb[3] = {tx, ty, tz};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    cb[d][0] = (tb[d] - 1 + c.nbin[d]) % c.nbin[d];
+    cb[d][1] = tb[d];
+    ncb[d] = (c.nbin[d] > 1 && c.ngd > 1) ? 2 : 1;
+    if (ncb[d] == 1) cb[d][0] = tb[d];
+  }
+  // gather candidate bead ranges (up to 8 bins)
+  int rs[8], re[8], nr = 0;
+  for (int a = 0; a < ncb[0]; ++a)
+    for (int b2 = 0; b2 < ncb[1]; ++b2)
+      for (int e = 0; e < ncb[2]; ++e) {
+        int bin = (cb[0][a] * c.nbin[1] + cb[1][b2]) * c.nbin[2] + cb[2][e];
+        rs[nr] = bin_start[bin];
+        re[nr] = bin_start[bin + 1];
+        nr++;
+      }
+  int total = 0;
+  for (int r = 0; r < nr; ++r) total += re[r] - rs[r];
+  __syncthreads();
+
+  const int ngd = c.ngd;
+  for (int base = 0; base < total; base += FS_SPREAD_CHUNK) {
+    const int nb = min(FS_SPREAD_CHUNK, total - base);
+    // stage: thread per (bead slot, axis, stencil index)
+    for (int it = tid; it < nb * 3 * ngd; it += nthr) {
+      const int s = it / (3 * ngd);
+      const int a = (it / ngd) % 3;
+      const int i = it % ngd;
+      int rank = base + s, r = 0;
+      while (rank >= re[r] - rs[r]) {
+        rank -= re[r] - rs[r];
+        ++r;
+      }
+      const int bead = sorted[rs[r] + rank];
+      const double Yv = Y[3 * bead + a];
+      const int xc = (int)(Yv / c.dx);
+      const int xg = xc - c.ngdh + (i + 1);
+      const double xx = ((double)xg) * c.dx - Yv;
+      R g, gd, rr;
+      if (sizeof(R) == 8) {
+        g = (R)(c.anorm * exp(-xx * xx / c.anorm2));
+        gd = (R)(c.anormdip * exp(-xx * xx / c.anormdip2));
+        rr = (R)(-xx / c.sigmadipsq);
+      } else {
+        const R xf = (R)xx;
+        g = (R)c.anorm * fs_exp<R>(-xf * xf / (R)c.anorm2);
+        gd = (R)c.anormdip * fs_exp<R>(-xf * xf / (R)c.anormdip2);
+        rr = -xf / (R)c.sigmadipsq;
+      }
+      const int Nn = c.N[a];
+      const int sw = wrap_int(xc - c.ngdh + 1, Nn);
+      const int aoff = wrap_int(X0[a] - sw, Nn);
+      if (a == 0) {
+        sm.ch.gx[s][i] = g;
+        sm.ch.dgx[s][i] = gd;
+        sm.ch.rx[s][i] = rr;
+        if (i == 0) {
+          sm.ch.ax[s] = aoff;
+          sm.ch.bead[s] = bead;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            sm.ch.f[s][d] = (R)F[3 * bead + d];
+            sm.ch.th[s][d] = (R)(0.5 * T[3 * bead + d]);
+          }
+        }
+      } else {
+        // compacted position among stencil indices that land in the tile
+        int pos = 0, cnt = 0, mine = -1;
+        for (int i2 = 0; i2 < ngd; ++i2) {
+          int l = wrap_int(i2 - aoff, Nn);
+          if (l < FS_TILE) {
+            if (i2 == i) mine = l;
+            if (i2 < i) pos++;
+            cnt++;
+          }
+        }
+        if (a == 1) {
+          if (mine >= 0) {
+            sm.ch.gy[s][pos] = g;
+            sm.ch.dgy[s][pos] = gd;
+            sm.ch.ry[s][pos] = rr;
+            sm.ch.ly[s][pos] = (unsigned char)mine;
+          }
+          if (i == 0) sm.ch.cy[s] = cnt;
+        } else {
+          if (mine >= 0) {
+            sm.ch.gz[s][pos] = g;
+            sm.ch.dgz[s][pos] = gd;
+            sm.ch.rz[s][pos] = rr;
+            sm.ch.lz[s][pos] = (unsigned char)mine;
+          }
+          if (i == 0) sm.ch.cz[s] = cnt;
+        }
+      }
+    }
+    __syncthreads();
+    // scatter: warp `warp` owns tile x-plane `warp`
+    for (int s = 0; s < nb; ++s) {
+      const int i = wrap_int(warp + sm.ch.ax[s], c.N[0]);
+      if (i < ngd) {
+        const R gxv = sm.ch.gx[s][i], dxv = sm.ch.dgx[s][i], rxv = sm.ch.rx[s][i];
+        const R F0 = sm.ch.f[s][0], F1 = sm.ch.f[s][1], F2 = sm.ch.f[s][2];
+        // g12 = T2/2, g13 = -T1/2, g21 = -T2/2, g23 = T0/2, g31 = T1/2, g32 = -T0/2 (GA_setup, :536-547)
+        const R h0 = sm.ch.th[s][0], h1 = sm.ch.th[s][1], h2 = sm.ch.th[s][2];
+        const int cy = sm.ch.cy[s], cz = sm.ch.cz[s];
+        const int cnt = cy * cz;
+        for (int pidx = lane; pidx < cnt; pidx += 32) {
+          const int jj = pidx / cz, kk = pidx - jj * cz;
+          const R gyv = sm.ch.gy[s][jj], dyv = sm.ch.dgy[s][jj], ryv = sm.ch.ry[s][jj];
+          const R gzv = sm.ch.gz[s][kk], dzv = sm.ch.dgz[s][kk], rzv = sm.ch.rz[s][kk];
+          const R temp = gxv * gyv * gzv;
+          const R temp2 = dxv * dyv * dzv;
+          const int ly = sm.ch.ly[s][jj], lz = sm.ch.lz[s][kk];
+          sm.acc.add(0, warp, ly, lz, F0 * temp + (h2 * ryv - h1 * rzv) * temp2);
+          sm.acc.add(1, warp, ly, lz, F1 * temp + (-h2 * rxv + h0 * rzv) * temp2);
+          sm.acc.add(2, warp, ly, lz, F2 * temp + (h1 * rxv - h0 * ryv) * temp2);
+        }
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+  }
+  // write the tile (each warp its plane; rows of FS_TILE contiguous z)
+  const size_t N = (size_t)c.N[0] * c.N[1] * c.N[2];
+  const int gx = X0[0] + warp;
+  for (int e = lane; e < 3 * FS_TILE * FS_TILE; e += 32) {
+    const int comp = e / (FS_TILE * FS_TILE);
+    const int y = (e / FS_TILE) % FS_TILE;
+    const int z = e % FS_TILE;
+    const size_t m = ((size_t)gx * c.N[1] + (X0[1] + y)) * c.N[2] + (X0[2] + z);
+    fgrid[comp * N + m] = sm.acc.result(comp, warp, y, z);
+  }
+}
+
+// ---- 4. Stokes projection -----------------------------------------------------
+template <typename R>
+struct Cplx;
+template <>
+struct Cplx<double> { typedef double2 T; };
+template <>
+struct Cplx<float> { typedef float2 T; };
+
+template <typename R>
+__device__ inline void project_mode(R q1, R q2, R q3, R a1, R a2, R a3, R total, R &u1, R &u2, R &u3) {
+  const R qq = q2 * q2 + q1 * q1 + (R)1e-18;
+  const R norm = (R)1.0 / (qq + q3 * q3);
+  const R kdotf = (q1 * a1 + q2 * a2 + q3 * a3) * norm;
+  u1 = norm * (a1 - q1 * kdotf) / total;
+  u2 = norm * (a2 - q2 * kdotf) / total;
+  u3 = norm * (a3 - q3 * kdotf) / total;
+}
+
+template <typename R>
+__device__ inline R wavenumber(int i, int n, R ff) {
+  return (R)((i <= n / 2) ? i : i - n) * ff;
+}
+
+// modes with 0 < kz < nz/2 (each stored once in the half spectrum)
+template <typename R>
+__global__ void k_project(typename Cplx<R>::T *__restrict__ fh, size_t NH, int nx, int ny, int nz, int nzh, R ffx,
+                          R ffy, R ffz, R total) {
+  typedef typename Cplx<R>::T C;
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= NH) return;
+  const int k = (int)(idx % nzh);
+  if (k == 0 || 2 * k == nz) return;
+  const int j = (int)((idx / nzh) % ny);
+  const int i = (int)(idx / ((size_t)nzh * ny));
+  const R q1 = wavenumber<R>(i, nx, ffx), q2 = wavenumber<R>(j, ny, ffy), q3 = (R)k * ffz;
+  C a = fh[idx], b = fh[NH + idx], d = fh[2 * NH + idx];
+  C ua, ub, ud;
+  project_mode<R>(q1, q2, q3, a.x, b.x, d.x, total, ua.x, ub.x, ud.x);
+  project_mode<R>(q1, q2, q3, a.y, b.y, d.y, total, ua.y, ub.y, ud.y);
+  fh[idx] = ua;
+  fh[NH + idx] = ub;
+  fh[2 * NH + idx] = ud;
+}
+
+// kz = 0 and kz = nz/2 planes. The reference's inverse real transform uses
+// only the real part of the last axis's DC and Nyquist coefficients after the
+// complex transforms of the other axes, which equals inverting the Hermitian
+// part of these planes: u_sym(i,j) = (u(i,j) + conj(u(-i,-j))) / 2. Writing
+// that exactly Hermitian plane makes the C2R result well defined.
+template <typename R>
+__global__ void k_project_planes(typename Cplx<R>::T *__restrict__ fh, size_t NH, int nx, int ny, int nz, int nzh,
+                                 R ffx, R ffy, R ffz, R total) {
+  typedef typename Cplx<R>::T C;
+  const int ij = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ij >= nx * ny) return;
+  const int kp = blockIdx.y == 0 ? 0 : nz / 2;
+  if (blockIdx.y == 1 && (nz % 2 != 0 || nz / 2 == 0)) return;
+  const int i = ij / ny, j = ij % ny;
+  const int ip = (nx - i) % nx, jp = (ny - j) % ny;
+  const int ijp = ip * ny + jp;
+  if (ijp < ij) return;  // the partner handles the pair
+  const size_t m = (size_t)ij * nzh + kp, mp = (size_t)ijp * nzh + kp;
+  const R q3 = (R)kp * ffz;
+  C u[3], up[3];
+  {
+    const R q1 = wavenumber<R>(i, nx, ffx), q2 = wavenumber<R>(j, ny, ffy);
+    C a = fh[m], b = fh[NH + m], d = fh[2 * NH + m];
+    project_mode<R>(q1, q2, q3, a.x, b.x, d.x, total, u[0].x, u[1].x, u[2].x);
+    project_mode<R>(q1, q2, q3, a.y, b.y, d.y, total, u[0].y, u[1].y, u[2].y);
+  }
+  {
+    const R q1 = wavenumber<R>(ip, nx, ffx), q2 = wavenumber<R>(jp, ny, ffy);
+    C a = fh[mp], b = fh[NH + mp], d = fh[2 * NH + mp];
+    project_mode<R>(q1, q2, q3, a.x, b.x, d.x, total, up[0].x, up[1].x, up[2].x);
+    project_mode<R>(q1, q2, q3, a.y, b.y, d.y, total, up[0].y, up[1].y, up[2].y);
+  }
+  const bool zero_mode = (kp == 0 && ij == 0);
+#pragma unroll
+  for (int cpt = 0; cpt < 3; ++cpt) {
+    C s;
+    s.x = (R)0.5 * (u[cpt].x + up[cpt].x);
+    s.y = (R)0.5 * (u[cpt].y - up[cpt].y);
+    if (zero_mode) s.x = s.y = (R)0;
+    if (ijp == ij) s.y = (R)0;
+    fh[(size_t)cpt * NH + m] = s;
+    if (ijp != ij) {
+      C sc;
+      sc.x = s.x;
+      sc.y = -s.y;
+      fh[(size_t)cpt * NH + mp] = sc;
+    }
+  }
+}
+
+// ---- 6. interpolation -------------------------------------------------------
+template <typename R>
+struct KSum;
+template <>
+struct KSum<double> {
+  double s;
+  __device__ void init() { s = 0.0; }
+  __device__ void add(double v) { s += v; }
+  __device__ double value() const { return s; }
+  __device__ void warp_reduce() {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  }
+};
+template <>
+struct KSum<float> {  // Kahan per lane, TwoSum across lanes
+  float s, c;
+  __device__ void init() { s = 0.f; c = 0.f; }
+  __device__ void add(float v) {
+    float y = v - c;
+    float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+  __device__ double value() const { return (double)s - (double)c; }
+  __device__ void warp_reduce() {
+    double v = (double)s - (double)c;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    s = (float)v;
+    c = (float)((double)s - v);
+  }
+};
+
+template <typename R>
+struct InterpWarp {
+  R g[3][16], gd[3][16], r[3][16];
+  int ind[3][16];
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_interp(const R *__restrict__ u, const double *__restrict__ Y,
+                                                const int *__restrict__ order, int np, FcmConsts c,
+                                                double *__restrict__ V, double *__restrict__ W) {
+  __shared__ InterpWarp<R> sw[8];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int wid = blockIdx.x * 8 + wl;
+  if (wid >= np) return;
+  const int b = order[wid];
+  InterpWarp<R> &s = sw[wl];
+  const int ngd = c.ngd;
+  for (int it = lane; it < 3 * ngd; it += 32) {
+    const int a = it / ngd, i = it % ngd;
+    const double Yv = Y[3 * b + a];
+    const int xc = (int)(Yv / c.dx);
+    const int xg = xc - c.ngdh + (i + 1);
+    s.ind[a][i] = xg - c.N[a] * ((int)floor(((double)xg) / ((double)c.N[a])));
+    const double xx = ((double)xg) * c.dx - Yv;
+    s.g[a][i] = (R)(c.anorm * exp(-xx * xx / c.anorm2));
+    s.gd[a][i] = (R)(c.anormdip * exp(-xx * xx / c.anormdip2));
+    s.r[a][i] = (R)(-xx / c.sigmadipsq);
+  }
+  __syncwarp();
+  const size_t N = (size_t)c.N[0] * c.N[1] * c.N[2];
+  const R *ux = u, *uy = u + N, *uz = u + 2 * N;
+  KSum<R> v0, v1, v2, w0, w1, w2;
+  v0.init(); v1.init(); v2.init(); w0.init(); w1.init(); w2.init();
+  const int ngd2 = ngd * ngd, ngd3 = ngd2 * ngd;
+  for (int p = lane; p < ngd3; p += 32) {
+    const int i = p / ngd2, rem = p - i * ngd2, j = rem / ngd, k = rem - j * ngd;
+    const size_t m = ((size_t)s.ind[0][i] * c.N[1] + s.ind[1][j]) * c.N[2] + s.ind[2][k];
+    const R a0 = ux[m], a1 = uy[m], a2 = uz[m];
+    const R temp = s.g[0][i] * s.g[1][j] * s.g[2][k];
+    const R tempd = s.gd[0][i] * s.gd[1][j] * s.gd[2][k];
+    const R xx = s.r[0][i], yy = s.r[1][j], zz = s.r[2][k];
+    v0.add(a0 * temp);
+    v1.add(a1 * temp);
+    v2.add(a2 * temp);
+    w0.add((a2 * yy - a1 * zz) * tempd);
+    w1.add((a0 * zz - a2 * xx) * tempd);
+    w2.add((a1 * xx - a0 * yy) * tempd);
+  }
+  v0.warp_reduce(); v1.warp_reduce(); v2.warp_reduce();
+  w0.warp_reduce(); w1.warp_reduce(); w2.warp_reduce();
+  if (lane == 0) {
+    const double norm = c.dx * c.dx * c.dx;
+    V[3 * b + 0] = v0.value() * norm;
+    V[3 * b + 1] = v1.value() * norm;
+    V[3 * b + 2] = v2.value() * norm;
+    W[3 * b + 0] = -0.5 * w0.value() * norm;
+    W[3 * b + 1] = -0.5 * w1.value() * norm;
+    W[3 * b + 2] = -0.5 * w2.value() * norm;
+  }
+}
+
+__global__ void k_friction(const double *__restrict__ F, const double *__restrict__ T, double *__restrict__ V,
+                           double *__restrict__ W, int n3, double a1, double a2) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n3) {
+    V[i] = a1 * F[i];
+    W[i] = a2 * T[i];
+  }
+}
+
+FcmConsts make_consts(const fs_ctx *c) {
+  FcmConsts k;
+  k.N[0] = c->nx;
+  k.N[1] = c->ny;
+  k.N[2] = c->nz;
+  k.ngd = c->p.ngd;
+  k.ngdh = c->p.ngd / 2;
+  for (int d = 0; d < 3; ++d) k.nbin[d] = c->nbin[d];
+  k.dx = c->p.dx;
+  const double PI = FS_PI;
+  k.sigmadipsq = c->p.sigma_dip * c->p.sigma_dip;
+  k.anormdip = 1.0 / sqrt(2.0 * PI * k.sigmadipsq);
+  k.anormdip2 = 2.0 * k.sigmadipsq;
+  const double sigmasq = c->p.sigma * c->p.sigma;
+  k.anorm = 1.0 / sqrt(2.0 * PI * sigmasq);
+  k.anorm2 = 2.0 * sigmasq;
+  return k;
+}
+
+fs_status ensure_plans(fs_ctx *c, int prec) {
+  if (c->plan_ok[prec]) return FS_OK;
+  int n[3] = {c->nx, c->ny, c->nz};
+  size_t ws = 0;
+  if (cufftCreate(&c->plan_fwd[prec]) != CUFFT_SUCCESS) return FS_ERR_CUFFT;
+  if (cufftCreate(&c->plan_inv[prec]) != CUFFT_SUCCESS) return FS_ERR_CUFFT;
+  cufftType tf = prec == FS_PREC_FP64 ? CUFFT_D2Z : CUFFT_R2C;
+  cufftType ti = prec == FS_PREC_FP64 ? CUFFT_Z2D : CUFFT_C2R;
+  if (cufftMakePlanMany(c->plan_fwd[prec], 3, n, NULL, 1, 0, NULL, 1, 0, tf, 3, &ws) != CUFFT_SUCCESS)
+    return FS_ERR_CUFFT;
+  c->bytes += ws;
+  if (cufftMakePlanMany(c->plan_inv[prec], 3, n, NULL, 1, 0, NULL, 1, 0, ti, 3, &ws) != CUFFT_SUCCESS)
+    return FS_ERR_CUFFT;
+  c->bytes += ws;
+  if (cufftSetStream(c->plan_fwd[prec], c->stream) != CUFFT_SUCCESS) return FS_ERR_CUFFT;
+  if (cufftSetStream(c->plan_inv[prec], c->stream) != CUFFT_SUCCESS) return FS_ERR_CUFFT;
+  c->plan_ok[prec] = true;
+  return FS_OK;
+}
+
+template <typename R>
+fs_status flow_solve_t(fs_ctx *c) {
+  const int prec = sizeof(R) == 8 ? FS_PREC_FP64 : FS_PREC_FP32;
+  FS_TRY(ensure_plans(c, prec));
+  cufftResult r;
+  if (prec == FS_PREC_FP64)
+    r = cufftExecD2Z(c->plan_fwd[prec], (cufftDoubleReal *)c->grid_real, (cufftDoubleComplex *)c->grid_cplx);
+  else
+    r = cufftExecR2C(c->plan_fwd[prec], (cufftReal *)c->grid_real, (cufftComplex *)c->grid_cplx);
+  if (r != CUFFT_SUCCESS) return FS_ERR_CUFFT;
+  const double TwoPI = 2. * FS_PI;
+  const R ffx = (R)(TwoPI / (c->nx * c->p.dx)), ffy = (R)(TwoPI / (c->ny * c->p.dx)),
+          ffz = (R)(TwoPI / (c->nz * c->p.dx));
+  const R total = (R)((double)c->nx * (double)c->ny * (double)c->nz);
+  typedef typename Cplx<R>::T C;
+  C *fh = (C *)c->grid_cplx;
+  k_project<R><<<fs_blocks((long long)c->NH, 256), 256, 0, c->stream>>>(fh, c->NH, c->nx, c->ny, c->nz, c->nzh, ffx,
+                                                                          ffy, ffz, total);
+  FS_LAUNCH_CHECK();
+  dim3 gp(fs_blocks((long long)c->nx * c->ny, 256), 2);
+  k_project_planes<R><<<gp, 256, 0, c->stream>>>(fh, c->NH, c->nx, c->ny, c->nz, c->nzh, ffx, ffy, ffz, total);
+  FS_LAUNCH_CHECK();
+  if (prec == FS_PREC_FP64)
+    r = cufftExecZ2D(c->plan_inv[prec], (cufftDoubleComplex *)c->grid_cplx, (cufftDoubleReal *)c->grid_real);
+  else
+    r = cufftExecC2R(c->plan_inv[prec], (cufftComplex *)c->grid_cplx, (cufftReal *)c->grid_real);
+  if (r != CUFFT_SUCCESS) return FS_ERR_CUFFT;
+  return FS_OK;
+}
+
+template <typename R>
+fs_status mobility_t(fs_ctx *c, const double *Y, const double *F, const double *T, double *V, double *W, int np) {
+  FcmConsts k = make_consts(c);
+  if (np > 0) {
+    k_fcm_bin_keys<<<fs_blocks(np, 256), 256, 0, c->stream>>>(Y, np, k, c->bins.key);
+    FS_LAUNCH_CHECK();
+  }
+  FS_TRY(fs_sort_run(&c->bins, np, c->stream));
+  const size_t smem = sizeof(SpreadSmem<R>);
+  k_spread<R><<<c->nbins, FS_TILE * 32, smem, c->stream>>>(Y, F, T, c->bins.start, c->bins.sorted, k,
+                                                            (R *)c->grid_real);
+  FS_LAUNCH_CHECK();
+  FS_TRY(flow_solve_t<R>(c));
+  if (np > 0) {
+    k_interp<R><<<fs_blocks(np, 8), 256, 0, c->stream>>>((const R *)c->grid_real, Y, c->bins.sorted, np, k, V, W);
+    FS_LAUNCH_CHECK();
+  }
+  c->last_grid_prec = sizeof(R) == 8 ? FS_PREC_FP64 : FS_PREC_FP32;
+  return FS_OK;
+}
+
+}  // namespace
+
+fs_status fcm_init(fs_ctx *c) {
+  c->nx = c->p.npts_x;
+  c->ny = c->p.npts_y;
+  c->nz = c->p.npts_z;
+  c->nzh = c->nz / 2 + 1;
+  c->N = (size_t)c->nx * c->ny * c->nz;
+  c->NH = (size_t)c->nx * c->ny * c->nzh;
+  for (int d = 0; d < 3; ++d) c->nbin[d] = (d == 0 ? c->nx : d == 1 ? c->ny : c->nz) / FS_TILE;
+  c->nbins = c->nbin[0] * c->nbin[1] * c->nbin[2];
+  c->last_grid_prec = -1;
+  FS_CUDA(cudaMalloc(&c->grid_real, sizeof(double) * 3 * c->N));
+  FS_CUDA(cudaMalloc(&c->grid_cplx, sizeof(double2) * 3 * c->NH));
+  c->bytes += sizeof(double) * 3 * c->N + sizeof(double2) * 3 * c->NH;
+  FS_TRY(fs_sort_alloc(&c->bins, c->nbins, c->max_beads, &c->bytes));
+  FS_CUDA(cudaFuncSetAttribute(k_spread<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(SpreadSmem<double>)));
+  FS_CUDA(cudaFuncSetAttribute(k_spread<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(SpreadSmem<float>)));
+  return FS_OK;
+}
+
+void fcm_free(fs_ctx *c) {
+  for (int p = 0; p < 2; ++p)
+    if (c->plan_ok[p]) {
+      cufftDestroy(c->plan_fwd[p]);
+      cufftDestroy(c->plan_inv[p]);
+      c->plan_ok[p] = false;
+    }
+  cudaFree(c->grid_real);
+  cudaFree(c->grid_cplx);
+  c->grid_real = c->grid_cplx = nullptr;
+  fs_sort_free(&c->bins);
+}
+
+fs_status fcm_mobility(fs_ctx *c, const double *Y, const double *F, const double *T, double *V, double *W, int np) {
+  if (c->precision == FS_PREC_FP32) return mobility_t<float>(c, Y, F, T, V, W, np);
+  return mobility_t<double>(c, Y, F, T, V, W, np);
+}
+
+fs_status fcm_friction(fs_ctx *c, const double *F, const double *T, double *V, double *W, int np) {
+  const double PI = FS_PI, a = c->p.a, mu = c->p.mu;
+  const double a1 = 1. / (6 * PI * a * mu);
+  const double a2 = 1. / (8 * PI * a * a * a * mu);
+  if (np > 0) {
+    k_friction<<<fs_blocks(3 * np, 256), 256, 0, c->stream>>>(F, T, V, W, 3 * np, a1, a2);
+    FS_LAUNCH_CHECK();
+  }
+  return FS_OK;
+}
+
+fs_status fcm_spread_only(fs_ctx *c, const double *Y, const double *F, const double *T, int np, double *f) {
+  FcmConsts k = make_consts(c);
+  if (np > 0) {
+    k_fcm_bin_keys<<<fs_blocks(np, 256), 256, 0, c->stream>>>(Y, np, k, c->bins.key);
+    FS_LAUNCH_CHECK();
+  }
+  FS_TRY(fs_sort_run(&c->bins, np, c->stream));
+  k_spread<double><<<c->nbins, FS_TILE * 32, sizeof(SpreadSmem<double>), c->stream>>>(
+      Y, F, T, c->bins.start, c->bins.sorted, k, (double *)c->grid_real);
+  FS_LAUNCH_CHECK();
+  FS_CUDA(cudaMemcpyAsync(f, c->grid_real, sizeof(double) * 3 * c->N, cudaMemcpyDeviceToDevice, c->stream));
+  c->last_grid_prec = -1;
+  return FS_OK;
+}
+
+fs_status fcm_flow_solve_only(fs_ctx *c, const double *f, double *u) {
+  const size_t n = 3 * c->N;
+  if (c->precision != FS_PREC_FP64) return FS_ERR_INVALID_ARG;  // the flow-only check is an FP64 entry point
+  FS_CUDA(cudaMemcpyAsync(c->grid_real, f, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+  FS_TRY(flow_solve_t<double>(c));
+  FS_CUDA(cudaMemcpyAsync(u, c->grid_real, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+  c->last_grid_prec = FS_PREC_FP64;
+  return FS_OK;
+}

@@ -1,0 +1,939 @@
+// fs_filament.cu -- filament mechanics, approximate Jacobian and Broyden
+// update of the implicit BDF2 step, FP64 on sm_100a.
+//
+//   k_initial_guess      Filament::initialGuess (Filament.hpp:227-237, Bead.hpp:202-217)
+//   k_unrobot_assign     Filament::unRobotArmify (Filament.hpp:489-505) +
+//                        Fcm::assign_filament_data's Y = fmod(Xs, L) (FCMfunctions.cpp:882-918)
+//   k_forces             setZeroForcesTorques, applyElasticTorques, applyConstraintForcesTorques,
+//                        applyExternalForcesTorques (Filament.hpp:271-402), one thread per bead
+//                        adding its links' terms in the reference's order
+//   k_jacobian           buildApproximateJacobian with BlockC/D/E/F (Filament.hpp:803-1120), then
+//                        LU with partial pivoting in place (one CTA per filament, column-major)
+//   k_error_check        ErrorCheckFCM + dexpinv (MobilityConstraints.cpp:109-143, 447-770)
+//   k_lu_apply           filamentJsolver::solve (FilamentJacobianSolver.hpp:49-73): J0^-1 b by
+//                        the LU factors, then the bad-Broyden history corrections
+//   k_broyden_cols       history update of main.cpp:640-663
+//   k_update / k_step    Filament::update (Filament.hpp:425-452), Filament::step (:455-478)
+#include "fs_internal.cuh"
+
+namespace {
+
+struct Q {
+  double s, v[3];
+};
+
+__device__ __forceinline__ Q qload(const double *a) {
+  Q q;
+  q.s = a[0];
+  q.v[0] = a[1];
+  q.v[1] = a[2];
+  q.v[2] = a[3];
+  return q;
+}
+__device__ __forceinline__ void qstore(const Q &q, double *a) {
+  a[0] = q.s;
+  a[1] = q.v[0];
+  a[2] = q.v[1];
+  a[3] = q.v[2];
+}
+__device__ __forceinline__ double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+__device__ __forceinline__ void cross3(const double *a, const double *b, double *c) {
+  double c0 = a[1] * b[2] - a[2] * b[1], c1 = a[2] * b[0] - a[0] * b[2], c2 = a[0] * b[1] - a[1] * b[0];
+  c[0] = c0;
+  c[1] = c1;
+  c[2] = c2;
+}
+__device__ __forceinline__ double norm3(const double *a) { return sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); }
+
+// expmInPlace (UnitQuaternion.hpp:227-242): q <- (cos(t/2), sin(t/2)/t v) * q
+__device__ Q q_expm(Q q, const double *v) {
+  double theta = norm3(v);
+  if (theta > 1.e-12) {
+    double tmp = sin(theta * .5) / theta;
+    Q p;
+    p.s = cos(theta * .5);
+    p.v[0] = tmp * v[0];
+    p.v[1] = tmp * v[1];
+    p.v[2] = tmp * v[2];
+    double scal_tmp = q.s * p.s - dot3(q.v, p.v);
+    double t[3];
+    cross3(p.v, q.v, t);
+    Q r;
+    for (int d = 0; d < 3; ++d) r.v[d] = q.s * p.v[d] + p.s * q.v[d] + t[d];
+    r.s = scal_tmp;
+    return r;
+  }
+  return q;
+}
+
+// tangent / normal / binormal (UnitQuaternion.hpp:341-378)
+__device__ __forceinline__ void q_tangent(const Q &q, double *v) {
+  double q22 = 2 * q.v[1] * q.v[1], q33 = 2 * q.v[2] * q.v[2];
+  v[0] = (1 - q22 - q33);
+  v[1] = 2 * (q.v[0] * q.v[1] + q.s * q.v[2]);
+  v[2] = 2 * (q.v[0] * q.v[2] - q.s * q.v[1]);
+}
+__device__ __forceinline__ void q_normal(const Q &q, double *v) {
+  double q11 = 2 * q.v[0] * q.v[0], q33 = 2 * q.v[2] * q.v[2];
+  v[0] = 2 * (q.v[0] * q.v[1] - q.s * q.v[2]);
+  v[1] = (1 - q11 - q33);
+  v[2] = 2 * (q.v[1] * q.v[2] + q.s * q.v[0]);
+}
+__device__ __forceinline__ void q_binormal(const Q &q, double *v) {
+  double q11 = 2 * q.v[0] * q.v[0], q22 = 2 * q.v[1] * q.v[1];
+  v[0] = 2 * (q.v[0] * q.v[2] + q.s * q.v[1]);
+  v[1] = 2 * (q.v[1] * q.v[2] - q.s * q.v[0]);
+  v[2] = (1 - q11 - q22);
+}
+// RotateVector (UnitQuaternion.hpp:323-338)
+__device__ void q_rotate(const Q &q, double *v) {
+  double vx = v[0], vy = v[1], vz = v[2];
+  const double *e = q.v;
+  double s = q.s;
+  double q11 = 2 * e[0] * e[0], q22 = 2 * e[1] * e[1], q33 = 2 * e[2] * e[2];
+  v[0] = (1 - q22 - q33) * vx + 2 * (e[0] * e[1] - s * e[2]) * vy + 2 * (e[0] * e[2] + s * e[1]) * vz;
+  v[1] = 2 * (e[0] * e[1] + s * e[2]) * vx + (1 - q11 - q33) * vy + 2 * (e[1] * e[2] - s * e[0]) * vz;
+  v[2] = 2 * (e[0] * e[2] - s * e[1]) * vx + 2 * (e[1] * e[2] + s * e[0]) * vy + (1 - q11 - q22) * vz;
+}
+// assignMidPointOf (UnitQuaternion.hpp:472-489) with quaSquareRootTimInPlace (:411-421)
+__device__ Q q_midpoint(const Q &p1, const Q &p2) {
+  Q m;
+  m.s = p2.s * p1.s + dot3(p2.v, p1.v);
+  double cr[3];
+  cross3(p2.v, p1.v, cr);
+  for (int d = 0; d < 3; ++d) m.v[d] = -p2.s * p1.v[d] + p1.s * p2.v[d] - cr[d];
+  if (m.s < -.9999999999999) {
+    m.s = 0.;
+    m.v[0] = 0.;
+    m.v[1] = 0.;
+    m.v[2] = 1.;
+  } else {
+    m.s = sqrt(0.5 * (m.s + 1.));
+    for (int d = 0; d < 3; ++d) m.v[d] /= (2. * m.s);
+  }
+  double scal_tmp = m.s * p1.s - dot3(m.v, p1.v);
+  double t[3];
+  cross3(m.v, p1.v, t);
+  Q o;
+  for (int d = 0; d < 3; ++d) o.v[d] = m.s * p1.v[d] + p1.s * m.v[d] + t[d];
+  o.s = scal_tmp;
+  return o;
+}
+
+// dexpinv (MobilityConstraints.cpp:109-143)
+__device__ void dexpinv(const double *u, const double *w, double *out) {
+  double tmp = norm3(u);
+  double cuw[3];
+  cross3(u, w, cuw);
+  if (tmp >= 1.e-12) {
+    double tmp2 = tmp / sin(.5 * tmp);
+    tmp2 *= cos(.5 * tmp);
+    tmp = .5 * tmp2 - 1.;
+    double nu = norm3(u);
+    double un[3] = {u[0] / nu, u[1] / nu, u[2] / nu};
+    double c1[3], c2[3];
+    cross3(un, w, c1);
+    cross3(un, c1, c2);
+    for (int d = 0; d < 3; ++d) {
+      out[d] = w[d] - .5 * cuw[d];
+      out[d] -= tmp * c2[d];
+    }
+  } else {
+    tmp = 1. / 12;
+    double c2[3];
+    cross3(u, cuw, c2);
+    for (int d = 0; d < 3; ++d) {
+      out[d] = w[d] - .5 * cuw[d];
+      out[d] += tmp * c2[d];
+    }
+  }
+}
+
+struct FilConsts {
+  double L[3];
+  double dt, dl, mu, tol;
+  double gravity[3], st[3];
+  int impl_euler_steps, lambda_extrap_step;
+};
+
+// ---- per-bead / per-filament kernels -----------------------------------------
+__global__ void k_initial_guess(int np, const int *__restrict__ seg_id, const double *__restrict__ X,
+                                const double *__restrict__ Xt, const double *__restrict__ U,
+                                const double *__restrict__ Ut, const double *__restrict__ q, double *__restrict__ Xs,
+                                double *__restrict__ Us, double *__restrict__ qs) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= np) return;
+  if (seg_id[b] == 0)
+    for (int d = 0; d < 3; ++d) Xs[3 * b + d] = 2. * X[3 * b + d] - Xt[3 * b + d];
+  double us[3];
+  for (int d = 0; d < 3; ++d) us[d] = 2. * U[3 * b + d] - Ut[3 * b + d];
+  for (int d = 0; d < 3; ++d) Us[3 * b + d] = us[d];
+  qstore(q_expm(qload(q + 4 * b), us), qs + 4 * b);
+}
+
+__global__ void k_unrobot_assign(int nfil, const int *__restrict__ fil_start, const double *__restrict__ qs,
+                                 double *__restrict__ Xs, double *__restrict__ Y, FilConsts k) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nfil) return;
+  int b0 = fil_start[f], b1 = fil_start[f + 1];
+  double Xsum[3] = {Xs[3 * b0], Xs[3 * b0 + 1], Xs[3 * b0 + 2]};
+  double t1[3], t2[3];
+  q_tangent(qload(qs + 4 * b0), t1);
+  const double half = 0.5 * k.dl;
+  for (int d = 0; d < 3; ++d) Y[3 * b0 + d] = fmod(Xsum[d], k.L[d]);
+  for (int b = b0 + 1; b < b1; ++b) {
+    q_tangent(qload(qs + 4 * b), t2);
+    for (int d = 0; d < 3; ++d) {
+      Xsum[d] += (t1[d] + t2[d]) * half;
+      Xs[3 * b + d] = Xsum[d];
+      Y[3 * b + d] = fmod(Xsum[d], k.L[d]);
+      t1[d] = t2[d];
+    }
+  }
+}
+
+// elastic torque of link (i, i+1) (Filament.hpp:297-340), before the +/- to the beads
+__device__ void elastic_link(const double *qi_, const double *qj_, double oneOverDL, double kap, double cmod,
+                             const double *st, double *vtmp) {
+  Q qi = qload(qi_), qj = qload(qj_);
+  Q qm = q_midpoint(qi, qj);
+  Q q2 = qj;
+  q2.s -= qi.s;
+  for (int d = 0; d < 3; ++d) q2.v[d] -= qi.v[d];
+  q2.s *= oneOverDL;
+  for (int d = 0; d < 3; ++d) q2.v[d] *= oneOverDL;
+  double tt[3];
+  cross3(q2.v, qm.v, tt);
+  double nv[3];
+  for (int d = 0; d < 3; ++d) nv[d] = -q2.s * qm.v[d] + qm.s * q2.v[d] + tt[d];
+  for (int d = 0; d < 3; ++d) vtmp[d] = 2. * nv[d] - st[d];
+  vtmp[0] *= cmod;
+  vtmp[1] *= kap;
+  vtmp[2] *= kap;
+  q_rotate(qm, vtmp);
+}
+
+__global__ void k_forces(int np, const int *__restrict__ fil_id, const int *__restrict__ seg_id,
+                         const int *__restrict__ fil_start, const double *__restrict__ qs,
+                         const double *__restrict__ lam, const double *__restrict__ kap,
+                         const double *__restrict__ cmod, double *__restrict__ F, double *__restrict__ TAU,
+                         FilConsts k) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= np) return;
+  const int f = fil_id[b], i = seg_id[b];
+  const int nw = fil_start[f + 1] - fil_start[f];
+  const int l0 = fil_start[f] - f;
+  const double oneOverDL = 1. / k.dl;
+  double tau[3] = {0.0, 0.0, 0.0}, fo[3] = {0.0, 0.0, 0.0}, v[3];
+  // elastic: link i-1 subtracts, link i adds (link order of Filament.hpp:297)
+  if (i >= 1) {
+    elastic_link(qs + 4 * (b - 1), qs + 4 * b, oneOverDL, kap[f], cmod[f], k.st, v);
+    for (int d = 0; d < 3; ++d) tau[d] -= v[d];
+  }
+  if (i < nw - 1) {
+    elastic_link(qs + 4 * b, qs + 4 * (b + 1), oneOverDL, kap[f], cmod[f], k.st, v);
+    for (int d = 0; d < 3; ++d) tau[d] += v[d];
+  }
+  // constraint forces and torques (Filament.hpp:351-368)
+  const double fac = -.5 * k.dl;
+  double t[3], c2[3];
+  q_tangent(qload(qs + 4 * b), t);
+  if (i >= 1) {
+    const double *lm = lam + 3 * (l0 + i - 1);
+    for (int d = 0; d < 3; ++d) fo[d] += lm[d];
+    cross3(t, lm, c2);
+    for (int d = 0; d < 3; ++d) tau[d] += fac * c2[d];
+  }
+  if (i < nw - 1) {
+    const double *lm = lam + 3 * (l0 + i);
+    for (int d = 0; d < 3; ++d) fo[d] -= lm[d];
+    cross3(t, lm, c2);
+    for (int d = 0; d < 3; ++d) tau[d] += fac * c2[d];
+  }
+  for (int d = 0; d < 3; ++d) {
+    F[3 * b + d] = fo[d] + k.gravity[d];
+    TAU[3 * b + d] = tau[d];
+  }
+}
+
+// ---- Jacobian ------------------------------------------------------------------
+struct M3 {
+  double m[9];
+};
+__device__ __forceinline__ M3 rcross(const double *x) {
+  M3 r;
+  r.m[0] = 0.;
+  r.m[1] = x[2];
+  r.m[2] = -x[1];
+  r.m[3] = -x[2];
+  r.m[4] = 0.;
+  r.m[5] = x[0];
+  r.m[6] = x[1];
+  r.m[7] = -x[0];
+  r.m[8] = 0.;
+  return r;
+}
+__device__ __forceinline__ M3 mt(const M3 &a) {
+  M3 r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r.m[3 * i + j] = a.m[3 * j + i];
+  return r;
+}
+__device__ M3 mmul(const M3 &a, const M3 &b) {
+  M3 r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double acc = 0.0;
+      for (int kk = 0; kk < 3; ++kk) acc += a.m[3 * i + kk] * b.m[3 * kk + j];
+      r.m[3 * i + j] = acc;
+    }
+  return r;
+}
+__device__ __forceinline__ M3 madd(M3 a, const M3 &b) {
+  for (int i = 0; i < 9; ++i) a.m[i] += b.m[i];
+  return a;
+}
+__device__ __forceinline__ M3 msub(M3 a, const M3 &b) {
+  for (int i = 0; i < 9; ++i) a.m[i] -= b.m[i];
+  return a;
+}
+__device__ __forceinline__ M3 msc(M3 a, double s) {
+  for (int i = 0; i < 9; ++i) a.m[i] *= s;
+  return a;
+}
+__device__ __forceinline__ M3 outer(const double *a, const double *b) {
+  M3 r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r.m[3 * i + j] = a[i] * b[j];
+  return r;
+}
+__device__ M3 blockE_diag(const M3 &dOmega, const M3 &LieMat, const M3 &OmegaMat, const double *Us, double dt) {
+  double ov[3];
+  for (int i = 0; i < 3; ++i) ov[i] = OmegaMat.m[3 * i] * Us[0] + OmegaMat.m[3 * i + 1] * Us[1] + OmegaMat.m[3 * i + 2] * Us[2];
+  M3 inner = msub(dOmega, msc(madd(OmegaMat, mmul(LieMat, dOmega)), 0.5));
+  M3 corr = madd(madd(rcross(ov), mmul(LieMat, OmegaMat)), mmul(mmul(LieMat, LieMat), dOmega));
+  inner = madd(inner, msc(corr, 1. / 12.));
+  return msc(inner, -2 * dt / 3.);
+}
+__device__ M3 blockE_off(const M3 &dOmega, const M3 &LieMat, double dt) {
+  M3 inner = msub(dOmega, msc(mmul(LieMat, dOmega), 0.5));
+  inner = madd(inner, msc(mmul(mmul(LieMat, LieMat), dOmega), 1. / 12.));
+  return msc(inner, -2 * dt / 3.);
+}
+__device__ __forceinline__ void frame(const double *qa, double *t, double *n, double *b) {
+  Q q = qload(qa);
+  q_tangent(q, t);
+  q_normal(q, n);
+  q_binormal(q, b);
+}
+// column-major store of a 3x3 block at (r0, c0)
+__device__ __forceinline__ void put3(double *J, int n, int r0, int c0, const M3 &a) {
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) J[(size_t)(c0 + j) * n + r0 + i] = a.m[3 * i + j];
+}
+
+// the three BlockE blocks of bead row k (Filament.hpp:958-1089)
+__device__ void blockE_row(int k, int nw, const double *qs, const double *Us, const double *TAU, const double *lam,
+                           double rad_k, double myC, double myKAP, const double *ST, double DL, double dt, double MU,
+                           double *J, int n) {
+  const double PI = FS_PI;
+  const int rE = 3 * nw, cE = 3;
+  double t[3], nn[3], b[3], tp1[3], np1[3], bp1[3], tm1[3], nm1[3], bm1[3];
+  const double Tfac = 1 / (8 * PI * MU * pow(rad_k, 3));
+  const M3 LieMat = mt(rcross(Us + 3 * k));
+  const double tT[3] = {Tfac * TAU[3 * k], Tfac * TAU[3 * k + 1], Tfac * TAU[3 * k + 2]};
+  const M3 OmegaMat = rcross(tT);
+  frame(qs + 4 * k, t, nn, b);
+  if (k == 0) {
+    frame(qs + 4, tp1, np1, bp1);
+    M3 ConstraintPart = mmul(msc(rcross(lam), -0.5 * DL), rcross(t));
+    double beta = -ST[2] + 0.5 * (np1[0] * b[0] + np1[1] * b[1] + np1[2] * b[2] - nn[0] * bp1[0] - nn[1] * bp1[1] - nn[2] * bp1[2]) / DL;
+    double CP[3] = {b[1] * np1[2] - b[2] * np1[1] - nn[1] * bp1[2] + nn[2] * bp1[1],
+                    b[2] * np1[0] - b[0] * np1[2] - nn[2] * bp1[0] + nn[0] * bp1[2],
+                    b[0] * np1[1] - b[1] * np1[0] - nn[0] * bp1[1] + nn[1] * bp1[0]};
+    double ttp[3] = {t[0] + tp1[0], t[1] + tp1[1], t[2] + tp1[2]};
+    M3 EP = msc(madd(msc(outer(ttp, CP), 0.5 / DL), msc(rcross(t), beta)), 0.5 * myC);
+    EP = madd(EP, msc(msub(msc(mmul(rcross(tp1), rcross(t)), 1. / DL),
+                           msc(madd(msc(rcross(nn), ST[0]), msc(rcross(b), ST[1])), 0.5)),
+                      0.5 * myKAP));
+    M3 dOmega = msc(madd(EP, ConstraintPart), Tfac);
+    put3(J, n, rE, cE, blockE_diag(dOmega, LieMat, OmegaMat, Us, dt));
+    EP = msc(msub(msc(rcross(tp1), beta), msc(outer(ttp, CP), 0.5 / DL)), 0.5 * myC);
+    EP = madd(EP, msc(msub(msc(mmul(mt(rcross(t)), rcross(tp1)), 1. / DL),
+                           msc(madd(msc(rcross(np1), ST[0]), msc(rcross(bp1), ST[1])), 0.5)),
+                      0.5 * myKAP));
+    dOmega = msc(EP, Tfac);
+    put3(J, n, rE, cE + 3, blockE_off(dOmega, LieMat, dt));
+    return;
+  }
+  if (k == nw - 1) {
+    frame(qs + 4 * (k - 1), tm1, nm1, bm1);
+    M3 ConstraintPart = mmul(msc(rcross(lam + 3 * (k - 1)), -0.5 * DL), rcross(t));
+    double beta = -ST[2] + 0.5 * (nn[0] * bm1[0] + nn[1] * bm1[1] + nn[2] * bm1[2] - nm1[0] * b[0] - nm1[1] * b[1] - nm1[2] * b[2]) / DL;
+    double CPm[3] = {bm1[1] * nn[2] - bm1[2] * nn[1] - nm1[1] * b[2] + nm1[2] * b[1],
+                     bm1[2] * nn[0] - bm1[0] * nn[2] - nm1[2] * b[0] + nm1[0] * b[2],
+                     bm1[0] * nn[1] - bm1[1] * nn[0] - nm1[0] * b[1] + nm1[1] * b[0]};
+    double ttm[3] = {t[0] + tm1[0], t[1] + tm1[1], t[2] + tm1[2]};
+    M3 EP = msc(msub(msc(rcross(t), beta), msc(outer(ttm, CPm), 0.5 / DL)), -0.5 * myC);
+    EP = msub(EP, msc(msub(msc(mmul(mt(rcross(tm1)), rcross(t)), 1. / DL),
+                           msc(madd(msc(rcross(nn), ST[0]), msc(rcross(b), ST[1])), 0.5)),
+                      0.5 * myKAP));
+    M3 dOmega = msc(madd(EP, ConstraintPart), Tfac);
+    put3(J, n, rE + 3 * k, cE + 3 * k, blockE_diag(dOmega, LieMat, OmegaMat, Us + 3 * k, dt));
+    EP = msc(msub(msc(rcross(tm1), beta), msc(outer(ttm, CPm), 0.5 / DL)), -0.5 * myC);
+    EP = msub(EP, msc(msub(msc(mmul(rcross(t), rcross(tm1)), 1. / DL),
+                           msc(madd(msc(rcross(nm1), ST[0]), msc(rcross(bm1), ST[1])), 0.5)),
+                      0.5 * myKAP));
+    dOmega = msc(EP, Tfac);
+    put3(J, n, rE + 3 * k, cE + 3 * k - 3, blockE_off(dOmega, LieMat, dt));
+    return;
+  }
+  frame(qs + 4 * (k - 1), tm1, nm1, bm1);
+  frame(qs + 4 * (k + 1), tp1, np1, bp1);
+  double lamvec[3] = {lam[3 * (k - 1)] + lam[3 * k], lam[3 * (k - 1) + 1] + lam[3 * k + 1], lam[3 * (k - 1) + 2] + lam[3 * k + 2]};
+  M3 ConstraintPart = mmul(msc(rcross(lamvec), -0.5 * DL), rcross(t));
+  double beta = -ST[2] + 0.5 * (np1[0] * b[0] + np1[1] * b[1] + np1[2] * b[2] - nn[0] * bp1[0] - nn[1] * bp1[1] - nn[2] * bp1[2]) / DL;
+  double CPk[3] = {b[1] * np1[2] - b[2] * np1[1] - nn[1] * bp1[2] + nn[2] * bp1[1],
+                   b[2] * np1[0] - b[0] * np1[2] - nn[2] * bp1[0] + nn[0] * bp1[2],
+                   b[0] * np1[1] - b[1] * np1[0] - nn[0] * bp1[1] + nn[1] * bp1[0]};
+  double tp[3] = {t[0] + tp1[0], t[1] + tp1[1], t[2] + tp1[2]};
+  double tm[3] = {t[0] + tm1[0], t[1] + tm1[1], t[2] + tm1[2]};
+  M3 EP = msc(madd(msc(outer(tp, CPk), 0.5 / DL), msc(rcross(t), beta)), 0.5 * myC);
+  EP = madd(EP, msc(msub(msc(mmul(rcross(tp1), rcross(t)), 1. / DL),
+                         msc(madd(msc(rcross(nn), ST[0]), msc(rcross(b), ST[1])), 0.5)),
+                    0.5 * myKAP));
+  // the k-1 side beta, with the k+1 side CrossPart kept (Filament.hpp:1068-1070)
+  beta = -ST[2] + 0.5 * (nn[0] * bm1[0] + nn[1] * bm1[1] + nn[2] * bm1[2] - nm1[0] * b[0] - nm1[1] * b[1] - nm1[2] * b[2]) / DL;
+  EP = msub(EP, msc(msub(msc(rcross(t), beta), msc(outer(tm, CPk), 0.5 / DL)), 0.5 * myC));
+  EP = msub(EP, msc(msub(msc(mmul(mt(rcross(tm1)), rcross(t)), 1. / DL),
+                         msc(madd(msc(rcross(nn), ST[0]), msc(rcross(b), ST[1])), 0.5)),
+                    0.5 * myKAP));
+  M3 dOmega = msc(madd(ConstraintPart, EP), Tfac);
+  put3(J, n, rE + 3 * k, cE + 3 * k, blockE_diag(dOmega, LieMat, OmegaMat, Us + 3 * k, dt));
+  EP = msc(msub(msc(rcross(tm1), beta), msc(outer(tm, CPk), 0.5 / DL)), -0.5 * myC);
+  EP = msub(EP, msc(msub(msc(mmul(rcross(t), rcross(tm1)), 1. / DL),
+                         msc(madd(msc(rcross(nm1), ST[0]), msc(rcross(bm1), ST[1])), 0.5)),
+                    0.5 * myKAP));
+  dOmega = msc(EP, Tfac);
+  put3(J, n, rE + 3 * k, cE + 3 * k - 3, blockE_off(dOmega, LieMat, dt));
+  // right block with the k-1 side beta (Filament.hpp:1083)
+  EP = msc(msub(msc(rcross(tp1), beta), msc(outer(tp, CPk), 0.5 / DL)), 0.5 * myC);
+  EP = madd(EP, msc(msub(msc(mmul(mt(rcross(t)), rcross(tp1)), 1. / DL),
+                         msc(madd(msc(rcross(np1), ST[0]), msc(rcross(bp1), ST[1])), 0.5)),
+                    0.5 * myKAP));
+  dOmega = msc(EP, Tfac);
+  put3(J, n, rE + 3 * k, cE + 3 * k + 3, blockE_off(dOmega, LieMat, dt));
+}
+
+// build J (column-major) then LU-factorise it in place; one CTA per filament
+__global__ void __launch_bounds__(256) k_jacobian(int nfil, const int *__restrict__ fil_start,
+                                                  const double *__restrict__ qs, const double *__restrict__ Us,
+                                                  const double *__restrict__ TAU, const double *__restrict__ lam,
+                                                  const double *__restrict__ kap, const double *__restrict__ cmod,
+                                                  const long long *__restrict__ joff, double *__restrict__ Jall,
+                                                  int *__restrict__ piv_all, int nt, FilConsts k, double a,
+                                                  double ah, int *__restrict__ flags) {
+  const int f = blockIdx.x;
+  const int b0 = fil_start[f], nw = fil_start[f + 1] - b0, l0 = b0 - f;
+  const int n = 6 * nw;
+  double *J = Jall + joff[f];
+  int *piv = piv_all + 6 * b0;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const double PI = FS_PI, dt = k.dt, DL = k.dl, MU = k.mu;
+  const double *q_f = qs + 4 * b0;
+  const double *Us_f = Us + 3 * b0;
+  const double *TAU_f = TAU + 3 * b0;
+  const double *lam_f = lam + 3 * l0;
+  // bead radius: ah for bead 0, a for the others
+#define RAD(kk) ((kk) == 0 ? ah : a)
+  for (long long e = tid; e < (long long)n * n; e += nthr) J[e] = 0.0;
+  __syncthreads();
+  const double Jprefac = 10.;
+  if (tid == 0) {
+    int j = 3 * nw + 3;
+    double temp = dt / (9 * PI * MU * RAD(0));
+    for (int d = 0; d < 3; ++d) J[(size_t)d * n + d] = 1;
+    if (nw > 1)
+      for (int d = 0; d < 3; ++d) J[(size_t)(j + d) * n + d] = temp / dt;
+    else
+      for (int d = 0; d < 3; ++d) J[(size_t)(3 + d) * n + 3 + d] = 1;
+  }
+  if (nw > 1) {
+    // BlockC(0.5*DL): row block r, col block m <= r+1
+    const double fac = 0.5 * DL;
+    const int ntask = (nw - 1) * (nw + 2);
+    for (int tsk = tid; tsk < ntask; tsk += nthr) {
+      const int r = tsk / (nw + 2), m = tsk % (nw + 2);
+      if (m > r + 1) continue;
+      double tv[3];
+      q_tangent(qload(q_f + 4 * m), tv);
+      M3 blk = msc(rcross(tv), fac);
+      if (!(m == 0 || m == r + 1)) blk = madd(blk, blk);
+      put3(J, n, 3 + 3 * r, 3 + 3 * m, blk);
+    }
+    // Jprefac * BlockD(nt) / dt
+    for (int m = tid; m < nw - 1; m += nthr) {
+      double facn = -2. * dt / (18. * PI * MU * RAD(m));
+      if (nt <= k.impl_euler_steps) facn *= (3. / 2.);
+      const int i = 3 * m;
+      for (int d = 0; d < 3; ++d) J[(size_t)(3 * nw + 3 + i + d) * n + 3 + i + d] = Jprefac * facn / dt;
+      if (m < nw - 2) {
+        facn = 2. * dt / (18. * PI * MU * RAD(m + 1));
+        if (nt <= k.impl_euler_steps) facn *= (3. / 2.);
+        for (int d = 0; d < 3; ++d) J[(size_t)(3 * nw + 3 + i + 3 + d) * n + 3 + i + d] = Jprefac * facn / dt;
+      }
+    }
+    // BlockE rows
+    for (int kk = tid; kk < nw; kk += nthr)
+      blockE_row(kk, nw, q_f, Us_f, TAU_f, lam_f, RAD(kk), cmod[f], kap[f], k.st, DL, dt, MU, J, n);
+    // BlockF / dt
+    for (int i = tid; i < nw - 1; i += nthr) {
+      const int jj = 3 * i;
+      double tv[3];
+      double fac2 = dt * DL / (24 * PI * MU * pow(RAD(i), 3.));
+      q_tangent(qload(q_f + 4 * i), tv);
+      M3 tmat = mt(rcross(tv));
+      M3 umat = rcross(Us_f + 3 * i);
+      M3 blk = madd(msub(tmat, msc(mmul(umat, tmat), 0.5)), msc(mmul(mmul(umat, umat), tmat), 1. / 12.));
+      put3(J, n, 3 * nw + jj, 3 * nw + 3 + jj, msc(blk, fac2 / dt));
+      fac2 = dt * DL / (24. * PI * MU * pow(RAD(i + 1), 3));
+      q_tangent(qload(q_f + 4 * (i + 1)), tv);
+      tmat = mt(rcross(tv));
+      umat = rcross(Us_f + 3 * (i + 1));
+      blk = madd(msub(tmat, msc(mmul(umat, tmat), 0.5)), msc(mmul(mmul(umat, umat), tmat), 1. / 12.));
+      put3(J, n, 3 * nw + jj + 3, 3 * nw + 3 + jj, msc(blk, fac2 / dt));
+    }
+  }
+#undef RAD
+  __syncthreads();
+  if (nw > 1)
+    for (int e = tid; e < 3 * nw; e += nthr) J[(size_t)(3 + e) * n + 3 * nw + e] += 1.;
+  __syncthreads();
+
+  // ---- LU with partial pivoting (first maximum wins, as the CPU loop) ----
+  __shared__ int s_piv;
+  __shared__ double s_inv;
+  const int lane = tid & 31, warp = tid >> 5;
+  for (int kc = 0; kc < n; ++kc) {
+    double *col = J + (size_t)kc * n;
+    if (warp == 0) {
+      double best = -1.0;
+      int bi = kc;
+      for (int r = kc + lane; r < n; r += 32) {
+        double v = fabs(col[r]);
+        if (v > best) {
+          best = v;
+          bi = r;
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      if (lane == 0) {
+        s_piv = bi;
+        piv[kc] = bi;
+        if (!(best > 0.0)) atomicOr(&flags[FLAG_PIVOT], 1);
+      }
+    }
+    __syncthreads();
+    const int p = s_piv;
+    if (p != kc)
+      for (int c = tid; c < n; c += nthr) {
+        double t = J[(size_t)c * n + kc];
+        J[(size_t)c * n + kc] = J[(size_t)c * n + p];
+        J[(size_t)c * n + p] = t;
+      }
+    __syncthreads();
+    if (tid == 0) s_inv = 1.0 / col[kc];
+    __syncthreads();
+    const double inv = s_inv;
+    for (int r = kc + 1 + tid; r < n; r += nthr) col[r] *= inv;
+    __syncthreads();
+    const int m = n - kc - 1;
+    for (int e = tid; e < m * m; e += nthr) {
+      const int r = kc + 1 + e % m, c = kc + 1 + e / m;
+      J[(size_t)c * n + r] -= col[r] * J[(size_t)c * n + kc];
+    }
+    __syncthreads();
+  }
+}
+
+// explicit inverse column e of filament f (test access), with the 1/dt row scaling
+__global__ void k_lu_inverse(const double *__restrict__ J, const int *__restrict__ piv, int n, int nw, double dt,
+                             double *__restrict__ out) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  double y[6 * 64];
+  for (int i = 0; i < n; ++i) y[i] = (i == e) ? 1.0 : 0.0;
+  for (int kc = 0; kc < n; ++kc)
+    if (piv[kc] != kc) {
+      double t = y[kc];
+      y[kc] = y[piv[kc]];
+      y[piv[kc]] = t;
+    }
+  for (int kc = 0; kc < n; ++kc)
+    for (int r = kc + 1; r < n; ++r) y[r] -= J[(size_t)kc * n + r] * y[kc];
+  for (int kc = n - 1; kc >= 0; --kc) {
+    y[kc] /= J[(size_t)kc * n + kc];
+    for (int r = 0; r < kc; ++r) y[r] -= J[(size_t)kc * n + r] * y[kc];
+  }
+  for (int r = 0; r < n; ++r) {
+    double v = y[r];
+    if (nw > 1 && r >= 3 * nw + 3) v /= dt;
+    out[(size_t)r * n + e] = v;  // row-major
+  }
+}
+
+// ---- error check ---------------------------------------------------------------
+__global__ void k_error_check(int np, const int *__restrict__ fil_id, const int *__restrict__ seg_id,
+                              const int *__restrict__ fil_start, const double *__restrict__ Xs,
+                              const double *__restrict__ X, const double *__restrict__ Xt,
+                              const double *__restrict__ Us, const double *__restrict__ U,
+                              const double *__restrict__ V, const double *__restrict__ W, double *__restrict__ err,
+                              int nt, FilConsts k, int *__restrict__ flags, unsigned long long *__restrict__ maxbits) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  bool over = false, nonfin = false, expl = false;
+  double mx = 0.0;
+  if (b < np) {
+    const int f = fil_id[b], i = seg_id[b];
+    const int b0 = fil_start[f], nw = fil_start[f + 1] - b0;
+    const int s0 = 6 * b0;
+    double dv[3];
+    dexpinv(Us + 3 * b, W + 3 * b, dv);
+    const double fourthirds = 4. / 3., onethird = 1. / 3., twothirdsDt = k.dt * 2. / 3.;
+    for (int d = 0; d < 3; ++d) {
+      double e1, e2;
+      if (nt <= k.impl_euler_steps) {
+        e1 = Xs[3 * b + d] - X[3 * b + d] - k.dt * V[3 * b + d];
+        e2 = Us[3 * b + d] - k.dt * dv[d];
+      } else {
+        e1 = Xs[3 * b + d] - fourthirds * X[3 * b + d] + onethird * Xt[3 * b + d] - twothirdsDt * V[3 * b + d];
+        e2 = Us[3 * b + d] - onethird * U[3 * b + d] - twothirdsDt * dv[d];
+      }
+      err[s0 + 3 * i + d] = e1;
+      err[s0 + 3 * nw + 3 * i + d] = e2;
+      over |= (fabs(e1) > k.tol) || (fabs(e2) > k.tol);
+      nonfin |= !isfinite(e1) || !isfinite(e2);
+      expl |= (fabs(e1) > 1e6) || (fabs(e2) > 1e6);
+      mx = fmax(mx, fmax(fabs(e1), fabs(e2)));
+    }
+  }
+  const unsigned full = 0xffffffffu;
+  if (__any_sync(full, over) && (threadIdx.x & 31) == 0) atomicOr(&flags[FLAG_CHECK], 1);
+  if (__any_sync(full, nonfin) && (threadIdx.x & 31) == 0) atomicOr(&flags[FLAG_NONFINITE], 1);
+  if (__any_sync(full, expl) && (threadIdx.x & 31) == 0) atomicOr(&flags[FLAG_EXPLODE], 1);
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(full, mx, o));
+  if ((threadIdx.x & 31) == 0 && maxbits) atomicMax(maxbits, fs_dbits(mx));
+}
+
+// ---- Broyden ---------------------------------------------------------------------
+#define RED_THREADS 256
+#define RED_BLOCKS 296
+
+// partial dot products D_i . b, i < iter: grid (RED_BLOCKS, iter)
+__global__ void __launch_bounds__(RED_THREADS) k_dots(const double *__restrict__ D, const double *__restrict__ b,
+                                                       size_t n6, double *__restrict__ partial) {
+  __shared__ double sh[RED_THREADS / 32];
+  const int i = blockIdx.y;
+  const double *d = D + (size_t)i * n6;
+  double acc = 0.0;
+  for (size_t k = (size_t)blockIdx.x * RED_THREADS + threadIdx.x; k < n6; k += (size_t)gridDim.x * RED_THREADS)
+    acc += d[k] * b[k];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < RED_THREADS / 32; ++w) s += sh[w];
+    partial[(size_t)i * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+// fixed-order final sums: one warp per output
+__global__ void k_reduce_rows(const double *__restrict__ partial, int nparts, int nrows, double *__restrict__ out,
+                              int do_sqrt) {
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= nrows) return;
+  double acc = 0.0;
+  for (int p = lane; p < nparts; p += 32) acc += partial[(size_t)row * nparts + p];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) out[row] = do_sqrt ? sqrt(acc) : acc;
+}
+
+// x_f = J0_f^-1 b_f (pivots, unit-L, U, 1/dt rows), then x += sum_i C_i dots_i
+__global__ void __launch_bounds__(256) k_lu_apply(const int *__restrict__ fil_start, const long long *__restrict__ joff,
+                                                  const double *__restrict__ Jall, const int *__restrict__ piv_all,
+                                                  const double *__restrict__ b, double *__restrict__ x,
+                                                  const double *__restrict__ C, const double *__restrict__ dots,
+                                                  int iter, size_t n6, double dt) {
+  extern __shared__ double y[];
+  const int f = blockIdx.x;
+  const int b0 = fil_start[f], nw = fil_start[f + 1] - b0, n = 6 * nw, s0 = 6 * b0;
+  const double *J = Jall + joff[f];
+  const int *piv = piv_all + s0;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  for (int r = tid; r < n; r += nthr) y[r] = b[s0 + r];
+  __syncthreads();
+  if (tid == 0)
+    for (int kc = 0; kc < n; ++kc) {
+      int p = piv[kc];
+      if (p != kc) {
+        double t = y[kc];
+        y[kc] = y[p];
+        y[p] = t;
+      }
+    }
+  __syncthreads();
+  for (int kc = 0; kc < n; ++kc) {
+    const double yk = y[kc];
+    const double *col = J + (size_t)kc * n;
+    for (int r = kc + 1 + tid; r < n; r += nthr) y[r] -= col[r] * yk;
+    __syncthreads();
+  }
+  for (int kc = n - 1; kc >= 0; --kc) {
+    const double *col = J + (size_t)kc * n;
+    const double yk = y[kc] / col[kc];
+    __syncthreads();
+    if (tid == 0) y[kc] = yk;
+    for (int r = tid; r < kc; r += nthr) y[r] -= col[r] * yk;
+    __syncthreads();
+  }
+  for (int r = tid; r < n; r += nthr) {
+    double v = y[r];
+    if (nw > 1 && r >= 3 * nw + 3) v /= dt;
+    for (int i = 0; i < iter; ++i) v += C[(size_t)i * n6 + s0 + r] * dots[i];
+    x[s0 + r] = v;
+  }
+}
+
+// dE = newerr - err and per-block sums of dE^2
+__global__ void __launch_bounds__(RED_THREADS) k_diff_sq(const double *__restrict__ ne, const double *__restrict__ e,
+                                                          double *__restrict__ dE, size_t n6,
+                                                          double *__restrict__ partial) {
+  __shared__ double sh[RED_THREADS / 32];
+  double acc = 0.0;
+  for (size_t k = (size_t)blockIdx.x * RED_THREADS + threadIdx.x; k < n6; k += (size_t)gridDim.x * RED_THREADS) {
+    double d = ne[k] - e[k];
+    dE[k] = d;
+    acc += d * d;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < RED_THREADS / 32; ++w) s += sh[w];
+    partial[blockIdx.x] = s;
+  }
+}
+
+// C_iter = -tmp/|dE| - upd/|dE|, D_iter = dE/|dE| (main.cpp:657-661)
+__global__ void k_broyden_cols(const double *__restrict__ tmp, const double *__restrict__ upd,
+                               const double *__restrict__ dE, const double *__restrict__ nrm, size_t n6,
+                               double *__restrict__ Ccol, double *__restrict__ Dcol) {
+  size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n6) return;
+  const double n = nrm[0];
+  double t = tmp[k] * (-1. / n);
+  t -= upd[k] / n;
+  Ccol[k] = t;
+  Dcol[k] = dE[k] / n;
+}
+
+// ---- update / step ----------------------------------------------------------------
+__global__ void k_update(int np, const int *__restrict__ fil_id, const int *__restrict__ seg_id,
+                         const int *__restrict__ fil_start, const double *__restrict__ u, double *__restrict__ Xs,
+                         double *__restrict__ Us, const double *__restrict__ q, double *__restrict__ qs,
+                         double *__restrict__ lam) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= np) return;
+  const int f = fil_id[b], i = seg_id[b];
+  const int b0 = fil_start[f], nw = fil_start[f + 1] - b0, l0 = b0 - f;
+  const int s = 6 * b0;
+  double us[3];
+  if (i == 0) {
+    for (int d = 0; d < 3; ++d) {
+      Xs[3 * b + d] -= u[s + d];
+      us[d] = Us[3 * b + d] - u[s + 3 + d];
+    }
+  } else {
+    for (int d = 0; d < 3; ++d) us[d] = Us[3 * b + d] - u[s + 6 + 3 * (i - 1) + d];
+  }
+  for (int d = 0; d < 3; ++d) Us[3 * b + d] = us[d];
+  qstore(q_expm(qload(q + 4 * b), us), qs + 4 * b);
+  if (i < nw - 1)
+    for (int d = 0; d < 3; ++d) lam[3 * (l0 + i) + d] -= u[s + 3 * nw + 3 + 3 * i + d];
+}
+
+__global__ void k_step(int np, int nlink, double *__restrict__ X, double *__restrict__ Xs, double *__restrict__ Xt,
+                       double *__restrict__ U, double *__restrict__ Us, double *__restrict__ Ut,
+                       double *__restrict__ q, double *__restrict__ qt, double *__restrict__ lam,
+                       double *__restrict__ lam1, double *__restrict__ lam2, int nt, int ex) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < np) {
+    const int b = t;
+    double uu[3];
+    for (int d = 0; d < 3; ++d) {
+      Xt[3 * b + d] = X[3 * b + d];
+      X[3 * b + d] = Xs[3 * b + d];
+      Ut[3 * b + d] = U[3 * b + d];
+      uu[d] = Us[3 * b + d];
+      U[3 * b + d] = uu[d];
+    }
+    Q qq = qload(q + 4 * b);
+    qstore(qq, qt + 4 * b);
+    qstore(q_expm(qq, uu), q + 4 * b);
+  }
+  if (t < 3 * nlink) {
+    const int kk = t;
+    if (nt > ex) {
+      double lamtmp = 3 * lam[kk] - 3 * lam1[kk] + lam2[kk];
+      lam2[kk] = lam1[kk];
+      lam1[kk] = lam[kk];
+      lam[kk] = lamtmp;
+    } else if (nt == ex) {
+      double lamtmp = 2. * lam[kk] - lam1[kk];
+      lam2[kk] = lam1[kk];
+      lam1[kk] = lam[kk];
+      lam[kk] = lamtmp;
+    } else {
+      lam1[kk] = lam[kk];
+    }
+  }
+}
+
+FilConsts make_fconsts(const fs_ctx *c) {
+  FilConsts k;
+  for (int d = 0; d < 3; ++d) {
+    k.L[d] = c->L[d];
+    k.gravity[d] = c->p.gravity[d];
+    k.st[d] = c->p.strain_twist[d];
+  }
+  k.dt = c->p.dt;
+  k.dl = c->p.dl;
+  k.mu = c->p.mu;
+  k.tol = c->p.tol;
+  k.impl_euler_steps = c->p.impl_euler_steps;
+  k.lambda_extrap_step = c->p.lambda_extrap_step;
+  return k;
+}
+
+}  // namespace
+
+fs_status fil_initial_guess(fs_ctx *c) {
+  if (!c->have_state) return FS_ERR_STATE;
+  k_initial_guess<<<fs_blocks(c->np, 256), 256, 0, c->stream>>>(c->np, c->seg_id, c->X, c->Xt, c->U, c->Ut, c->q,
+                                                                 c->Xs, c->Us, c->qs);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+fs_status fil_forces(fs_ctx *c, int nt) {
+  (void)nt;
+  if (!c->have_state) return FS_ERR_STATE;
+  FilConsts k = make_fconsts(c);
+  k_unrobot_assign<<<fs_blocks(c->nfil, 128), 128, 0, c->stream>>>(c->nfil, c->fil_start, c->qs, c->Xs, c->Y, k);
+  FS_LAUNCH_CHECK();
+  k_forces<<<fs_blocks(c->np, 256), 256, 0, c->stream>>>(c->np, c->fil_id, c->seg_id, c->fil_start, c->qs, c->lam,
+                                                          c->kap, c->cc, c->F, c->TAU, k);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+fs_status fil_jacobian_build(fs_ctx *c, int nt) {
+  if (!c->have_state) return FS_ERR_STATE;
+  FilConsts k = make_fconsts(c);
+  k_jacobian<<<c->nfil, 256, 0, c->stream>>>(c->nfil, c->fil_start, c->qs, c->Us, c->TAU, c->lam, c->kap, c->cc,
+                                             c->joff, c->J, c->jpiv, nt, k, c->p.a, c->p.ah, c->flags);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+fs_status fil_jacobian_inverse(fs_ctx *c, int f, double *out_d) {
+  int fs_h[2];
+  long long off;
+  FS_CUDA(cudaMemcpyAsync(fs_h, c->fil_start + f, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  FS_CUDA(cudaMemcpyAsync(&off, c->joff + f, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+  FS_CUDA(cudaStreamSynchronize(c->stream));
+  const int nw = fs_h[1] - fs_h[0], n = 6 * nw;
+  if (nw > 64) return FS_ERR_INVALID_ARG;
+  k_lu_inverse<<<fs_blocks(n, 64), 64, 0, c->stream>>>(c->J + off, c->jpiv + 6 * fs_h[0], n, nw, c->p.dt, out_d);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+fs_status fil_error_check(fs_ctx *c, const double *V, const double *W, double *err, int nt) {
+  if (!c->have_state) return FS_ERR_STATE;
+  FilConsts k = make_fconsts(c);
+  FS_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(int) * 3, c->stream));  // check, nonfinite, explode
+  FS_CUDA(cudaMemsetAsync(c->maxerr_bits, 0, sizeof(unsigned long long), c->stream));
+  k_error_check<<<fs_blocks(c->np, 256), 256, 0, c->stream>>>(c->np, c->fil_id, c->seg_id, c->fil_start, c->Xs, c->X,
+                                                               c->Xt, c->Us, c->U, V, W, err, nt, k, c->flags,
+                                                               c->maxerr_bits);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+fs_status fil_broyden_apply(fs_ctx *c, const double *b, double *x, int iter) {
+  if (!c->have_state) return FS_ERR_STATE;
+  const size_t n6 = (size_t)6 * c->np;
+  if (iter > 0) {
+    dim3 g(RED_BLOCKS, iter);
+    k_dots<<<g, RED_THREADS, 0, c->stream>>>(c->Dmat, b, n6, c->partials);
+    FS_LAUNCH_CHECK();
+    k_reduce_rows<<<fs_blocks(iter, 8), 256, 0, c->stream>>>(c->partials, RED_BLOCKS, iter, c->dots, 0);
+    FS_LAUNCH_CHECK();
+  }
+  const size_t smem = sizeof(double) * 6 * (size_t)c->max_nw;
+  k_lu_apply<<<c->nfil, 256, smem, c->stream>>>(c->fil_start, c->joff, c->J, c->jpiv, b, x, c->Cmat, c->dots, iter,
+                                                n6, c->p.dt);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+// main.cpp:641-663 with the current err/newerr/upd: history column `iter`
+fs_status fil_broyden_update(fs_ctx *c, int iter) {
+  const size_t n6 = (size_t)6 * c->np;
+  k_diff_sq<<<RED_BLOCKS, RED_THREADS, 0, c->stream>>>(c->newerr, c->err, c->dE, n6, c->partials);
+  FS_LAUNCH_CHECK();
+  k_reduce_rows<<<1, 32, 0, c->stream>>>(c->partials, RED_BLOCKS, 1, c->scalars, 1);
+  FS_LAUNCH_CHECK();
+  FS_TRY(fil_broyden_apply(c, c->dE, c->tmp, iter));
+  k_broyden_cols<<<fs_blocks((long long)n6, 256), 256, 0, c->stream>>>(c->tmp, c->upd, c->dE, c->scalars, n6,
+                                                                       c->Cmat + (size_t)iter * n6,
+                                                                       c->Dmat + (size_t)iter * n6);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+fs_status fil_state_update(fs_ctx *c, const double *upd) {
+  if (!c->have_state) return FS_ERR_STATE;
+  k_update<<<fs_blocks(c->np, 256), 256, 0, c->stream>>>(c->np, c->fil_id, c->seg_id, c->fil_start, upd, c->Xs,
+                                                          c->Us, c->q, c->qs, c->lam);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+fs_status fil_step(fs_ctx *c, int nt) {
+  if (!c->have_state) return FS_ERR_STATE;
+  int n = c->np > 3 * c->nlink ? c->np : 3 * c->nlink;
+  k_step<<<fs_blocks(n, 256), 256, 0, c->stream>>>(c->np, c->nlink, c->X, c->Xs, c->Xt, c->U, c->Us, c->Ut, c->q,
+                                                    c->qt, c->lam, c->lam1, c->lam2, nt, c->p.lambda_extrap_step);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+fs_status fil_max_abs_err(fs_ctx *c, const double *err, double *out_h) {
+  (void)err;
+  unsigned long long bits;
+  FS_CUDA(cudaMemcpyAsync(&bits, c->maxerr_bits, sizeof bits, cudaMemcpyDeviceToHost, c->stream));
+  FS_CUDA(cudaStreamSynchronize(c->stream));
+  memcpy(out_h, &bits, sizeof bits);
+  return FS_OK;
+}

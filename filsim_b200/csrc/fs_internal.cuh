@@ -1,0 +1,143 @@
+// fs_internal.cuh -- context layout and helpers shared by the sm_100a kernels
+// of libfilsim_gpu.
+#pragma once
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+#include "../../include/filsim_gpu.h"
+
+#define FS_PI 3.14159265358979323846264338327950288
+
+// Spread tile edge (grid points) and warps per spread CTA (one x-plane each).
+#define FS_TILE 16
+// Beads staged in shared memory per spread pass.
+#define FS_SPREAD_CHUNK 16
+// Collision events kept per bead (pairs inside the barrier range).
+#define FS_MAX_EVENTS 64
+// Flag words (device int array ctx->flags).
+enum { FLAG_CHECK = 0, FLAG_NONFINITE = 1, FLAG_EXPLODE = 2, FLAG_CAPACITY = 3, FLAG_PIVOT = 4, FLAG_COUNT = 8 };
+
+struct fs_sort {
+  // counting sort of `n` items by integer key in [0, nkeys)
+  int nkeys;
+  int *key;      // per item
+  int *count;    // nkeys
+  int *start;    // nkeys + 1
+  int *cursor;   // nkeys
+  int *sorted;   // items in (key, id) order
+  int *block_sums;
+};
+
+struct fs_ctx {
+  fs_params p;
+  int device;
+  cudaStream_t stream;
+  bool own_stream;
+  int max_beads, max_fil;
+  int precision;
+
+  // FCM grid
+  int nx, ny, nz, nzh;
+  size_t N, NH;
+  double L[3];
+  void *grid_real;   // 3 x N reals (force grid f, then velocity grid u)
+  void *grid_cplx;   // 3 x NH complex
+  cufftHandle plan_fwd[2], plan_inv[2];  // [precision]
+  bool plan_ok[2];
+  int nbin[3], nbins;  // spread bins (FS_TILE wide in stencil-start space)
+  fs_sort bins;
+  int last_grid_prec;  // precision of the grids from the last solve (-1: none)
+
+  // collision cells
+  int M[3], ncell;
+  fs_sort cells;
+  int *head, *list, *map;
+  int *cell_rank;      // descending-id rank of each bead inside its cell
+  int *pair_count, *pair_off, *pair_scan_tmp;
+  int cells_np;        // beads in the last link (-1: none)
+  double *min_dist2;   // device scalar
+  unsigned long long *min_dist2_bits;
+
+  // filament suspension (device)
+  int nfil, np, nlink;
+  bool have_state;
+  int *fil_start, *fil_id, *seg_id;
+  double *X, *Xs, *Xt, *U, *Us, *Ut, *q, *qs, *qt, *F, *TAU, *lam, *lam1, *lam2, *kap, *cc, *radius;
+  double *Y, *V, *W;
+  double *err, *newerr, *upd, *tmp, *dE;
+  double *Cmat, *Dmat;   // broyden_maxiter x 6Np
+  double *J;             // per-filament LU factors (column-major), offsets joff
+  long long *joff;
+  int *jpiv;             // per-filament pivots, offset 6*fil_start[f]
+  int max_nw;
+  double *dots;          // broyden_maxiter partial dots
+  double *partials;      // reduction scratch
+  double *scalars;       // [0] = ||dE||
+  int *flags;            // FLAG_COUNT ints
+  int *flags_h;          // pinned host copy
+  unsigned long long *maxerr_bits;
+  fs_diag diag;
+  size_t bytes;
+};
+
+#define FS_CUDA(call)                                                         \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess) {                                                  \
+      fprintf(stderr, "filsim_gpu: %s failed: %s (%s:%d)\n", #call,          \
+              cudaGetErrorString(e_), __FILE__, __LINE__);                    \
+      return e_ == cudaErrorMemoryAllocation ? FS_ERR_OOM : FS_ERR_CUDA;      \
+    }                                                                         \
+  } while (0)
+
+#define FS_LAUNCH_CHECK()                                                     \
+  do {                                                                        \
+    cudaError_t e_ = cudaGetLastError();                                      \
+    if (e_ != cudaSuccess) {                                                  \
+      fprintf(stderr, "filsim_gpu: launch failed: %s (%s:%d)\n",             \
+              cudaGetErrorString(e_), __FILE__, __LINE__);                    \
+      return FS_ERR_CUDA;                                                     \
+    }                                                                         \
+  } while (0)
+
+#define FS_TRY(call)                   \
+  do {                                 \
+    fs_status s_ = (call);             \
+    if (s_ != FS_OK) return s_;        \
+  } while (0)
+
+static inline int fs_blocks(long long n, int threads) { return (int)((n + threads - 1) / threads); }
+
+// ---- entry points implemented across the .cu files (internal C++ linkage) ----
+fs_status fs_sort_alloc(fs_sort *s, int nkeys, int max_items, size_t *bytes);
+void fs_sort_free(fs_sort *s);
+fs_status fs_sort_run(fs_sort *s, int n, cudaStream_t st);  // keys in s->key must be set
+
+fs_status fcm_init(fs_ctx *c);
+void fcm_free(fs_ctx *c);
+fs_status fcm_mobility(fs_ctx *c, const double *Y, const double *F, const double *T, double *V, double *W, int np);
+fs_status fcm_friction(fs_ctx *c, const double *F, const double *T, double *V, double *W, int np);
+fs_status fcm_flow_solve_only(fs_ctx *c, const double *f, double *u);
+fs_status fcm_spread_only(fs_ctx *c, const double *Y, const double *F, const double *T, int np, double *f);
+
+fs_status cells_init(fs_ctx *c);
+void cells_free(fs_ctx *c);
+fs_status cells_link(fs_ctx *c, const double *Xs, int np);
+fs_status cells_barrier(fs_ctx *c, const double *Y, double *F, int np, int nt, const int *fil_id, const int *seg_id,
+                        int *pairs_d, int max_pairs, int *npairs_h);
+
+fs_status fil_initial_guess(fs_ctx *c);
+fs_status fil_forces(fs_ctx *c, int nt);
+fs_status fil_jacobian_build(fs_ctx *c, int nt);
+fs_status fil_jacobian_inverse(fs_ctx *c, int f, double *out_d);
+fs_status fil_error_check(fs_ctx *c, const double *V, const double *W, double *err, int nt);
+fs_status fil_broyden_apply(fs_ctx *c, const double *b, double *x, int iter);
+fs_status fil_broyden_update(fs_ctx *c, int iter);
+fs_status fil_state_update(fs_ctx *c, const double *upd);
+fs_status fil_step(fs_ctx *c, int nt);
+fs_status fil_max_abs_err(fs_ctx *c, const double *err, double *out_h);
+
+// ordered bit patterns for atomicMin/Max on non-negative doubles
+__device__ __forceinline__ unsigned long long fs_dbits(double x) { return (unsigned long long)__double_as_longlong(x); }

@@ -1,0 +1,247 @@
+/*
+ * filsim_gpu.h -- C-ABI of libfilsim_gpu, the sm_100a (B200) implementation of
+ * FilSim's hot path: the Force Coupling Method (FCM) mobility solve, the
+ * cell-linked-list collision barrier, and the implicit BDF2 + Broyden step that
+ * drives them.
+ *
+ * Conventions (shared by every entry point):
+ *   - All arrays are plain contiguous C arrays. Per-bead vectors are Np x 3
+ *     row-major doubles (x0 y0 z0 x1 y1 z1 ...), exactly the storage behind the
+ *     reference's `double**` bead arrays (c_array_functions.cpp:12-21), so a
+ *     caller passes `&fcm.Y[0][0]`.
+ *   - Pointers are DEVICE pointers unless the parameter name ends in `_h`
+ *     (host memory).
+ *   - Every entry point returns an fs_status (0 = FS_OK). No C++ exception
+ *     crosses the ABI. fs_status_string() gives a message.
+ *   - One fs_ctx per CUDA stream; a context is not thread-safe. Work is queued
+ *     on the context's stream; entry points that return host values
+ *     synchronise that stream.
+ *   - There is no CPU fallback: on a machine without a usable sm_100 GPU,
+ *     fs_create returns FS_ERR_NO_DEVICE.
+ *
+ * Reference interfaces replaced (file:line inside the FilSim sources):
+ *   struct Fcm               FCMfunctions.hpp:7-59
+ *   struct LinkedList        CollisionBarrierFilament.hpp:19-57
+ *   class filamentJsolver    FilamentJacobianSolver.hpp:14-87
+ *   Filament per-step calls  Filament.hpp:227-505, 803-1120
+ *   ErrorCheckFCM            MobilityConstraints.cpp:447-770
+ *   time loop                main.cpp:284-754
+ */
+#ifndef FILSIM_GPU_H
+#define FILSIM_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FS_ABI_VERSION 1
+
+typedef int fs_status;
+enum {
+  FS_OK = 0,
+  FS_ERR_INVALID_ARG = 1,     /* bad size, null pointer, unsupported parameter */
+  FS_ERR_NO_DEVICE = 2,       /* no CUDA device, or not sm_100 */
+  FS_ERR_CUDA = 3,            /* a CUDA runtime call failed */
+  FS_ERR_CUFFT = 4,           /* a cuFFT call failed */
+  FS_ERR_OOM = 5,             /* device allocation failed */
+  FS_ERR_NOT_CONVERGED = 6,   /* Broyden reached broyden_maxiter (state is still advanced, as the reference does) */
+  FS_ERR_NONFINITE = 7,       /* NaN/Inf met in a residual */
+  FS_ERR_CAPACITY = 8,        /* an internal fixed-size list overflowed (reported, never written out of bounds) */
+  FS_ERR_STATE = 9            /* call order violated (e.g. barrier before link) */
+};
+
+/* Precision of the FCM spread / FFT / interpolation chain. */
+enum { FS_PREC_FP64 = 0, FS_PREC_FP32 = 1 };
+
+/*
+ * Runtime parameters. They replace the compile-time macros of config.hpp and the
+ * derived constants of multi_filament_header.hpp:32-81. fs_params_default()
+ * fills the values the reference derives (sigma = a/sqrt(pi),
+ * sigma_dip = a/(36 pi)^(1/6), dx = sigma_dip/1.5, cell width 2.5a, ...).
+ */
+typedef struct fs_params {
+  int npts_x, npts_y, npts_z;   /* NPTS_X/Y/Z: periodic FCM grid */
+  int ngd;                      /* Gaussian support points per axis (reference `ngd`) */
+  double a;                     /* bead radius (FCM kernels, drag) */
+  double ah;                    /* radius of bead 0 of each filament (Jacobian, `ah`) */
+  double mu;                    /* viscosity MU */
+  double dx;                    /* grid spacing; box length = npts * dx */
+  double sigma;                 /* monopole Gaussian width */
+  double sigma_dip;             /* dipole Gaussian width */
+  double dl;                    /* bead spacing DL */
+  double dt;                    /* time step */
+  double gravity[3];            /* external force added to every bead (WeightPerLength*DL) */
+  double strain_twist[3];       /* intrinsic strain-twist (STRAINTWISTZ, X, Y) */
+  double tol;                   /* Broyden tolerance: any(|Err| > tol) keeps iterating */
+  int broyden_maxiter;          /* Broyden iteration cap (reference: 300) */
+  int impl_euler_steps;         /* ImplEulerSteps: nt <= this uses implicit Euler */
+  int initial_friction_steps;   /* initialFrictionSteps: nt <= this uses Stokes drag only */
+  int precision;                /* FS_PREC_FP64 or FS_PREC_FP32 for the FCM chain */
+  double barrier_fs_over_2a;    /* Barrier_FS_over_2a */
+  double barrier_distance_cap;  /* Barrier_distance_cap */
+  double cell_width;            /* Rref: ideal collision cell width (2.5a) */
+  int lambda_extrap_step;       /* nt at which lambda extrapolation turns linear (reference: 12) */
+  int reserved0;
+} fs_params;
+
+/* Per-call diagnostics of the last fs_run_steps / fs_step_implicit call. */
+typedef struct fs_diag {
+  int last_nt;                  /* last completed time step */
+  int last_iters;               /* Broyden iterations of the last step */
+  long long total_iters;        /* Broyden iterations summed over the call */
+  long long mobility_solves;    /* FCM (or friction) solves issued */
+  int not_converged_steps;      /* steps that stopped at broyden_maxiter */
+  int nonfinite;                /* 1 if a NaN/Inf residual was seen */
+  int explosion;                /* 1 if any |Err| > 1e6 was seen (reference warning) */
+  int reserved;
+  double min_dist2;             /* last collision-barrier minimum squared distance */
+  double last_max_abs_err;      /* max |Err| at the end of the last step */
+} fs_diag;
+
+/*
+ * Host-side view of the filament suspension, used to upload and download the
+ * device-resident state. Layouts (all host pointers):
+ *   fil_start[nfil+1]   bead prefix: filament f owns beads [fil_start[f], fil_start[f+1])
+ *   X, Xs, Xt, U, Us, Ut, F, TAU   np*3   (Bead.hpp:33-44; Xs/Us/qs = iterate, X/U/q = current, Xt/Ut/qt = previous)
+ *   q, qs, qt                      np*4   (scalar first)
+ *   lam, lam1, lam2                (np-nfil)*3, link l of filament f at fil_start[f]-f+l
+ *   kap, c                         nfil   (bending, twist moduli: myKAP, myC)
+ * Any pointer may be NULL on download to skip that field.
+ */
+typedef struct fs_host_state {
+  int nfil;
+  int np;
+  const int *fil_start;
+  double *X, *Xs, *Xt;
+  double *U, *Us, *Ut;
+  double *q, *qs, *qt;
+  double *F, *TAU;
+  double *lam, *lam1, *lam2;
+  double *kap, *c;
+} fs_host_state;
+
+typedef struct fs_ctx fs_ctx;
+
+/* ---- library / context ---------------------------------------------------- */
+
+int fs_abi_version(void);
+const char *fs_status_string(fs_status s);
+void fs_params_default(fs_params *p, int npts_x, int npts_y, int npts_z);
+
+/* Allocates grids, cuFFT plans and bead buffers for up to max_beads beads and
+ * max_filaments filaments (the suspension itself is uploaded later).
+ * Replaces Fcm::initialise (FCMfunctions.cpp:10-168) and
+ * LinkedList::initialise (CollisionBarrierFilament.cpp:274-304).
+ * stream: a cudaStream_t or NULL for a context-owned stream. */
+fs_status fs_create(const fs_params *p, int max_beads, int max_filaments, void *stream, fs_ctx **out);
+/* Replaces Fcm::free_memory (FCMfunctions.cpp:468-519). */
+fs_status fs_destroy(fs_ctx *ctx);
+fs_status fs_get_params(const fs_ctx *ctx, fs_params *p_h);
+fs_status fs_set_precision(fs_ctx *ctx, int precision);
+fs_status fs_synchronize(fs_ctx *ctx);
+/* Bytes of device memory the context holds. */
+fs_status fs_device_bytes(const fs_ctx *ctx, size_t *bytes_h);
+
+/* ---- FCM mobility (struct Fcm) -------------------------------------------- */
+
+/* V, W (np x 3) from positions Y, forces F and torques T (np x 3), periodic
+ * Stokes flow. Replaces Fcm::mobility_solve (FCMfunctions.cpp:175-464):
+ * GA_setup :536-547, gaussian_setup :549-593, spread :596-646, forward FFT
+ * :360-372, flow_solve :648-736, inverse FFT :403-406, particle_velocities
+ * :740-770, particle_rotations :774-808. Y may lie anywhere in (-L, L) per axis
+ * (the reference's fmod output). Precision follows fs_set_precision. */
+fs_status fs_fcm_mobility(fs_ctx *ctx, const double *Y, const double *F, const double *T,
+                          double *V, double *W, int np);
+/* Same call on HOST buffers: copies in, solves, copies out, synchronises. */
+fs_status fs_fcm_mobility_host(fs_ctx *ctx, const double *Y_h, const double *F_h, const double *T_h,
+                               double *V_h, double *W_h, int np);
+/* Stokes drag only: V = F/(6 pi mu a), W = T/(8 pi mu a^3).
+ * Replaces Fcm::friction_mobility_solve (FCMfunctions.cpp:865-880). */
+fs_status fs_fcm_friction(fs_ctx *ctx, const double *F, const double *T, double *V, double *W, int np);
+/* The force-distribution step alone (GA_setup + gaussian_setup +
+ * mono_and_dipole_force_distribution, FCMfunctions.cpp:536-646) in FP64:
+ * writes the spread force grid f (device, 3 x Nx x Ny x Nz doubles,
+ * component-major, z fastest). */
+fs_status fs_fcm_spread(fs_ctx *ctx, const double *Y, const double *F, const double *T, int np, double *f);
+/* Copies the velocity grid u of the last FP64 mobility solve (3 x Nx x Ny x Nz
+ * doubles) to host; count is the number of doubles grid_h holds. */
+fs_status fs_fcm_get_grid(fs_ctx *ctx, double *grid_h, size_t count);
+/* Runs flow_solve alone on a given force grid (3 x Nx x Ny x Nz, device):
+ * forward FFT, projection, inverse FFT, result written to u (same layout).
+ * Used for the reference's sinusoidal-forcing check (FCMfunctions.cpp:252-275). */
+fs_status fs_fcm_flow_solve(fs_ctx *ctx, const double *f, double *u);
+
+/* ---- collision barrier (struct LinkedList) -------------------------------- */
+
+/* Cell grid sizes M_X, M_Y, M_Z (CollisionBarrierFilament.cpp:277-281). */
+fs_status fs_cells_dims(const fs_ctx *ctx, int *mxyz_h);
+/* Bins beads into cells from unwrapped positions Xs (np x 3) with a counting
+ * sort; the result is the reference's head/list linked list.
+ * Replaces LinkedList::link (CollisionBarrierFilament.cpp:370-433). */
+fs_status fs_cells_link(fs_ctx *ctx, const double *Xs, int np);
+/* Copies the linked list out: head (ncell), list (np), map (13*ncell); any may be NULL. */
+fs_status fs_cells_get_lists(fs_ctx *ctx, int *head_h, int *list_h, int *map_h);
+/* Adds the barrier forces for positions Y into F_inout (both np x 3, device)
+ * using the cells of the last fs_cells_link. min_dist2_h (may be NULL)
+ * receives the minimum squared separation examined.
+ * fil_id, seg_id: per-bead filament/segment number (device ints) or NULL to
+ * use the uploaded suspension.
+ * Replaces LinkedList::apply_collision_barrier (CollisionBarrierFilament.cpp:24-271). */
+fs_status fs_collision_barrier(fs_ctx *ctx, const double *Y, double *F_inout, int np, int nt,
+                               const int *fil_id, const int *seg_id, double *min_dist2_h);
+/* Lists the interacting pairs (i, j) in the reference's visiting order
+ * (pairs_h: 2*max_pairs ints); *npairs_h receives the total count. */
+fs_status fs_collision_pairs(fs_ctx *ctx, const double *Y, int np, int nt,
+                             const int *fil_id, const int *seg_id,
+                             int *pairs_h, int max_pairs, int *npairs_h);
+
+/* ---- filament suspension and the implicit step ----------------------------- */
+
+/* Uploads / downloads the suspension (fs_host_state layouts). */
+fs_status fs_state_upload(fs_ctx *ctx, const fs_host_state *s_h);
+fs_status fs_state_download(fs_ctx *ctx, fs_host_state *s_h);
+/* Device pointers of the resident bead arrays, for callers that drive the
+ * step themselves: which = "Xs", "X", "Xt", "Us", "U", "Ut", "qs", "q", "qt",
+ * "F", "TAU", "Y", "V", "W", "lam", "err", "update". */
+fs_status fs_state_device_ptr(fs_ctx *ctx, const char *which, double **ptr_h);
+
+/* Filament::initialGuess (Filament.hpp:227-237, Bead.hpp:202-217). */
+fs_status fs_initial_guess(fs_ctx *ctx);
+/* Filament::unRobotArmify, setZeroForcesTorques, applyElasticTorques,
+ * applyConstraintForcesTorques, applyExternalForcesTorques
+ * (Filament.hpp:271-402, 489-505), then Fcm::assign_filament_data
+ * (FCMfunctions.cpp:882-918): Y = fmod(Xs, L), F, T into the FCM arrays. */
+fs_status fs_filament_forces(fs_ctx *ctx, int nt);
+/* filamentJsolver::buildJacobian (FilamentJacobianSolver.hpp:36-47 and
+ * Filament.hpp:803-1120): per filament the approximate Jacobian is built and
+ * LU-factorised; Broyden history is cleared. */
+fs_status fs_jacobian_build(fs_ctx *ctx, int nt);
+/* Copies the explicit inverse J0^-1 of filament f (6Nw x 6Nw row-major, with
+ * the reference's 1/dt row scaling, Filament.hpp:862-865) to host. */
+fs_status fs_jacobian_get_inverse(fs_ctx *ctx, int f, double *jinv_h, int n);
+/* ErrorCheckFCM (MobilityConstraints.cpp:447-770): err (6Np) from V, W (np x 3);
+ * *check_h = 1 if any |err| > tol. */
+fs_status fs_error_check(fs_ctx *ctx, const double *V, const double *W, double *err, int nt, int *check_h);
+/* filamentJsolver::solve (FilamentJacobianSolver.hpp:49-73): x = J0^-1 b plus
+ * the bad-Broyden corrections of the first `iter` history columns. */
+fs_status fs_broyden_apply(fs_ctx *ctx, const double *b, double *x, int iter);
+/* addCmatCol / addDmatCol (FilamentJacobianSolver.hpp:76-84). */
+fs_status fs_broyden_set_cols(fs_ctx *ctx, const double *c, const double *d, int iter);
+/* Filament::update (Filament.hpp:425-452): state -= update (6Np). */
+fs_status fs_state_update(fs_ctx *ctx, const double *update);
+/* Filament::step (Filament.hpp:455-478). */
+fs_status fs_step(fs_ctx *ctx, int nt);
+/* One full implicit time step nt (main.cpp:284-754 loop body). */
+fs_status fs_step_implicit(fs_ctx *ctx, int nt, int *iters_h);
+/* nsteps implicit steps from nt_start; iters_h (may be NULL) receives the
+ * Broyden iteration count of each step. */
+fs_status fs_run_steps(fs_ctx *ctx, int nt_start, int nsteps, int *iters_h);
+fs_status fs_get_diag(fs_ctx *ctx, fs_diag *d_h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FILSIM_GPU_H */

@@ -1,0 +1,168 @@
+"""FCM mobility on the GPU against the CPU oracle (FCMfunctions.cpp:175-880).
+
+Tolerances: FP64 mode U/Omega within 1e-10 of the oracle relative to the
+largest component; FP32 mode within 1e-5 of FP64.
+"""
+import numpy as np
+import pytest
+import torch
+
+from filsim_b200 import abi
+from filsim_b200.configs import make_mobility_case, params_for
+from filsim_b200.fcm import Context, Fcm, mobility_host
+
+pytestmark = pytest.mark.gpu
+
+FP64_REL = 1e-10
+FP32_REL = 1e-5
+
+
+def rel_err(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+def gpu_mobility(p, Y, F, T, prec=abi.FS_PREC_FP64):
+    ctx = Context(p, max_beads=max(1, Y.shape[0]))
+    ctx.set_precision(prec)
+    fcm = Fcm(ctx, Y.shape[0])
+    fcm.set(Y, F, T)
+    fcm.mobility_solve()
+    ctx.synchronize()
+    out = fcm.V.cpu().numpy(), fcm.W.cpu().numpy()
+    ctx.close()
+    return out
+
+
+@pytest.fixture(scope="module")
+def case64(gpu_lib):
+    return make_mobility_case(64, 32, 15, seed=1000)
+
+
+def test_mobility_64_fp64_matches_oracle(oracle, case64):
+    p, s, Y, F, T = case64
+    V0, W0 = oracle.fcm_mobility(p, Y, F, T)
+    V, W = gpu_mobility(p, Y, F, T)
+    assert rel_err(V, V0) < FP64_REL
+    assert rel_err(W, W0) < FP64_REL
+
+
+def test_mobility_golden_fixture(case64):
+    g = np.load(__import__("os").path.join(__import__("os").path.dirname(__file__), "golden", "mobility_64.npz"))
+    p = params_for(64)
+    V, W = gpu_mobility(p, g["Y"], g["F"], g["T"])
+    assert rel_err(V, g["V"]) < FP64_REL
+    assert rel_err(W, g["W"]) < FP64_REL
+
+
+def test_spread_grid_matches_oracle(oracle):
+    p, s, Y, F, T = make_mobility_case(32, 6, 5, seed=7)
+    _, _, f0, _ = oracle.fcm_mobility(p, Y, F, T, return_grids=True)
+    ctx = Context(p, max_beads=Y.shape[0])
+    fcm = Fcm(ctx, Y.shape[0])
+    fcm.set(Y, F, T)
+    f = fcm.spread().cpu().numpy()
+    assert np.abs(f - f0).max() / np.abs(f0).max() < 1e-13
+
+
+def test_velocity_grid_matches_oracle(oracle):
+    p, s, Y, F, T = make_mobility_case(32, 6, 5, seed=8)
+    _, _, _, u0 = oracle.fcm_mobility(p, Y, F, T, return_grids=True)
+    ctx = Context(p, max_beads=Y.shape[0])
+    fcm = Fcm(ctx, Y.shape[0])
+    fcm.set(Y, F, T)
+    fcm.mobility_solve()
+    u = fcm.velocity_grid()
+    assert np.abs(u - u0).max() / np.abs(u0).max() < 1e-11
+
+
+def test_sinusoidal_forcing_known_answer():
+    """FCMfunctions.cpp:252-275: fz = sin(2 pi x / Nx) gives uz = fz / k^2 (mu = 1)."""
+    p = params_for(32)
+    N = 32
+    f = np.zeros((3, N, N, N))
+    f[2] = np.sin(2 * np.pi * np.arange(N) / N)[:, None, None]
+    ctx = Context(p, max_beads=1)
+    fcm = Fcm(ctx, 1)
+    u = fcm.flow_solve(f).cpu().numpy()
+    k = 2 * np.pi / (N * p.dx)
+    assert np.abs(u[2] - f[2] / k ** 2).max() < 1e-12
+    assert np.abs(u[:2]).max() < 1e-12
+
+
+def test_fp32_within_1e5_of_fp64(case64):
+    p, s, Y, F, T = case64
+    V64, W64 = gpu_mobility(p, Y, F, T)
+    V32, W32 = gpu_mobility(p, Y, F, T, abi.FS_PREC_FP32)
+    assert rel_err(V32, V64) < FP32_REL
+    assert rel_err(W32, W64) < FP32_REL
+
+
+def test_repeat_is_bitwise_identical(case64):
+    p, s, Y, F, T = case64
+    V1, W1 = gpu_mobility(p, Y, F, T)
+    V2, W2 = gpu_mobility(p, Y, F, T)
+    assert np.array_equal(V1, V2) and np.array_equal(W1, W2)
+
+
+def test_host_entry_equals_device_entry(case64):
+    p, s, Y, F, T = case64
+    ctx = Context(p, max_beads=Y.shape[0])
+    V, W = mobility_host(ctx, Y, F, T)
+    Vd, Wd = gpu_mobility(p, Y, F, T)
+    assert np.array_equal(V, Vd) and np.array_equal(W, Wd)
+
+
+def test_negative_and_boundary_positions(oracle):
+    """fmod leaves Y in (-L, L); (int)(Y/dx) truncates toward zero (FCMfunctions.cpp:565-567)."""
+    p = params_for(32)
+    L = 32 * p.dx
+    rng = np.random.default_rng(3)
+    Y = np.array([[-0.3 * p.dx, 0.2, 5.0], [-L + 0.01, L - 0.01, -2.5 * p.dx], [0.0, -1e-14, 3 * p.dx],
+                  [L / 2, -L / 2, 7.25], [-4.0 * p.dx, 11.0, -0.5]])
+    F = rng.standard_normal(Y.shape)
+    T = rng.standard_normal(Y.shape)
+    V0, W0 = oracle.fcm_mobility(p, Y, F, T)
+    V, W = gpu_mobility(p, Y, F, T)
+    assert rel_err(V, V0) < FP64_REL
+    assert rel_err(W, W0) < FP64_REL
+
+
+def test_friction_mobility(oracle, case64):
+    p, s, Y, F, T = case64
+    V0, W0 = oracle.fcm_friction(p, F, T)
+    ctx = Context(p, max_beads=Y.shape[0])
+    fcm = Fcm(ctx, Y.shape[0])
+    fcm.set(Y, F, T)
+    fcm.friction_mobility_solve()
+    assert np.array_equal(fcm.V.cpu().numpy(), V0)
+    assert np.array_equal(fcm.W.cpu().numpy(), W0)
+
+
+def test_single_bead_self_mobility():
+    """Periodic self-mobility approaches 1/(6 pi mu a) with Hasimoto's O(a/L) correction."""
+    p = params_for(64)
+    L = 64 * p.dx
+    Y = np.array([[L / 2 + 0.1, L / 2 - 0.2, L / 2 + 0.3]])
+    V, W = gpu_mobility(p, Y, np.array([[0, 0, 1.0]]), np.zeros((1, 3)))
+    expect = 1 / (6 * np.pi) * (1 - 2.8373 / L)
+    assert abs(V[0, 2] / expect - 1) < 1e-3
+    V, W = gpu_mobility(p, Y, np.zeros((1, 3)), np.array([[0, 0, 1.0]]))
+    assert abs(W[0, 2] * 8 * np.pi - 1) < 1e-3
+
+
+def test_empty_call():
+    p = params_for(32)
+    ctx = Context(p, max_beads=4)
+    fcm = Fcm(ctx, 0)
+    fcm.mobility_solve()
+    ctx.synchronize()
+
+
+def test_too_many_beads_rejected():
+    p = params_for(32)
+    ctx = Context(p, max_beads=2)
+    fcm = Fcm(ctx, 3)
+    with pytest.raises(abi.FsError):
+        fcm.mobility_solve()
