@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Benchmark: implicit BDF2 time steps of sedimenting elastic filaments.
+
+Workload sediment_512: 512^3 periodic FCM grid, 4096 filaments x 32 beads
+(131,072 beads) placed by seeded rejection sampling, gravity (0,0,-1) per bead,
+K_B = K_T = 1, dt = 0.05, Broyden tolerance 1e-6 (the reference's absolute
+max-norm test), barrier below 2.2a. One "step" is one implicit time step
+(main.cpp:284-754): initial guess, forces, Jacobian build, cell link, then
+Broyden iterations each with a collision barrier and an FCM mobility solve,
+until converged. The metric is bead-steps per second.
+
+value      mixed precision (FP32 spread/FFT/interpolation, FP64 Broyden and
+           filament mechanics), inputs resident in HBM, device-timed with CUDA
+           events on the context's stream, max over ranks; weak scaling (one
+           independent replica per GPU).
+e2e        the same steps through the C-ABI with HOST state: every step uploads
+           the suspension from pinned host memory (fs_state_upload), steps, and
+           downloads it (fs_state_download).
+plain_fp64 the same steps with the FCM chain in FP64.
+--impl reference times the CPU restatement of the reference (the reference
+           itself, MPI + FFTW 2.1.5 + Armadillo, cannot be built here).
+
+Grids (3 x 512^3 reals + 3 x 512^2 x 257 complex, several GB) exceed the 126 MB
+L2, so no flush is needed between steps.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "bead-steps/s & Broyden iters/step: learned+FP32 vs plain FP64 GPU, resid<=1e-6"
+UNIT = "bead-steps/s"
+WORKLOAD = dict(npts=512, nfil=4096, nw=32, seed=1002)
+# Broyden iterations per step of sediment_512 used to scale the CPU baseline's
+# per-iteration sample to whole steps when the GPU run is not available (the
+# reference arm); the GPU FP64 path matches the oracle's iteration counts.
+REFERENCE_ITERS_PER_STEP = 20.0
+# DRAM bytes per launch from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum);
+# the kernels and captures are listed in profiles/.
+NCU_TRAFFIC = {}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-stride", type=int, default=64)
+    return ap.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + ",".join(self.FIELDS), "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def state_bytes(s):
+    n = 0
+    for k, v in s.arrays.items():
+        n += v.nbytes
+    return n + s.fil_start.nbytes
+
+
+def run_ours(args, rank, world):
+    import numpy as np
+    import torch
+    from filsim_b200 import abi
+    from filsim_b200.configs import make_sediment_case
+    from filsim_b200.fcm import Context, Simulation
+    from filsim_b200.suspension import Suspension
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", dev))
+    K, W = args.steps, args.warmup
+    p, susp = make_sediment_case(WORKLOAD["npts"], WORKLOAD["nfil"], WORKLOAD["nw"], seed=WORKLOAD["seed"] + rank)
+    npb = susp.np
+    stream = torch.cuda.Stream()
+    ctx = Context(p, max_beads=npb, max_filaments=susp.nfil, stream=stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_steps(prec, profile=False):
+        ctx.set_precision(prec)
+        sim = Simulation(ctx, susp.copy())
+        sim.run_steps(1, W)
+        barrier()
+        if profile:
+            ctx.profile_enable(True)
+        launches0 = abi.lib().fs_kernel_launches()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(dev) as clk:
+            ev0.record(stream)
+            its, st = sim.run_steps(W + 1, K)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        launches = abi.lib().fs_kernel_launches() - launches0
+        prof = ctx.profile() if profile else None
+        if profile:
+            ctx.profile_enable(False)
+        barrier()
+        return max_over_ranks(ms), its, st, prof, clk.summary(), launches, sim
+
+    # mixed precision (headline)
+    ms, its, st, prof, clocks, launches, sim = timed_steps(abi.FS_PREC_FP32, profile=True)
+    value = world * npb * K / (ms / 1e3)
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 FCM chain + f64 Broyden/mechanics", "data": "synthetic (seeded rejection-placed filaments)",
+        "config": {"workload": "sediment_512", "grid": [512, 512, 512], "filaments": WORKLOAD["nfil"],
+                   "beads_per_filament": WORKLOAD["nw"], "beads": npb, "dt": p.dt, "tol": p.tol,
+                   "precision": "mixed", "learned_warm_start": False, "parallelism": "replicas x%d" % world,
+                   "l2": "inputs larger than L2 (grids ~10 GB)"},
+        "iters_per_step": float(np.mean(its)), "status": abi.STATUS_NAMES.get(st, st),
+        "clocks": clocks, "gpu_launches": int(launches),
+    }
+    stage_ms = {k: v[0] for k, v in prof.items()}
+    stage_calls = {k: v[1] for k, v in prof.items()}
+    out["stage_ms_per_step"] = {k: v / K for k, v in stage_ms.items() if v > 0}
+
+    # roofline of the dominant kernel stage of this library (cuFFT is a library call)
+    peak, peak_kind = measured_peaks()
+    N = 512 ** 3
+    NH = 512 * 512 * 257
+    s_real = 4  # FP32 grids in the mixed path
+    alg_bytes = {
+        "spread": 3 * s_real * N + npb * 9 * 8,          # write f once, read bead Y, F, T
+        "project": 2 * 3 * NH * 2 * s_real,              # read and write 3 complex spectra
+        "interp": 3 * s_real * N + npb * 9 * 8,          # read u once, bead Y in, V, W out
+        "jacobian": 2 * susp.nfil * (6 * WORKLOAD["nw"]) ** 2 * 8,  # write J, then LU in place (one pass)
+        "broyden": susp.nfil * (6 * WORKLOAD["nw"]) ** 2 * 8,       # read the LU factors once per application
+    }
+    cands = {k: stage_ms[k] for k in alg_bytes if stage_ms.get(k, 0) > 0}
+    dom = max(cands, key=cands.get)
+    per_launch_ms = stage_ms[dom] / max(1, stage_calls[dom])
+    achieved = alg_bytes[dom] / (per_launch_ms / 1e3) / 1e9
+    out["roofline"] = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                       "frac": achieved / peak, "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind,
+                       "traffic": NCU_TRAFFIC.get(dom), "algorithmic_bytes": alg_bytes[dom],
+                       "launch_ms": per_launch_ms}
+    fcm_ms = sum(stage_ms.get(k, 0) for k in ("spread", "fft_fwd", "project", "fft_inv", "interp"))
+    solves = max(1, stage_calls.get("interp", 0))
+    b_fcm = 24 * s_real * N
+    out["fcm_chain"] = {"ms_per_solve": fcm_ms / solves, "bytes_per_solve": b_fcm,
+                        "GBps": b_fcm / (fcm_ms / solves / 1e3) / 1e9, "frac": b_fcm / (fcm_ms / solves / 1e3) / 1e9 / peak}
+
+    # plain FP64 FCM chain on the same suspension
+    if not args.no_fp64:
+        ms64, its64, st64, _, clocks64, _, _ = timed_steps(abi.FS_PREC_FP64)
+        out["plain_fp64"] = {"value": world * npb * K / (ms64 / 1e3), "ms_per_step": ms64 / K,
+                             "iters_per_step": float(np.mean(its64)), "status": abi.STATUS_NAMES.get(st64, st64)}
+        out["speedup_vs_plain_fp64"] = out["value"] / out["plain_fp64"]["value"]
+
+    # end to end through the C-ABI with pinned host state
+    if not args.no_e2e:
+        ctx.set_precision(abi.FS_PREC_FP32)
+        host = susp.copy()
+        pinned = {}
+        for k, v in host.arrays.items():
+            t = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)
+            t.numpy()[...] = v
+            pinned[k] = t
+        host.arrays = {k: t.numpy() for k, t in pinned.items()}
+        sim = Simulation(ctx, host)
+        sim.run_steps(1, W)
+        host.set_arrays(sim.download())
+        barrier()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for k in range(K):
+            sim.upload(host)                      # H2D of the step's input state
+            sim.step_implicit(W + 1 + k)
+            host.set_arrays(sim.download())       # D2H of the step's result
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms_e2e = max_over_ranks(ev0.elapsed_time(ev1))
+        nbytes = state_bytes(host)
+        out["e2e"] = {"value": world * npb * K / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                      "d2h_bytes_per_step": nbytes, "ms_per_step": ms_e2e / K}
+
+    # CPU baseline: the oracle on this host's cores, sampled
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(p, susp, out.get("plain_fp64", {}).get("iters_per_step",
+                                                                                   out["iters_per_step"]),
+                                           args.cpu_stride)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def cpu_baseline(p, susp, iters_per_step, stride):
+    """Oracle stage costs of one Broyden iteration of this workload, each stage
+    run on 1/stride of its independent work units and scaled back; a step is
+    the Jacobian build plus (iters+1) iterations."""
+    from oracle import oracle_py
+    sysw = oracle_py.System(p, susp)
+    sysw.initial_guess()
+    sysw.filament_forces(1)
+    t0 = time.time()
+    parts, nth = sysw.sample_costs(stride)
+    wall = time.time() - t0
+    per_iter = sum(v for k, v in parts.items() if k != "jacobian")
+    step_s = parts["jacobian"] + (iters_per_step + 1) * per_iter
+    sysw.close()
+    return {"value": susp.np / step_s, "unit": UNIT, "cores": nth, "kind": "port",
+            "sample": "oracle stage costs of one Broyden iteration of sediment_512 on 1/%d of each stage's work "
+                      "units (lines, beads, modes, filaments), scaled by %d; step = Jacobian + (%.1f+1) "
+                      "iterations; %.1f s wall" % (stride, stride, iters_per_step, wall),
+            "seconds_per_step": step_s, "stage_seconds": parts}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    from filsim_b200.configs import make_sediment_case
+    p, susp = make_sediment_case(WORKLOAD["npts"], WORKLOAD["nfil"], WORKLOAD["nw"], seed=WORKLOAD["seed"])
+    from oracle import oracle_py
+    sysw = oracle_py.System(p, susp)
+    sysw.initial_guess()
+    sysw.filament_forces(1)
+    for _ in range(args.warmup):
+        sysw.sample_costs(args.cpu_stride)
+    times = []
+    nth = 1
+    for _ in range(args.steps):
+        parts, nth = sysw.sample_costs(args.cpu_stride)
+        per_iter = sum(v for k, v in parts.items() if k != "jacobian")
+        times.append(parts["jacobian"] + (REFERENCE_ITERS_PER_STEP + 1) * per_iter)
+    step_s = statistics.mean(times)
+    value = susp.np / step_s
+    sample = ("CPU restatement of the reference (oracle/fs_oracle.c, OpenMP, %d threads): stage costs of one "
+              "Broyden iteration of sediment_512 on 1/%d of each stage's work units scaled back; step = Jacobian "
+              "+ (%.0f+1) iterations. The reference binary (MPI + FFTW 2.1.5 + Armadillo) is not buildable here."
+              % (nth, args.cpu_stride, REFERENCE_ITERS_PER_STEP))
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded rejection-placed filaments)",
+            "config": {"workload": "sediment_512", "grid": [512, 512, 512], "filaments": WORKLOAD["nfil"],
+                       "beads_per_filament": WORKLOAD["nw"], "beads": susp.np},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+    else:
+        out = run_ours(args, rank, world)
+    if rank == 0 and out is not None:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

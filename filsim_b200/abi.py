@@ -50,6 +50,15 @@ class FsDiag(ctypes.Structure):
     ]
 
 
+STAGES = ["spread", "fft_fwd", "project", "fft_inv", "interp", "link", "barrier", "forces", "jacobian",
+          "error_check", "broyden", "update", "friction"]
+FS_STAGE_COUNT = 16
+
+
+class FsProfile(ctypes.Structure):
+    _fields_ = [("ms", c_double * FS_STAGE_COUNT), ("calls", c_longlong * FS_STAGE_COUNT)]
+
+
 class FsHostState(ctypes.Structure):
     _fields_ = [
         ("nfil", c_int), ("np", c_int), ("fil_start", P_int),
@@ -129,7 +138,8 @@ def _declare(L):
         "fs_fcm_mobility": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
         "fs_fcm_mobility_host": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
         "fs_fcm_friction": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
-        "fs_fcm_get_grid": (c_int, [c_void_p, c_int, c_void_p, c_size_t]),
+        "fs_fcm_get_grid": (c_int, [c_void_p, c_void_p, c_size_t]),
+        "fs_fcm_spread": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
         "fs_fcm_flow_solve": (c_int, [c_void_p, c_void_p, c_void_p]),
         "fs_cells_dims": (c_int, [c_void_p, c_void_p]),
         "fs_cells_link": (c_int, [c_void_p, c_void_p, c_int]),
@@ -151,6 +161,11 @@ def _declare(L):
         "fs_step_implicit": (c_int, [c_void_p, c_int, c_void_p]),
         "fs_run_steps": (c_int, [c_void_p, c_int, c_int, c_void_p]),
         "fs_get_diag": (c_int, [c_void_p, ctypes.POINTER(FsDiag)]),
+        "fs_suspension_random": (c_int, [ctypes.POINTER(FsParams), c_int, c_int, ctypes.c_ulonglong, c_double,
+                                         c_int, c_void_p, c_void_p]),
+        "fs_kernel_launches": (ctypes.c_ulonglong, []),
+        "fs_profile_enable": (c_int, [c_void_p, c_int]),
+        "fs_profile_get": (c_int, [c_void_p, ctypes.POINTER(FsProfile)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -7,6 +7,34 @@
 #include <vector>
 #include "fs_internal.cuh"
 
+unsigned long long g_fs_kernel_launches = 0;
+
+int prof_begin(fs_ctx *c, int stage) {
+  if (!c->prof.on) return -1;
+  if (c->prof.n == FS_PROF_SLOTS) prof_flush(c);
+  const int s = c->prof.n++;
+  c->prof.stage[s] = stage;
+  cudaEventRecord(c->prof.ev[2 * s], c->stream);
+  return s;
+}
+
+void prof_end(fs_ctx *c, int slot) {
+  if (slot >= 0) cudaEventRecord(c->prof.ev[2 * slot + 1], c->stream);
+}
+
+void prof_flush(fs_ctx *c) {
+  if (!c->prof.n) return;
+  cudaStreamSynchronize(c->stream);
+  for (int i = 0; i < c->prof.n; ++i) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c->prof.ev[2 * i], c->prof.ev[2 * i + 1]) == cudaSuccess) {
+      c->prof.ms[c->prof.stage[i]] += ms;
+      c->prof.calls[c->prof.stage[i]]++;
+    }
+  }
+  c->prof.n = 0;
+}
+
 namespace {
 
 fs_status validate_params(const fs_params *p) {
@@ -65,6 +93,7 @@ void free_state(fs_ctx *c) {
 fs_status read_flags(fs_ctx *c) {
   FS_CUDA(cudaMemcpyAsync(c->flags_h, c->flags, sizeof(int) * FLAG_COUNT, cudaMemcpyDeviceToHost, c->stream));
   FS_CUDA(cudaStreamSynchronize(c->stream));
+  prof_flush(c);
   if (c->flags_h[FLAG_NONFINITE]) c->diag.nonfinite = 1;
   if (c->flags_h[FLAG_EXPLODE]) c->diag.explosion = 1;
   if (c->flags_h[FLAG_CAPACITY]) return FS_ERR_CAPACITY;
@@ -119,6 +148,8 @@ fs_status step_implicit(fs_ctx *c, int nt, int *iters_out) {
 extern "C" {
 
 int fs_abi_version(void) { return FS_ABI_VERSION; }
+
+unsigned long long fs_kernel_launches(void) { return __atomic_load_n(&g_fs_kernel_launches, __ATOMIC_RELAXED); }
 
 const char *fs_status_string(fs_status s) {
   switch (s) {
@@ -189,7 +220,9 @@ fs_status fs_create(const fs_params *p, int max_beads, int max_filaments, void *
   if (stream) {
     c->stream = (cudaStream_t)stream;
   } else {
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) st = FS_ERR_CUDA;
+    // a blocking stream: work on it is ordered against the legacy default
+    // stream, which callers' own copies (and torch's) use
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault) != cudaSuccess) st = FS_ERR_CUDA;
     c->own_stream = true;
   }
   if (st == FS_OK) st = alloc_state(c);
@@ -204,9 +237,33 @@ fs_status fs_create(const fs_params *p, int max_beads, int max_filaments, void *
   return FS_OK;
 }
 
+fs_status fs_profile_enable(fs_ctx *c, int on) {
+  if (!c) return FS_ERR_INVALID_ARG;
+  if (on && !c->prof.created) {
+    for (int i = 0; i < 2 * FS_PROF_SLOTS; ++i) FS_CUDA(cudaEventCreate(&c->prof.ev[i]));
+    c->prof.created = true;
+  }
+  prof_flush(c);
+  memset(c->prof.ms, 0, sizeof c->prof.ms);
+  memset(c->prof.calls, 0, sizeof c->prof.calls);
+  c->prof.on = on != 0;
+  return FS_OK;
+}
+
+fs_status fs_profile_get(fs_ctx *c, fs_profile *out) {
+  if (!c || !out) return FS_ERR_INVALID_ARG;
+  prof_flush(c);
+  FS_CUDA(cudaStreamSynchronize(c->stream));
+  memcpy(out->ms, c->prof.ms, sizeof out->ms);
+  memcpy(out->calls, c->prof.calls, sizeof out->calls);
+  return FS_OK;
+}
+
 fs_status fs_destroy(fs_ctx *c) {
   if (!c) return FS_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->prof.created)
+    for (int i = 0; i < 2 * FS_PROF_SLOTS; ++i) cudaEventDestroy(c->prof.ev[i]);
   fcm_free(c);
   cells_free(c);
   free_state(c);

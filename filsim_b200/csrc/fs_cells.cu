@@ -327,6 +327,7 @@ void cells_free(fs_ctx *c) {
 }
 
 fs_status cells_link(fs_ctx *c, const double *Xs, int np) {
+  ProfScope ps(c, FS_STAGE_LINK);
   BarrierConsts k = make_bconsts(c, 0);
   if (np > 0) {
     k_cell_keys<<<fs_blocks(np, 256), 256, 0, c->stream>>>(Xs, np, k, c->cells.key);
@@ -343,6 +344,7 @@ fs_status cells_link(fs_ctx *c, const double *Xs, int np) {
 fs_status cells_barrier(fs_ctx *c, const double *Y, double *F, int np, int nt, const int *fil_id,
                         const int *seg_id, int *pairs_d, int max_pairs, int *npairs_h) {
   if (c->cells_np != np) return FS_ERR_STATE;
+  ProfScope ps(c, FS_STAGE_BARRIER);
   BarrierConsts k = make_bconsts(c, nt);
   k_set_min_init<<<1, 1, 0, c->stream>>>(c->min_dist2_bits);
   FS_LAUNCH_CHECK();

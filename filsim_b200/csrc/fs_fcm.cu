@@ -502,10 +502,13 @@ fs_status flow_solve_t(fs_ctx *c) {
   const int prec = sizeof(R) == 8 ? FS_PREC_FP64 : FS_PREC_FP32;
   FS_TRY(ensure_plans(c, prec));
   cufftResult r;
-  if (prec == FS_PREC_FP64)
-    r = cufftExecD2Z(c->plan_fwd[prec], (cufftDoubleReal *)c->grid_real, (cufftDoubleComplex *)c->grid_cplx);
-  else
-    r = cufftExecR2C(c->plan_fwd[prec], (cufftReal *)c->grid_real, (cufftComplex *)c->grid_cplx);
+  {
+    ProfScope ps(c, FS_STAGE_FFT_FWD);
+    if (prec == FS_PREC_FP64)
+      r = cufftExecD2Z(c->plan_fwd[prec], (cufftDoubleReal *)c->grid_real, (cufftDoubleComplex *)c->grid_cplx);
+    else
+      r = cufftExecR2C(c->plan_fwd[prec], (cufftReal *)c->grid_real, (cufftComplex *)c->grid_cplx);
+  }
   if (r != CUFFT_SUCCESS) return FS_ERR_CUFFT;
   const double TwoPI = 2. * FS_PI;
   const R ffx = (R)(TwoPI / (c->nx * c->p.dx)), ffy = (R)(TwoPI / (c->ny * c->p.dx)),
@@ -513,16 +516,22 @@ fs_status flow_solve_t(fs_ctx *c) {
   const R total = (R)((double)c->nx * (double)c->ny * (double)c->nz);
   typedef typename Cplx<R>::T C;
   C *fh = (C *)c->grid_cplx;
-  k_project<R><<<fs_blocks((long long)c->NH, 256), 256, 0, c->stream>>>(fh, c->NH, c->nx, c->ny, c->nz, c->nzh, ffx,
-                                                                          ffy, ffz, total);
-  FS_LAUNCH_CHECK();
-  dim3 gp(fs_blocks((long long)c->nx * c->ny, 256), 2);
-  k_project_planes<R><<<gp, 256, 0, c->stream>>>(fh, c->NH, c->nx, c->ny, c->nz, c->nzh, ffx, ffy, ffz, total);
-  FS_LAUNCH_CHECK();
-  if (prec == FS_PREC_FP64)
-    r = cufftExecZ2D(c->plan_inv[prec], (cufftDoubleComplex *)c->grid_cplx, (cufftDoubleReal *)c->grid_real);
-  else
-    r = cufftExecC2R(c->plan_inv[prec], (cufftComplex *)c->grid_cplx, (cufftReal *)c->grid_real);
+  {
+    ProfScope ps(c, FS_STAGE_PROJECT);
+    k_project<R><<<fs_blocks((long long)c->NH, 256), 256, 0, c->stream>>>(fh, c->NH, c->nx, c->ny, c->nz, c->nzh,
+                                                                            ffx, ffy, ffz, total);
+    FS_LAUNCH_CHECK();
+    dim3 gp(fs_blocks((long long)c->nx * c->ny, 256), 2);
+    k_project_planes<R><<<gp, 256, 0, c->stream>>>(fh, c->NH, c->nx, c->ny, c->nz, c->nzh, ffx, ffy, ffz, total);
+    FS_LAUNCH_CHECK();
+  }
+  {
+    ProfScope ps(c, FS_STAGE_FFT_INV);
+    if (prec == FS_PREC_FP64)
+      r = cufftExecZ2D(c->plan_inv[prec], (cufftDoubleComplex *)c->grid_cplx, (cufftDoubleReal *)c->grid_real);
+    else
+      r = cufftExecC2R(c->plan_inv[prec], (cufftComplex *)c->grid_cplx, (cufftReal *)c->grid_real);
+  }
   if (r != CUFFT_SUCCESS) return FS_ERR_CUFFT;
   return FS_OK;
 }
@@ -530,17 +539,21 @@ fs_status flow_solve_t(fs_ctx *c) {
 template <typename R>
 fs_status mobility_t(fs_ctx *c, const double *Y, const double *F, const double *T, double *V, double *W, int np) {
   FcmConsts k = make_consts(c);
-  if (np > 0) {
-    k_fcm_bin_keys<<<fs_blocks(np, 256), 256, 0, c->stream>>>(Y, np, k, c->bins.key);
+  {
+    ProfScope ps(c, FS_STAGE_SPREAD);
+    if (np > 0) {
+      k_fcm_bin_keys<<<fs_blocks(np, 256), 256, 0, c->stream>>>(Y, np, k, c->bins.key);
+      FS_LAUNCH_CHECK();
+    }
+    FS_TRY(fs_sort_run(&c->bins, np, c->stream));
+    const size_t smem = sizeof(SpreadSmem<R>);
+    k_spread<R><<<c->nbins, FS_TILE * 32, smem, c->stream>>>(Y, F, T, c->bins.start, c->bins.sorted, k,
+                                                              (R *)c->grid_real);
     FS_LAUNCH_CHECK();
   }
-  FS_TRY(fs_sort_run(&c->bins, np, c->stream));
-  const size_t smem = sizeof(SpreadSmem<R>);
-  k_spread<R><<<c->nbins, FS_TILE * 32, smem, c->stream>>>(Y, F, T, c->bins.start, c->bins.sorted, k,
-                                                            (R *)c->grid_real);
-  FS_LAUNCH_CHECK();
   FS_TRY(flow_solve_t<R>(c));
   if (np > 0) {
+    ProfScope ps(c, FS_STAGE_INTERP);
     k_interp<R><<<fs_blocks(np, 8), 256, 0, c->stream>>>((const R *)c->grid_real, Y, c->bins.sorted, np, k, V, W);
     FS_LAUNCH_CHECK();
   }
@@ -594,6 +607,7 @@ fs_status fcm_friction(fs_ctx *c, const double *F, const double *T, double *V, d
   const double a1 = 1. / (6 * PI * a * mu);
   const double a2 = 1. / (8 * PI * a * a * a * mu);
   if (np > 0) {
+    ProfScope ps(c, FS_STAGE_FRICTION);
     k_friction<<<fs_blocks(3 * np, 256), 256, 0, c->stream>>>(F, T, V, W, 3 * np, a1, a2);
     FS_LAUNCH_CHECK();
   }

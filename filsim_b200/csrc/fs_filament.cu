@@ -828,6 +828,7 @@ FilConsts make_fconsts(const fs_ctx *c) {
 
 fs_status fil_initial_guess(fs_ctx *c) {
   if (!c->have_state) return FS_ERR_STATE;
+  ProfScope ps(c, FS_STAGE_UPDATE);
   k_initial_guess<<<fs_blocks(c->np, 256), 256, 0, c->stream>>>(c->np, c->seg_id, c->X, c->Xt, c->U, c->Ut, c->q,
                                                                  c->Xs, c->Us, c->qs);
   FS_LAUNCH_CHECK();
@@ -837,6 +838,7 @@ fs_status fil_initial_guess(fs_ctx *c) {
 fs_status fil_forces(fs_ctx *c, int nt) {
   (void)nt;
   if (!c->have_state) return FS_ERR_STATE;
+  ProfScope ps(c, FS_STAGE_FORCES);
   FilConsts k = make_fconsts(c);
   k_unrobot_assign<<<fs_blocks(c->nfil, 128), 128, 0, c->stream>>>(c->nfil, c->fil_start, c->qs, c->Xs, c->Y, k);
   FS_LAUNCH_CHECK();
@@ -848,6 +850,7 @@ fs_status fil_forces(fs_ctx *c, int nt) {
 
 fs_status fil_jacobian_build(fs_ctx *c, int nt) {
   if (!c->have_state) return FS_ERR_STATE;
+  ProfScope ps(c, FS_STAGE_JACOBIAN);
   FilConsts k = make_fconsts(c);
   k_jacobian<<<c->nfil, 256, 0, c->stream>>>(c->nfil, c->fil_start, c->qs, c->Us, c->TAU, c->lam, c->kap, c->cc,
                                              c->joff, c->J, c->jpiv, nt, k, c->p.a, c->p.ah, c->flags);
@@ -870,6 +873,7 @@ fs_status fil_jacobian_inverse(fs_ctx *c, int f, double *out_d) {
 
 fs_status fil_error_check(fs_ctx *c, const double *V, const double *W, double *err, int nt) {
   if (!c->have_state) return FS_ERR_STATE;
+  ProfScope ps(c, FS_STAGE_ERROR_CHECK);
   FilConsts k = make_fconsts(c);
   FS_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(int) * 3, c->stream));  // check, nonfinite, explode
   FS_CUDA(cudaMemsetAsync(c->maxerr_bits, 0, sizeof(unsigned long long), c->stream));
@@ -882,6 +886,7 @@ fs_status fil_error_check(fs_ctx *c, const double *V, const double *W, double *e
 
 fs_status fil_broyden_apply(fs_ctx *c, const double *b, double *x, int iter) {
   if (!c->have_state) return FS_ERR_STATE;
+  ProfScope ps(c, FS_STAGE_BROYDEN);
   const size_t n6 = (size_t)6 * c->np;
   if (iter > 0) {
     dim3 g(RED_BLOCKS, iter);
@@ -900,11 +905,15 @@ fs_status fil_broyden_apply(fs_ctx *c, const double *b, double *x, int iter) {
 // main.cpp:641-663 with the current err/newerr/upd: history column `iter`
 fs_status fil_broyden_update(fs_ctx *c, int iter) {
   const size_t n6 = (size_t)6 * c->np;
-  k_diff_sq<<<RED_BLOCKS, RED_THREADS, 0, c->stream>>>(c->newerr, c->err, c->dE, n6, c->partials);
-  FS_LAUNCH_CHECK();
-  k_reduce_rows<<<1, 32, 0, c->stream>>>(c->partials, RED_BLOCKS, 1, c->scalars, 1);
-  FS_LAUNCH_CHECK();
+  {
+    ProfScope ps(c, FS_STAGE_BROYDEN);
+    k_diff_sq<<<RED_BLOCKS, RED_THREADS, 0, c->stream>>>(c->newerr, c->err, c->dE, n6, c->partials);
+    FS_LAUNCH_CHECK();
+    k_reduce_rows<<<1, 32, 0, c->stream>>>(c->partials, RED_BLOCKS, 1, c->scalars, 1);
+    FS_LAUNCH_CHECK();
+  }
   FS_TRY(fil_broyden_apply(c, c->dE, c->tmp, iter));
+  ProfScope ps(c, FS_STAGE_BROYDEN);
   k_broyden_cols<<<fs_blocks((long long)n6, 256), 256, 0, c->stream>>>(c->tmp, c->upd, c->dE, c->scalars, n6,
                                                                        c->Cmat + (size_t)iter * n6,
                                                                        c->Dmat + (size_t)iter * n6);
@@ -914,6 +923,7 @@ fs_status fil_broyden_update(fs_ctx *c, int iter) {
 
 fs_status fil_state_update(fs_ctx *c, const double *upd) {
   if (!c->have_state) return FS_ERR_STATE;
+  ProfScope ps(c, FS_STAGE_UPDATE);
   k_update<<<fs_blocks(c->np, 256), 256, 0, c->stream>>>(c->np, c->fil_id, c->seg_id, c->fil_start, upd, c->Xs,
                                                           c->Us, c->q, c->qs, c->lam);
   FS_LAUNCH_CHECK();
@@ -922,6 +932,7 @@ fs_status fil_state_update(fs_ctx *c, const double *upd) {
 
 fs_status fil_step(fs_ctx *c, int nt) {
   if (!c->have_state) return FS_ERR_STATE;
+  ProfScope ps(c, FS_STAGE_UPDATE);
   int n = c->np > 3 * c->nlink ? c->np : 3 * c->nlink;
   k_step<<<fs_blocks(n, 256), 256, 0, c->stream>>>(c->np, c->nlink, c->X, c->Xs, c->Xt, c->U, c->Us, c->Ut, c->q,
                                                     c->qt, c->lam, c->lam1, c->lam2, nt, c->p.lambda_extrap_step);

@@ -13,7 +13,7 @@
 // Spread tile edge (grid points) and warps per spread CTA (one x-plane each).
 #define FS_TILE 16
 // Beads staged in shared memory per spread pass.
-#define FS_SPREAD_CHUNK 16
+#define FS_SPREAD_CHUNK 12
 // Collision events kept per bead (pairs inside the barrier range).
 #define FS_MAX_EVENTS 64
 // Flag words (device int array ctx->flags).
@@ -30,8 +30,19 @@ struct fs_sort {
   int *block_sums;
 };
 
+#define FS_PROF_SLOTS 512
+struct fs_prof {
+  bool on, created;
+  cudaEvent_t ev[2 * FS_PROF_SLOTS];
+  int stage[FS_PROF_SLOTS];
+  int n;  // pending slots
+  double ms[FS_STAGE_COUNT];
+  long long calls[FS_STAGE_COUNT];
+};
+
 struct fs_ctx {
   fs_params p;
+  fs_prof prof;
   int device;
   cudaStream_t stream;
   bool own_stream;
@@ -92,8 +103,12 @@ struct fs_ctx {
     }                                                                         \
   } while (0)
 
+// kernels this library has launched in the process (every launch is followed by FS_LAUNCH_CHECK)
+extern unsigned long long g_fs_kernel_launches;
+
 #define FS_LAUNCH_CHECK()                                                     \
   do {                                                                        \
+    __atomic_fetch_add(&g_fs_kernel_launches, 1ull, __ATOMIC_RELAXED);        \
     cudaError_t e_ = cudaGetLastError();                                      \
     if (e_ != cudaSuccess) {                                                  \
       fprintf(stderr, "filsim_gpu: launch failed: %s (%s:%d)\n",             \
@@ -109,6 +124,17 @@ struct fs_ctx {
   } while (0)
 
 static inline int fs_blocks(long long n, int threads) { return (int)((n + threads - 1) / threads); }
+
+// ---- stage timing (fs_capi.cu) ----
+int prof_begin(fs_ctx *c, int stage);
+void prof_end(fs_ctx *c, int slot);
+void prof_flush(fs_ctx *c);
+struct ProfScope {
+  fs_ctx *c;
+  int slot;
+  ProfScope(fs_ctx *ctx, int stage) : c(ctx), slot(prof_begin(ctx, stage)) {}
+  ~ProfScope() { prof_end(c, slot); }
+};
 
 // ---- entry points implemented across the .cu files (internal C++ linkage) ----
 fs_status fs_sort_alloc(fs_sort *s, int nkeys, int max_items, size_t *bytes);

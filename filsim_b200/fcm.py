@@ -2,13 +2,16 @@
 
 Class and method names follow the reference so a main.cpp-shaped driver reads
 the same:
-  Fcm            struct Fcm (FCMfunctions.hpp:7-59)
-  LinkedList     struct LinkedList (CollisionBarrierFilament.hpp:19-57)
-  FilamentJsolver class filamentJsolver (FilamentJacobianSolver.hpp:14-87)
-  Simulation     the filament suspension and the time loop of main.cpp:284-754
+  Fcm             struct Fcm (FCMfunctions.hpp:7-59)
+  LinkedList      struct LinkedList (CollisionBarrierFilament.hpp:19-57)
+  Simulation      the filament suspension with Filament's per-step calls,
+                  filamentJsolver (FilamentJacobianSolver.hpp:14-87) and the
+                  time loop of main.cpp:284-754
 
 Device buffers are torch CUDA tensors (plumbing only); every computation runs
-in the library's kernels. Errors raise FsError with the library's status.
+in the library's kernels. Each wrapper call keeps its argument tensors alive
+and synchronises the context before returning, so torch may reuse or read the
+memory afterwards. Errors raise FsError with the library's status.
 """
 import ctypes
 
@@ -17,17 +20,24 @@ import torch
 
 from . import abi
 from .abi import check, lib
-from .suspension import Suspension
 
 
 def _dptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else None
 
 
-def _dev(x, device="cuda"):
+def _dev(x, dtype=torch.float64):
     if isinstance(x, torch.Tensor):
-        return x.to(device=device, dtype=torch.float64).contiguous()
-    return torch.as_tensor(np.ascontiguousarray(x, dtype=np.float64), device=device)
+        return x.to(device="cuda", dtype=dtype).contiguous()
+    npdt = np.float64 if dtype == torch.float64 else np.int32
+    return torch.as_tensor(np.ascontiguousarray(x, dtype=npdt), device="cuda")
+
+
+class _DeviceView:
+    """__cuda_array_interface__ over a library-owned device array."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 2}
 
 
 class Context:
@@ -57,6 +67,11 @@ class Context:
     def synchronize(self):
         check(lib().fs_synchronize(self.h), "fs_synchronize")
 
+    def call(self, name, *args):
+        """Calls fs_<name>(ctx, *args), then synchronises the context."""
+        check(getattr(lib(), name)(self.h, *args), name)
+        self.synchronize()
+
     def set_precision(self, prec):
         check(lib().fs_set_precision(self.h, prec), "fs_set_precision")
 
@@ -64,6 +79,15 @@ class Context:
         n = ctypes.c_size_t()
         check(lib().fs_device_bytes(self.h, ctypes.byref(n)), "fs_device_bytes")
         return n.value
+
+    def profile_enable(self, on=True):
+        check(lib().fs_profile_enable(self.h, 1 if on else 0), "fs_profile_enable")
+
+    def profile(self):
+        """{stage: (milliseconds, calls)} since the last profile_enable."""
+        pr = abi.FsProfile()
+        check(lib().fs_profile_get(self.h, ctypes.byref(pr)), "fs_profile_get")
+        return {name: (pr.ms[i], pr.calls[i]) for i, name in enumerate(abi.STAGES)}
 
 
 class Fcm:
@@ -77,39 +101,38 @@ class Fcm:
 
     def mobility_solve(self):
         """Fcm::mobility_solve (FCMfunctions.cpp:175-464)."""
-        check(lib().fs_fcm_mobility(self.ctx.h, _dptr(self.Y), _dptr(self.F), _dptr(self.T), _dptr(self.V),
-                                    _dptr(self.W), self.np), "fs_fcm_mobility")
+        self.ctx.call("fs_fcm_mobility", _dptr(self.Y), _dptr(self.F), _dptr(self.T), _dptr(self.V),
+                      _dptr(self.W), self.np)
 
     def friction_mobility_solve(self):
         """Fcm::friction_mobility_solve (FCMfunctions.cpp:865-880)."""
-        check(lib().fs_fcm_friction(self.ctx.h, _dptr(self.F), _dptr(self.T), _dptr(self.V), _dptr(self.W),
-                                    self.np), "fs_fcm_friction")
+        self.ctx.call("fs_fcm_friction", _dptr(self.F), _dptr(self.T), _dptr(self.V), _dptr(self.W), self.np)
 
     def spread(self):
         """The force grid f (3, Nx, Ny, Nz) of the current Y, F, T (FP64)."""
         p = self.ctx.params
         f = torch.empty((3, p.npts_x, p.npts_y, p.npts_z), dtype=torch.float64, device="cuda")
-        check(lib().fs_fcm_spread(self.ctx.h, _dptr(self.Y), _dptr(self.F), _dptr(self.T), self.np, _dptr(f)),
-              "fs_fcm_spread")
+        self.ctx.call("fs_fcm_spread", _dptr(self.Y), _dptr(self.F), _dptr(self.T), self.np, _dptr(f))
         return f
 
     def velocity_grid(self):
         p = self.ctx.params
         n = 3 * p.npts_x * p.npts_y * p.npts_z
         out = np.zeros(n)
-        check(lib().fs_fcm_get_grid(self.ctx.h, out.ctypes.data_as(ctypes.c_void_p), n), "fs_fcm_get_grid")
+        self.ctx.call("fs_fcm_get_grid", out.ctypes.data_as(ctypes.c_void_p), n)
         return out.reshape(3, p.npts_x, p.npts_y, p.npts_z)
 
     def flow_solve(self, f):
         f = _dev(f)
         u = torch.empty_like(f)
-        check(lib().fs_fcm_flow_solve(self.ctx.h, _dptr(f), _dptr(u)), "fs_fcm_flow_solve")
+        self.ctx.call("fs_fcm_flow_solve", _dptr(f), _dptr(u))
         return u
 
     def set(self, Y=None, F=None, T=None):
         for name, val in (("Y", Y), ("F", F), ("T", T)):
             if val is not None:
                 getattr(self, name).copy_(_dev(val).reshape(self.np, 3))
+        torch.cuda.synchronize()
 
 
 def mobility_host(ctx, Y, F, T):
@@ -120,8 +143,7 @@ def mobility_host(ctx, Y, F, T):
     V = np.zeros_like(Y)
     W = np.zeros_like(Y)
     vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
-    check(lib().fs_fcm_mobility_host(ctx.h, vp(Y), vp(F), vp(T), vp(V), vp(W), Y.shape[0]),
-          "fs_fcm_mobility_host")
+    ctx.call("fs_fcm_mobility_host", vp(Y), vp(F), vp(T), vp(V), vp(W), Y.shape[0])
     return V, W
 
 
@@ -140,33 +162,32 @@ class LinkedList:
         """LinkedList::link (CollisionBarrierFilament.cpp:370-433) from unwrapped positions."""
         Xs = _dev(Xs)
         self.np = Xs.shape[0]
-        check(lib().fs_cells_link(self.ctx.h, _dptr(Xs), self.np), "fs_cells_link")
+        self.ctx.call("fs_cells_link", _dptr(Xs), self.np)
 
     def lists(self):
         head = np.zeros(self.ncell, dtype=np.int32)
         lst = np.zeros(max(self.np, 1), dtype=np.int32)
         mp = np.zeros(13 * self.ncell, dtype=np.int32)
         vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
-        check(lib().fs_cells_get_lists(self.ctx.h, vp(head), vp(lst), vp(mp)), "fs_cells_get_lists")
+        self.ctx.call("fs_cells_get_lists", vp(head), vp(lst), vp(mp))
         return head, lst[: self.np], mp
 
     def apply_collision_barrier(self, Y, F, nt, fil_id=None, seg_id=None):
         """Adds barrier forces into F (device tensor, modified in place); returns min_dist2."""
-        fid = torch.as_tensor(fil_id, dtype=torch.int32, device="cuda") if fil_id is not None else None
-        sid = torch.as_tensor(seg_id, dtype=torch.int32, device="cuda") if seg_id is not None else None
+        fid = _dev(fil_id, torch.int32) if fil_id is not None else None
+        sid = _dev(seg_id, torch.int32) if seg_id is not None else None
         md = ctypes.c_double()
-        check(lib().fs_collision_barrier(self.ctx.h, _dptr(Y), _dptr(F), Y.shape[0], nt, _dptr(fid), _dptr(sid),
-                                         ctypes.byref(md)), "fs_collision_barrier")
+        self.ctx.call("fs_collision_barrier", _dptr(Y), _dptr(F), Y.shape[0], nt, _dptr(fid), _dptr(sid),
+                      ctypes.byref(md))
         return md.value
 
     def pairs(self, Y, nt, fil_id=None, seg_id=None, max_pairs=1 << 20):
-        fid = torch.as_tensor(fil_id, dtype=torch.int32, device="cuda") if fil_id is not None else None
-        sid = torch.as_tensor(seg_id, dtype=torch.int32, device="cuda") if seg_id is not None else None
+        fid = _dev(fil_id, torch.int32) if fil_id is not None else None
+        sid = _dev(seg_id, torch.int32) if seg_id is not None else None
         out = np.zeros(2 * max_pairs, dtype=np.int32)
         n = ctypes.c_int()
-        check(lib().fs_collision_pairs(self.ctx.h, _dptr(Y), Y.shape[0], nt, _dptr(fid), _dptr(sid),
-                                       out.ctypes.data_as(ctypes.c_void_p), max_pairs, ctypes.byref(n)),
-              "fs_collision_pairs")
+        self.ctx.call("fs_collision_pairs", _dptr(Y), Y.shape[0], nt, _dptr(fid), _dptr(sid),
+                      out.ctypes.data_as(ctypes.c_void_p), max_pairs, ctypes.byref(n))
         return out[: 2 * min(n.value, max_pairs)].reshape(-1, 2), n.value
 
 
@@ -181,60 +202,59 @@ class Simulation:
     def upload(self, susp):
         self.susp = susp
         self._hs = susp.host_state()
-        check(lib().fs_state_upload(self.ctx.h, ctypes.byref(self._hs.struct)), "fs_state_upload")
+        self.ctx.call("fs_state_upload", ctypes.byref(self._hs.struct))
 
     def download(self):
         out = self.susp.empty_like_state()
-        check(lib().fs_state_download(self.ctx.h, ctypes.byref(out.struct)), "fs_state_download")
+        self.ctx.call("fs_state_download", ctypes.byref(out.struct))
         return out.arrays
 
     def device_array(self, which, shape):
+        """A copy of a library-resident array (Y, V, W, err, ...)."""
         ptr = ctypes.c_void_p()
         check(lib().fs_state_device_ptr(self.ctx.h, which.encode(), ctypes.byref(ptr)), "fs_state_device_ptr")
-        n = int(np.prod(shape))
         self.ctx.synchronize()
-        # device-to-device copy (kind 3) through the CUDA runtime torch links
-        t = torch.empty(n, dtype=torch.float64, device="cuda")
-        torch.cuda.cudart().cudaMemcpy(t.data_ptr(), ptr.value, n * 8, 3)
-        return t.reshape(shape)
+        n = int(np.prod(shape))
+        return torch.as_tensor(_DeviceView(ptr.value, n), device="cuda").clone().reshape(shape)
 
     def initial_guess(self):
-        check(lib().fs_initial_guess(self.ctx.h), "fs_initial_guess")
+        self.ctx.call("fs_initial_guess")
 
     def filament_forces(self, nt):
-        check(lib().fs_filament_forces(self.ctx.h, nt), "fs_filament_forces")
+        self.ctx.call("fs_filament_forces", nt)
 
     def build_jacobian(self, nt):
-        check(lib().fs_jacobian_build(self.ctx.h, nt), "fs_jacobian_build")
+        self.ctx.call("fs_jacobian_build", nt)
 
     def jinv(self, f):
         nw = int(self.susp.fil_start[f + 1] - self.susp.fil_start[f])
         out = np.zeros((6 * nw, 6 * nw))
-        check(lib().fs_jacobian_get_inverse(self.ctx.h, f, out.ctypes.data_as(ctypes.c_void_p), 6 * nw),
-              "fs_jacobian_get_inverse")
+        self.ctx.call("fs_jacobian_get_inverse", f, out.ctypes.data_as(ctypes.c_void_p), 6 * nw)
         return out
 
     def error_check(self, V, W, nt):
+        V, W = _dev(V), _dev(W)
         err = torch.zeros(6 * self.susp.np, dtype=torch.float64, device="cuda")
         chk = ctypes.c_int()
-        check(lib().fs_error_check(self.ctx.h, _dptr(_dev(V)), _dptr(_dev(W)), _dptr(err), nt, ctypes.byref(chk)),
-              "fs_error_check")
+        self.ctx.call("fs_error_check", _dptr(V), _dptr(W), _dptr(err), nt, ctypes.byref(chk))
         return err, bool(chk.value)
 
     def broyden_apply(self, b, iter_):
         b = _dev(b)
         x = torch.zeros_like(b)
-        check(lib().fs_broyden_apply(self.ctx.h, _dptr(b), _dptr(x), iter_), "fs_broyden_apply")
+        self.ctx.call("fs_broyden_apply", _dptr(b), _dptr(x), iter_)
         return x
 
     def set_cols(self, c, d, iter_):
-        check(lib().fs_broyden_set_cols(self.ctx.h, _dptr(_dev(c)), _dptr(_dev(d)), iter_), "fs_broyden_set_cols")
+        c, d = _dev(c), _dev(d)
+        self.ctx.call("fs_broyden_set_cols", _dptr(c), _dptr(d), iter_)
 
     def update(self, u):
-        check(lib().fs_state_update(self.ctx.h, _dptr(_dev(u))), "fs_state_update")
+        u = _dev(u)
+        self.ctx.call("fs_state_update", _dptr(u))
 
     def step(self, nt):
-        check(lib().fs_step(self.ctx.h, nt), "fs_step")
+        self.ctx.call("fs_step", nt)
 
     def step_implicit(self, nt):
         it = ctypes.c_int()

@@ -10,7 +10,8 @@ to an accepted bead or to a periodic image of its own beads, the test of
 Filament::checkOverlapWithPeriodic (Filament.cpp:126-153) with the separation
 the benchmark configurations state (2.2a) instead of the reference's 2(a+a).
 
-The random stream is numpy's PCG64 seeded with `seed`; the reference's
+The generator runs as host code in libfilsim_gpu (fs_suspension_random):
+xoshiro256** seeded through splitmix64, Box-Muller normals. The reference's
 Armadillo RNG is not reproduced.
 """
 import ctypes
@@ -100,67 +101,18 @@ class Suspension:
             self.arrays[k][...] = v
 
 
-def random_suspension(p, nfil, nw, seed, min_sep=None, kap=1.0, c=1.0, max_tries=2000):
-    """Rejection-placed straight filaments in the periodic box of params p."""
-    rng = np.random.Generator(np.random.PCG64(seed))
-    L = np.array(box_lengths(p))
-    dl = p.dl
+def random_suspension(p, nfil, nw, seed, min_sep=None, kap=1.0, c=1.0, max_tries=1000000):
+    """Rejection-placed straight filaments in the periodic box of params p
+    (fs_suspension_random, host code of libfilsim_gpu)."""
+    import ctypes
+    from .abi import lib, check
     if min_sep is None:
         min_sep = 2.2 * p.a
-    M = np.maximum((L / min_sep).astype(int), 1)
-    cell = L / M
-    cap = 8
-    grid = -np.ones((M[0], M[1], M[2], cap), dtype=np.int64)
-    fill = np.zeros((M[0], M[1], M[2]), dtype=np.int64)
     X = np.zeros((nfil * nw, 3))
     Q = np.zeros((nfil * nw, 4))
-    offs = np.array([(i, j, k) for i in (-1, 0, 1) for j in (-1, 0, 1) for k in (-1, 0, 1)])
-    n_idx = np.arange(nw)
-    placed = 0
-    for f in range(nfil):
-        for _ in range(max_tries):
-            q = rng.standard_normal(4)
-            q = q / np.sqrt(np.sum(q * q))
-            centre = rng.random(3) * L
-            t = quat_tangent(q[None, :])[0]
-            pos = centre[None, :] + (n_idx[:, None] * dl - nw * dl / 2.0) * t[None, :]
-            # own periodic images
-            d = pos[:, None, :] - pos[None, :, :]
-            dmi = d - L * np.floor(d / L + 0.5)
-            wrapped = np.any(np.abs(dmi - d) > 1e-9, axis=2)
-            r2 = np.sum(dmi * dmi, axis=2)
-            if np.any(wrapped & (r2 < min_sep * min_sep)):
-                continue
-            if placed:
-                wpos = pos - L * np.floor(pos / L)
-                ci = np.minimum((wpos / cell).astype(int), M - 1)
-                nb = (ci[:, None, :] + offs[None, :, :]) % M
-                cand = grid[nb[..., 0], nb[..., 1], nb[..., 2]].reshape(nw, -1)
-                ok = True
-                if np.any(cand >= 0):
-                    cidx = np.where(cand >= 0, cand, 0)
-                    dd = pos[:, None, :] - X[cidx]
-                    dd = dd - L * np.floor(dd / L + 0.5)
-                    rr = np.sum(dd * dd, axis=2)
-                    if np.any((cand >= 0) & (rr < min_sep * min_sep)):
-                        ok = False
-                if not ok:
-                    continue
-            wpos = pos - L * np.floor(pos / L)
-            ci = np.minimum((wpos / cell).astype(int), M - 1)
-            for b in range(nw):
-                cx, cy, cz = ci[b]
-                k = fill[cx, cy, cz]
-                if k >= cap:
-                    raise RuntimeError("placement grid cell overflow")
-                grid[cx, cy, cz, k] = placed + b
-                fill[cx, cy, cz] = k + 1
-            X[placed:placed + nw] = pos
-            Q[placed:placed + nw] = q[None, :]
-            placed += nw
-            break
-        else:
-            raise RuntimeError("could not place filament %d after %d tries" % (f, max_tries))
+    check(lib().fs_suspension_random(ctypes.byref(p), nfil, nw, seed, min_sep, max_tries,
+                                     X.ctypes.data_as(ctypes.c_void_p), Q.ctypes.data_as(ctypes.c_void_p)),
+          "fs_suspension_random")
     fil_start = np.arange(nfil + 1, dtype=np.int32) * nw
     return Suspension(fil_start, X, Q, kap=kap, c=c)
 

@@ -135,7 +135,8 @@ void fs_params_default(fs_params *p, int npts_x, int npts_y, int npts_z);
  * max_filaments filaments (the suspension itself is uploaded later).
  * Replaces Fcm::initialise (FCMfunctions.cpp:10-168) and
  * LinkedList::initialise (CollisionBarrierFilament.cpp:274-304).
- * stream: a cudaStream_t or NULL for a context-owned stream. */
+ * stream: a cudaStream_t, or NULL for a context-owned blocking stream (ordered
+ * against the legacy default stream). */
 fs_status fs_create(const fs_params *p, int max_beads, int max_filaments, void *stream, fs_ctx **out);
 /* Replaces Fcm::free_memory (FCMfunctions.cpp:468-519). */
 fs_status fs_destroy(fs_ctx *ctx);
@@ -240,6 +241,50 @@ fs_status fs_step_implicit(fs_ctx *ctx, int nt, int *iters_h);
  * Broyden iteration count of each step. */
 fs_status fs_run_steps(fs_ctx *ctx, int nt_start, int nsteps, int *iters_h);
 fs_status fs_get_diag(fs_ctx *ctx, fs_diag *d_h);
+
+/* ---- stage profiling ---------------------------------------------------------- */
+
+/* Device time per stage, taken with CUDA events on the context's stream. The
+ * stages follow the columns of the reference's profiler (profilers.hpp:22-60,
+ * printed per step by profilers.cpp:46-65). */
+enum {
+  FS_STAGE_SPREAD = 0,      /* binning + force distribution (FCMGauss + FCMForcD) */
+  FS_STAGE_FFT_FWD = 1,     /* cuFFT R2C x3 (FCMFFTFw) */
+  FS_STAGE_PROJECT = 2,     /* Stokes projection (FCMFlowS) */
+  FS_STAGE_FFT_INV = 3,     /* cuFFT C2R x3 (FCMFFTBk) */
+  FS_STAGE_INTERP = 4,      /* U and Omega interpolation (FCMParVR) */
+  FS_STAGE_LINK = 5,        /* cell binning (ColBarri, link) */
+  FS_STAGE_BARRIER = 6,     /* pair forces (ColBarri) */
+  FS_STAGE_FORCES = 7,      /* unRobotArmify + filament forces + assign (Assign F) */
+  FS_STAGE_JACOBIAN = 8,    /* J build + LU (Bld Jinv) */
+  FS_STAGE_ERROR_CHECK = 9, /* ErrorChk */
+  FS_STAGE_BROYDEN = 10,    /* J0^-1 applications + history (Slv Jinv) */
+  FS_STAGE_UPDATE = 11,     /* state update + step */
+  FS_STAGE_FRICTION = 12,   /* Stokes-drag mobility */
+  FS_STAGE_COUNT = 16
+};
+typedef struct fs_profile {
+  double ms[FS_STAGE_COUNT];     /* summed device milliseconds */
+  long long calls[FS_STAGE_COUNT];
+} fs_profile;
+/* Turns stage timing on (1) or off (0); either resets the sums. */
+fs_status fs_profile_enable(fs_ctx *ctx, int on);
+/* Synchronises and returns the sums since the last enable. */
+fs_status fs_profile_get(fs_ctx *ctx, fs_profile *out_h);
+/* Number of kernels this library has launched in the process (cuFFT's own
+ * kernels are not counted). */
+unsigned long long fs_kernel_launches(void);
+
+/* ---- synthetic inputs (host only, no GPU needed) ------------------------------ */
+
+/* Seeded straight-filament suspension: nfil filaments of nw beads with the
+ * placement of Filament::initialFilamentSetupIsoRandCentred (Filament.cpp:47-66)
+ * and the periodic overlap rejection of Filament::checkOverlapWithPeriodic
+ * (Filament.cpp:126-153) at separation min_sep. X_h: nfil*nw*3 unwrapped bead
+ * positions; q_h: nfil*nw*4 quaternions (all beads of a filament share one).
+ * Returns FS_ERR_CAPACITY if a filament cannot be placed in max_tries. */
+fs_status fs_suspension_random(const fs_params *p, int nfil, int nw, unsigned long long seed, double min_sep,
+                               int max_tries, double *X_h, double *q_h);
 
 #ifdef __cplusplus
 }

@@ -119,8 +119,9 @@ static void or_fft_line(or_cpx *data, size_t stride, const or_fftplan *pl, int s
   for (int i = 0; i < n; ++i) data[(size_t)i * stride] = work_out[i];
 }
 
-/* Unnormalised 3-D real-to-complex transform; out is [nx][ny][nz/2+1]. */
-void or_fft_r2c_3d(const double *in, or_cpx *out, int nx, int ny, int nz) {
+/* Unnormalised 3-D real-to-complex transform; out is [nx][ny][nz/2+1].
+ * stride > 1 transforms the first 1/stride of the lines of each pass only (timing samples). */
+static void fft_r2c_3d_s(const double *in, or_cpx *out, int nx, int ny, int nz, long stride) {
   int nzh = nz / 2 + 1;
   or_fftplan px, py, pz;
   or_plan_init(&px, nx);
@@ -133,7 +134,7 @@ void or_fft_r2c_3d(const double *in, or_cpx *out, int nx, int ny, int nz) {
     or_cpx *wa = (or_cpx *)malloc(sizeof(or_cpx) * (size_t)nmax);
     or_cpx *wb = (or_cpx *)malloc(sizeof(or_cpx) * (size_t)nmax);
 #pragma omp for schedule(static)
-    for (long line = 0; line < (long)nx * ny; ++line) {
+    for (long line = 0; line < (long)nx * ny / stride; ++line) {
       const double *src = in + (size_t)line * nz;
       for (int k = 0; k < nz; ++k) { wa[k].re = src[k]; wa[k].im = 0.0; }
       or_fft_rec(wa, wb, nz, 1, &pz, 1, pz.fac, -1);
@@ -141,12 +142,12 @@ void or_fft_r2c_3d(const double *in, or_cpx *out, int nx, int ny, int nz) {
       for (int k = 0; k < nzh; ++k) dst[k] = wb[k];
     }
 #pragma omp for schedule(static)
-    for (long line = 0; line < (long)nx * nzh; ++line) {
+    for (long line = 0; line < (long)nx * nzh / stride; ++line) {
       long i = line / nzh, k = line % nzh;
       or_fft_line(out + (size_t)i * ny * nzh + k, nzh, &py, -1, wa, wb);
     }
 #pragma omp for schedule(static)
-    for (long line = 0; line < (long)ny * nzh; ++line) {
+    for (long line = 0; line < (long)ny * nzh / stride; ++line) {
       or_fft_line(out + line, (size_t)ny * nzh, &px, -1, wa, wb);
     }
     free(wa);
@@ -160,7 +161,7 @@ void or_fft_r2c_3d(const double *in, or_cpx *out, int nx, int ny, int nz) {
 /* Unnormalised 3-D complex-to-real inverse. Complex transforms along x and y
  * first, then a real inverse along z that, like FFTW's halfcomplex format,
  * uses only the real parts of the k=0 and k=nz/2 coefficients. in is destroyed. */
-void or_fft_c2r_3d(or_cpx *in, double *out, int nx, int ny, int nz) {
+static void fft_c2r_3d_s(or_cpx *in, double *out, int nx, int ny, int nz, long stride) {
   int nzh = nz / 2 + 1;
   or_fftplan px, py, pz;
   or_plan_init(&px, nx);
@@ -173,16 +174,16 @@ void or_fft_c2r_3d(or_cpx *in, double *out, int nx, int ny, int nz) {
     or_cpx *wa = (or_cpx *)malloc(sizeof(or_cpx) * (size_t)nmax);
     or_cpx *wb = (or_cpx *)malloc(sizeof(or_cpx) * (size_t)nmax);
 #pragma omp for schedule(static)
-    for (long line = 0; line < (long)ny * nzh; ++line) {
+    for (long line = 0; line < (long)ny * nzh / stride; ++line) {
       or_fft_line(in + line, (size_t)ny * nzh, &px, +1, wa, wb);
     }
 #pragma omp for schedule(static)
-    for (long line = 0; line < (long)nx * nzh; ++line) {
+    for (long line = 0; line < (long)nx * nzh / stride; ++line) {
       long i = line / nzh, k = line % nzh;
       or_fft_line(in + (size_t)i * ny * nzh + k, nzh, &py, +1, wa, wb);
     }
 #pragma omp for schedule(static)
-    for (long line = 0; line < (long)nx * ny; ++line) {
+    for (long line = 0; line < (long)nx * ny / stride; ++line) {
       const or_cpx *src = in + (size_t)line * nzh;
       wa[0].re = src[0].re;
       wa[0].im = 0.0;
@@ -202,6 +203,9 @@ void or_fft_c2r_3d(or_cpx *in, double *out, int nx, int ny, int nz) {
   or_plan_free(&py);
   or_plan_free(&pz);
 }
+
+void or_fft_r2c_3d(const double *in, or_cpx *out, int nx, int ny, int nz) { fft_r2c_3d_s(in, out, nx, ny, nz, 1); }
+void or_fft_c2r_3d(or_cpx *in, double *out, int nx, int ny, int nz) { fft_c2r_3d_s(in, out, nx, ny, nz, 1); }
 
 /* ------------------------------------------------------------------------ */
 /* FCM: FCMfunctions.cpp                                                    */
@@ -1421,3 +1425,159 @@ int or_run_steps(or_system *s, int nt_start, int nsteps, int *iters) {
 
 double or_last_min_dist2(or_system *s) { return s->min_dist2; }
 long long or_mobility_solves(or_system *s) { return s->nsolves; }
+
+/* ------------------------------------------------------------------------ */
+/* CPU-baseline sampling                                                     */
+/* ------------------------------------------------------------------------ */
+static double or_now(void) {
+#ifdef _OPENMP
+  return omp_get_wtime();
+#else
+  return (double)clock() / CLOCKS_PER_SEC;
+#endif
+}
+
+/* Wall time of the stages of one implicit-step iteration of the current
+ * suspension, each run on every stride-th of its independent work units
+ * (beads, FFT lines, modes, filaments) and multiplied back by stride:
+ * parts[0] spread, [1] forward FFTs, [2] projection, [3] inverse FFTs,
+ * [4] interpolation, [5] Jacobian build + inversion (once per step),
+ * [6] forces + error check + two J0^-1 applications with 10 history columns
+ * (full, not sampled), [7] link + barrier (full). Returns the thread count. */
+int or_sample_costs(or_system *s, int stride, double *parts) {
+  const fs_params *p = &s->p;
+  or_consts c;
+  or_consts_init(p, &c);
+  const int nx = p->npts_x, ny = p->npts_y, nz = p->npts_z, nzh = nz / 2 + 1, ngd = p->ngd, np = s->np;
+  const size_t N = (size_t)nx * ny * nz, NH = (size_t)nx * ny * nzh;
+  double *f = (double *)calloc(3 * N, sizeof(double));
+  double *u = (double *)calloc(3 * N, sizeof(double));
+  or_cpx *fh = (or_cpx *)calloc(3 * NH, sizeof(or_cpx));
+  double *g = (double *)malloc(sizeof(double) * (size_t)np * 3 * ngd);
+  double *gd = (double *)malloc(sizeof(double) * (size_t)np * 3 * ngd);
+  double *gr = (double *)malloc(sizeof(double) * (size_t)np * 3 * ngd);
+  int *ind = (int *)malloc(sizeof(int) * (size_t)np * 3 * ngd);
+  const double *Y = s->Y, *F = s->F, *T = s->TAU;
+  double sink = 0.0;
+  /* pass 0 is an untimed warm-up (first-touch page faults are not part of a
+   * solve); pass 1 is timed. The samples touch about 1/stride of the grids. */
+  for (int rep = 0; rep < 2; ++rep) {
+  double t0 = or_now();
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < np / stride; ++b)
+    or_gauss_bead(p, &c, Y + 3 * b, g + (size_t)b * 3 * ngd, gd + (size_t)b * 3 * ngd, gr + (size_t)b * 3 * ngd,
+                  ind + (size_t)b * 3 * ngd);
+#pragma omp parallel
+  {
+    int nth = 1, tid = 0;
+#ifdef _OPENMP
+    nth = omp_get_num_threads();
+    tid = omp_get_thread_num();
+#endif
+    int x0 = (int)((long)nx * tid / nth), x1 = (int)((long)nx * (tid + 1) / nth);
+    for (int b = 0; b < np / stride; ++b) {
+      const double *gx = g + (size_t)b * 3 * ngd, *gy = gx + ngd, *gz = gy + ngd;
+      const double *dgx = gd + (size_t)b * 3 * ngd, *dgy = dgx + ngd, *dgz = dgy + ngd;
+      const double *rx = gr + (size_t)b * 3 * ngd, *ry = rx + ngd, *rz = ry + ngd;
+      const int *ix = ind + (size_t)b * 3 * ngd, *iy = ix + ngd, *iz = iy + ngd;
+      const double g12 = 0.5 * T[3 * b + 2], g13 = -0.5 * T[3 * b + 1], g23 = 0.5 * T[3 * b];
+      for (int i = 0; i < ngd; ++i) {
+        int ii = ix[i];
+        if (ii < x0 || ii >= x1) continue;
+        for (int j = 0; j < ngd; ++j)
+          for (int k = 0; k < ngd; ++k) {
+            size_t m = ((size_t)ii * ny + iy[j]) * nz + iz[k];
+            double temp = gx[i] * gy[j] * gz[k], temp2 = dgx[i] * dgy[j] * dgz[k];
+            f[m] += F[3 * b] * temp + (g12 * ry[j] + g13 * rz[k]) * temp2;
+            f[N + m] += F[3 * b + 1] * temp + (-g12 * rx[i] + g23 * rz[k]) * temp2;
+            f[2 * N + m] += F[3 * b + 2] * temp + (-g13 * rx[i] - g23 * ry[j]) * temp2;
+          }
+      }
+    }
+  }
+  parts[0] = (or_now() - t0) * stride;
+  t0 = or_now();
+  for (int cpt = 0; cpt < 3; ++cpt) fft_r2c_3d_s(f + cpt * N, fh + cpt * NH, nx, ny, nz, stride);
+  parts[1] = (or_now() - t0) * stride;
+  t0 = or_now();
+  {
+    const double TwoPI = 2. * OR_PI;
+    const double ffx = TwoPI / (nx * p->dx), ffy = TwoPI / (ny * p->dx), ffz = TwoPI / (nz * p->dx);
+    const double totalpts = (double)N;
+#pragma omp parallel for schedule(static)
+    for (long ij = 0; ij < (long)nx * ny / stride; ++ij) {
+      int i = (int)(ij / ny), j = (int)(ij % ny);
+      double q1 = (i <= nx / 2 ? i : i - nx) * ffx, q2 = (j <= ny / 2 ? j : j - ny) * ffy;
+      double qq = q2 * q2 + q1 * q1 + 1e-18;
+      for (int k = 0; k < nzh; ++k) {
+        size_t m = (size_t)ij * nzh + k;
+        double q3 = k * ffz, norm = 1.0 / (qq + q3 * q3);
+        for (int part = 0; part < 2; ++part) {
+          double *a1 = part ? &fh[m].im : &fh[m].re, *a2 = part ? &fh[NH + m].im : &fh[NH + m].re,
+                 *a3 = part ? &fh[2 * NH + m].im : &fh[2 * NH + m].re;
+          double kdotf = (q1 * *a1 + q2 * *a2 + q3 * *a3) * norm;
+          *a1 = norm * (*a1 - q1 * kdotf) / totalpts;
+          *a2 = norm * (*a2 - q2 * kdotf) / totalpts;
+          *a3 = norm * (*a3 - q3 * kdotf) / totalpts;
+        }
+      }
+    }
+  }
+  parts[2] = (or_now() - t0) * stride;
+  t0 = or_now();
+  for (int cpt = 0; cpt < 3; ++cpt) fft_c2r_3d_s(fh + cpt * NH, u + cpt * N, nx, ny, nz, stride);
+  parts[3] = (or_now() - t0) * stride;
+  t0 = or_now();
+#pragma omp parallel for schedule(static) reduction(+ : sink)
+  for (int b = 0; b < np / stride; ++b) {
+    const double *gx = g + (size_t)b * 3 * ngd, *gy = gx + ngd, *gz = gy + ngd;
+    const double *dgx = gd + (size_t)b * 3 * ngd, *dgy = dgx + ngd, *dgz = dgy + ngd;
+    const double *rx = gr + (size_t)b * 3 * ngd, *ry = rx + ngd, *rz = ry + ngd;
+    const int *ix = ind + (size_t)b * 3 * ngd, *iy = ix + ngd, *iz = iy + ngd;
+    double v[3] = {0, 0, 0}, w[3] = {0, 0, 0};
+    for (int i = 0; i < ngd; ++i)
+      for (int j = 0; j < ngd; ++j)
+        for (int k = 0; k < ngd; ++k) {
+          size_t m = ((size_t)ix[i] * ny + iy[j]) * nz + iz[k];
+          double temp = gx[i] * gy[j] * gz[k], tempd = dgx[i] * dgy[j] * dgz[k];
+          v[0] += u[m] * temp;
+          v[1] += u[N + m] * temp;
+          v[2] += u[2 * N + m] * temp;
+          w[0] -= 0.5 * (u[2 * N + m] * ry[j] - u[N + m] * rz[k]) * tempd;
+          w[1] -= 0.5 * (u[m] * rz[k] - u[2 * N + m] * rx[i]) * tempd;
+          w[2] -= 0.5 * (u[N + m] * rx[i] - u[m] * ry[j]) * tempd;
+        }
+    sink += v[0] + v[1] + v[2] + w[0] + w[1] + w[2];
+  }
+  parts[4] = (or_now() - t0) * stride;
+  t0 = or_now();
+#pragma omp parallel for schedule(dynamic)
+  for (int fl = 0; fl < s->nfil / stride; ++fl) {
+    int nw = s->fil_start[fl + 1] - s->fil_start[fl];
+    int n = 6 * nw;
+    double *J = (double *)malloc(sizeof(double) * (size_t)n * n);
+    or_build_J(s, fl, 2, J);
+    or_invert(J, n, s->Jinv + s->joff[fl]);
+    free(J);
+  }
+  parts[5] = (or_now() - t0) * stride;
+  t0 = or_now();
+  or_filament_forces(s, 2);
+  or_error_check(s, s->V, s->W, s->NewErr, 2);
+  int hist = p->broyden_maxiter < 10 ? p->broyden_maxiter : 10;
+  or_jsolve(s, s->Err, s->Upd, hist);
+  or_jsolve(s, s->NewErr, s->tmp, hist);
+  parts[6] = or_now() - t0;
+  t0 = or_now();
+  or_cells_link(p, np, s->Xs, s->head, s->list);
+  or_collision_barrier(p, np, s->fil_id, s->seg_id, s->Y, s->head, s->list, s->map, 2, s->F, &s->min_dist2, NULL, 0);
+  parts[7] = or_now() - t0;
+  }
+  parts[8] = sink;
+  free(f); free(u); free(fh); free(g); free(gd); free(gr); free(ind);
+  int nth = 1;
+#ifdef _OPENMP
+  nth = omp_get_max_threads();
+#endif
+  return nth;
+}

@@ -55,6 +55,9 @@ void or_update(or_system *sys, const double *upd);
 void or_step(or_system *sys, int nt);
 int or_step_implicit(or_system *sys, int nt, int *iters);
 int or_run_steps(or_system *sys, int nt_start, int nsteps, int *iters);
+/* CPU-baseline timing sample: stage wall times of one iteration, each stage run
+ * on every stride-th work unit and scaled back (parts: 9 doubles) */
+int or_sample_costs(or_system *sys, int stride, double *parts);
 /* last step's barrier minimum squared distance */
 double or_last_min_dist2(or_system *sys);
 long long or_mobility_solves(or_system *sys);

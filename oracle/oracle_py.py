@@ -61,6 +61,8 @@ def lib():
         L.or_last_min_dist2.argtypes = [vp]
         L.or_mobility_solves.restype = ctypes.c_longlong
         L.or_mobility_solves.argtypes = [vp]
+        L.or_sample_costs.restype = ctypes.c_int
+        L.or_sample_costs.argtypes = [vp, ctypes.c_int, vp]
         _lib = L
     return _lib
 
@@ -242,3 +244,12 @@ class System:
 
     def min_dist2(self):
         return lib().or_last_min_dist2(self.h)
+
+    STAGE_NAMES = ("spread", "fft_fwd", "project", "fft_inv", "interp", "jacobian", "iteration_other", "barrier")
+
+    def sample_costs(self, stride):
+        """Stage wall seconds of one iteration, sampled on 1/stride of the work
+        units and scaled back; returns (dict, threads)."""
+        parts = np.zeros(9)
+        nth = lib().or_sample_costs(self.h, stride, _ptr(parts))
+        return dict(zip(self.STAGE_NAMES, parts[:8].tolist())), int(nth)
