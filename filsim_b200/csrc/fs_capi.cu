@@ -64,8 +64,8 @@ fs_status alloc_state(fs_ctx *c) {
   FS_CUDA(cudaMalloc(&c->fil_start, sizeof(int) * (nf + 1)));
   FS_CUDA(cudaMalloc(&c->fil_id, sizeof(int) * nb));
   FS_CUDA(cudaMalloc(&c->seg_id, sizeof(int) * nb));
-  FS_CUDA(cudaMalloc(&c->jpiv, sizeof(int) * 6 * nb));
-  FS_CUDA(cudaMalloc(&c->joff, sizeof(long long) * (nf + 1)));
+  FS_CUDA(cudaMalloc(&c->soff, sizeof(long long) * (nf + 1)));
+  FS_CUDA(cudaMalloc(&c->aoff, sizeof(long long) * (nf + 1)));
   const size_t hist = (size_t)c->p.broyden_maxiter * 6 * nb;
   FS_CUDA(cudaMalloc(&c->Cmat, sizeof(double) * hist));
   FS_CUDA(cudaMalloc(&c->Dmat, sizeof(double) * hist));
@@ -84,8 +84,8 @@ fs_status alloc_state(fs_ctx *c) {
 void free_state(fs_ctx *c) {
   void *ptrs[] = {c->X, c->Xs, c->Xt, c->U, c->Us, c->Ut, c->F, c->TAU, c->Y, c->V, c->W, c->lam, c->lam1,
                   c->lam2, c->q, c->qs, c->qt, c->err, c->newerr, c->upd, c->tmp, c->dE, c->kap, c->cc,
-                  c->fil_start, c->fil_id, c->seg_id, c->jpiv, c->joff, c->Cmat, c->Dmat, c->dots, c->partials,
-                  c->scalars, c->flags, c->maxerr_bits, c->J};
+                  c->fil_start, c->fil_id, c->seg_id, c->soff, c->aoff, c->Cmat, c->Dmat, c->dots, c->partials,
+                  c->scalars, c->flags, c->maxerr_bits, c->Sinv, c->aux};
   for (void *p : ptrs) cudaFree(p);
   if (c->flags_h) cudaFreeHost(c->flags_h);
 }
@@ -413,9 +413,9 @@ fs_status fs_state_upload(fs_ctx *c, const fs_host_state *s) {
   const int nf = s->nfil, np = s->np;
   if (s->fil_start[0] != 0 || s->fil_start[nf] != np) return FS_ERR_INVALID_ARG;
   std::vector<int> fid(np > 0 ? np : 1), sid(np > 0 ? np : 1);
-  std::vector<long long> joff(nf + 1);
+  std::vector<long long> soff(nf + 1), aoff(nf + 1);
   int max_nw = 1;
-  joff[0] = 0;
+  soff[0] = aoff[0] = 0;
   for (int f = 0; f < nf; ++f) {
     const int nw = s->fil_start[f + 1] - s->fil_start[f];
     if (nw < 1) return FS_ERR_INVALID_ARG;
@@ -424,21 +424,29 @@ fs_status fs_state_upload(fs_ctx *c, const fs_host_state *s) {
       fid[s->fil_start[f] + i] = f;
       sid[s->fil_start[f] + i] = i;
     }
-    joff[f + 1] = joff[f] + 36LL * nw * nw;
+    soff[f + 1] = soff[f] + 9LL * nw * nw;
+    aoff[f + 1] = aoff[f] + fil_aux_size(nw);
   }
-  if (max_nw > 1024) return FS_ERR_INVALID_ARG;  // one filament's solve vector lives in shared memory
+  const int prev_max_nw = c->max_nw;
+  c->max_nw = max_nw;
+  if (fil_jacobian_prepare(c) != FS_OK) {  // the Schur complement of a filament lives in shared memory
+    c->max_nw = prev_max_nw;
+    return FS_ERR_INVALID_ARG;
+  }
   c->nfil = nf;
   c->np = np;
   c->nlink = np - nf;
-  c->max_nw = max_nw;
-  cudaFree(c->J);
-  c->J = nullptr;
-  FS_CUDA(cudaMalloc(&c->J, sizeof(double) * (size_t)(joff[nf] > 0 ? joff[nf] : 1)));
+  cudaFree(c->Sinv);
+  cudaFree(c->aux);
+  c->Sinv = c->aux = nullptr;
+  FS_CUDA(cudaMalloc(&c->Sinv, sizeof(double) * (size_t)(soff[nf] > 0 ? soff[nf] : 1)));
+  FS_CUDA(cudaMalloc(&c->aux, sizeof(double) * (size_t)(aoff[nf] > 0 ? aoff[nf] : 1)));
   cudaStream_t st = c->stream;
   FS_CUDA(cudaMemcpyAsync(c->fil_start, s->fil_start, sizeof(int) * (nf + 1), cudaMemcpyHostToDevice, st));
   FS_CUDA(cudaMemcpyAsync(c->fil_id, fid.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
   FS_CUDA(cudaMemcpyAsync(c->seg_id, sid.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
-  FS_CUDA(cudaMemcpyAsync(c->joff, joff.data(), sizeof(long long) * (nf + 1), cudaMemcpyHostToDevice, st));
+  FS_CUDA(cudaMemcpyAsync(c->soff, soff.data(), sizeof(long long) * (nf + 1), cudaMemcpyHostToDevice, st));
+  FS_CUDA(cudaMemcpyAsync(c->aoff, aoff.data(), sizeof(long long) * (nf + 1), cudaMemcpyHostToDevice, st));
   struct F3 {
     double *d;
     const double *h;

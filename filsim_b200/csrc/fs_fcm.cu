@@ -32,9 +32,18 @@ __host__ __device__ inline int wrap_int(int x, int n) {
   int r = x % n;
   return r < 0 ? r + n : r;
 }
+// x in (-n, 2n): one conditional add or subtract
+__device__ __forceinline__ int wrap_near(int x, int n) {
+  x += (x < 0) ? n : 0;
+  return x >= n ? x - n : x;
+}
 
 // ---- 1. binning -------------------------------------------------------------
-__global__ void k_fcm_bin_keys(const double *__restrict__ Y, int np, FcmConsts c, int *__restrict__ key) {
+// key: the tile bin of the wrapped stencil start; sw: the wrapped stencil
+// start per axis (gaussian_setup's index rule, FCMfunctions.cpp:565-585), kept
+// for the spread and interpolation kernels so they need no integer division.
+__global__ void k_fcm_bin_keys(const double *__restrict__ Y, int np, FcmConsts c, int *__restrict__ key,
+                               int *__restrict__ sw_out) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= np) return;
   int bi[3];
@@ -42,6 +51,7 @@ __global__ void k_fcm_bin_keys(const double *__restrict__ Y, int np, FcmConsts c
   for (int d = 0; d < 3; ++d) {
     int xc = (int)(Y[3 * b + d] / c.dx);
     int sw = wrap_int(xc - c.ngdh + 1, c.N[d]);
+    sw_out[3 * b + d] = sw;
     bi[d] = sw / FS_TILE;
   }
   key[b] = (bi[0] * c.nbin[1] + bi[1]) * c.nbin[2] + bi[2];
@@ -57,7 +67,7 @@ struct SpreadChunk {
   R th[FS_SPREAD_CHUNK][3];  // half torque (0.5 T)
   unsigned char ly[FS_SPREAD_CHUNK][16], lz[FS_SPREAD_CHUNK][16];
   int ax[FS_SPREAD_CHUNK];   // (X0 - stencil start) mod N
-  int cy[FS_SPREAD_CHUNK], cz[FS_SPREAD_CHUNK];
+  int cy[FS_SPREAD_CHUNK], cz[FS_SPREAD_CHUNK], mcz[FS_SPREAD_CHUNK];
   int bead[FS_SPREAD_CHUNK];
 };
 
@@ -111,7 +121,8 @@ __device__ inline float fs_exp<float>(float x) { return expf(x); }
 template <typename R>
 __global__ void __launch_bounds__(FS_TILE * 32, 2)
     k_spread(const double *__restrict__ Y, const double *__restrict__ F, const double *__restrict__ T,
-             const int *__restrict__ bin_start, const int *__restrict__ sorted, FcmConsts c, R *__restrict__ fgrid) {
+             const int *__restrict__ bin_start, const int *__restrict__ sorted, const int *__restrict__ bead_sw,
+             FcmConsts c, R *__restrict__ fgrid) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SpreadSmem<R> &sm = *reinterpret_cast<SpreadSmem<R> *>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -176,8 +187,9 @@ __global__ void __launch_bounds__(FS_TILE * 32, 2)
         rr = -xf / (R)c.sigmadipsq;
       }
       const int Nn = c.N[a];
-      const int sw = wrap_int(xc - c.ngdh + 1, Nn);
-      const int aoff = wrap_int(X0[a] - sw, Nn);
+      const int sw = bead_sw[3 * bead + a];  // wrapped stencil start, in [0, N)
+      // stencil index i lands on tile-local l = (i - aoff) mod N; valid if l < FS_TILE
+      const int aoff = wrap_near(X0[a] - sw, Nn);
       if (a == 0) {
         sm.ch.gx[s][i] = g;
         sm.ch.dgx[s][i] = gd;
@@ -192,18 +204,17 @@ __global__ void __launch_bounds__(FS_TILE * 32, 2)
           }
         }
       } else {
-        // compacted position among stencil indices that land in the tile
-        int pos = 0, cnt = 0, mine = -1;
-        for (int i2 = 0; i2 < ngd; ++i2) {
-          int l = wrap_int(i2 - aoff, Nn);
-          if (l < FS_TILE) {
-            if (i2 == i) mine = l;
-            if (i2 < i) pos++;
-            cnt++;
-          }
-        }
+        // the valid indices form [0, e2) (stencil wrapped around the box) and
+        // [aoff, e1); compact them in index order
+        const int e1 = min(ngd, aoff + FS_TILE);
+        const int e2 = max(0, min(ngd, aoff + FS_TILE - Nn));
+        const int n1 = max(0, e1 - aoff);
+        const bool in2 = i < e2, in1 = i >= aoff && i < e1;
+        const int pos = in2 ? i : e2 + (i - aoff);
+        const int mine = in2 ? i - aoff + Nn : i - aoff;
+        const int cnt = n1 + e2;
         if (a == 1) {
-          if (mine >= 0) {
+          if (in1 || in2) {
             sm.ch.gy[s][pos] = g;
             sm.ch.dgy[s][pos] = gd;
             sm.ch.ry[s][pos] = rr;
@@ -211,29 +222,34 @@ __global__ void __launch_bounds__(FS_TILE * 32, 2)
           }
           if (i == 0) sm.ch.cy[s] = cnt;
         } else {
-          if (mine >= 0) {
+          if (in1 || in2) {
             sm.ch.gz[s][pos] = g;
             sm.ch.dgz[s][pos] = gd;
             sm.ch.rz[s][pos] = rr;
             sm.ch.lz[s][pos] = (unsigned char)mine;
           }
-          if (i == 0) sm.ch.cz[s] = cnt;
+          if (i == 0) {
+            sm.ch.cz[s] = cnt;
+            sm.ch.mcz[s] = cnt > 0 ? (4096 + cnt - 1) / cnt : 0;
+          }
         }
       }
     }
     __syncthreads();
     // scatter: warp `warp` owns tile x-plane `warp`
     for (int s = 0; s < nb; ++s) {
-      const int i = wrap_int(warp + sm.ch.ax[s], c.N[0]);
+      int i = warp + sm.ch.ax[s];
+      i = i >= c.N[0] ? i - c.N[0] : i;
       if (i < ngd) {
         const R gxv = sm.ch.gx[s][i], dxv = sm.ch.dgx[s][i], rxv = sm.ch.rx[s][i];
         const R F0 = sm.ch.f[s][0], F1 = sm.ch.f[s][1], F2 = sm.ch.f[s][2];
         // g12 = T2/2, g13 = -T1/2, g21 = -T2/2, g23 = T0/2, g31 = T1/2, g32 = -T0/2 (GA_setup, :536-547)
         const R h0 = sm.ch.th[s][0], h1 = sm.ch.th[s][1], h2 = sm.ch.th[s][2];
-        const int cy = sm.ch.cy[s], cz = sm.ch.cz[s];
+        const int cy = sm.ch.cy[s], cz = sm.ch.cz[s], mcz = sm.ch.mcz[s];
         const int cnt = cy * cz;
         for (int pidx = lane; pidx < cnt; pidx += 32) {
-          const int jj = pidx / cz, kk = pidx - jj * cz;
+          // pidx / cz by multiply-shift: exact for pidx < 256, cz <= 16
+          const int jj = (pidx * mcz) >> 12, kk = pidx - jj * cz;
           const R gyv = sm.ch.gy[s][jj], dyv = sm.ch.dgy[s][jj], ryv = sm.ch.ry[s][jj];
           const R gzv = sm.ch.gz[s][kk], dzv = sm.ch.dgz[s][kk], rzv = sm.ch.rz[s][kk];
           const R temp = gxv * gyv * gzv;
@@ -396,8 +412,8 @@ struct InterpWarp {
 
 template <typename R>
 __global__ void __launch_bounds__(256) k_interp(const R *__restrict__ u, const double *__restrict__ Y,
-                                                const int *__restrict__ order, int np, FcmConsts c,
-                                                double *__restrict__ V, double *__restrict__ W) {
+                                                const int *__restrict__ order, const int *__restrict__ bead_sw,
+                                                int np, FcmConsts c, double *__restrict__ V, double *__restrict__ W) {
   __shared__ InterpWarp<R> sw[8];
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const int wid = blockIdx.x * 8 + wl;
@@ -405,36 +421,53 @@ __global__ void __launch_bounds__(256) k_interp(const R *__restrict__ u, const d
   const int b = order[wid];
   InterpWarp<R> &s = sw[wl];
   const int ngd = c.ngd;
-  for (int it = lane; it < 3 * ngd; it += 32) {
-    const int a = it / ngd, i = it % ngd;
+  for (int it = lane; it < 3 * 16; it += 32) {
+    const int a = it >> 4, i = it & 15;
+    if (i >= ngd) continue;
     const double Yv = Y[3 * b + a];
     const int xc = (int)(Yv / c.dx);
     const int xg = xc - c.ngdh + (i + 1);
-    s.ind[a][i] = xg - c.N[a] * ((int)floor(((double)xg) / ((double)c.N[a])));
+    const int ix = bead_sw[3 * b + a] + i;  // (stencil start + i) mod N, as gaussian_setup's indx
+    s.ind[a][i] = ix >= c.N[a] ? ix - c.N[a] : ix;
     const double xx = ((double)xg) * c.dx - Yv;
-    s.g[a][i] = (R)(c.anorm * exp(-xx * xx / c.anorm2));
-    s.gd[a][i] = (R)(c.anormdip * exp(-xx * xx / c.anormdip2));
-    s.r[a][i] = (R)(-xx / c.sigmadipsq);
+    if (sizeof(R) == 8) {
+      s.g[a][i] = (R)(c.anorm * exp(-xx * xx / c.anorm2));
+      s.gd[a][i] = (R)(c.anormdip * exp(-xx * xx / c.anormdip2));
+      s.r[a][i] = (R)(-xx / c.sigmadipsq);
+    } else {
+      const R xf = (R)xx;
+      s.g[a][i] = (R)c.anorm * fs_exp<R>(-xf * xf / (R)c.anorm2);
+      s.gd[a][i] = (R)c.anormdip * fs_exp<R>(-xf * xf / (R)c.anormdip2);
+      s.r[a][i] = -xf / (R)c.sigmadipsq;
+    }
   }
   __syncwarp();
   const size_t N = (size_t)c.N[0] * c.N[1] * c.N[2];
   const R *ux = u, *uy = u + N, *uz = u + 2 * N;
   KSum<R> v0, v1, v2, w0, w1, w2;
   v0.init(); v1.init(); v2.init(); w0.init(); w1.init(); w2.init();
-  const int ngd2 = ngd * ngd, ngd3 = ngd2 * ngd;
-  for (int p = lane; p < ngd3; p += 32) {
-    const int i = p / ngd2, rem = p - i * ngd2, j = rem / ngd, k = rem - j * ngd;
-    const size_t m = ((size_t)s.ind[0][i] * c.N[1] + s.ind[1][j]) * c.N[2] + s.ind[2][k];
-    const R a0 = ux[m], a1 = uy[m], a2 = uz[m];
-    const R temp = s.g[0][i] * s.g[1][j] * s.g[2][k];
-    const R tempd = s.gd[0][i] * s.gd[1][j] * s.gd[2][k];
-    const R xx = s.r[0][i], yy = s.r[1][j], zz = s.r[2][k];
-    v0.add(a0 * temp);
-    v1.add(a1 * temp);
-    v2.add(a2 * temp);
-    w0.add((a2 * yy - a1 * zz) * tempd);
-    w1.add((a0 * zz - a2 * xx) * tempd);
-    w2.add((a1 * xx - a0 * yy) * tempd);
+  // lane -> (row parity, z index): two stencil rows (i, j) per pass, z contiguous
+  const int k = lane & 15, jsub = lane >> 4;
+  if (k < ngd) {
+    const R gzk = s.g[2][k], dzk = s.gd[2][k], zz = s.r[2][k];
+    const int iz = s.ind[2][k];
+    for (int i = 0; i < ngd; ++i) {
+      const R gx = s.g[0][i], dxv = s.gd[0][i], xx = s.r[0][i];
+      const size_t plane = (size_t)s.ind[0][i] * c.N[1];
+      for (int j = jsub; j < ngd; j += 2) {
+        const size_t m = (plane + s.ind[1][j]) * c.N[2] + iz;
+        const R a0 = ux[m], a1 = uy[m], a2 = uz[m];
+        const R temp = gx * s.g[1][j] * gzk;
+        const R tempd = dxv * s.gd[1][j] * dzk;
+        const R yy = s.r[1][j];
+        v0.add(a0 * temp);
+        v1.add(a1 * temp);
+        v2.add(a2 * temp);
+        w0.add((a2 * yy - a1 * zz) * tempd);
+        w1.add((a0 * zz - a2 * xx) * tempd);
+        w2.add((a1 * xx - a0 * yy) * tempd);
+      }
+    }
   }
   v0.warp_reduce(); v1.warp_reduce(); v2.warp_reduce();
   w0.warp_reduce(); w1.warp_reduce(); w2.warp_reduce();
@@ -542,19 +575,20 @@ fs_status mobility_t(fs_ctx *c, const double *Y, const double *F, const double *
   {
     ProfScope ps(c, FS_STAGE_SPREAD);
     if (np > 0) {
-      k_fcm_bin_keys<<<fs_blocks(np, 256), 256, 0, c->stream>>>(Y, np, k, c->bins.key);
+      k_fcm_bin_keys<<<fs_blocks(np, 256), 256, 0, c->stream>>>(Y, np, k, c->bins.key, c->bead_sw);
       FS_LAUNCH_CHECK();
     }
     FS_TRY(fs_sort_run(&c->bins, np, c->stream));
     const size_t smem = sizeof(SpreadSmem<R>);
-    k_spread<R><<<c->nbins, FS_TILE * 32, smem, c->stream>>>(Y, F, T, c->bins.start, c->bins.sorted, k,
+    k_spread<R><<<c->nbins, FS_TILE * 32, smem, c->stream>>>(Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k,
                                                               (R *)c->grid_real);
     FS_LAUNCH_CHECK();
   }
   FS_TRY(flow_solve_t<R>(c));
   if (np > 0) {
     ProfScope ps(c, FS_STAGE_INTERP);
-    k_interp<R><<<fs_blocks(np, 8), 256, 0, c->stream>>>((const R *)c->grid_real, Y, c->bins.sorted, np, k, V, W);
+    k_interp<R><<<fs_blocks(np, 8), 256, 0, c->stream>>>((const R *)c->grid_real, Y, c->bins.sorted, c->bead_sw, np, k,
+                                                          V, W);
     FS_LAUNCH_CHECK();
   }
   c->last_grid_prec = sizeof(R) == 8 ? FS_PREC_FP64 : FS_PREC_FP32;
@@ -577,6 +611,8 @@ fs_status fcm_init(fs_ctx *c) {
   FS_CUDA(cudaMalloc(&c->grid_cplx, sizeof(double2) * 3 * c->NH));
   c->bytes += sizeof(double) * 3 * c->N + sizeof(double2) * 3 * c->NH;
   FS_TRY(fs_sort_alloc(&c->bins, c->nbins, c->max_beads, &c->bytes));
+  FS_CUDA(cudaMalloc(&c->bead_sw, sizeof(int) * 3 * (size_t)(c->max_beads > 0 ? c->max_beads : 1)));
+  c->bytes += sizeof(int) * 3 * (size_t)c->max_beads;
   FS_CUDA(cudaFuncSetAttribute(k_spread<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(SpreadSmem<double>)));
   FS_CUDA(cudaFuncSetAttribute(k_spread<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -595,6 +631,8 @@ void fcm_free(fs_ctx *c) {
   cudaFree(c->grid_cplx);
   c->grid_real = c->grid_cplx = nullptr;
   fs_sort_free(&c->bins);
+  cudaFree(c->bead_sw);
+  c->bead_sw = nullptr;
 }
 
 fs_status fcm_mobility(fs_ctx *c, const double *Y, const double *F, const double *T, double *V, double *W, int np) {
@@ -617,12 +655,12 @@ fs_status fcm_friction(fs_ctx *c, const double *F, const double *T, double *V, d
 fs_status fcm_spread_only(fs_ctx *c, const double *Y, const double *F, const double *T, int np, double *f) {
   FcmConsts k = make_consts(c);
   if (np > 0) {
-    k_fcm_bin_keys<<<fs_blocks(np, 256), 256, 0, c->stream>>>(Y, np, k, c->bins.key);
+    k_fcm_bin_keys<<<fs_blocks(np, 256), 256, 0, c->stream>>>(Y, np, k, c->bins.key, c->bead_sw);
     FS_LAUNCH_CHECK();
   }
   FS_TRY(fs_sort_run(&c->bins, np, c->stream));
   k_spread<double><<<c->nbins, FS_TILE * 32, sizeof(SpreadSmem<double>), c->stream>>>(
-      Y, F, T, c->bins.start, c->bins.sorted, k, (double *)c->grid_real);
+      Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k, (double *)c->grid_real);
   FS_LAUNCH_CHECK();
   FS_CUDA(cudaMemcpyAsync(f, c->grid_real, sizeof(double) * 3 * c->N, cudaMemcpyDeviceToDevice, c->stream));
   c->last_grid_prec = -1;

@@ -7,11 +7,12 @@
 //   k_forces             setZeroForcesTorques, applyElasticTorques, applyConstraintForcesTorques,
 //                        applyExternalForcesTorques (Filament.hpp:271-402), one thread per bead
 //                        adding its links' terms in the reference's order
-//   k_jacobian           buildApproximateJacobian with BlockC/D/E/F (Filament.hpp:803-1120), then
-//                        LU with partial pivoting in place (one CTA per filament, column-major)
+//   k_jacobian_schur     buildApproximateJacobian with BlockC/D/E/F (Filament.hpp:803-1120) reduced
+//                        to the 3Nw x 3Nw Schur complement of its constraint block, inverted in
+//                        shared memory (one CTA per filament)
 //   k_error_check        ErrorCheckFCM + dexpinv (MobilityConstraints.cpp:109-143, 447-770)
-//   k_lu_apply           filamentJsolver::solve (FilamentJacobianSolver.hpp:49-73): J0^-1 b by
-//                        the LU factors, then the bad-Broyden history corrections
+//   k_schur_apply        filamentJsolver::solve (FilamentJacobianSolver.hpp:49-73): J0^-1 b from
+//                        the Schur inverse, then the bad-Broyden history corrections
 //   k_broyden_cols       history update of main.cpp:640-663
 //   k_update / k_step    Filament::update (Filament.hpp:425-452), Filament::step (:455-478)
 #include "fs_internal.cuh"
@@ -326,18 +327,19 @@ __device__ __forceinline__ void frame(const double *qa, double *t, double *n, do
   q_normal(q, n);
   q_binormal(q, b);
 }
-// column-major store of a 3x3 block at (r0, c0)
+// row-major store of a 3x3 block at (r0, c0) of an n-column matrix
 __device__ __forceinline__ void put3(double *J, int n, int r0, int c0, const M3 &a) {
   for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) J[(size_t)(c0 + j) * n + r0 + i] = a.m[3 * i + j];
+    for (int j = 0; j < 3; ++j) J[(size_t)(r0 + i) * n + c0 + j] = a.m[3 * i + j];
 }
 
-// the three BlockE blocks of bead row k (Filament.hpp:958-1089)
+// the three BlockE blocks of bead row k (Filament.hpp:958-1089), stored into
+// the 3nw x 3nw matrix J (row-major, leading dimension n = 3nw)
 __device__ void blockE_row(int k, int nw, const double *qs, const double *Us, const double *TAU, const double *lam,
                            double rad_k, double myC, double myKAP, const double *ST, double DL, double dt, double MU,
                            double *J, int n) {
   const double PI = FS_PI;
-  const int rE = 3 * nw, cE = 3;
+  const int rE = 0, cE = 0;
   double t[3], nn[3], b[3], tp1[3], np1[3], bp1[3], tm1[3], nm1[3], bm1[3];
   const double Tfac = 1 / (8 * PI * MU * pow(rad_k, 3));
   const M3 LieMat = mt(rcross(Us + 3 * k));
@@ -425,168 +427,296 @@ __device__ void blockE_row(int k, int nw, const double *qs, const double *Us, co
   put3(J, n, rE + 3 * k, cE + 3 * k + 3, blockE_off(dOmega, LieMat, dt));
 }
 
-// build J (column-major) then LU-factorise it in place; one CTA per filament
-__global__ void __launch_bounds__(256) k_jacobian(int nfil, const int *__restrict__ fil_start,
-                                                  const double *__restrict__ qs, const double *__restrict__ Us,
-                                                  const double *__restrict__ TAU, const double *__restrict__ lam,
-                                                  const double *__restrict__ kap, const double *__restrict__ cmod,
-                                                  const long long *__restrict__ joff, double *__restrict__ Jall,
-                                                  int *__restrict__ piv_all, int nt, FilConsts k, double a,
-                                                  double ah, int *__restrict__ flags) {
-  const int f = blockIdx.x;
-  const int b0 = fil_start[f], nw = fil_start[f + 1] - b0, l0 = b0 - f;
-  const int n = 6 * nw;
-  double *J = Jall + joff[f];
-  int *piv = piv_all + 6 * b0;
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  const double PI = FS_PI, dt = k.dt, DL = k.dl, MU = k.mu;
-  const double *q_f = qs + 4 * b0;
-  const double *Us_f = Us + 3 * b0;
-  const double *TAU_f = TAU + 3 * b0;
-  const double *lam_f = lam + 3 * l0;
-  // bead radius: ah for bead 0, a for the others
-#define RAD(kk) ((kk) == 0 ? ah : a)
-  for (long long e = tid; e < (long long)n * n; e += nthr) J[e] = 0.0;
-  __syncthreads();
-  const double Jprefac = 10.;
-  if (tid == 0) {
-    int j = 3 * nw + 3;
-    double temp = dt / (9 * PI * MU * RAD(0));
-    for (int d = 0; d < 3; ++d) J[(size_t)d * n + d] = 1;
-    if (nw > 1)
-      for (int d = 0; d < 3; ++d) J[(size_t)(j + d) * n + d] = temp / dt;
-    else
-      for (int d = 0; d < 3; ++d) J[(size_t)(3 + d) * n + 3 + d] = 1;
-  }
-  if (nw > 1) {
-    // BlockC(0.5*DL): row block r, col block m <= r+1
-    const double fac = 0.5 * DL;
-    const int ntask = (nw - 1) * (nw + 2);
-    for (int tsk = tid; tsk < ntask; tsk += nthr) {
-      const int r = tsk / (nw + 2), m = tsk % (nw + 2);
-      if (m > r + 1) continue;
-      double tv[3];
-      q_tangent(qload(q_f + 4 * m), tv);
-      M3 blk = msc(rcross(tv), fac);
-      if (!(m == 0 || m == r + 1)) blk = madd(blk, blk);
-      put3(J, n, 3 + 3 * r, 3 + 3 * m, blk);
-    }
-    // Jprefac * BlockD(nt) / dt
-    for (int m = tid; m < nw - 1; m += nthr) {
-      double facn = -2. * dt / (18. * PI * MU * RAD(m));
-      if (nt <= k.impl_euler_steps) facn *= (3. / 2.);
-      const int i = 3 * m;
-      for (int d = 0; d < 3; ++d) J[(size_t)(3 * nw + 3 + i + d) * n + 3 + i + d] = Jprefac * facn / dt;
-      if (m < nw - 2) {
-        facn = 2. * dt / (18. * PI * MU * RAD(m + 1));
-        if (nt <= k.impl_euler_steps) facn *= (3. / 2.);
-        for (int d = 0; d < 3; ++d) J[(size_t)(3 * nw + 3 + i + 3 + d) * n + 3 + i + d] = Jprefac * facn / dt;
-      }
-    }
-    // BlockE rows
-    for (int kk = tid; kk < nw; kk += nthr)
-      blockE_row(kk, nw, q_f, Us_f, TAU_f, lam_f, RAD(kk), cmod[f], kap[f], k.st, DL, dt, MU, J, n);
-    // BlockF / dt
-    for (int i = tid; i < nw - 1; i += nthr) {
-      const int jj = 3 * i;
-      double tv[3];
-      double fac2 = dt * DL / (24 * PI * MU * pow(RAD(i), 3.));
-      q_tangent(qload(q_f + 4 * i), tv);
-      M3 tmat = mt(rcross(tv));
-      M3 umat = rcross(Us_f + 3 * i);
-      M3 blk = madd(msub(tmat, msc(mmul(umat, tmat), 0.5)), msc(mmul(mmul(umat, umat), tmat), 1. / 12.));
-      put3(J, n, 3 * nw + jj, 3 * nw + 3 + jj, msc(blk, fac2 / dt));
-      fac2 = dt * DL / (24. * PI * MU * pow(RAD(i + 1), 3));
-      q_tangent(qload(q_f + 4 * (i + 1)), tv);
-      tmat = mt(rcross(tv));
-      umat = rcross(Us_f + 3 * (i + 1));
-      blk = madd(msub(tmat, msc(mmul(umat, tmat), 0.5)), msc(mmul(mmul(umat, umat), tmat), 1. / 12.));
-      put3(J, n, 3 * nw + jj + 3, 3 * nw + 3 + jj, msc(blk, fac2 / dt));
-    }
-  }
-#undef RAD
-  __syncthreads();
-  if (nw > 1)
-    for (int e = tid; e < 3 * nw; e += nthr) J[(size_t)(3 + e) * n + 3 * nw + e] += 1.;
-  __syncthreads();
+// ---- approximate Jacobian by the Schur complement of the constraint block --------
+//
+// With columns [X0 (3) | U (3nw) | lambda (3nw-3)] and rows [first-bead
+// position (3) | constraints (3nw-3) | Lie updates (3nw)], the reference's J
+// (Filament.hpp:803-867) is
+//     J = [ I  0  P  ]    P  = (temp/dt) [I 0 ... 0]
+//         [ 0  C  D' ]    C  = BlockC(DL/2), D' = 10 BlockD/dt (block bidiagonal, scalar blocks)
+//         [ 0  E  F' ]    E  = BlockE,       F' = BlockF/dt (block bidiagonal)
+// Eliminating lambda = D'^-1 (b1 - C u) leaves S u = b2 - F' D'^-1 b1 with
+// S = E - F' D'^-1 C (3nw x 3nw). k_jacobian_schur builds S in shared memory and
+// inverts it (Gauss-Jordan, partial pivoting); k_schur_apply then applies J^-1
+// exactly, with the reference's 1/dt scaling of the lambda rows (:864).
+//
+// Per-filament auxiliary data (aux, nw >= 2): d[nw-1], e[nw-1] (D' blocks),
+// Fd[nw-1][9] = F'(k,k), Fl[nw-1][9] = F'(k+1,k), t[nw][3] tangents, pcoef.
+#define FS_MAX_NW 48
 
-  // ---- LU with partial pivoting (first maximum wins, as the CPU loop) ----
+// column cc of rcross(t) (Av = cross(v, t))
+__device__ __forceinline__ void rcross_col(const double *t, int cc, double *col) {
+  if (cc == 0) { col[0] = 0.; col[1] = -t[2]; col[2] = t[1]; }
+  else if (cc == 1) { col[0] = t[2]; col[1] = 0.; col[2] = -t[0]; }
+  else { col[0] = -t[1]; col[1] = t[0]; col[2] = 0.; }
+}
+
+__global__ void __launch_bounds__(256) k_jacobian_schur(
+    const int *__restrict__ fil_start, const double *__restrict__ qs, const double *__restrict__ Us,
+    const double *__restrict__ TAU, const double *__restrict__ lam, const double *__restrict__ kap,
+    const double *__restrict__ cmod, const long long *__restrict__ soff, const long long *__restrict__ aoff,
+    double *__restrict__ Sinv_all, double *__restrict__ aux_all, int nt, FilConsts k, double a, double ah,
+    int *__restrict__ flags) {
+  extern __shared__ double S[];  // 3nw x 3nw, row-major
+  __shared__ int perm[3 * FS_MAX_NW];
+  __shared__ double fcol[3 * FS_MAX_NW];
   __shared__ int s_piv;
   __shared__ double s_inv;
-  const int lane = tid & 31, warp = tid >> 5;
-  for (int kc = 0; kc < n; ++kc) {
-    double *col = J + (size_t)kc * n;
+  const int f = blockIdx.x;
+  const int b0 = fil_start[f], nw = fil_start[f + 1] - b0, l0 = b0 - f;
+  if (nw < 2) return;  // J0 is the identity
+  const int m = 3 * nw, nl = nw - 1;
+  const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const double PI = FS_PI, dt = k.dt, DL = k.dl, MU = k.mu;
+  const double *q_f = qs + 4 * b0, *Us_f = Us + 3 * b0, *TAU_f = TAU + 3 * b0, *lam_f = lam + 3 * l0;
+  double *aux = aux_all + aoff[f];
+  double *dd = aux, *ee = aux + nl, *Fd = aux + 2 * nl, *Fl = Fd + 9 * nl, *tt = Fl + 9 * nl, *pcoef = tt + 3 * nw;
+#define RAD(kk) ((kk) == 0 ? ah : a)
+  for (int e = tid; e < m * m; e += nthr) S[e] = 0.0;
+  for (int kk = tid; kk < nw; kk += nthr) {
+    double tv[3];
+    q_tangent(qload(q_f + 4 * kk), tv);
+    for (int d = 0; d < 3; ++d) tt[3 * kk + d] = tv[d];
+  }
+  const double Jprefac = 10.;
+  for (int r = tid; r < nl; r += nthr) {
+    // Jprefac * BlockD(nt) / dt (Filament.hpp:912-949)
+    double facn = -2. * dt / (18. * PI * MU * RAD(r));
+    if (nt <= k.impl_euler_steps) facn *= (3. / 2.);
+    dd[r] = Jprefac * facn / dt;
+    double facu = 0.0;
+    if (r < nw - 2) {
+      facu = 2. * dt / (18. * PI * MU * RAD(r + 1));
+      if (nt <= k.impl_euler_steps) facu *= (3. / 2.);
+      facu = Jprefac * facu / dt;
+    }
+    ee[r] = facu;
+    // BlockF / dt (Filament.hpp:1099-1120)
+    double tv[3];
+    double fac2 = dt * DL / (24 * PI * MU * pow(RAD(r), 3.));
+    q_tangent(qload(q_f + 4 * r), tv);
+    M3 tmat = mt(rcross(tv));
+    M3 umat = rcross(Us_f + 3 * r);
+    M3 blk = msc(madd(msub(tmat, msc(mmul(umat, tmat), 0.5)), msc(mmul(mmul(umat, umat), tmat), 1. / 12.)), fac2 / dt);
+    for (int e = 0; e < 9; ++e) Fd[9 * r + e] = blk.m[e];
+    fac2 = dt * DL / (24. * PI * MU * pow(RAD(r + 1), 3));
+    q_tangent(qload(q_f + 4 * (r + 1)), tv);
+    tmat = mt(rcross(tv));
+    umat = rcross(Us_f + 3 * (r + 1));
+    blk = msc(madd(msub(tmat, msc(mmul(umat, tmat), 0.5)), msc(mmul(mmul(umat, umat), tmat), 1. / 12.)), fac2 / dt);
+    for (int e = 0; e < 9; ++e) Fl[9 * r + e] = blk.m[e];
+  }
+  if (tid == 0) *pcoef = (dt / (9 * PI * MU * RAD(0))) / dt;
+  __syncthreads();
+  for (int kk = tid; kk < nw; kk += nthr)
+    blockE_row(kk, nw, q_f, Us_f, TAU_f, lam_f, RAD(kk), cmod[f], kap[f], k.st, DL, dt, MU, S, m);
+#undef RAD
+  __syncthreads();
+  for (int e = tid; e < m; e += nthr) S[e * m + e] += 1.;  // BlockE's identity (Filament.hpp:1092-1094)
+  __syncthreads();
+  // S -= F' D'^-1 C, one column of C per thread
+  const double fac = 0.5 * DL;
+  for (int j = tid; j < m; j += nthr) {
+    const int mb = j / 3, cc = j % 3;
+    double col[3];
+    rcross_col(tt + 3 * mb, cc, col);
+    double y[3 * (FS_MAX_NW - 1)];
+    for (int r = nl - 1; r >= 0; --r) {  // y = D'^-1 C[:, j] (upper bidiagonal back substitution)
+      double cf = 0.0;
+      if (mb == 0 || mb == r + 1) cf = 1.0;
+      else if (mb >= 1 && mb <= r) cf = 2.0;
+      for (int d = 0; d < 3; ++d) {
+        double cv = (cf == 0.0) ? 0.0 : (cf == 1.0 ? fac * col[d] : fac * col[d] + fac * col[d]);
+        double nxt = (r + 1 < nl) ? ee[r] * y[3 * (r + 1) + d] : 0.0;
+        y[3 * r + d] = (cv - nxt) / dd[r];
+      }
+    }
+    for (int kb = 0; kb < nw; ++kb) {  // g = F' y, S[:, j] -= g
+      double g[3] = {0.0, 0.0, 0.0};
+      if (kb < nl)
+        for (int i2 = 0; i2 < 3; ++i2)
+          g[i2] += Fd[9 * kb + 3 * i2] * y[3 * kb] + Fd[9 * kb + 3 * i2 + 1] * y[3 * kb + 1] +
+                   Fd[9 * kb + 3 * i2 + 2] * y[3 * kb + 2];
+      if (kb >= 1)
+        for (int i2 = 0; i2 < 3; ++i2)
+          g[i2] += Fl[9 * (kb - 1) + 3 * i2] * y[3 * (kb - 1)] + Fl[9 * (kb - 1) + 3 * i2 + 1] * y[3 * (kb - 1) + 1] +
+                   Fl[9 * (kb - 1) + 3 * i2 + 2] * y[3 * (kb - 1) + 2];
+      for (int i2 = 0; i2 < 3; ++i2) S[(3 * kb + i2) * m + j] -= g[i2];
+    }
+  }
+  __syncthreads();
+  // Gauss-Jordan inversion in place with partial pivoting (first maximum wins)
+  for (int kc = 0; kc < m; ++kc) {
     if (warp == 0) {
       double best = -1.0;
       int bi = kc;
-      for (int r = kc + lane; r < n; r += 32) {
-        double v = fabs(col[r]);
-        if (v > best) {
-          best = v;
-          bi = r;
-        }
+      for (int r = kc + lane; r < m; r += 32) {
+        double v = fabs(S[r * m + kc]);
+        if (v > best) { best = v; bi = r; }
       }
       for (int o = 16; o > 0; o >>= 1) {
         double ob = __shfl_xor_sync(0xffffffffu, best, o);
         int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) {
-          best = ob;
-          bi = oi;
-        }
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
       }
       if (lane == 0) {
         s_piv = bi;
-        piv[kc] = bi;
+        perm[kc] = bi;
         if (!(best > 0.0)) atomicOr(&flags[FLAG_PIVOT], 1);
       }
     }
     __syncthreads();
     const int p = s_piv;
     if (p != kc)
-      for (int c = tid; c < n; c += nthr) {
-        double t = J[(size_t)c * n + kc];
-        J[(size_t)c * n + kc] = J[(size_t)c * n + p];
-        J[(size_t)c * n + p] = t;
+      for (int c = tid; c < m; c += nthr) {
+        double t = S[kc * m + c];
+        S[kc * m + c] = S[p * m + c];
+        S[p * m + c] = t;
       }
     __syncthreads();
-    if (tid == 0) s_inv = 1.0 / col[kc];
-    __syncthreads();
-    const double inv = s_inv;
-    for (int r = kc + 1 + tid; r < n; r += nthr) col[r] *= inv;
-    __syncthreads();
-    const int m = n - kc - 1;
-    for (int e = tid; e < m * m; e += nthr) {
-      const int r = kc + 1 + e % m, c = kc + 1 + e / m;
-      J[(size_t)c * n + r] -= col[r] * J[(size_t)c * n + kc];
+    if (tid == 0) {
+      s_inv = 1.0 / S[kc * m + kc];
+      S[kc * m + kc] = 1.0;
     }
     __syncthreads();
+    for (int c = tid; c < m; c += nthr) S[kc * m + c] *= s_inv;
+    for (int r = tid; r < m; r += nthr) fcol[r] = S[r * m + kc];
+    __syncthreads();
+    for (int e = tid; e < m * m; e += nthr) {
+      const int r = e / m, c = e - r * m;
+      if (r == kc) continue;
+      const double base = (c == kc) ? 0.0 : S[e];
+      S[e] = base - fcol[r] * S[kc * m + c];
+    }
+    __syncthreads();
+  }
+  for (int kc = m - 1; kc >= 0; --kc) {  // undo the row interchanges on the columns
+    const int p = perm[kc];
+    if (p != kc)
+      for (int r = tid; r < m; r += nthr) {
+        double t = S[r * m + kc];
+        S[r * m + kc] = S[r * m + p];
+        S[r * m + p] = t;
+      }
+    __syncthreads();
+  }
+  double *Sinv = Sinv_all + soff[f];
+  for (int e = tid; e < m * m; e += nthr) Sinv[e] = S[e];
+}
+
+// x = J0^-1 b for one filament (shared-memory vectors; 128 threads)
+// b: 6nw entries [first-bead position rows | constraint rows | Lie rows]
+// x: 6nw entries [X0 | U | lambda/dt]
+__device__ void schur_apply_one(int nw, const double *__restrict__ Sinv, const double *__restrict__ aux,
+                                const double *bb, double *x, double *y, double *w, double dt, double fac) {
+  const int m = 3 * nw, nl = nw - 1;
+  const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarp = nthr >> 5;
+  const double *dd = aux, *ee = aux + nl, *Fd = aux + 2 * nl, *Fl = Fd + 9 * nl, *tt = Fl + 9 * nl;
+  const double pcoef = tt[3 * nw];
+  const double *b1 = bb + 3, *b2 = bb + m;
+  // y = D'^-1 b1
+  if (tid < 3) {
+    const int d = tid;
+    for (int r = nl - 1; r >= 0; --r) {
+      double nxt = (r + 1 < nl) ? ee[r] * y[3 * (r + 1) + d] : 0.0;
+      y[3 * r + d] = (b1[3 * r + d] - nxt) / dd[r];
+    }
+  }
+  __syncthreads();
+  // w = b2 - F' y
+  for (int row = tid; row < m; row += nthr) {
+    const int kb = row / 3, i2 = row % 3;
+    double g = 0.0;
+    if (kb < nl) g += Fd[9 * kb + 3 * i2] * y[3 * kb] + Fd[9 * kb + 3 * i2 + 1] * y[3 * kb + 1] + Fd[9 * kb + 3 * i2 + 2] * y[3 * kb + 2];
+    if (kb >= 1)
+      g += Fl[9 * (kb - 1) + 3 * i2] * y[3 * (kb - 1)] + Fl[9 * (kb - 1) + 3 * i2 + 1] * y[3 * (kb - 1) + 1] +
+           Fl[9 * (kb - 1) + 3 * i2 + 2] * y[3 * (kb - 1) + 2];
+    w[row] = b2[row] - g;
+  }
+  __syncthreads();
+  // u = S^-1 w: one warp per row, coalesced row reads
+  double *u = x + 3;
+  for (int row = warp; row < m; row += nwarp) {
+    const double *srow = Sinv + (size_t)row * m;
+    double acc = 0.0;
+    for (int c = lane; c < m; c += 32) acc += srow[c] * w[c];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) u[row] = acc;
+  }
+  __syncthreads();
+  // z = b1 - C u, (C u)_r = fac c_0 + 2 fac sum_{1<=q<=r} c_q + fac c_{r+1}, c_q = cross(u_q, t_q)
+  // (y is reused for z, then for lambda)
+  if (tid < 3) {
+    const int d = tid;
+    const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
+    double c0 = u[d1] * tt[d2] - u[d2] * tt[d1];
+    double run = 0.0;
+    for (int r = 0; r < nl; ++r) {
+      const int q = r + 1;
+      double cq = u[3 * q + d1] * tt[3 * q + d2] - u[3 * q + d2] * tt[3 * q + d1];
+      double cu = fac * c0 + 2.0 * fac * run + fac * cq;
+      y[3 * r + d] = b1[3 * r + d] - cu;
+      run += cq;
+    }
+  }
+  __syncthreads();
+  // lambda = D'^-1 z (in place), then X0 = b0 - P lambda
+  if (tid < 3) {
+    const int d = tid;
+    for (int r = nl - 1; r >= 0; --r) {
+      double nxt = (r + 1 < nl) ? ee[r] * y[3 * (r + 1) + d] : 0.0;
+      y[3 * r + d] = (y[3 * r + d] - nxt) / dd[r];
+    }
+    x[d] = bb[d] - pcoef * y[d];
+  }
+  __syncthreads();
+  for (int i = tid; i < 3 * nl; i += nthr) x[3 + m + i] = y[i] / dt;
+  __syncthreads();
+}
+
+// x_f = J0_f^-1 b_f, then x += sum_i C_i dots_i (FilamentJacobianSolver.hpp:49-73)
+__global__ void __launch_bounds__(128) k_schur_apply(const int *__restrict__ fil_start,
+                                                     const long long *__restrict__ soff,
+                                                     const long long *__restrict__ aoff,
+                                                     const double *__restrict__ Sinv_all,
+                                                     const double *__restrict__ aux_all, const double *__restrict__ b,
+                                                     double *__restrict__ x, const double *__restrict__ C,
+                                                     const double *__restrict__ dots, int iter, size_t n6, double dt,
+                                                     double fac) {
+  __shared__ double bb[6 * FS_MAX_NW], xs[6 * FS_MAX_NW], y[3 * FS_MAX_NW], w[3 * FS_MAX_NW];
+  const int f = blockIdx.x;
+  const int b0 = fil_start[f], nw = fil_start[f + 1] - b0, s0 = 6 * b0, n = 6 * nw;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  for (int r = tid; r < n; r += nthr) bb[r] = b[s0 + r];
+  __syncthreads();
+  if (nw < 2) {
+    for (int r = tid; r < n; r += nthr) xs[r] = bb[r];
+    __syncthreads();
+  } else {
+    schur_apply_one(nw, Sinv_all + soff[f], aux_all + aoff[f], bb, xs, y, w, dt, fac);
+  }
+  for (int r = tid; r < n; r += nthr) {
+    double v = xs[r];
+    for (int i = 0; i < iter; ++i) v += C[(size_t)i * n6 + s0 + r] * dots[i];
+    x[s0 + r] = v;
   }
 }
 
-// explicit inverse column e of filament f (test access), with the 1/dt row scaling
-__global__ void k_lu_inverse(const double *__restrict__ J, const int *__restrict__ piv, int n, int nw, double dt,
-                             double *__restrict__ out) {
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n) return;
-  double y[6 * 64];
-  for (int i = 0; i < n; ++i) y[i] = (i == e) ? 1.0 : 0.0;
-  for (int kc = 0; kc < n; ++kc)
-    if (piv[kc] != kc) {
-      double t = y[kc];
-      y[kc] = y[piv[kc]];
-      y[piv[kc]] = t;
-    }
-  for (int kc = 0; kc < n; ++kc)
-    for (int r = kc + 1; r < n; ++r) y[r] -= J[(size_t)kc * n + r] * y[kc];
-  for (int kc = n - 1; kc >= 0; --kc) {
-    y[kc] /= J[(size_t)kc * n + kc];
-    for (int r = 0; r < kc; ++r) y[r] -= J[(size_t)kc * n + r] * y[kc];
+// explicit inverse of filament f's J0 (with the 1/dt rows), one column per CTA (test access)
+__global__ void __launch_bounds__(128) k_schur_inverse(int nw, const double *__restrict__ Sinv,
+                                                       const double *__restrict__ aux, double dt, double fac,
+                                                       double *__restrict__ out) {
+  __shared__ double bb[6 * FS_MAX_NW], xs[6 * FS_MAX_NW], y[3 * FS_MAX_NW], w[3 * FS_MAX_NW];
+  const int n = 6 * nw, e = blockIdx.x, tid = threadIdx.x;
+  for (int r = tid; r < n; r += blockDim.x) bb[r] = (r == e) ? 1.0 : 0.0;
+  __syncthreads();
+  if (nw < 2) {
+    for (int r = tid; r < n; r += blockDim.x) xs[r] = bb[r];
+    __syncthreads();
+  } else {
+    schur_apply_one(nw, Sinv, aux, bb, xs, y, w, dt, fac);
   }
-  for (int r = 0; r < n; ++r) {
-    double v = y[r];
-    if (nw > 1 && r >= 3 * nw + 3) v /= dt;
-    out[(size_t)r * n + e] = v;  // row-major
-  }
+  for (int r = tid; r < n; r += blockDim.x) out[(size_t)r * n + e] = xs[r];
 }
 
 // ---- error check ---------------------------------------------------------------
@@ -664,52 +794,6 @@ __global__ void k_reduce_rows(const double *__restrict__ partial, int nparts, in
   for (int p = lane; p < nparts; p += 32) acc += partial[(size_t)row * nparts + p];
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
   if (lane == 0) out[row] = do_sqrt ? sqrt(acc) : acc;
-}
-
-// x_f = J0_f^-1 b_f (pivots, unit-L, U, 1/dt rows), then x += sum_i C_i dots_i
-__global__ void __launch_bounds__(256) k_lu_apply(const int *__restrict__ fil_start, const long long *__restrict__ joff,
-                                                  const double *__restrict__ Jall, const int *__restrict__ piv_all,
-                                                  const double *__restrict__ b, double *__restrict__ x,
-                                                  const double *__restrict__ C, const double *__restrict__ dots,
-                                                  int iter, size_t n6, double dt) {
-  extern __shared__ double y[];
-  const int f = blockIdx.x;
-  const int b0 = fil_start[f], nw = fil_start[f + 1] - b0, n = 6 * nw, s0 = 6 * b0;
-  const double *J = Jall + joff[f];
-  const int *piv = piv_all + s0;
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  for (int r = tid; r < n; r += nthr) y[r] = b[s0 + r];
-  __syncthreads();
-  if (tid == 0)
-    for (int kc = 0; kc < n; ++kc) {
-      int p = piv[kc];
-      if (p != kc) {
-        double t = y[kc];
-        y[kc] = y[p];
-        y[p] = t;
-      }
-    }
-  __syncthreads();
-  for (int kc = 0; kc < n; ++kc) {
-    const double yk = y[kc];
-    const double *col = J + (size_t)kc * n;
-    for (int r = kc + 1 + tid; r < n; r += nthr) y[r] -= col[r] * yk;
-    __syncthreads();
-  }
-  for (int kc = n - 1; kc >= 0; --kc) {
-    const double *col = J + (size_t)kc * n;
-    const double yk = y[kc] / col[kc];
-    __syncthreads();
-    if (tid == 0) y[kc] = yk;
-    for (int r = tid; r < kc; r += nthr) y[r] -= col[r] * yk;
-    __syncthreads();
-  }
-  for (int r = tid; r < n; r += nthr) {
-    double v = y[r];
-    if (nw > 1 && r >= 3 * nw + 3) v /= dt;
-    for (int i = 0; i < iter; ++i) v += C[(size_t)i * n6 + s0 + r] * dots[i];
-    x[s0 + r] = v;
-  }
 }
 
 // dE = newerr - err and per-block sums of dE^2
@@ -852,21 +936,32 @@ fs_status fil_jacobian_build(fs_ctx *c, int nt) {
   if (!c->have_state) return FS_ERR_STATE;
   ProfScope ps(c, FS_STAGE_JACOBIAN);
   FilConsts k = make_fconsts(c);
-  k_jacobian<<<c->nfil, 256, 0, c->stream>>>(c->nfil, c->fil_start, c->qs, c->Us, c->TAU, c->lam, c->kap, c->cc,
-                                             c->joff, c->J, c->jpiv, nt, k, c->p.a, c->p.ah, c->flags);
+  const size_t smem = sizeof(double) * 9 * (size_t)c->max_nw * c->max_nw;
+  k_jacobian_schur<<<c->nfil, 256, smem, c->stream>>>(c->fil_start, c->qs, c->Us, c->TAU, c->lam, c->kap, c->cc,
+                                                      c->soff, c->aoff, c->Sinv, c->aux, nt, k, c->p.a, c->p.ah,
+                                                      c->flags);
   FS_LAUNCH_CHECK();
   return FS_OK;
 }
 
+fs_status fil_jacobian_prepare(fs_ctx *c) {
+  if (c->max_nw > FS_MAX_NW) return FS_ERR_INVALID_ARG;
+  const size_t smem = sizeof(double) * 9 * (size_t)c->max_nw * c->max_nw;
+  FS_CUDA(cudaFuncSetAttribute(k_jacobian_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  return FS_OK;
+}
+
+int fil_aux_size(int nw) { return nw < 2 ? 1 : 20 * (nw - 1) + 3 * nw + 1; }
+
 fs_status fil_jacobian_inverse(fs_ctx *c, int f, double *out_d) {
   int fs_h[2];
-  long long off;
+  long long so, ao;
   FS_CUDA(cudaMemcpyAsync(fs_h, c->fil_start + f, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  FS_CUDA(cudaMemcpyAsync(&off, c->joff + f, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+  FS_CUDA(cudaMemcpyAsync(&so, c->soff + f, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+  FS_CUDA(cudaMemcpyAsync(&ao, c->aoff + f, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
   FS_CUDA(cudaStreamSynchronize(c->stream));
   const int nw = fs_h[1] - fs_h[0], n = 6 * nw;
-  if (nw > 64) return FS_ERR_INVALID_ARG;
-  k_lu_inverse<<<fs_blocks(n, 64), 64, 0, c->stream>>>(c->J + off, c->jpiv + 6 * fs_h[0], n, nw, c->p.dt, out_d);
+  k_schur_inverse<<<n, 128, 0, c->stream>>>(nw, c->Sinv + so, c->aux + ao, c->p.dt, 0.5 * c->p.dl, out_d);
   FS_LAUNCH_CHECK();
   return FS_OK;
 }
@@ -895,9 +990,8 @@ fs_status fil_broyden_apply(fs_ctx *c, const double *b, double *x, int iter) {
     k_reduce_rows<<<fs_blocks(iter, 8), 256, 0, c->stream>>>(c->partials, RED_BLOCKS, iter, c->dots, 0);
     FS_LAUNCH_CHECK();
   }
-  const size_t smem = sizeof(double) * 6 * (size_t)c->max_nw;
-  k_lu_apply<<<c->nfil, 256, smem, c->stream>>>(c->fil_start, c->joff, c->J, c->jpiv, b, x, c->Cmat, c->dots, iter,
-                                                n6, c->p.dt);
+  k_schur_apply<<<c->nfil, 128, 0, c->stream>>>(c->fil_start, c->soff, c->aoff, c->Sinv, c->aux, b, x, c->Cmat,
+                                                 c->dots, iter, n6, c->p.dt, 0.5 * c->p.dl);
   FS_LAUNCH_CHECK();
   return FS_OK;
 }

@@ -59,6 +59,7 @@ struct fs_ctx {
   bool plan_ok[2];
   int nbin[3], nbins;  // spread bins (FS_TILE wide in stencil-start space)
   fs_sort bins;
+  int *bead_sw;        // per bead, wrapped Gaussian stencil start per axis
   int last_grid_prec;  // precision of the grids from the last solve (-1: none)
 
   // collision cells
@@ -79,9 +80,9 @@ struct fs_ctx {
   double *Y, *V, *W;
   double *err, *newerr, *upd, *tmp, *dE;
   double *Cmat, *Dmat;   // broyden_maxiter x 6Np
-  double *J;             // per-filament LU factors (column-major), offsets joff
-  long long *joff;
-  int *jpiv;             // per-filament pivots, offset 6*fil_start[f]
+  double *Sinv;          // per-filament inverse Schur complement (3Nw x 3Nw row-major) at soff[f]
+  double *aux;           // per-filament D', F' blocks, tangents, P coefficient at aoff[f]
+  long long *soff, *aoff;
   int max_nw;
   double *dots;          // broyden_maxiter partial dots
   double *partials;      // reduction scratch
@@ -157,6 +158,8 @@ fs_status cells_barrier(fs_ctx *c, const double *Y, double *F, int np, int nt, c
 fs_status fil_initial_guess(fs_ctx *c);
 fs_status fil_forces(fs_ctx *c, int nt);
 fs_status fil_jacobian_build(fs_ctx *c, int nt);
+fs_status fil_jacobian_prepare(fs_ctx *c);  // after an upload: kernel attributes for the filament lengths
+int fil_aux_size(int nw);
 fs_status fil_jacobian_inverse(fs_ctx *c, int f, double *out_d);
 fs_status fil_error_check(fs_ctx *c, const double *V, const double *W, double *err, int nt);
 fs_status fil_broyden_apply(fs_ctx *c, const double *b, double *x, int iter);
