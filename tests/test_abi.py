@@ -88,3 +88,34 @@ def test_sources_have_no_cpu_fallback():
             if f.endswith((".py", ".cu", ".cuh")):
                 text = open(os.path.join(dirpath, f)).read()
                 assert "oracle" not in text.replace("the oracle", ""), f
+
+
+def test_cpp_mirror_header_compiles_and_links(libpath, tmp_path):
+    """include/filsim_gpu.hpp builds against the library; without a GPU the
+    context constructor reports FS_ERR_NO_DEVICE through filsim::Error."""
+    src = tmp_path / "drv.cpp"
+    src.write_text(textwrap.dedent("""
+        #include <cstdio>
+        #include "filsim_gpu.hpp"
+        int main() {
+          fs_params p;
+          fs_params_default(&p, 32, 32, 32);
+          try {
+            filsim::Context ctx(p, 8, 2);
+            filsim::FcmGpu fcm(ctx, 8);
+            filsim::LinkedListGpu ll(ctx);
+            std::printf("context %d %d %d\\n", ll.cells()[0], ll.cells()[1], ll.cells()[2]);
+          } catch (const filsim::Error &e) {
+            std::printf("error %d\\n", e.status);
+          }
+          return 0;
+        }
+    """))
+    exe = tmp_path / "drv"
+    libdir = os.path.dirname(libpath)
+    subprocess.run(["g++", "-std=c++14", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L" + libdir, "-lfilsim_gpu", "-Wl,-rpath," + libdir], check=True)
+    import torch
+    if not torch.cuda.is_available():
+        out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+        assert out.strip() == "error 2"
