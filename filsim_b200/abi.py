@@ -164,6 +164,8 @@ def _declare(L):
         "fs_suspension_random": (c_int, [ctypes.POINTER(FsParams), c_int, c_int, ctypes.c_ulonglong, c_double,
                                          c_int, c_void_p, c_void_p]),
         "fs_kernel_launches": (ctypes.c_ulonglong, []),
+        "fs_collision_barrier_noalloc": (c_int, [ctypes.POINTER(FsParams), c_void_p, c_void_p, c_void_p, c_int, c_int,
+                                                 c_void_p, c_void_p, c_void_p, c_void_p]),
         "fs_profile_enable": (c_int, [c_void_p, c_int]),
         "fs_profile_get": (c_int, [c_void_p, ctypes.POINTER(FsProfile)]),
     }

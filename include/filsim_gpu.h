@@ -199,6 +199,28 @@ fs_status fs_collision_pairs(fs_ctx *ctx, const double *Y, int np, int nt,
                              const int *fil_id, const int *seg_id,
                              int *pairs_h, int max_pairs, int *npairs_h);
 
+/* ---- collision barrier without device allocation --------------------------- */
+
+/* No counterpart in the reference. For callers that cannot allocate device
+ * memory -- a host program that hands this library a fixed budget through its
+ * own memory pool, or a step loop that must not pay cudaMalloc's device-wide
+ * synchronisation -- this one call bins beads into cells from unwrapped
+ * positions Xs and adds the barrier forces for positions Y into F_inout, as
+ * fs_cells_link followed by fs_collision_barrier do, without a context. It
+ * allocates nothing: its working memory is one static 4 MiB device array that
+ * every GPU loading this library holds until the process exits, which limits
+ * a call to FS_NOALLOC_MAX_BEADS beads and FS_NOALLOC_MAX_CELLS cells (larger
+ * calls return FS_ERR_INVALID_ARG). The first call on a device looks up the
+ * array's device address on that device, so make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU (different streams or
+ * host threads) race. stream: a cudaStream_t or NULL; the call synchronises it.
+ * All array arguments are device pointers; min_dist2_h (may be NULL) is host. */
+#define FS_NOALLOC_MAX_BEADS 65536
+#define FS_NOALLOC_MAX_CELLS 262144
+fs_status fs_collision_barrier_noalloc(const fs_params *p, const double *Xs, const double *Y, double *F_inout,
+                                       int np, int nt, const int *fil_id, const int *seg_id, void *stream,
+                                       double *min_dist2_h);
+
 /* ---- filament suspension and the implicit step ----------------------------- */
 
 /* Uploads / downloads the suspension (fs_host_state layouts). */
