@@ -250,7 +250,7 @@ def run_ours(args, rank, world):
         host.arrays = {k: t.numpy() for k, t in pinned.items()}
         sim = Simulation(ctx, host)
         sim.run_steps(1, W)
-        host.set_arrays(sim.download())
+        sim.download_into(host)
         barrier()
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
@@ -258,7 +258,7 @@ def run_ours(args, rank, world):
         for k in range(K):
             sim.upload(host)                      # H2D of the step's input state
             sim.step_implicit(W + 1 + k)
-            host.set_arrays(sim.download())       # D2H of the step's result
+            sim.download_into(host)               # D2H of the step's result
         ev1.record(stream)
         torch.cuda.synchronize()
         ms_e2e = max_over_ranks(ev0.elapsed_time(ev1))

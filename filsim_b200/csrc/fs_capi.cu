@@ -268,6 +268,7 @@ fs_status fs_destroy(fs_ctx *c) {
   cells_free(c);
   free_state(c);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  free(c->fil_start_h);
   free(c);
   return FS_OK;
 }
@@ -407,11 +408,54 @@ fs_status fs_collision_pairs(fs_ctx *c, const double *Y, int np, int nt, const i
   return st;
 }
 
+static fs_status upload_layout(fs_ctx *c, const fs_host_state *s);
+
+// state arrays always; the filament layout (ids, offsets, Schur buffers) only
+// when it differs from the previous upload's
 fs_status fs_state_upload(fs_ctx *c, const fs_host_state *s) {
   if (!c || !s || !s->fil_start || s->nfil < 0 || s->np < 0) return FS_ERR_INVALID_ARG;
   if (s->np > c->max_beads || s->nfil > c->max_fil) return FS_ERR_INVALID_ARG;
   const int nf = s->nfil, np = s->np;
   if (s->fil_start[0] != 0 || s->fil_start[nf] != np) return FS_ERR_INVALID_ARG;
+  cudaStream_t st = c->stream;
+  const bool same_layout = c->have_state && c->fil_start_h && c->nfil == nf && c->np == np &&
+                           memcmp(c->fil_start_h, s->fil_start, sizeof(int) * (nf + 1)) == 0;
+  if (!same_layout) FS_TRY(upload_layout(c, s));
+  struct F3 {
+    double *d;
+    const double *h;
+    size_t n;
+  } fields[] = {{c->X, s->X, 3}, {c->Xs, s->Xs, 3}, {c->Xt, s->Xt, 3}, {c->U, s->U, 3}, {c->Us, s->Us, 3},
+                {c->Ut, s->Ut, 3}, {c->q, s->q, 4}, {c->qs, s->qs, 4}, {c->qt, s->qt, 4}, {c->F, s->F, 3},
+                {c->TAU, s->TAU, 3}};
+  for (auto &fl : fields) {
+    if (fl.h) FS_CUDA(cudaMemcpyAsync(fl.d, fl.h, sizeof(double) * fl.n * np, cudaMemcpyHostToDevice, st));
+    else FS_CUDA(cudaMemsetAsync(fl.d, 0, sizeof(double) * fl.n * np, st));
+  }
+  const size_t nl3 = sizeof(double) * 3 * (size_t)c->nlink;
+  double *lams[] = {c->lam, c->lam1, c->lam2};
+  double *lams_h[] = {s->lam, s->lam1, s->lam2};
+  for (int i = 0; i < 3; ++i) {
+    if (lams_h[i]) FS_CUDA(cudaMemcpyAsync(lams[i], lams_h[i], nl3, cudaMemcpyHostToDevice, st));
+    else FS_CUDA(cudaMemsetAsync(lams[i], 0, nl3, st));
+  }
+  if (s->kap) FS_CUDA(cudaMemcpyAsync(c->kap, s->kap, sizeof(double) * nf, cudaMemcpyHostToDevice, st));
+  if (s->c) FS_CUDA(cudaMemcpyAsync(c->cc, s->c, sizeof(double) * nf, cudaMemcpyHostToDevice, st));
+  if (!same_layout || !s->kap || !s->c) {
+    std::vector<double> ones(nf > 0 ? nf : 1, 1.0);
+    if (!s->kap) FS_CUDA(cudaMemcpyAsync(c->kap, ones.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, st));
+    if (!s->c) FS_CUDA(cudaMemcpyAsync(c->cc, ones.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, st));
+    FS_CUDA(cudaStreamSynchronize(st));
+  } else {
+    FS_CUDA(cudaStreamSynchronize(st));
+  }
+  c->have_state = true;
+  return FS_OK;
+}
+
+// the filament layout of an upload: ids, offsets, Schur buffers (fs_state_upload)
+static fs_status upload_layout(fs_ctx *c, const fs_host_state *s) {
+  const int nf = s->nfil, np = s->np;
   std::vector<int> fid(np > 0 ? np : 1), sid(np > 0 ? np : 1);
   std::vector<long long> soff(nf + 1), aoff(nf + 1);
   int max_nw = 1;
@@ -447,29 +491,11 @@ fs_status fs_state_upload(fs_ctx *c, const fs_host_state *s) {
   FS_CUDA(cudaMemcpyAsync(c->seg_id, sid.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
   FS_CUDA(cudaMemcpyAsync(c->soff, soff.data(), sizeof(long long) * (nf + 1), cudaMemcpyHostToDevice, st));
   FS_CUDA(cudaMemcpyAsync(c->aoff, aoff.data(), sizeof(long long) * (nf + 1), cudaMemcpyHostToDevice, st));
-  struct F3 {
-    double *d;
-    const double *h;
-    size_t n;
-  } fields[] = {{c->X, s->X, 3}, {c->Xs, s->Xs, 3}, {c->Xt, s->Xt, 3}, {c->U, s->U, 3}, {c->Us, s->Us, 3},
-                {c->Ut, s->Ut, 3}, {c->q, s->q, 4}, {c->qs, s->qs, 4}, {c->qt, s->qt, 4}, {c->F, s->F, 3},
-                {c->TAU, s->TAU, 3}};
-  for (auto &fl : fields) {
-    if (fl.h) FS_CUDA(cudaMemcpyAsync(fl.d, fl.h, sizeof(double) * fl.n * np, cudaMemcpyHostToDevice, st));
-    else FS_CUDA(cudaMemsetAsync(fl.d, 0, sizeof(double) * fl.n * np, st));
-  }
-  const size_t nl3 = sizeof(double) * 3 * (size_t)c->nlink;
-  double *lams[] = {c->lam, c->lam1, c->lam2};
-  double *lams_h[] = {s->lam, s->lam1, s->lam2};
-  for (int i = 0; i < 3; ++i) {
-    if (lams_h[i]) FS_CUDA(cudaMemcpyAsync(lams[i], lams_h[i], nl3, cudaMemcpyHostToDevice, st));
-    else FS_CUDA(cudaMemsetAsync(lams[i], 0, nl3, st));
-  }
-  std::vector<double> ones(nf > 0 ? nf : 1, 1.0);
-  FS_CUDA(cudaMemcpyAsync(c->kap, s->kap ? s->kap : ones.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, st));
-  FS_CUDA(cudaMemcpyAsync(c->cc, s->c ? s->c : ones.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, st));
-  FS_CUDA(cudaStreamSynchronize(st));
-  c->have_state = true;
+  FS_CUDA(cudaStreamSynchronize(st));  // the host vectors above go out of scope
+  free(c->fil_start_h);
+  c->fil_start_h = (int *)malloc(sizeof(int) * (nf + 1));
+  if (!c->fil_start_h) return FS_ERR_OOM;
+  memcpy(c->fil_start_h, s->fil_start, sizeof(int) * (nf + 1));
   return FS_OK;
 }
 

@@ -1,14 +1,13 @@
 // fs_fcm.cu -- Force Coupling Method mobility solve on sm_100a.
 //
 // Replaces Fcm::mobility_solve (FCMfunctions.cpp:175-464):
-//   1. k_fcm_bin_keys + counting sort: beads binned by the 16-point tile that
+//   1. k_fcm_bin_keys + counting sort: beads binned by the 8-point tile that
 //      holds the start of their Gaussian stencil (gaussian_setup's index rule,
 //      FCMfunctions.cpp:565-589).
-//   2. k_spread: one CTA per 16^3 grid tile gathers the monopole + rotlet
+//   2. k_spread: one CTA per 8^3 grid tile gathers the monopole + rotlet
 //      Gaussians of every bead whose stencil reaches the tile
-//      (mono_and_dipole_force_distribution, :596-646). Each warp owns one
-//      x-plane of the tile in shared memory, so every grid point is written by
-//      one warp in bead order: no atomics, bit-reproducible.
+//      (mono_and_dipole_force_distribution, :596-646) into per-warp private
+//      copies of the tile, summed in fixed order: no atomics, bit-reproducible.
 //   3. cuFFT R2C (batched x3), 4. k_project / k_project_planes: the Stokes
 //      projection of flow_solve (:648-736), 5. cuFFT C2R (batched x3).
 //   6. k_interp: one warp per bead (in spread-bin order for L2 locality)
@@ -58,47 +57,61 @@ __global__ void k_fcm_bin_keys(const double *__restrict__ Y, int np, FcmConsts c
 }
 
 // ---- 2. spread ----------------------------------------------------------------
+// One CTA (4 warps) per 8^3 grid tile. Candidate beads are those whose stencil
+// start lies in the 3 bins before and at the tile per axis; they are staged in
+// chunks (per axis: the stencil indices landing in the tile, compacted, with
+// their Gaussian weights). Warp w takes chunk beads w, w+4, ... in sorted order
+// and adds each bead's clipped footprint (lanes over its (y, z) patch, a loop
+// over x) into its own private copy of the tile in shared memory. The four
+// copies are then summed in fixed order and written once: dense lane use, no
+// atomics, bit-reproducible.
+#define FS_SPREAD_WARPS 4
+
 template <typename R>
 struct SpreadChunk {
-  R gx[FS_SPREAD_CHUNK][16], dgx[FS_SPREAD_CHUNK][16], rx[FS_SPREAD_CHUNK][16];  // x by stencil index i
-  R gy[FS_SPREAD_CHUNK][16], dgy[FS_SPREAD_CHUNK][16], ry[FS_SPREAD_CHUNK][16];  // y compacted to the tile
-  R gz[FS_SPREAD_CHUNK][16], dgz[FS_SPREAD_CHUNK][16], rz[FS_SPREAD_CHUNK][16];  // z compacted to the tile
+  R g[3][FS_SPREAD_CHUNK][FS_TILE], d[3][FS_SPREAD_CHUNK][FS_TILE], r[3][FS_SPREAD_CHUNK][FS_TILE];
   R f[FS_SPREAD_CHUNK][3];   // force
-  R th[FS_SPREAD_CHUNK][3];  // half torque (0.5 T)
-  unsigned char ly[FS_SPREAD_CHUNK][16], lz[FS_SPREAD_CHUNK][16];
-  int ax[FS_SPREAD_CHUNK];   // (X0 - stencil start) mod N
-  int cy[FS_SPREAD_CHUNK], cz[FS_SPREAD_CHUNK], mcz[FS_SPREAD_CHUNK];
-  int bead[FS_SPREAD_CHUNK];
+  R th[FS_SPREAD_CHUNK][3];  // half torque (GA_setup, :536-547)
+  unsigned char l[3][FS_SPREAD_CHUNK][FS_TILE];  // tile-local coordinate of each compacted entry
+  int cnt[3][FS_SPREAD_CHUNK];
+  int mcz[FS_SPREAD_CHUNK];  // multiply-shift divisor for the (y, z) patch
 };
 
 template <typename R>
 struct SpreadAcc;
 template <>
-struct SpreadAcc<double> {
-  double v[3][FS_TILE][FS_TILE][FS_TILE];
-  __device__ void add(int c, int x, int y, int z, double val) { v[c][x][y][z] += val; }
-  __device__ double result(int c, int x, int y, int z) const { return v[c][x][y][z]; }
+struct SpreadAcc<double> {  // FP64 mode: plain double sums
+  double v[FS_SPREAD_WARPS][3][FS_TILE * FS_TILE * FS_TILE];
+  __device__ void add(int w, int c, int e, double val) { v[w][c][e] += val; }
+  __device__ double total(int c, int e) const {
+    double s = v[0][c][e];
+    for (int w = 1; w < FS_SPREAD_WARPS; ++w) s += v[w][c][e];
+    return s;
+  }
   __device__ void zero(int t, int nt) {
-    double *p = &v[0][0][0][0];
-    for (int i = t; i < 3 * FS_TILE * FS_TILE * FS_TILE; i += nt) p[i] = 0.0;
+    double *p = &v[0][0][0];
+    for (int i = t; i < FS_SPREAD_WARPS * 3 * FS_TILE * FS_TILE * FS_TILE; i += nt) p[i] = 0.0;
   }
 };
 template <>
-struct SpreadAcc<float> {
-  float v[3][FS_TILE][FS_TILE][FS_TILE];
-  float cmp[3][FS_TILE][FS_TILE][FS_TILE];  // Kahan compensation
-  __device__ void add(int c, int x, int y, int z, float val) {
-    float s = v[c][x][y][z];
-    float yv = val - cmp[c][x][y][z];
+struct SpreadAcc<float> {  // FP32 mode: Kahan-compensated float sums
+  float v[FS_SPREAD_WARPS][3][FS_TILE * FS_TILE * FS_TILE];
+  float cmp[FS_SPREAD_WARPS][3][FS_TILE * FS_TILE * FS_TILE];
+  __device__ void add(int w, int c, int e, float val) {
+    float s = v[w][c][e];
+    float yv = val - cmp[w][c][e];
     float t = s + yv;
-    cmp[c][x][y][z] = (t - s) - yv;
-    v[c][x][y][z] = t;
+    cmp[w][c][e] = (t - s) - yv;
+    v[w][c][e] = t;
   }
-  __device__ float result(int c, int x, int y, int z) const { return v[c][x][y][z] - cmp[c][x][y][z]; }
+  __device__ float total(int c, int e) const {
+    double s = 0.0;
+    for (int w = 0; w < FS_SPREAD_WARPS; ++w) s += (double)v[w][c][e] - (double)cmp[w][c][e];
+    return (float)s;
+  }
   __device__ void zero(int t, int nt) {
-    float *p = &v[0][0][0][0];
-    float *q = &cmp[0][0][0][0];
-    for (int i = t; i < 3 * FS_TILE * FS_TILE * FS_TILE; i += nt) {
+    float *p = &v[0][0][0], *q = &cmp[0][0][0];
+    for (int i = t; i < FS_SPREAD_WARPS * 3 * FS_TILE * FS_TILE * FS_TILE; i += nt) {
       p[i] = 0.f;
       q[i] = 0.f;
     }
@@ -119,7 +132,7 @@ template <>
 __device__ inline float fs_exp<float>(float x) { return expf(x); }
 
 template <typename R>
-__global__ void __launch_bounds__(FS_TILE * 32, 2)
+__global__ void __launch_bounds__(FS_SPREAD_WARPS * 32)
     k_spread(const double *__restrict__ Y, const double *__restrict__ F, const double *__restrict__ T,
              const int *__restrict__ bin_start, const int *__restrict__ sorted, const int *__restrict__ bead_sw,
              FcmConsts c, R *__restrict__ fgrid) {
@@ -130,31 +143,32 @@ __global__ void __launch_bounds__(FS_TILE * 32, 2)
   const int tile = blockIdx.x;
   const int tz = tile % c.nbin[2], ty = (tile / c.nbin[2]) % c.nbin[1], tx = tile / (c.nbin[2] * c.nbin[1]);
   const int X0[3] = {tx * FS_TILE, ty * FS_TILE, tz * FS_TILE};
-
   sm.acc.zero(tid, nthr);
 
-  // candidate bins per axis: the tile's own bin and the one before it
-  int cb[3][2], ncb[3];
+  // candidate bins per axis: stencil starts in [X0 - ngd + 1, X0 + FS_TILE), wrapped
+  int cb[3][4], ncb[3];
   const int tb[3] = {tx, ty, tz};
+  const int back = (c.ngd - 1 + FS_TILE - 1) / FS_TILE;
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    cb[d][0] = (tb[d] - 1 + c.nbin[d]) % c.nbin[d];
-    cb[d][1] = tb[d];
-    ncb[d] = (c.nbin[d] > 1 && c.ngd > 1) ? 2 : 1;
-    if (ncb[d] == 1) cb[d][0] = tb[d];
+  for (int dd = 0; dd < 3; ++dd) {
+    ncb[dd] = 0;
+    for (int k = back; k >= 0; --k) {
+      int b = wrap_int(tb[dd] - k, c.nbin[dd]);
+      bool dup = false;
+      for (int q = 0; q < ncb[dd]; ++q) dup |= (cb[dd][q] == b);
+      if (!dup && ncb[dd] < 4) cb[dd][ncb[dd]++] = b;
+    }
   }
-  // gather candidate bead ranges (up to 8 bins)
-  int rs[8], re[8], nr = 0;
+  int rs[64], re[64], nr = 0, total = 0;
   for (int a = 0; a < ncb[0]; ++a)
     for (int b2 = 0; b2 < ncb[1]; ++b2)
       for (int e = 0; e < ncb[2]; ++e) {
         int bin = (cb[0][a] * c.nbin[1] + cb[1][b2]) * c.nbin[2] + cb[2][e];
         rs[nr] = bin_start[bin];
         re[nr] = bin_start[bin + 1];
+        total += re[nr] - rs[nr];
         nr++;
       }
-  int total = 0;
-  for (int r = 0; r < nr; ++r) total += re[r] - rs[r];
   __syncthreads();
 
   const int ngd = c.ngd;
@@ -175,104 +189,80 @@ __global__ void __launch_bounds__(FS_TILE * 32, 2)
       const int xc = (int)(Yv / c.dx);
       const int xg = xc - c.ngdh + (i + 1);
       const double xx = ((double)xg) * c.dx - Yv;
-      R g, gd, rr;
-      if (sizeof(R) == 8) {
-        g = (R)(c.anorm * exp(-xx * xx / c.anorm2));
-        gd = (R)(c.anormdip * exp(-xx * xx / c.anormdip2));
-        rr = (R)(-xx / c.sigmadipsq);
-      } else {
-        const R xf = (R)xx;
-        g = (R)c.anorm * fs_exp<R>(-xf * xf / (R)c.anorm2);
-        gd = (R)c.anormdip * fs_exp<R>(-xf * xf / (R)c.anormdip2);
-        rr = -xf / (R)c.sigmadipsq;
-      }
       const int Nn = c.N[a];
-      const int sw = bead_sw[3 * bead + a];  // wrapped stencil start, in [0, N)
-      // stencil index i lands on tile-local l = (i - aoff) mod N; valid if l < FS_TILE
+      const int sw = bead_sw[3 * bead + a];
+      // stencil index i lands on tile-local l = (i - aoff) mod N; valid if l < FS_TILE.
+      // The valid indices form [0, e2) (wrapped around the box) and [aoff, e1).
       const int aoff = wrap_near(X0[a] - sw, Nn);
-      if (a == 0) {
-        sm.ch.gx[s][i] = g;
-        sm.ch.dgx[s][i] = gd;
-        sm.ch.rx[s][i] = rr;
-        if (i == 0) {
-          sm.ch.ax[s] = aoff;
-          sm.ch.bead[s] = bead;
-#pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            sm.ch.f[s][d] = (R)F[3 * bead + d];
-            sm.ch.th[s][d] = (R)(0.5 * T[3 * bead + d]);
-          }
-        }
-      } else {
-        // the valid indices form [0, e2) (stencil wrapped around the box) and
-        // [aoff, e1); compact them in index order
-        const int e1 = min(ngd, aoff + FS_TILE);
-        const int e2 = max(0, min(ngd, aoff + FS_TILE - Nn));
-        const int n1 = max(0, e1 - aoff);
-        const bool in2 = i < e2, in1 = i >= aoff && i < e1;
+      const int e1 = min(ngd, aoff + FS_TILE);
+      const int e2 = max(0, min(ngd, aoff + FS_TILE - Nn));
+      const bool in2 = i < e2, in1 = i >= aoff && i < e1;
+      if (in1 || in2) {
         const int pos = in2 ? i : e2 + (i - aoff);
-        const int mine = in2 ? i - aoff + Nn : i - aoff;
-        const int cnt = n1 + e2;
-        if (a == 1) {
-          if (in1 || in2) {
-            sm.ch.gy[s][pos] = g;
-            sm.ch.dgy[s][pos] = gd;
-            sm.ch.ry[s][pos] = rr;
-            sm.ch.ly[s][pos] = (unsigned char)mine;
-          }
-          if (i == 0) sm.ch.cy[s] = cnt;
+        R g, gd, rr;
+        if (sizeof(R) == 8) {
+          g = (R)(c.anorm * exp(-xx * xx / c.anorm2));
+          gd = (R)(c.anormdip * exp(-xx * xx / c.anormdip2));
+          rr = (R)(-xx / c.sigmadipsq);
         } else {
-          if (in1 || in2) {
-            sm.ch.gz[s][pos] = g;
-            sm.ch.dgz[s][pos] = gd;
-            sm.ch.rz[s][pos] = rr;
-            sm.ch.lz[s][pos] = (unsigned char)mine;
-          }
-          if (i == 0) {
-            sm.ch.cz[s] = cnt;
-            sm.ch.mcz[s] = cnt > 0 ? (4096 + cnt - 1) / cnt : 0;
-          }
+          const R xf = (R)xx;
+          g = (R)c.anorm * fs_exp<R>(-xf * xf / (R)c.anorm2);
+          gd = (R)c.anormdip * fs_exp<R>(-xf * xf / (R)c.anormdip2);
+          rr = -xf / (R)c.sigmadipsq;
         }
+        sm.ch.g[a][s][pos] = g;
+        sm.ch.d[a][s][pos] = gd;
+        sm.ch.r[a][s][pos] = rr;
+        sm.ch.l[a][s][pos] = (unsigned char)(in2 ? i - aoff + Nn : i - aoff);
+      }
+      if (i == 0) {
+        const int cntv = max(0, e1 - aoff) + e2;
+        sm.ch.cnt[a][s] = cntv;
+        if (a == 2) sm.ch.mcz[s] = cntv > 0 ? (4096 + cntv - 1) / cntv : 0;
+        if (a == 0)
+#pragma unroll
+          for (int dd = 0; dd < 3; ++dd) {
+            sm.ch.f[s][dd] = (R)F[3 * bead + dd];
+            sm.ch.th[s][dd] = (R)(0.5 * T[3 * bead + dd]);
+          }
       }
     }
     __syncthreads();
-    // scatter: warp `warp` owns tile x-plane `warp`
-    for (int s = 0; s < nb; ++s) {
-      int i = warp + sm.ch.ax[s];
-      i = i >= c.N[0] ? i - c.N[0] : i;
-      if (i < ngd) {
-        const R gxv = sm.ch.gx[s][i], dxv = sm.ch.dgx[s][i], rxv = sm.ch.rx[s][i];
-        const R F0 = sm.ch.f[s][0], F1 = sm.ch.f[s][1], F2 = sm.ch.f[s][2];
-        // g12 = T2/2, g13 = -T1/2, g21 = -T2/2, g23 = T0/2, g31 = T1/2, g32 = -T0/2 (GA_setup, :536-547)
-        const R h0 = sm.ch.th[s][0], h1 = sm.ch.th[s][1], h2 = sm.ch.th[s][2];
-        const int cy = sm.ch.cy[s], cz = sm.ch.cz[s], mcz = sm.ch.mcz[s];
-        const int cnt = cy * cz;
-        for (int pidx = lane; pidx < cnt; pidx += 32) {
-          // pidx / cz by multiply-shift: exact for pidx < 256, cz <= 16
-          const int jj = (pidx * mcz) >> 12, kk = pidx - jj * cz;
-          const R gyv = sm.ch.gy[s][jj], dyv = sm.ch.dgy[s][jj], ryv = sm.ch.ry[s][jj];
-          const R gzv = sm.ch.gz[s][kk], dzv = sm.ch.dgz[s][kk], rzv = sm.ch.rz[s][kk];
+    for (int s = warp; s < nb; s += FS_SPREAD_WARPS) {
+      const int cx = sm.ch.cnt[0][s], cy = sm.ch.cnt[1][s], cz = sm.ch.cnt[2][s], mcz = sm.ch.mcz[s];
+      const int cyz = cy * cz;
+      if (cx == 0 || cyz == 0) continue;
+      // g12 = T2/2, g13 = -T1/2, g21 = -T2/2, g23 = T0/2, g31 = T1/2, g32 = -T0/2 (GA_setup, :536-547)
+      const R F0 = sm.ch.f[s][0], F1 = sm.ch.f[s][1], F2 = sm.ch.f[s][2];
+      const R h0 = sm.ch.th[s][0], h1 = sm.ch.th[s][1], h2 = sm.ch.th[s][2];
+      for (int ix = 0; ix < cx; ++ix) {
+        const R gxv = sm.ch.g[0][s][ix], dxv = sm.ch.d[0][s][ix], rxv = sm.ch.r[0][s][ix];
+        const int lx = sm.ch.l[0][s][ix];
+        for (int p = lane; p < cyz; p += 32) {
+          // p / cz by multiply-shift: exact for p < 256, cz <= 16
+          const int iy = (p * mcz) >> 12, iz = p - iy * cz;
+          const R gyv = sm.ch.g[1][s][iy], dyv = sm.ch.d[1][s][iy], ryv = sm.ch.r[1][s][iy];
+          const R gzv = sm.ch.g[2][s][iz], dzv = sm.ch.d[2][s][iz], rzv = sm.ch.r[2][s][iz];
           const R temp = gxv * gyv * gzv;
           const R temp2 = dxv * dyv * dzv;
-          const int ly = sm.ch.ly[s][jj], lz = sm.ch.lz[s][kk];
-          sm.acc.add(0, warp, ly, lz, F0 * temp + (h2 * ryv - h1 * rzv) * temp2);
-          sm.acc.add(1, warp, ly, lz, F1 * temp + (-h2 * rxv + h0 * rzv) * temp2);
-          sm.acc.add(2, warp, ly, lz, F2 * temp + (h1 * rxv - h0 * ryv) * temp2);
+          const int e = (lx * FS_TILE + sm.ch.l[1][s][iy]) * FS_TILE + sm.ch.l[2][s][iz];
+          sm.acc.add(warp, 0, e, F0 * temp + (h2 * ryv - h1 * rzv) * temp2);
+          sm.acc.add(warp, 1, e, F1 * temp + (-h2 * rxv + h0 * rzv) * temp2);
+          sm.acc.add(warp, 2, e, F2 * temp + (h1 * rxv - h0 * ryv) * temp2);
         }
       }
       __syncwarp();
     }
     __syncthreads();
   }
-  // write the tile (each warp its plane; rows of FS_TILE contiguous z)
+  // sum the private copies and write the tile (rows of FS_TILE contiguous z)
   const size_t N = (size_t)c.N[0] * c.N[1] * c.N[2];
-  const int gx = X0[0] + warp;
-  for (int e = lane; e < 3 * FS_TILE * FS_TILE; e += 32) {
-    const int comp = e / (FS_TILE * FS_TILE);
-    const int y = (e / FS_TILE) % FS_TILE;
-    const int z = e % FS_TILE;
-    const size_t m = ((size_t)gx * c.N[1] + (X0[1] + y)) * c.N[2] + (X0[2] + z);
-    fgrid[comp * N + m] = sm.acc.result(comp, warp, y, z);
+  for (int q = tid; q < 3 * FS_TILE * FS_TILE * FS_TILE; q += nthr) {
+    const int comp = q / (FS_TILE * FS_TILE * FS_TILE);
+    const int e = q - comp * FS_TILE * FS_TILE * FS_TILE;
+    const int x = e / (FS_TILE * FS_TILE), y = (e / FS_TILE) % FS_TILE, z = e % FS_TILE;
+    const size_t m = ((size_t)(X0[0] + x) * c.N[1] + (X0[1] + y)) * c.N[2] + (X0[2] + z);
+    fgrid[comp * N + m] = sm.acc.total(comp, e);
   }
 }
 
@@ -580,7 +570,7 @@ fs_status mobility_t(fs_ctx *c, const double *Y, const double *F, const double *
     }
     FS_TRY(fs_sort_run(&c->bins, np, c->stream));
     const size_t smem = sizeof(SpreadSmem<R>);
-    k_spread<R><<<c->nbins, FS_TILE * 32, smem, c->stream>>>(Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k,
+    k_spread<R><<<c->nbins, FS_SPREAD_WARPS * 32, smem, c->stream>>>(Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k,
                                                               (R *)c->grid_real);
     FS_LAUNCH_CHECK();
   }
@@ -659,7 +649,7 @@ fs_status fcm_spread_only(fs_ctx *c, const double *Y, const double *F, const dou
     FS_LAUNCH_CHECK();
   }
   FS_TRY(fs_sort_run(&c->bins, np, c->stream));
-  k_spread<double><<<c->nbins, FS_TILE * 32, sizeof(SpreadSmem<double>), c->stream>>>(
+  k_spread<double><<<c->nbins, FS_SPREAD_WARPS * 32, sizeof(SpreadSmem<double>), c->stream>>>(
       Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k, (double *)c->grid_real);
   FS_LAUNCH_CHECK();
   FS_CUDA(cudaMemcpyAsync(f, c->grid_real, sizeof(double) * 3 * c->N, cudaMemcpyDeviceToDevice, c->stream));

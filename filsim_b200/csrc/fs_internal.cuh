@@ -10,10 +10,10 @@
 
 #define FS_PI 3.14159265358979323846264338327950288
 
-// Spread tile edge (grid points) and warps per spread CTA (one x-plane each).
-#define FS_TILE 16
+// Spread tile edge (grid points); spread bins have the same width.
+#define FS_TILE 8
 // Beads staged in shared memory per spread pass.
-#define FS_SPREAD_CHUNK 12
+#define FS_SPREAD_CHUNK 32
 // Collision events kept per bead (pairs inside the barrier range).
 #define FS_MAX_EVENTS 64
 // Flag words (device int array ctx->flags).
@@ -75,6 +75,7 @@ struct fs_ctx {
   // filament suspension (device)
   int nfil, np, nlink;
   bool have_state;
+  int *fil_start_h;      // host copy of the uploaded layout (nfil + 1)
   int *fil_start, *fil_id, *seg_id;
   double *X, *Xs, *Xt, *U, *Us, *Ut, *q, *qs, *qt, *F, *TAU, *lam, *lam1, *lam2, *kap, *cc, *radius;
   double *Y, *V, *W;

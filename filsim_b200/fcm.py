@@ -209,6 +209,11 @@ class Simulation:
         self.ctx.call("fs_state_download", ctypes.byref(out.struct))
         return out.arrays
 
+    def download_into(self, susp):
+        """Downloads the device state into susp's own arrays (e.g. pinned ones)."""
+        hs = susp.host_state()
+        self.ctx.call("fs_state_download", ctypes.byref(hs.struct))
+
     def device_array(self, which, shape):
         """A copy of a library-resident array (Y, V, W, err, ...)."""
         ptr = ctypes.c_void_p()
