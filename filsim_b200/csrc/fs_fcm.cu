@@ -1,13 +1,13 @@
 // fs_fcm.cu -- Force Coupling Method mobility solve on sm_100a.
 //
 // Replaces Fcm::mobility_solve (FCMfunctions.cpp:175-464):
-//   1. k_fcm_bin_keys + counting sort: beads binned by the 8-point tile that
+//   1. k_fcm_bin_keys + counting sort: beads binned by the 16-point tile that
 //      holds the start of their Gaussian stencil (gaussian_setup's index rule,
 //      FCMfunctions.cpp:565-589).
-//   2. k_spread: one CTA per 8^3 grid tile gathers the monopole + rotlet
+//   2. k_spread: one CTA per 16^3 grid tile gathers the monopole + rotlet
 //      Gaussians of every bead whose stencil reaches the tile
-//      (mono_and_dipole_force_distribution, :596-646) into per-warp private
-//      copies of the tile, summed in fixed order: no atomics, bit-reproducible.
+//      (mono_and_dipole_force_distribution, :596-646); each lane owns grid
+//      points and sums in registers: no atomics, bit-reproducible.
 //   3. cuFFT R2C (batched x3), 4. k_project / k_project_planes: the Stokes
 //      projection of flow_solve (:648-736), 5. cuFFT C2R (batched x3).
 //   6. k_interp: one warp per bead (in spread-bin order for L2 locality)
@@ -57,71 +57,51 @@ __global__ void k_fcm_bin_keys(const double *__restrict__ Y, int np, FcmConsts c
 }
 
 // ---- 2. spread ----------------------------------------------------------------
-// One CTA (4 warps) per 8^3 grid tile. Candidate beads are those whose stencil
-// start lies in the 3 bins before and at the tile per axis; they are staged in
-// chunks (per axis: the stencil indices landing in the tile, compacted, with
-// their Gaussian weights). Warp w takes chunk beads w, w+4, ... in sorted order
-// and adds each bead's clipped footprint (lanes over its (y, z) patch, a loop
-// over x) into its own private copy of the tile in shared memory. The four
-// copies are then summed in fixed order and written once: dense lane use, no
-// atomics, bit-reproducible.
-#define FS_SPREAD_WARPS 4
+// One CTA (16 warps) per 16^3 grid tile; the tile is cut into 2x2x8 blocks and
+// warp w owns the 8 blocks of column (bx, bz) = (w/2, w%2), one grid point per
+// lane. Candidate beads (stencil start in the tile's bin or the one before it,
+// per axis) are staged as per-axis weight tables indexed by tile coordinate
+// (zero outside the bead's stencil). Each warp builds, by ballots, the set of
+// staged beads that reach its column and, per block, those that reach the
+// block; every lane then sums those beads' contributions to its point in
+// registers, in sorted bead order, and writes the point once. No atomics and no
+// shared-memory read-modify-write; bit-reproducible. FP32 mode keeps Kahan
+// compensated register sums.
+#define FS_SPREAD_THREADS 512
 
 template <typename R>
-struct SpreadChunk {
-  R g[3][FS_SPREAD_CHUNK][FS_TILE], d[3][FS_SPREAD_CHUNK][FS_TILE], r[3][FS_SPREAD_CHUNK][FS_TILE];
-  R f[FS_SPREAD_CHUNK][3];   // force
-  R th[FS_SPREAD_CHUNK][3];  // half torque (GA_setup, :536-547)
-  unsigned char l[3][FS_SPREAD_CHUNK][FS_TILE];  // tile-local coordinate of each compacted entry
-  int cnt[3][FS_SPREAD_CHUNK];
-  int mcz[FS_SPREAD_CHUNK];  // multiply-shift divisor for the (y, z) patch
+struct W4 {
+  R g, d, r, pad;
 };
 
 template <typename R>
-struct SpreadAcc;
+struct SpreadStage {
+  W4<R> w[FS_SPREAD_CHUNK][3][FS_TILE];  // weights by tile-local coordinate
+  R f[FS_SPREAD_CHUNK][4];                // force
+  R th[FS_SPREAD_CHUNK][4];               // half torque (GA_setup, :536-547)
+  unsigned mask[FS_SPREAD_CHUNK][3];      // per axis: tile-local coordinates covered
+};
+
+template <typename R>
+struct KAcc;
 template <>
-struct SpreadAcc<double> {  // FP64 mode: plain double sums
-  double v[FS_SPREAD_WARPS][3][FS_TILE * FS_TILE * FS_TILE];
-  __device__ void add(int w, int c, int e, double val) { v[w][c][e] += val; }
-  __device__ double total(int c, int e) const {
-    double s = v[0][c][e];
-    for (int w = 1; w < FS_SPREAD_WARPS; ++w) s += v[w][c][e];
-    return s;
-  }
-  __device__ void zero(int t, int nt) {
-    double *p = &v[0][0][0];
-    for (int i = t; i < FS_SPREAD_WARPS * 3 * FS_TILE * FS_TILE * FS_TILE; i += nt) p[i] = 0.0;
-  }
+struct KAcc<double> {
+  double s;
+  __device__ void init() { s = 0.0; }
+  __device__ void add(double v) { s += v; }
+  __device__ double value() const { return s; }
 };
 template <>
-struct SpreadAcc<float> {  // FP32 mode: Kahan-compensated float sums
-  float v[FS_SPREAD_WARPS][3][FS_TILE * FS_TILE * FS_TILE];
-  float cmp[FS_SPREAD_WARPS][3][FS_TILE * FS_TILE * FS_TILE];
-  __device__ void add(int w, int c, int e, float val) {
-    float s = v[w][c][e];
-    float yv = val - cmp[w][c][e];
-    float t = s + yv;
-    cmp[w][c][e] = (t - s) - yv;
-    v[w][c][e] = t;
+struct KAcc<float> {
+  float s, c;
+  __device__ void init() { s = 0.f; c = 0.f; }
+  __device__ void add(float v) {
+    float y = v - c;
+    float t = s + y;
+    c = (t - s) - y;
+    s = t;
   }
-  __device__ float total(int c, int e) const {
-    double s = 0.0;
-    for (int w = 0; w < FS_SPREAD_WARPS; ++w) s += (double)v[w][c][e] - (double)cmp[w][c][e];
-    return (float)s;
-  }
-  __device__ void zero(int t, int nt) {
-    float *p = &v[0][0][0], *q = &cmp[0][0][0];
-    for (int i = t; i < FS_SPREAD_WARPS * 3 * FS_TILE * FS_TILE * FS_TILE; i += nt) {
-      p[i] = 0.f;
-      q[i] = 0.f;
-    }
-  }
-};
-
-template <typename R>
-struct SpreadSmem {
-  SpreadAcc<R> acc;
-  SpreadChunk<R> ch;
+  __device__ float value() const { return s - c; }
 };
 
 template <typename R>
@@ -132,34 +112,27 @@ template <>
 __device__ inline float fs_exp<float>(float x) { return expf(x); }
 
 template <typename R>
-__global__ void __launch_bounds__(FS_SPREAD_WARPS * 32)
+__global__ void __launch_bounds__(FS_SPREAD_THREADS)
     k_spread(const double *__restrict__ Y, const double *__restrict__ F, const double *__restrict__ T,
              const int *__restrict__ bin_start, const int *__restrict__ sorted, const int *__restrict__ bead_sw,
              FcmConsts c, R *__restrict__ fgrid) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  SpreadSmem<R> &sm = *reinterpret_cast<SpreadSmem<R> *>(smem_raw);
+  SpreadStage<R> &st = *reinterpret_cast<SpreadStage<R> *>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nthr = blockDim.x;
   const int tile = blockIdx.x;
   const int tz = tile % c.nbin[2], ty = (tile / c.nbin[2]) % c.nbin[1], tx = tile / (c.nbin[2] * c.nbin[1]);
   const int X0[3] = {tx * FS_TILE, ty * FS_TILE, tz * FS_TILE};
-  sm.acc.zero(tid, nthr);
-
-  // candidate bins per axis: stencil starts in [X0 - ngd + 1, X0 + FS_TILE), wrapped
-  int cb[3][4], ncb[3];
+  // candidate bins per axis: the tile's own bin and the one before it
+  int cb[3][2], ncb[3];
   const int tb[3] = {tx, ty, tz};
-  const int back = (c.ngd - 1 + FS_TILE - 1) / FS_TILE;
 #pragma unroll
-  for (int dd = 0; dd < 3; ++dd) {
-    ncb[dd] = 0;
-    for (int k = back; k >= 0; --k) {
-      int b = wrap_int(tb[dd] - k, c.nbin[dd]);
-      bool dup = false;
-      for (int q = 0; q < ncb[dd]; ++q) dup |= (cb[dd][q] == b);
-      if (!dup && ncb[dd] < 4) cb[dd][ncb[dd]++] = b;
-    }
+  for (int d = 0; d < 3; ++d) {
+    cb[d][0] = wrap_int(tb[d] - 1, c.nbin[d]);
+    cb[d][1] = tb[d];
+    ncb[d] = (c.nbin[d] > 1) ? 2 : 1;
+    if (ncb[d] == 1) cb[d][0] = tb[d];
   }
-  int rs[64], re[64], nr = 0, total = 0;
+  int rs[8], re[8], nr = 0, total = 0;
   for (int a = 0; a < ncb[0]; ++a)
     for (int b2 = 0; b2 < ncb[1]; ++b2)
       for (int e = 0; e < ncb[2]; ++e) {
@@ -169,101 +142,124 @@ __global__ void __launch_bounds__(FS_SPREAD_WARPS * 32)
         total += re[nr] - rs[nr];
         nr++;
       }
-  __syncthreads();
-
+  // this lane's point in block (bx, by, bz): x = 2bx + (lane&1), y = 2by + ((lane>>1)&1), z = 8bz + (lane>>2)
+  const int bx = warp >> 1, bz = warp & 1;
+  const int px = 2 * bx + (lane & 1), pyo = (lane >> 1) & 1, pz = 8 * bz + (lane >> 2);
+  const size_t N = (size_t)c.N[0] * c.N[1] * c.N[2];
   const int ngd = c.ngd;
   for (int base = 0; base < total; base += FS_SPREAD_CHUNK) {
     const int nb = min(FS_SPREAD_CHUNK, total - base);
-    // stage: thread per (bead slot, axis, stencil index)
-    for (int it = tid; it < nb * 3 * ngd; it += nthr) {
-      const int s = it / (3 * ngd);
-      const int a = (it / ngd) % 3;
-      const int i = it % ngd;
-      int rank = base + s, r = 0;
-      while (rank >= re[r] - rs[r]) {
-        rank -= re[r] - rs[r];
-        ++r;
-      }
-      const int bead = sorted[rs[r] + rank];
-      const double Yv = Y[3 * bead + a];
-      const int xc = (int)(Yv / c.dx);
-      const int xg = xc - c.ngdh + (i + 1);
-      const double xx = ((double)xg) * c.dx - Yv;
-      const int Nn = c.N[a];
-      const int sw = bead_sw[3 * bead + a];
-      // stencil index i lands on tile-local l = (i - aoff) mod N; valid if l < FS_TILE.
-      // The valid indices form [0, e2) (wrapped around the box) and [aoff, e1).
-      const int aoff = wrap_near(X0[a] - sw, Nn);
-      const int e1 = min(ngd, aoff + FS_TILE);
-      const int e2 = max(0, min(ngd, aoff + FS_TILE - Nn));
-      const bool in2 = i < e2, in1 = i >= aoff && i < e1;
-      if (in1 || in2) {
-        const int pos = in2 ? i : e2 + (i - aoff);
-        R g, gd, rr;
-        if (sizeof(R) == 8) {
-          g = (R)(c.anorm * exp(-xx * xx / c.anorm2));
-          gd = (R)(c.anormdip * exp(-xx * xx / c.anormdip2));
-          rr = (R)(-xx / c.sigmadipsq);
-        } else {
-          const R xf = (R)xx;
-          g = (R)c.anorm * fs_exp<R>(-xf * xf / (R)c.anorm2);
-          gd = (R)c.anormdip * fs_exp<R>(-xf * xf / (R)c.anormdip2);
-          rr = -xf / (R)c.sigmadipsq;
+    __syncthreads();  // the previous chunk's tables are no longer read
+    // stage: one half-warp per (bead slot, axis), lane l -> tile-local coordinate l
+    const int nitems = nb * 3 * FS_TILE;
+    for (int it0 = warp * 32; it0 < nitems; it0 += FS_SPREAD_THREADS) {
+      const int it = it0 + lane;
+      const bool act = it < nitems;
+      const int s = act ? it / (3 * FS_TILE) : 0;
+      const int a = act ? (it / FS_TILE) % 3 : 0;
+      const int l = it % FS_TILE;
+      bool valid = false;
+      W4<R> wv = {(R)0, (R)0, (R)0, (R)0};
+      int bead = 0;
+      if (act) {
+        int rank = base + s, r = 0;
+        while (rank >= re[r] - rs[r]) {
+          rank -= re[r] - rs[r];
+          ++r;
         }
-        sm.ch.g[a][s][pos] = g;
-        sm.ch.d[a][s][pos] = gd;
-        sm.ch.r[a][s][pos] = rr;
-        sm.ch.l[a][s][pos] = (unsigned char)(in2 ? i - aoff + Nn : i - aoff);
+        bead = sorted[rs[r] + rank];
+        const int Nn = c.N[a];
+        // tile-local l holds stencil index i = (l + X0 - sw) mod N if i < ngd
+        const int i = wrap_near(l + wrap_near(X0[a] - bead_sw[3 * bead + a], Nn), Nn);
+        if (i < ngd) {
+          valid = true;
+          const double Yv = Y[3 * bead + a];
+          const int xc = (int)(Yv / c.dx);
+          const int xg = xc - c.ngdh + (i + 1);
+          const double xx = ((double)xg) * c.dx - Yv;
+          if (sizeof(R) == 8) {
+            wv.g = (R)(c.anorm * exp(-xx * xx / c.anorm2));
+            wv.d = (R)(c.anormdip * exp(-xx * xx / c.anormdip2));
+            wv.r = (R)(-xx / c.sigmadipsq);
+          } else {
+            const R xf = (R)xx;
+            wv.g = (R)c.anorm * fs_exp<R>(-xf * xf / (R)c.anorm2);
+            wv.d = (R)c.anormdip * fs_exp<R>(-xf * xf / (R)c.anormdip2);
+            wv.r = -xf / (R)c.sigmadipsq;
+          }
+        }
+        st.w[s][a][l] = wv;
       }
-      if (i == 0) {
-        const int cntv = max(0, e1 - aoff) + e2;
-        sm.ch.cnt[a][s] = cntv;
-        if (a == 2) sm.ch.mcz[s] = cntv > 0 ? (4096 + cntv - 1) / cntv : 0;
+      const unsigned bal = __ballot_sync(0xffffffffu, valid);
+      if (act && l == 0) {
+        st.mask[s][a] = (bal >> (lane & 16)) & 0xffffu;
         if (a == 0)
-#pragma unroll
-          for (int dd = 0; dd < 3; ++dd) {
-            sm.ch.f[s][dd] = (R)F[3 * bead + dd];
-            sm.ch.th[s][dd] = (R)(0.5 * T[3 * bead + dd]);
+          for (int d = 0; d < 3; ++d) {
+            st.f[s][d] = (R)F[3 * bead + d];
+            st.th[s][d] = (R)(0.5 * T[3 * bead + d]);
           }
       }
     }
     __syncthreads();
-    for (int s = warp; s < nb; s += FS_SPREAD_WARPS) {
-      const int cx = sm.ch.cnt[0][s], cy = sm.ch.cnt[1][s], cz = sm.ch.cnt[2][s], mcz = sm.ch.mcz[s];
-      const int cyz = cy * cz;
-      if (cx == 0 || cyz == 0) continue;
-      // g12 = T2/2, g13 = -T1/2, g21 = -T2/2, g23 = T0/2, g31 = T1/2, g32 = -T0/2 (GA_setup, :536-547)
-      const R F0 = sm.ch.f[s][0], F1 = sm.ch.f[s][1], F2 = sm.ch.f[s][2];
-      const R h0 = sm.ch.th[s][0], h1 = sm.ch.th[s][1], h2 = sm.ch.th[s][2];
-      for (int ix = 0; ix < cx; ++ix) {
-        const R gxv = sm.ch.g[0][s][ix], dxv = sm.ch.d[0][s][ix], rxv = sm.ch.r[0][s][ix];
-        const int lx = sm.ch.l[0][s][ix];
-        for (int p = lane; p < cyz; p += 32) {
-          // p / cz by multiply-shift: exact for p < 256, cz <= 16
-          const int iy = (p * mcz) >> 12, iz = p - iy * cz;
-          const R gyv = sm.ch.g[1][s][iy], dyv = sm.ch.d[1][s][iy], ryv = sm.ch.r[1][s][iy];
-          const R gzv = sm.ch.g[2][s][iz], dzv = sm.ch.d[2][s][iz], rzv = sm.ch.r[2][s][iz];
-          const R temp = gxv * gyv * gzv;
-          const R temp2 = dxv * dyv * dzv;
-          const int e = (lx * FS_TILE + sm.ch.l[1][s][iy]) * FS_TILE + sm.ch.l[2][s][iz];
-          sm.acc.add(warp, 0, e, F0 * temp + (h2 * ryv - h1 * rzv) * temp2);
-          sm.acc.add(warp, 1, e, F1 * temp + (-h2 * rxv + h0 * rzv) * temp2);
-          sm.acc.add(warp, 2, e, F2 * temp + (h1 * rxv - h0 * ryv) * temp2);
+    // beads reaching this warp's column, and per y-block those reaching the block
+    unsigned col[FS_SPREAD_CHUNK / 32], ym[8][FS_SPREAD_CHUNK / 32];
+#pragma unroll
+    for (int h = 0; h < FS_SPREAD_CHUNK / 32; ++h) {
+      const int s = 32 * h + lane;
+      unsigned mx = 0, my = 0, mz = 0;
+      if (s < nb) {
+        mx = st.mask[s][0];
+        my = st.mask[s][1];
+        mz = st.mask[s][2];
+      }
+      col[h] = __ballot_sync(0xffffffffu, ((mx >> (2 * bx)) & 3u) && ((mz >> (8 * bz)) & 0xffu));
+#pragma unroll
+      for (int by = 0; by < 8; ++by) ym[by][h] = __ballot_sync(0xffffffffu, (my >> (2 * by)) & 3u);
+    }
+    const W4<R> *wxp = &st.w[0][0][px];
+    const W4<R> *wzp = &st.w[0][2][pz];
+#pragma unroll 1
+    for (int by = 0; by < 8; ++by) {
+      const int py = 2 * by + pyo;
+      KAcc<R> a0, a1, a2;
+      a0.init();
+      a1.init();
+      a2.init();
+#pragma unroll
+      for (int h = 0; h < FS_SPREAD_CHUNK / 32; ++h) {
+        unsigned m = col[h] & ym[by][h];
+        while (m) {
+          const int s = 32 * h + __ffs(m) - 1;
+          m &= m - 1;
+          const W4<R> wx = wxp[s * 3 * FS_TILE], wy = st.w[s][1][py], wz = wzp[s * 3 * FS_TILE];
+          const R F0 = st.f[s][0], F1 = st.f[s][1], F2 = st.f[s][2];
+          const R h0 = st.th[s][0], h1 = st.th[s][1], h2 = st.th[s][2];
+          const R temp = wx.g * wy.g * wz.g;
+          const R temp2 = wx.d * wy.d * wz.d;
+          a0.add(F0 * temp + (h2 * wy.r - h1 * wz.r) * temp2);
+          a1.add(F1 * temp + (-h2 * wx.r + h0 * wz.r) * temp2);
+          a2.add(F2 * temp + (h1 * wx.r - h0 * wy.r) * temp2);
         }
       }
-      __syncwarp();
+      const size_t m0 = ((size_t)(X0[0] + px) * c.N[1] + (X0[1] + py)) * c.N[2] + (X0[2] + pz);
+      if (base == 0) {
+        fgrid[m0] = a0.value();
+        fgrid[N + m0] = a1.value();
+        fgrid[2 * N + m0] = a2.value();
+      } else {  // more candidates than one chunk: add in chunk order
+        fgrid[m0] += a0.value();
+        fgrid[N + m0] += a1.value();
+        fgrid[2 * N + m0] += a2.value();
+      }
     }
-    __syncthreads();
   }
-  // sum the private copies and write the tile (rows of FS_TILE contiguous z)
-  const size_t N = (size_t)c.N[0] * c.N[1] * c.N[2];
-  for (int q = tid; q < 3 * FS_TILE * FS_TILE * FS_TILE; q += nthr) {
-    const int comp = q / (FS_TILE * FS_TILE * FS_TILE);
-    const int e = q - comp * FS_TILE * FS_TILE * FS_TILE;
-    const int x = e / (FS_TILE * FS_TILE), y = (e / FS_TILE) % FS_TILE, z = e % FS_TILE;
-    const size_t m = ((size_t)(X0[0] + x) * c.N[1] + (X0[1] + y)) * c.N[2] + (X0[2] + z);
-    fgrid[comp * N + m] = sm.acc.total(comp, e);
-  }
+  if (total == 0)
+    for (int by = 0; by < 8; ++by) {
+      const size_t m0 = ((size_t)(X0[0] + px) * c.N[1] + (X0[1] + 2 * by + pyo)) * c.N[2] + (X0[2] + pz);
+      fgrid[m0] = (R)0;
+      fgrid[N + m0] = (R)0;
+      fgrid[2 * N + m0] = (R)0;
+    }
 }
 
 // ---- 4. Stokes projection -----------------------------------------------------
@@ -569,8 +565,8 @@ fs_status mobility_t(fs_ctx *c, const double *Y, const double *F, const double *
       FS_LAUNCH_CHECK();
     }
     FS_TRY(fs_sort_run(&c->bins, np, c->stream));
-    const size_t smem = sizeof(SpreadSmem<R>);
-    k_spread<R><<<c->nbins, FS_SPREAD_WARPS * 32, smem, c->stream>>>(Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k,
+    const size_t smem = sizeof(SpreadStage<R>);
+    k_spread<R><<<c->nbins, FS_SPREAD_THREADS, smem, c->stream>>>(Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k,
                                                               (R *)c->grid_real);
     FS_LAUNCH_CHECK();
   }
@@ -604,9 +600,9 @@ fs_status fcm_init(fs_ctx *c) {
   FS_CUDA(cudaMalloc(&c->bead_sw, sizeof(int) * 3 * (size_t)(c->max_beads > 0 ? c->max_beads : 1)));
   c->bytes += sizeof(int) * 3 * (size_t)c->max_beads;
   FS_CUDA(cudaFuncSetAttribute(k_spread<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)sizeof(SpreadSmem<double>)));
+                               (int)sizeof(SpreadStage<double>)));
   FS_CUDA(cudaFuncSetAttribute(k_spread<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)sizeof(SpreadSmem<float>)));
+                               (int)sizeof(SpreadStage<float>)));
   return FS_OK;
 }
 
@@ -649,7 +645,7 @@ fs_status fcm_spread_only(fs_ctx *c, const double *Y, const double *F, const dou
     FS_LAUNCH_CHECK();
   }
   FS_TRY(fs_sort_run(&c->bins, np, c->stream));
-  k_spread<double><<<c->nbins, FS_SPREAD_WARPS * 32, sizeof(SpreadSmem<double>), c->stream>>>(
+  k_spread<double><<<c->nbins, FS_SPREAD_THREADS, sizeof(SpreadStage<double>), c->stream>>>(
       Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k, (double *)c->grid_real);
   FS_LAUNCH_CHECK();
   FS_CUDA(cudaMemcpyAsync(f, c->grid_real, sizeof(double) * 3 * c->N, cudaMemcpyDeviceToDevice, c->stream));

@@ -11,9 +11,9 @@
 #define FS_PI 3.14159265358979323846264338327950288
 
 // Spread tile edge (grid points); spread bins have the same width.
-#define FS_TILE 8
-// Beads staged in shared memory per spread pass.
-#define FS_SPREAD_CHUNK 32
+#define FS_TILE 16
+// Beads staged in shared memory per spread pass (a multiple of 32).
+#define FS_SPREAD_CHUNK 64
 // Collision events kept per bead (pairs inside the barrier range).
 #define FS_MAX_EVENTS 64
 // Flag words (device int array ctx->flags).
