@@ -41,10 +41,13 @@ WORKLOAD = dict(npts=512, nfil=4096, nw=32, seed=1002)
 # Broyden iterations per step of sediment_512 used to scale the CPU baseline's
 # per-iteration sample to whole steps when the GPU run is not available (the
 # reference arm); the GPU FP64 path matches the oracle's iteration counts.
-REFERENCE_ITERS_PER_STEP = 20.0
+REFERENCE_ITERS_PER_STEP = 26.0
 # DRAM bytes per launch from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum);
 # the kernels and captures are listed in profiles/.
-NCU_TRAFFIC = {}
+NCU_TRAFFIC = {
+    # mobility_256 capture of k_spread<float>: 307.9 MB, scaled x8 to the 512^3 grid it writes
+    "spread": 2.463e9,
+}
 
 
 def parse():
@@ -57,6 +60,9 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-stride", type=int, default=64)
+    ap.add_argument("--workload", default="sediment_512", choices=["sediment_512", "mobility_256"],
+                    help="sediment_512: implicit steps (the headline); mobility_256: FCM mobility solves, "
+                         "FP32 against FP64, on 256^3 with 1024 x 30 beads")
     return ap.parse_args()
 
 
@@ -175,10 +181,12 @@ def run_ours(args, rank, world):
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         with ClockSampler(dev) as clk:
+            torch.cuda.nvtx.range_push("timed_steps")
             ev0.record(stream)
             its, st = sim.run_steps(W + 1, K)
             ev1.record(stream)
             torch.cuda.synchronize()
+            torch.cuda.nvtx.range_pop()
         ms = ev0.elapsed_time(ev1)
         launches = abi.lib().fs_kernel_launches() - launches0
         prof = ctx.profile() if profile else None
@@ -210,12 +218,14 @@ def run_ours(args, rank, world):
     N = 512 ** 3
     NH = 512 * 512 * 257
     s_real = 4  # FP32 grids in the mixed path
+    nw = WORKLOAD["nw"]
+    aux = 20 * (nw - 1) + 3 * nw + 1  # doubles of D', F', tangents and P per filament (fil_aux_size)
     alg_bytes = {
         "spread": 3 * s_real * N + npb * 9 * 8,          # write f once, read bead Y, F, T
         "project": 2 * 3 * NH * 2 * s_real,              # read and write 3 complex spectra
         "interp": 3 * s_real * N + npb * 9 * 8,          # read u once, bead Y in, V, W out
-        "jacobian": 2 * susp.nfil * (6 * WORKLOAD["nw"]) ** 2 * 8,  # write J, then LU in place (one pass)
-        "broyden": susp.nfil * (6 * WORKLOAD["nw"]) ** 2 * 8,       # read the LU factors once per application
+        "jacobian": susp.nfil * ((3 * nw) ** 2 + aux) * 8,  # write the Schur inverse and the D', F' blocks
+        "broyden": susp.nfil * ((3 * nw) ** 2 + aux) * 8 + 2 * 6 * npb * 8,  # read them, read b, write x
     }
     cands = {k: stage_ms[k] for k in alg_bytes if stage_ms.get(k, 0) > 0}
     dom = max(cands, key=cands.get)
@@ -278,6 +288,58 @@ def run_ours(args, rank, world):
     return out
 
 
+def run_mobility(args, rank, world):
+    """Workload mobility_256: one step is one FCM mobility solve (spread, FFT,
+    projection, inverse FFT, interpolation) of 30,720 beads on 256^3, timed in
+    FP32 (value) and FP64; the FP32 velocities are compared with the FP64 ones."""
+    import numpy as np
+    import torch
+    from filsim_b200 import abi
+    from filsim_b200.configs import WORKLOADS, make_mobility_case
+    from filsim_b200.fcm import Context, Fcm
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    w = WORKLOADS["mobility_256"]
+    p, s, Y, F, T = make_mobility_case(w["npts"], w["nfil"], w["nw"], w["seed"] + rank)
+    stream = torch.cuda.Stream()
+    ctx = Context(p, max_beads=s.np, max_filaments=s.nfil, stream=stream)
+    fcm = Fcm(ctx, s.np)
+    fcm.set(Y, F, T)
+    K, W = args.steps, args.warmup
+    res = {}
+    for name, prec in (("fp32", abi.FS_PREC_FP32), ("fp64", abi.FS_PREC_FP64)):
+        ctx.set_precision(prec)
+        for _ in range(W):
+            fcm.mobility_solve()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        launches0 = abi.lib().fs_kernel_launches()
+        with ClockSampler(dev) as clk:
+            torch.cuda.nvtx.range_push("timed_steps")
+            ev0.record(stream)
+            for _ in range(K):
+                fcm.mobility_solve()
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            torch.cuda.nvtx.range_pop()
+        res[name] = dict(ms=ev0.elapsed_time(ev1), V=fcm.V.cpu().numpy(), W=fcm.W.cpu().numpy(),
+                         clocks=clk.summary(), launches=abi.lib().fs_kernel_launches() - launches0)
+    ctx.close()
+    relerr = lambda a, b: float(np.abs(a - b).max() / np.abs(b).max())
+    ms = res["fp32"]["ms"]
+    return {"metric": "FCM mobility bead-solves/s (FP32 chain; FP64 beside it)", "value": s.np * K / (ms / 1e3),
+            "unit": "bead-solves/s", "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded rejection-placed filaments, F, T ~ N(0,1))",
+            "config": {"workload": "mobility_256", "grid": [256, 256, 256], "filaments": w["nfil"],
+                       "beads_per_filament": w["nw"], "beads": s.np, "l2": "grids (~0.4 GB) larger than L2"},
+            "fp64": {"value": s.np * K / (res["fp64"]["ms"] / 1e3), "ms_per_step": res["fp64"]["ms"] / K},
+            "fp32_error_vs_fp64": {"U": relerr(res["fp32"]["V"], res["fp64"]["V"]),
+                                   "Omega": relerr(res["fp32"]["W"], res["fp64"]["W"])},
+            "clocks": res["fp32"]["clocks"], "gpu_launches": int(res["fp32"]["launches"])}
+
+
 def cpu_baseline(p, susp, iters_per_step, stride):
     """Oracle stage costs of one Broyden iteration of this workload, each stage
     run on 1/stride of its independent work units and scaled back; a step is
@@ -338,6 +400,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
     if args.impl == "reference":
         out = run_reference(args, rank, world)
+    elif args.workload == "mobility_256":
+        out = run_mobility(args, rank, world) if rank == 0 else None
     else:
         out = run_ours(args, rank, world)
     if rank == 0 and out is not None:
