@@ -468,6 +468,12 @@ __global__ void __launch_bounds__(256) k_interp(const R *__restrict__ u, const d
   }
 }
 
+template <typename A, typename B>
+__global__ void k_convert(const A *__restrict__ in, B *__restrict__ out, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (B)in[i];
+}
+
 __global__ void k_friction(const double *__restrict__ F, const double *__restrict__ T, double *__restrict__ V,
                            double *__restrict__ W, int n3, double a1, double a2) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -519,6 +525,7 @@ fs_status ensure_plans(fs_ctx *c, int prec) {
 template <typename R>
 fs_status flow_solve_t(fs_ctx *c) {
   const int prec = sizeof(R) == 8 ? FS_PREC_FP64 : FS_PREC_FP32;
+  if (prec == FS_PREC_FP32 && c->fft_tw) return fft32_flow_solve(c);
   FS_TRY(ensure_plans(c, prec));
   cufftResult r;
   {
@@ -603,7 +610,7 @@ fs_status fcm_init(fs_ctx *c) {
                                (int)sizeof(SpreadStage<double>)));
   FS_CUDA(cudaFuncSetAttribute(k_spread<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(SpreadStage<float>)));
-  return FS_OK;
+  return fft32_init(c);
 }
 
 void fcm_free(fs_ctx *c) {
@@ -616,6 +623,7 @@ void fcm_free(fs_ctx *c) {
   cudaFree(c->grid_real);
   cudaFree(c->grid_cplx);
   c->grid_real = c->grid_cplx = nullptr;
+  fft32_free(c);
   fs_sort_free(&c->bins);
   cudaFree(c->bead_sw);
   c->bead_sw = nullptr;
@@ -655,7 +663,16 @@ fs_status fcm_spread_only(fs_ctx *c, const double *Y, const double *F, const dou
 
 fs_status fcm_flow_solve_only(fs_ctx *c, const double *f, double *u) {
   const size_t n = 3 * c->N;
-  if (c->precision != FS_PREC_FP64) return FS_ERR_INVALID_ARG;  // the flow-only check is an FP64 entry point
+  if (c->precision == FS_PREC_FP32) {
+    // FP32 chain: f rounded to float, solved, widened back
+    k_convert<double, float><<<fs_blocks((long long)n, 256), 256, 0, c->stream>>>(f, (float *)c->grid_real, n);
+    FS_LAUNCH_CHECK();
+    FS_TRY(flow_solve_t<float>(c));
+    k_convert<float, double><<<fs_blocks((long long)n, 256), 256, 0, c->stream>>>((const float *)c->grid_real, u, n);
+    FS_LAUNCH_CHECK();
+    c->last_grid_prec = FS_PREC_FP32;
+    return FS_OK;
+  }
   FS_CUDA(cudaMemcpyAsync(c->grid_real, f, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
   FS_TRY(flow_solve_t<double>(c));
   FS_CUDA(cudaMemcpyAsync(u, c->grid_real, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));

@@ -1,0 +1,626 @@
+// fs_fft.cu -- FP32 periodic Stokes solve on power-of-two grids for sm_100a:
+// the forward real 3-D transform, the projection of flow_solve
+// (FCMfunctions.cpp:648-736) and the inverse real transform in five passes
+// over HBM, replacing cuFFT R2C + projection + C2R in the mixed-precision path.
+//
+//   f[c][x][y][z] (real)  --z_r2c-->    A[c][kz][x][y]   z lines, real-to-half-complex
+//                         --y_fwd-->    B[c][kz][ky][x]  y lines, written transposed
+//                         --x_project-> B (in place)     x lines: forward, Stokes
+//                                                        projection, inverse, with the
+//                                                        three components in registers
+//                         --y_inv-->    A[c][kz][x][y]
+//                         --z_c2r-->    u[c][x][y][z] (real)
+// Each pass reads and writes the grid once with 128-byte rows. Every line is
+// transformed by one warp in registers: N = 32*M points, M per lane, an
+// M-point radix-2 DFT per lane, a transpose through a padded per-warp shared
+// buffer, a second M-point DFT and log2(32/M) radix-2 stages across lanes with
+// shuffles. Transforms are unnormalised; the projection divides by Nx*Ny*Nz as
+// the reference does. The half-complex inverse along z takes only the real part
+// of the kz = 0 and kz = Nz/2 coefficients after the complex inverse transforms
+// along x and y, the semantics of the reference's multi-dimensional real
+// inverse transform.
+#include "fs_internal.cuh"
+
+namespace {
+
+constexpr int FFT_WARPS = 8;
+constexpr int FFT_THREADS = 32 * FFT_WARPS;
+constexpr int FFT_TILE = 16;             // lines per transposing tile (16 complex = 128 bytes)
+constexpr int FFT_TS = FFT_TILE + 1;     // padded tile row (conflict-free column access)
+constexpr int TW_FULL = 1024;            // tw[j] = exp(-2 pi i j / 1024)
+#define FULL_MASK 0xffffffffu
+
+// Row of spectrum index k in a shared buffer that receives a warp's output in
+// register order (k = c + M k' + M^2 t across lanes): k + (k / M^2) (16 / G)
+// spreads the lanes of each half-warp over distinct banks.
+template <int N>
+__host__ __device__ constexpr int prow(int k) {
+  return N == 32 ? k + (k >> 4) : k + (k / ((N / 32) * (N / 32))) * (16 / (32 / (N / 32)));
+}
+
+template <int N>
+struct Fft {
+  static constexpr int M = N / 32;                       // points per lane
+  static constexpr int G = 32 / M;                       // lanes per column in the second stage
+  static constexpr int RS = 32 + (G < 16 ? G : 0);       // padded transpose row
+  static constexpr int PEXT = prow<N>(N - 1) + 1;        // rows of a swizzled N-point buffer
+  static constexpr int SW = (PEXT > M * RS ? PEXT : M * RS);  // per-warp scratch (float2)
+  static constexpr int LANE_TAB = TW_FULL + N - 32;      // offset of the per-lane twiddle table
+};
+
+__host__ __device__ constexpr int bitrev_c(int i, int n) {
+  int r = 0;
+  for (int b = 1, rb = n >> 1; b < n; b <<= 1, rb >>= 1)
+    if (i & b) r |= rb;
+  return r;
+}
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// table twiddle for direction D (+1 forward, -1 inverse)
+template <int D>
+__device__ __forceinline__ float2 twd(const float2 *__restrict__ tw, int j) {
+  float2 w = __ldg(tw + j);
+  if (D < 0) w.y = -w.y;
+  return w;
+}
+
+// a * exp(-D 2 pi i j / 16) for j in [0, 8); j is a compile-time constant after unrolling
+__device__ __forceinline__ float cos16(int j) {
+  switch (j) {
+    case 1: return 0.92387953251128676f;
+    case 2: return 0.70710678118654752f;
+    case 3: return 0.38268343236508977f;
+    case 5: return -0.38268343236508977f;
+    case 6: return -0.70710678118654752f;
+    case 7: return -0.92387953251128676f;
+    default: return 0.f;
+  }
+}
+__device__ __forceinline__ float sin16(int j) {
+  switch (j) {
+    case 1: case 7: return 0.38268343236508977f;
+    case 2: case 6: return 0.70710678118654752f;
+    case 3: case 5: return 0.92387953251128676f;
+    default: return 0.f;
+  }
+}
+// exp(-2 pi i k / 32), k in [0, 16); k is a compile-time constant after unrolling
+__device__ __forceinline__ float2 w32(int k) {
+  switch (k) {
+    case 1: return make_float2(0.98078528040323043f, -0.19509032201612826f);
+    case 2: return make_float2(0.92387953251128674f, -0.38268343236508978f);
+    case 3: return make_float2(0.83146961230254524f, -0.55557023301960218f);
+    case 4: return make_float2(0.70710678118654752f, -0.70710678118654752f);
+    case 5: return make_float2(0.55557023301960218f, -0.83146961230254524f);
+    case 6: return make_float2(0.38268343236508978f, -0.92387953251128674f);
+    case 7: return make_float2(0.19509032201612826f, -0.98078528040323043f);
+    case 8: return make_float2(0.f, -1.f);
+    case 9: return make_float2(-0.19509032201612826f, -0.98078528040323043f);
+    case 10: return make_float2(-0.38268343236508978f, -0.92387953251128674f);
+    case 11: return make_float2(-0.55557023301960218f, -0.83146961230254524f);
+    case 12: return make_float2(-0.70710678118654752f, -0.70710678118654752f);
+    case 13: return make_float2(-0.83146961230254524f, -0.55557023301960218f);
+    case 14: return make_float2(-0.92387953251128674f, -0.38268343236508978f);
+    case 15: return make_float2(-0.98078528040323043f, -0.19509032201612826f);
+    default: return make_float2(1.f, 0.f);
+  }
+}
+
+template <int D>
+__device__ __forceinline__ float2 tw16(float2 a, int j) {
+  if (j == 0) return a;
+  if (j == 4) return D > 0 ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
+  const float c = cos16(j), s = D > 0 ? sin16(j) : -sin16(j);
+  return make_float2(a.x * c + a.y * s, a.y * c - a.x * s);
+}
+
+// M-point decimation in frequency: natural input, bit-reversed output
+template <int M, int D>
+__device__ __forceinline__ void dif_reg(float2 (&v)[M]) {
+#pragma unroll
+  for (int span = M / 2; span >= 1; span >>= 1) {
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      if ((i & span) == 0) {
+        const float2 a = v[i], b = v[i + span];
+        v[i] = cadd(a, b);
+        v[i + span] = tw16<D>(csub(a, b), (i & (span - 1)) * (8 / span));
+      }
+    }
+  }
+}
+// M-point decimation in time: bit-reversed input, natural output (the inverse
+// of dif_reg<M, -D> up to the factor M)
+template <int M, int D>
+__device__ __forceinline__ void dit_reg(float2 (&v)[M]) {
+#pragma unroll
+  for (int span = 1; span < M; span <<= 1) {
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      if ((i & span) == 0) {
+        const float2 t = tw16<D>(v[i + span], (i & (span - 1)) * (8 / span));
+        const float2 u = v[i];
+        v[i] = cadd(u, t);
+        v[i + span] = csub(u, t);
+      }
+    }
+  }
+}
+
+// 8-byte asynchronous global->shared copies (no register staging), so a CTA has
+// its whole tile of loads in flight at once
+__device__ __forceinline__ void cp_async8(float2 *smem, const float2 *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+__device__ __forceinline__ float2 shfl_xor2(float2 a, int m) {
+  return make_float2(__shfl_xor_sync(FULL_MASK, a.x, m), __shfl_xor_sync(FULL_MASK, a.y, m));
+}
+
+template <int N>
+__device__ __forceinline__ int lane_bitrev_g(int h) {
+  constexpr int G = Fft<N>::G;
+  constexpr int LG = G == 2 ? 1 : G == 4 ? 2 : G == 8 ? 3 : G == 16 ? 4 : 5;
+  return (int)(__brev((unsigned)h) >> (32 - LG));
+}
+// second-stage twiddles exp(-D 2 pi i h k' / 32) of register i (k' = bitrev(i));
+// with two lanes per column (N = 512) they are constants selected by h
+template <int N, int D>
+__device__ __forceinline__ void stage2_twiddle(float2 (&v)[Fft<N>::M], const float2 *__restrict__ tw, int h) {
+  constexpr int M = Fft<N>::M, G = Fft<N>::G;
+#pragma unroll
+  for (int i = 1; i < M; ++i) {
+    float2 w;
+    if (G == 2) {
+      w = w32(bitrev_c(i, M));
+      if (D < 0) w.y = -w.y;
+      if (h == 0) w = make_float2(1.f, 0.f);
+    } else {
+      w = twd<D>(tw, h * bitrev_c(i, M) * (TW_FULL / 32));
+    }
+    v[i] = cmul(v[i], w);
+  }
+}
+
+__device__ __forceinline__ float2 add_signed(float2 o, float sgn, float2 v) {
+  return make_float2(fmaf(sgn, v.x, o.x), fmaf(sgn, v.y, o.y));
+}
+
+// index of register i of this lane after fft_n2p (and before fft_p2n)
+template <int N>
+__device__ __forceinline__ int out_index(int lane, int i) {
+  constexpr int M = Fft<N>::M, G = Fft<N>::G;
+  const int c = lane / G, h = lane & (G - 1);
+  return c + M * (bitrev_c(i, M) + M * lane_bitrev_g<N>(h));
+}
+
+// N-point DFT of one line held by a warp. Input v[m] = x[lane + 32 m];
+// output v[i] = X[out_index<N>(lane, i)]. D = +1: exp(-2 pi i jk/N); D = -1: the
+// unnormalised inverse. S: this warp's scratch (Fft<N>::SW float2).
+template <int N, int D>
+__device__ __forceinline__ void fft_n2p(float2 (&v)[Fft<N>::M], float2 *S, const float2 *__restrict__ tw, int lane) {
+  constexpr int M = Fft<N>::M, G = Fft<N>::G, RS = Fft<N>::RS;
+  dif_reg<M, D>(v);
+#pragma unroll
+  for (int i = 1; i < M; ++i) v[i] = cmul(v[i], twd<D>(tw + Fft<N>::LANE_TAB, bitrev_c(i, M) * 32 + lane));
+  const int c = lane / G, h = lane & (G - 1);
+  if (M > 1) {
+#pragma unroll
+    for (int i = 0; i < M; ++i) S[bitrev_c(i, M) * RS + lane] = v[i];
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < M; ++j) v[j] = S[c * RS + h + G * j];
+    __syncwarp();
+  }
+  dif_reg<M, D>(v);
+  stage2_twiddle<N, D>(v, tw, h);
+  // radix-2 stages across lanes: lower lane a + b, upper lane (a - b) w
+#pragma unroll
+  for (int span = G / 2; span >= 1; span >>= 1) {
+    const bool upper = (h & span) != 0;
+    const float sgn = upper ? -1.f : 1.f;
+    float2 w = make_float2(1.f, 0.f);
+    if (span > 1 && upper) w = twd<D>(tw, (h & (span - 1)) * (TW_FULL / (2 * span)));
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const float2 t = add_signed(shfl_xor2(v[i], span), sgn, v[i]);
+      v[i] = span > 1 ? cmul(t, w) : t;
+    }
+  }
+}
+
+// The adjoint pipeline: input v[i] = X[out_index<N>(lane, i)], output
+// v[m] = x[lane + 32 m]; fft_p2n<N, -1> inverts fft_n2p<N, +1> up to the factor N.
+template <int N, int D>
+__device__ __forceinline__ void fft_p2n(float2 (&v)[Fft<N>::M], float2 *S, const float2 *__restrict__ tw, int lane) {
+  constexpr int M = Fft<N>::M, G = Fft<N>::G, RS = Fft<N>::RS;
+  const int c = lane / G, h = lane & (G - 1);
+  // radix-2 stages across lanes: the upper lane scales its value by w, then
+  // lower lane a + w b, upper lane a - w b
+#pragma unroll
+  for (int span = 1; span < G; span <<= 1) {
+    const bool upper = (h & span) != 0;
+    const float sgn = upper ? -1.f : 1.f;
+    float2 w = make_float2(1.f, 0.f);
+    if (span > 1 && upper) w = twd<D>(tw, (h & (span - 1)) * (TW_FULL / (2 * span)));
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const float2 z = span > 1 ? cmul(v[i], w) : v[i];
+      v[i] = add_signed(shfl_xor2(z, span), sgn, z);
+    }
+  }
+  stage2_twiddle<N, D>(v, tw, h);
+  dit_reg<M, D>(v);
+  if (M > 1) {
+#pragma unroll
+    for (int j = 0; j < M; ++j) S[c * RS + h + G * j] = v[j];
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < M; ++i) v[i] = S[bitrev_c(i, M) * RS + lane];
+    __syncwarp();
+  }
+#pragma unroll
+  for (int i = 1; i < M; ++i) v[i] = cmul(v[i], twd<D>(tw + Fft<N>::LANE_TAB, bitrev_c(i, M) * 32 + lane));
+  dit_reg<M, D>(v);
+}
+
+// ---- pass 1: real-to-half-complex along z ------------------------------------
+// CTA: component c, plane x, 16 consecutive y lines; output rows of 16 y values.
+template <int NZ>
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_z_r2c(const float *__restrict__ f, float2 *__restrict__ A,
+                                                           int nx, int ny, const float2 *__restrict__ tw) {
+  constexpr int H = NZ / 2, M = Fft<H>::M, SW = Fft<H>::SW;
+  extern __shared__ float2 fft_smem[];
+  float2 *T = fft_smem;  // (H + 1) x FFT_TS
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2 *S = fft_smem + (H + 1) * FFT_TS + warp * SW;
+  const int nyt = ny / FFT_TILE;
+  const int yt = blockIdx.x % nyt;
+  const int x = (blockIdx.x / nyt) % nx;
+  const int c = blockIdx.x / (nyt * nx);
+#pragma unroll 1
+  for (int r = 0; r < FFT_TILE / FFT_WARPS; ++r) {
+    const int wy = warp + FFT_WARPS * r;
+    const float2 *line =
+        reinterpret_cast<const float2 *>(f + (((size_t)c * nx + x) * ny + (size_t)yt * FFT_TILE + wy) * NZ);
+    float2 v[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) v[m] = __ldg(line + lane + 32 * m);
+    fft_n2p<H, 1>(v, S, tw, lane);
+#pragma unroll
+    for (int i = 0; i < M; ++i) S[prow<H>(out_index<H>(lane, i))] = v[i];
+    __syncwarp();
+    // X_k = ((Z_k + conj Z_{H-k}) - i W_NZ^k (Z_k - conj Z_{H-k})) / 2
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const int k = lane + 32 * m;
+      const float2 zk = S[prow<H>(k)], zr = S[prow<H>((H - k) & (H - 1))];
+      const float2 d = make_float2(zk.x - zr.x, zk.y + zr.y);
+      const float2 e = cmul(d, twd<1>(tw, k * (TW_FULL / NZ)));
+      T[k * FFT_TS + wy] = make_float2(0.5f * (zk.x + zr.x + e.y), 0.5f * (zk.y - zr.y - e.x));
+    }
+    if (lane == 0) {
+      const float2 z0 = S[0];
+      T[H * FFT_TS + wy] = make_float2(z0.x - z0.y, 0.f);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  float2 *out = A + ((size_t)c * (H + 1) * nx + x) * ny + (size_t)yt * FFT_TILE;
+  const size_t plane = (size_t)nx * ny;
+  for (int idx = threadIdx.x; idx < (H + 1) * FFT_TILE; idx += FFT_THREADS) {
+    const int k = idx / FFT_TILE, j = idx % FFT_TILE;
+    out[(size_t)k * plane + j] = T[k * FFT_TS + j];
+  }
+}
+
+// ---- pass 2: forward y, written transposed -----------------------------------
+// CTA: (c, kz) plane, 16 consecutive x lines; output rows of 16 x values per ky.
+template <int NY>
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_y_fwd(const float2 *__restrict__ A, float2 *__restrict__ B,
+                                                           int nx, const float2 *__restrict__ tw) {
+  constexpr int M = Fft<NY>::M, SW = Fft<NY>::SW;
+  extern __shared__ float2 fft_smem[];
+  float2 *T = fft_smem;  // Fft<NY>::PEXT swizzled rows x FFT_TS
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2 *S = fft_smem + Fft<NY>::PEXT * FFT_TS + warp * SW;
+  const int nxt = nx / FFT_TILE;
+  const int xt = blockIdx.x % nxt;
+  const size_t ckz = blockIdx.x / nxt;
+#pragma unroll 1
+  for (int r = 0; r < FFT_TILE / FFT_WARPS; ++r) {
+    const int wx = warp + FFT_WARPS * r;
+    const float2 *line = A + (ckz * nx + (size_t)xt * FFT_TILE + wx) * NY;
+    float2 v[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) v[m] = __ldg(line + lane + 32 * m);
+    fft_n2p<NY, 1>(v, S, tw, lane);
+#pragma unroll
+    for (int i = 0; i < M; ++i) T[prow<NY>(out_index<NY>(lane, i)) * FFT_TS + wx] = v[i];
+  }
+  __syncthreads();
+  float2 *out = B + ckz * NY * nx + (size_t)xt * FFT_TILE;
+  for (int idx = threadIdx.x; idx < NY * FFT_TILE; idx += FFT_THREADS) {
+    const int ky = idx / FFT_TILE, j = idx % FFT_TILE;
+    out[(size_t)ky * nx + j] = T[prow<NY>(ky) * FFT_TS + j];
+  }
+}
+
+__device__ __forceinline__ float wavenumber_f(int i, int n, float ff) { return (float)((i <= n / 2) ? i : i - n) * ff; }
+
+// ---- pass 3: x lines: forward, projection, inverse ---------------------------------
+// Three warps per (kz, ky), one per component. After the forward transforms each
+// warp leaves its spectrum in its scratch in register order (the same
+// lane/register -> kx map for all three), every warp reads the three values of
+// its modes and keeps its own projected component. Arithmetic of the projection
+// as in flow_solve (FCMfunctions.cpp:668-722): norm = 1/(|q|^2 + 1e-18),
+// u = norm (f - q (q.f) norm) / (Nx Ny Nz); the k = 0 mode is zeroed. The
+// reciprocal is the fast one (2 ulp), well inside the FP32 chain's error.
+constexpr int XP_PAIRS = 2;                    // (kz, ky) lines per CTA
+constexpr int XP_THREADS = 3 * 32 * XP_PAIRS;  // one warp per component and line
+template <int NX>
+__global__ void __launch_bounds__(XP_THREADS) k_fft_x_project(float2 *__restrict__ B, int ny, int nzh,
+                                                              size_t cstride, float ffx, float ffy, float ffz,
+                                                              float inv_total, const float2 *__restrict__ tw) {
+  constexpr int M = Fft<NX>::M, SW = Fft<NX>::SW;
+  __shared__ float2 Sall[3 * XP_PAIRS * SW];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int comp = warp % 3, pl = warp / 3;
+  float2 *S = Sall + warp * SW;
+  const int pair = blockIdx.x * XP_PAIRS + pl;
+  const bool active = pair < nzh * ny;  // warp-uniform; inactive warps still reach the barriers
+  const int kz = pair / ny, ky = pair % ny;
+  float2 *line = B + comp * cstride + (size_t)pair * NX;
+  float2 v[M];
+  if (active) {
+#pragma unroll
+    for (int m = 0; m < M; ++m) v[m] = line[lane + 32 * m];
+    fft_n2p<NX, 1>(v, S, tw, lane);
+#pragma unroll
+    for (int i = 0; i < M; ++i) S[lane + 32 * i] = v[i];
+  }
+  __syncthreads();
+  if (active) {
+    const float2 *S0 = Sall + (3 * pl) * SW, *S1 = S0 + SW, *S2 = S1 + SW;
+    const float q2 = wavenumber_f(ky, ny, ffy), q3 = (float)kz * ffz;
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const int kx = out_index<NX>(lane, i);
+      const float q1 = wavenumber_f(kx, NX, ffx);
+      const float qq = q2 * q2 + q1 * q1 + 1e-18f;
+      const float norm = __fdividef(1.0f, qq + q3 * q3);
+      const float2 a = S0[lane + 32 * i], b = S1[lane + 32 * i], d = S2[lane + 32 * i];
+      const float kfr = (q1 * a.x + q2 * b.x + q3 * d.x) * norm;
+      const float kfi = (q1 * a.y + q2 * b.y + q3 * d.y) * norm;
+      const float qc = comp == 0 ? q1 : comp == 1 ? q2 : q3;
+      const float sc = (kx | ky | kz) == 0 ? 0.f : norm * inv_total;
+      v[i] = make_float2(sc * (v[i].x - qc * kfr), sc * (v[i].y - qc * kfi));
+    }
+  }
+  __syncthreads();
+  if (active) {
+    fft_p2n<NX, -1>(v, S, tw, lane);
+#pragma unroll
+    for (int m = 0; m < M; ++m) line[lane + 32 * m] = v[m];
+  }
+}
+
+// ---- pass 4: inverse y, read transposed ---------------------------------------
+template <int NY>
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_y_inv(const float2 *__restrict__ B, float2 *__restrict__ A,
+                                                           int nx, const float2 *__restrict__ tw) {
+  constexpr int M = Fft<NY>::M, SW = Fft<NY>::SW;
+  extern __shared__ float2 fft_smem[];
+  float2 *T = fft_smem;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2 *S = fft_smem + NY * FFT_TS + warp * SW;
+  const int nxt = nx / FFT_TILE;
+  const int xt = blockIdx.x % nxt;
+  const size_t ckz = blockIdx.x / nxt;
+  const float2 *in = B + ckz * NY * nx + (size_t)xt * FFT_TILE;
+  for (int idx = threadIdx.x; idx < NY * FFT_TILE; idx += FFT_THREADS) {
+    const int ky = idx / FFT_TILE, j = idx % FFT_TILE;
+    cp_async8(T + ky * FFT_TS + j, in + (size_t)ky * nx + j);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+#pragma unroll 1
+  for (int r = 0; r < FFT_TILE / FFT_WARPS; ++r) {
+    const int wx = warp + FFT_WARPS * r;
+    float2 v[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) v[m] = T[(lane + 32 * m) * FFT_TS + wx];
+    fft_n2p<NY, -1>(v, S, tw, lane);
+    float2 *line = A + (ckz * nx + (size_t)xt * FFT_TILE + wx) * NY;
+#pragma unroll
+    for (int i = 0; i < M; ++i) line[out_index<NY>(lane, i)] = v[i];
+  }
+}
+
+// ---- pass 5: half-complex-to-real along z ---------------------------------------
+// Z'_k = (X_k + conj X_{H-k}) + i W_NZ^{-k} (X_k - conj X_{H-k}), k < H, with the
+// imaginary parts of X_0 and X_H dropped; z = unnormalised inverse H-point DFT
+// of Z'; u[2n] = Re z_n, u[2n+1] = Im z_n.
+template <int NZ>
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_z_c2r(const float2 *__restrict__ A, float *__restrict__ u,
+                                                           int nx, int ny, const float2 *__restrict__ tw) {
+  constexpr int H = NZ / 2, M = Fft<H>::M, SW = Fft<H>::SW;
+  extern __shared__ float2 fft_smem[];
+  float2 *T = fft_smem;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2 *S = fft_smem + (H + 1) * FFT_TS + warp * SW;
+  const int nyt = ny / FFT_TILE;
+  const int yt = blockIdx.x % nyt;
+  const int x = (blockIdx.x / nyt) % nx;
+  const int c = blockIdx.x / (nyt * nx);
+  const float2 *in = A + ((size_t)c * (H + 1) * nx + x) * ny + (size_t)yt * FFT_TILE;
+  const size_t plane = (size_t)nx * ny;
+  for (int idx = threadIdx.x; idx < (H + 1) * FFT_TILE; idx += FFT_THREADS) {
+    const int k = idx / FFT_TILE, j = idx % FFT_TILE;
+    cp_async8(T + k * FFT_TS + j, in + (size_t)k * plane + j);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+#pragma unroll 1
+  for (int r = 0; r < FFT_TILE / FFT_WARPS; ++r) {
+    const int wy = warp + FFT_WARPS * r;
+    float2 v[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const int k = lane + 32 * m;
+      float2 xk = T[k * FFT_TS + wy], xr = T[(H - k) * FFT_TS + wy];
+      if (k == 0) xk.y = xr.y = 0.f;
+      const float2 d = make_float2(xk.x - xr.x, xk.y + xr.y);
+      const float2 e = cmul(d, twd<-1>(tw, k * (TW_FULL / NZ)));
+      v[m] = make_float2(xk.x + xr.x - e.y, xk.y - xr.y + e.x);
+    }
+    fft_n2p<H, -1>(v, S, tw, lane);
+    float2 *line = reinterpret_cast<float2 *>(u + (((size_t)c * nx + x) * ny + (size_t)yt * FFT_TILE + wy) * NZ);
+#pragma unroll
+    for (int i = 0; i < M; ++i) line[out_index<H>(lane, i)] = v[i];
+  }
+}
+
+template <int NZ>
+constexpr size_t smem_z() { return sizeof(float2) * ((NZ / 2 + 1) * FFT_TS + FFT_WARPS * Fft<NZ / 2>::SW); }
+template <int NY>
+constexpr size_t smem_y() { return sizeof(float2) * (Fft<NY>::PEXT * FFT_TS + FFT_WARPS * Fft<NY>::SW); }
+
+bool pow2_in(int n, int lo, int hi) { return n >= lo && n <= hi && (n & (n - 1)) == 0; }
+
+template <int NZ>
+fs_status z_attr() {
+  FS_CUDA(cudaFuncSetAttribute(k_fft_z_r2c<NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z<NZ>()));
+  FS_CUDA(cudaFuncSetAttribute(k_fft_z_c2r<NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z<NZ>()));
+  return FS_OK;
+}
+template <int NY>
+fs_status y_attr() {
+  FS_CUDA(cudaFuncSetAttribute(k_fft_y_fwd<NY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y<NY>()));
+  FS_CUDA(cudaFuncSetAttribute(k_fft_y_inv<NY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y<NY>()));
+  return FS_OK;
+}
+
+template <int NZ>
+fs_status z_fwd(fs_ctx *c, const float *f, float2 *A, const float2 *tw) {
+  k_fft_z_r2c<NZ><<<3 * c->nx * (c->ny / FFT_TILE), FFT_THREADS, smem_z<NZ>(), c->stream>>>(f, A, c->nx, c->ny, tw);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+template <int NZ>
+fs_status z_inv(fs_ctx *c, const float2 *A, float *u, const float2 *tw) {
+  k_fft_z_c2r<NZ><<<3 * c->nx * (c->ny / FFT_TILE), FFT_THREADS, smem_z<NZ>(), c->stream>>>(A, u, c->nx, c->ny, tw);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+template <int NY>
+fs_status y_fwd(fs_ctx *c, const float2 *A, float2 *B, const float2 *tw) {
+  k_fft_y_fwd<NY><<<3 * c->nzh * (c->nx / FFT_TILE), FFT_THREADS, smem_y<NY>(), c->stream>>>(A, B, c->nx, tw);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+template <int NY>
+fs_status y_inv(fs_ctx *c, const float2 *B, float2 *A, const float2 *tw) {
+  k_fft_y_inv<NY><<<3 * c->nzh * (c->nx / FFT_TILE), FFT_THREADS, smem_y<NY>(), c->stream>>>(B, A, c->nx, tw);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+template <int NX>
+fs_status x_project(fs_ctx *c, float2 *B, const float2 *tw) {
+  const double TwoPI = 2. * FS_PI;
+  const float ffx = (float)(TwoPI / (c->nx * c->p.dx)), ffy = (float)(TwoPI / (c->ny * c->p.dx)),
+              ffz = (float)(TwoPI / (c->nz * c->p.dx));
+  // 1 / (Nx Ny Nz) is a power of two here, so the product equals the reference's quotient
+  const float inv_total = (float)(1.0 / ((double)c->nx * (double)c->ny * (double)c->nz));
+  const int pairs = c->nzh * c->ny;
+  const size_t cstride = (size_t)c->nzh * c->ny * c->nx;
+  k_fft_x_project<NX><<<fs_blocks(pairs, XP_PAIRS), XP_THREADS, 0, c->stream>>>(B, c->ny, c->nzh, cstride, ffx, ffy,
+                                                                                ffz, inv_total, tw);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+#define FS_FFT_SWITCH(n, fn, ...)                    \
+  switch (n) {                                       \
+    case 32: FS_TRY(fn<32>(__VA_ARGS__)); break;     \
+    case 64: FS_TRY(fn<64>(__VA_ARGS__)); break;     \
+    case 128: FS_TRY(fn<128>(__VA_ARGS__)); break;   \
+    case 256: FS_TRY(fn<256>(__VA_ARGS__)); break;   \
+    case 512: FS_TRY(fn<512>(__VA_ARGS__)); break;   \
+    default: return FS_ERR_INVALID_ARG;              \
+  }
+#define FS_FFT_SWITCH_Z(n, fn, ...)                  \
+  switch (n) {                                       \
+    case 64: FS_TRY(fn<64>(__VA_ARGS__)); break;     \
+    case 128: FS_TRY(fn<128>(__VA_ARGS__)); break;   \
+    case 256: FS_TRY(fn<256>(__VA_ARGS__)); break;   \
+    case 512: FS_TRY(fn<512>(__VA_ARGS__)); break;   \
+    default: return FS_ERR_INVALID_ARG;              \
+  }
+
+}  // namespace
+
+bool fft32_supported(const fs_ctx *c) {
+  return pow2_in(c->nx, 32, 512) && pow2_in(c->ny, 32, 512) && pow2_in(c->nz, 64, 512);
+}
+
+fs_status fft32_init(fs_ctx *c) {
+  c->fft_tw = nullptr;
+  if (!fft32_supported(c)) return FS_OK;
+  // [0, 1024): exp(-2 pi i j / 1024); then per N in {32, ..., 512}, at 1024 + N - 32,
+  // the lane table [k2 * 32 + lane] = exp(-2 pi i lane k2 / N), k2 < N / 32.
+  const int ntw = TW_FULL + 512 - 32 + 512;
+  float2 *h = (float2 *)malloc(sizeof(float2) * ntw);
+  if (!h) return FS_ERR_OOM;
+  const double TwoPI = 2. * FS_PI;
+  for (int j = 0; j < TW_FULL; ++j) h[j] = make_float2((float)cos(TwoPI * j / TW_FULL), (float)-sin(TwoPI * j / TW_FULL));
+  for (int n = 32; n <= 512; n <<= 1)
+    for (int k2 = 0; k2 < n / 32; ++k2)
+      for (int l = 0; l < 32; ++l) {
+        const long long j = (long long)l * k2;
+        h[TW_FULL + n - 32 + k2 * 32 + l] = make_float2((float)cos(TwoPI * j / n), (float)-sin(TwoPI * j / n));
+      }
+  cudaError_t e = cudaMalloc(&c->fft_tw, sizeof(float2) * ntw);
+  if (e == cudaSuccess) e = cudaMemcpy(c->fft_tw, h, sizeof(float2) * ntw, cudaMemcpyHostToDevice);
+  free(h);
+  if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? FS_ERR_OOM : FS_ERR_CUDA;
+  c->bytes += sizeof(float2) * ntw;
+  FS_FFT_SWITCH_Z(c->nz, z_attr);
+  FS_FFT_SWITCH(c->ny, y_attr);
+  return FS_OK;
+}
+
+void fft32_free(fs_ctx *c) {
+  cudaFree(c->fft_tw);
+  c->fft_tw = nullptr;
+}
+
+// u = Stokes solve of f, both FP32 [3][nx][ny][nz] in c->grid_real (in place);
+// c->grid_cplx holds the two half spectra A and B.
+fs_status fft32_flow_solve(fs_ctx *c) {
+  const float2 *tw = (const float2 *)c->fft_tw;
+  float *g = (float *)c->grid_real;
+  float2 *A = (float2 *)c->grid_cplx;
+  float2 *B = A + (size_t)3 * c->nzh * c->nx * c->ny;
+  {
+    ProfScope ps(c, FS_STAGE_FFT_FWD);
+    FS_FFT_SWITCH_Z(c->nz, z_fwd, c, g, A, tw);
+    FS_FFT_SWITCH(c->ny, y_fwd, c, A, B, tw);
+  }
+  {
+    ProfScope ps(c, FS_STAGE_PROJECT);
+    FS_FFT_SWITCH(c->nx, x_project, c, B, tw);
+  }
+  {
+    ProfScope ps(c, FS_STAGE_FFT_INV);
+    FS_FFT_SWITCH(c->ny, y_inv, c, B, A, tw);
+    FS_FFT_SWITCH_Z(c->nz, z_inv, c, A, g, tw);
+  }
+  return FS_OK;
+}

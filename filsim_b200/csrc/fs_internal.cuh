@@ -61,6 +61,7 @@ struct fs_ctx {
   fs_sort bins;
   int *bead_sw;        // per bead, wrapped Gaussian stencil start per axis
   int last_grid_prec;  // precision of the grids from the last solve (-1: none)
+  void *fft_tw;        // FP32 transform twiddle tables (null: grid not handled by fs_fft.cu, cuFFT is used)
 
   // collision cells
   int M[3], ncell;
@@ -149,6 +150,11 @@ fs_status fcm_mobility(fs_ctx *c, const double *Y, const double *F, const double
 fs_status fcm_friction(fs_ctx *c, const double *F, const double *T, double *V, double *W, int np);
 fs_status fcm_flow_solve_only(fs_ctx *c, const double *f, double *u);
 fs_status fcm_spread_only(fs_ctx *c, const double *Y, const double *F, const double *T, int np, double *f);
+
+bool fft32_supported(const fs_ctx *c);
+fs_status fft32_init(fs_ctx *c);
+void fft32_free(fs_ctx *c);
+fs_status fft32_flow_solve(fs_ctx *c);
 
 fs_status cells_init(fs_ctx *c);
 void cells_free(fs_ctx *c);

@@ -91,6 +91,65 @@ def test_sinusoidal_forcing_known_answer():
     assert np.abs(u[:2]).max() < 1e-12
 
 
+def numpy_flow_solve(p, f):
+    """flow_solve (FCMfunctions.cpp:648-736) in numpy FP64: unnormalised transforms,
+    norm = 1/(|q|^2 + 1e-18), u = norm (f - q (q.f) norm) / N, k = 0 zeroed, the
+    Nyquist index taking +k; irfftn drops the imaginary parts of the kz = 0 and
+    kz = Nz/2 coefficients as the reference's real inverse transform does."""
+    nx, ny, nz = f.shape[1:]
+    fh = np.fft.rfftn(f, axes=(1, 2, 3))
+
+    def wn(n):
+        i = np.arange(n)
+        return np.where(i <= n // 2, i, i - n) * 2 * np.pi / (n * p.dx)
+
+    q1 = wn(nx)[:, None, None]
+    q2 = wn(ny)[None, :, None]
+    q3 = (np.arange(nz // 2 + 1) * 2 * np.pi / (nz * p.dx))[None, None, :]
+    qq = q2 * q2 + q1 * q1 + 1e-18
+    norm = 1.0 / (qq + q3 * q3)
+    kdotf = (q1 * fh[0] + q2 * fh[1] + q3 * fh[2]) * norm
+    total = nx * ny * nz
+    u = np.stack([norm * (fh[0] - q1 * kdotf), norm * (fh[1] - q2 * kdotf), norm * (fh[2] - q3 * kdotf)]) / total
+    u[:, 0, 0, 0] = 0
+    return np.fft.irfftn(u, s=(nx, ny, nz), axes=(1, 2, 3)) * total
+
+
+def flow_input(kind, dims, seed):
+    """White noise, or fields whose spectrum lies only in the kz = 0, kz = Nz/2 or
+    kx = Nx/2 planes (the modes the real inverse transform treats specially)."""
+    nx, ny, nz = dims
+    rng = np.random.default_rng(seed)
+    if kind == "noise":
+        return rng.standard_normal((3, nx, ny, nz))
+    if kind == "kz0":
+        return np.repeat(rng.standard_normal((3, nx, ny, 1)), nz, axis=3)
+    if kind == "kzN":
+        return rng.standard_normal((3, nx, ny, 1)) * ((-1.0) ** np.arange(nz))[None, None, None, :]
+    if kind == "kxN":
+        return rng.standard_normal((3, 1, ny, nz)) * ((-1.0) ** np.arange(nx))[None, :, None, None]
+    raise ValueError(kind)
+
+
+@pytest.mark.parametrize("dims", [(64, 64, 64), (32, 128, 64), (128, 32, 256), (32, 32, 32)])
+@pytest.mark.parametrize("kind", ["noise", "kz0", "kzN", "kxN"])
+def test_flow_solve_fp64_and_fp32_against_numpy(dims, kind):
+    """Power-of-two grids with nz >= 64 run the FP32 five-pass transform
+    (fs_fft.cu); 32^3 runs cuFFT. FP64 within 1e-12, FP32 within 1e-5 of the
+    largest velocity component."""
+    p = params_for(dims)
+    f = flow_input(kind, dims, seed=sum(dims) + len(kind))
+    ref = numpy_flow_solve(p, f)
+    ctx = Context(p, max_beads=1)
+    fcm = Fcm(ctx, 1)
+    u64 = fcm.flow_solve(f).cpu().numpy()
+    ctx.set_precision(abi.FS_PREC_FP32)
+    u32 = fcm.flow_solve(f).cpu().numpy()
+    ctx.close()
+    assert rel_err(u64, ref) < 1e-12
+    assert rel_err(u32, ref) < FP32_REL
+
+
 def test_fp32_within_1e5_of_fp64(case64):
     p, s, Y, F, T = case64
     V64, W64 = gpu_mobility(p, Y, F, T)
