@@ -23,7 +23,9 @@ STATUS_NAMES = {
     0: "FS_OK", 1: "FS_ERR_INVALID_ARG", 2: "FS_ERR_NO_DEVICE", 3: "FS_ERR_CUDA", 4: "FS_ERR_CUFFT",
     5: "FS_ERR_OOM", 6: "FS_ERR_NOT_CONVERGED", 7: "FS_ERR_NONFINITE", 8: "FS_ERR_CAPACITY", 9: "FS_ERR_STATE",
 }
+FS_ERR_INVALID_ARG = 1
 FS_ERR_NOT_CONVERGED = 6
+FS_ERR_STATE = 9
 FS_PREC_FP64 = 0
 FS_PREC_FP32 = 1
 
@@ -47,11 +49,12 @@ class FsDiag(ctypes.Structure):
         ("last_nt", c_int), ("last_iters", c_int), ("total_iters", c_longlong), ("mobility_solves", c_longlong),
         ("not_converged_steps", c_int), ("nonfinite", c_int), ("explosion", c_int), ("reserved", c_int),
         ("min_dist2", c_double), ("last_max_abs_err", c_double),
+        ("learned_filaments", c_longlong), ("fallback_filaments", c_longlong),
     ]
 
 
 STAGES = ["spread", "fft_fwd", "project", "fft_inv", "interp", "link", "barrier", "forces", "jacobian",
-          "error_check", "broyden", "update", "friction"]
+          "error_check", "broyden", "update", "friction", "learn"]
 FS_STAGE_COUNT = 16
 
 
@@ -168,6 +171,20 @@ def _declare(L):
                                                  c_void_p, c_void_p, c_void_p, c_void_p]),
         "fs_profile_enable": (c_int, [c_void_p, c_int]),
         "fs_profile_get": (c_int, [c_void_p, ctypes.POINTER(FsProfile)]),
+        "fs_mlp_create": (c_int, [c_void_p, c_int, c_int, c_int, ctypes.c_ulonglong]),
+        "fs_mlp_dims": (c_int, [c_void_p, c_void_p]),
+        "fs_mlp_set_normalization": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+        "fs_mlp_get_params": (c_int, [c_void_p, c_void_p, c_size_t]),
+        "fs_mlp_set_params": (c_int, [c_void_p, c_void_p, c_size_t]),
+        "fs_mlp_forward": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
+        "fs_mlp_gradients": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_size_t, c_void_p]),
+        "fs_mlp_train_step": (c_int, [c_void_p, c_void_p, c_void_p, c_int, ctypes.c_float, c_void_p]),
+        "fs_learn_features": (c_int, [c_void_p, c_void_p]),
+        "fs_learn_record": (c_int, [c_void_p, c_int]),
+        "fs_learn_targets": (c_int, [c_void_p, c_void_p]),
+        "fs_set_warm_start": (c_int, [c_void_p, c_int]),
+        "fs_learn_override": (c_int, [c_void_p, c_void_p]),
+        "fs_gemm_bf16": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

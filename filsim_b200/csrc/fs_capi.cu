@@ -113,11 +113,17 @@ fs_status barrier_and_mobility(fs_ctx *c, int nt) {
 // one implicit step (main.cpp:334-707)
 fs_status step_implicit(fs_ctx *c, int nt, int *iters_out) {
   FS_TRY(fil_initial_guess(c));
+  const bool learned = learn_active(c) && nt > c->p.initial_friction_steps;
+  if (learned || learn_recording(c)) FS_TRY(learn_save_guess(c));
   FS_TRY(fil_forces(c, nt));
   FS_TRY(fil_jacobian_build(c, nt));
   FS_TRY(cells_link(c, c->Xs, c->np));
-  FS_TRY(barrier_and_mobility(c, nt));
-  FS_TRY(fil_error_check(c, c->V, c->W, c->err, nt));
+  if (learned) {
+    FS_TRY(learn_warm_start(c, nt, barrier_and_mobility));
+  } else {
+    FS_TRY(barrier_and_mobility(c, nt));
+    FS_TRY(fil_error_check(c, c->V, c->W, c->err, nt));
+  }
   FS_TRY(read_flags(c));
   if (c->flags_h[FLAG_PIVOT]) return FS_ERR_NONFINITE;
   int check = c->flags_h[FLAG_CHECK];
@@ -134,6 +140,8 @@ fs_status step_implicit(fs_ctx *c, int nt, int *iters_out) {
     FS_TRY(read_flags(c));
     check = c->flags_h[FLAG_CHECK];
   }
+  if (learn_recording(c)) FS_TRY(learn_capture_targets(c, iter));
+  FS_TRY(learn_end_step(c));
   FS_TRY(fil_step(c, nt));
   c->diag.last_nt = nt;
   c->diag.last_iters = iter;
@@ -264,6 +272,7 @@ fs_status fs_destroy(fs_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->prof.created)
     for (int i = 0; i < 2 * FS_PROF_SLOTS; ++i) cudaEventDestroy(c->prof.ev[i]);
+  mlp_free(c);
   fcm_free(c);
   cells_free(c);
   free_state(c);
@@ -420,6 +429,7 @@ fs_status fs_state_upload(fs_ctx *c, const fs_host_state *s) {
   cudaStream_t st = c->stream;
   const bool same_layout = c->have_state && c->fil_start_h && c->nfil == nf && c->np == np &&
                            memcmp(c->fil_start_h, s->fil_start, sizeof(int) * (nf + 1)) == 0;
+  FS_TRY(learn_before_upload(c, same_layout));
   if (!same_layout) FS_TRY(upload_layout(c, s));
   struct F3 {
     double *d;
@@ -439,6 +449,7 @@ fs_status fs_state_upload(fs_ctx *c, const fs_host_state *s) {
     if (lams_h[i]) FS_CUDA(cudaMemcpyAsync(lams[i], lams_h[i], nl3, cudaMemcpyHostToDevice, st));
     else FS_CUDA(cudaMemsetAsync(lams[i], 0, nl3, st));
   }
+  FS_TRY(learn_after_upload(c));
   if (s->kap) FS_CUDA(cudaMemcpyAsync(c->kap, s->kap, sizeof(double) * nf, cudaMemcpyHostToDevice, st));
   if (s->c) FS_CUDA(cudaMemcpyAsync(c->cc, s->c, sizeof(double) * nf, cudaMemcpyHostToDevice, st));
   if (!same_layout || !s->kap || !s->c) {

@@ -993,7 +993,7 @@ fs_status fil_broyden_apply(fs_ctx *c, const double *b, double *x, int iter) {
   k_schur_apply<<<c->nfil, 128, 0, c->stream>>>(c->fil_start, c->soff, c->aoff, c->Sinv, c->aux, b, x, c->Cmat,
                                                  c->dots, iter, n6, c->p.dt, 0.5 * c->p.dl);
   FS_LAUNCH_CHECK();
-  return FS_OK;
+  return learn_diag_apply(c, b, x);  // learned initial inverse-Jacobian diagonal, when on
 }
 
 // main.cpp:641-663 with the current err/newerr/upd: history column `iter`

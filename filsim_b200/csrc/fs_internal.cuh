@@ -94,6 +94,7 @@ struct fs_ctx {
   unsigned long long *maxerr_bits;
   fs_diag diag;
   size_t bytes;
+  struct fs_mlp *mlp;    // learned warm start (fs_mlp.cu); null until fs_mlp_create
 };
 
 #define FS_CUDA(call)                                                         \
@@ -174,6 +175,18 @@ fs_status fil_broyden_update(fs_ctx *c, int iter);
 fs_status fil_state_update(fs_ctx *c, const double *upd);
 fs_status fil_step(fs_ctx *c, int nt);
 fs_status fil_max_abs_err(fs_ctx *c, const double *err, double *out_h);
+
+// ---- learned warm start (fs_mlp.cu) ----
+bool learn_active(const fs_ctx *c);
+bool learn_recording(const fs_ctx *c);
+fs_status learn_save_guess(fs_ctx *c);
+fs_status learn_warm_start(fs_ctx *c, int nt, fs_status (*solve)(fs_ctx *, int));
+fs_status learn_diag_apply(fs_ctx *c, const double *b, double *x);
+fs_status learn_capture_targets(fs_ctx *c, int iters);
+fs_status learn_end_step(fs_ctx *c);
+fs_status learn_before_upload(fs_ctx *c, bool same_layout);
+fs_status learn_after_upload(fs_ctx *c);
+void mlp_free(fs_ctx *c);
 
 // ordered bit patterns for atomicMin/Max on non-negative doubles
 __device__ __forceinline__ unsigned long long fs_dbits(double x) { return (unsigned long long)__double_as_longlong(x); }

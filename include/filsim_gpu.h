@@ -99,6 +99,8 @@ typedef struct fs_diag {
   int reserved;
   double min_dist2;             /* last collision-barrier minimum squared distance */
   double last_max_abs_err;      /* max |Err| at the end of the last step */
+  long long learned_filaments;  /* filament-steps started from the learned iterate */
+  long long fallback_filaments; /* filament-steps put back to the plain start (worse first residual) */
 } fs_diag;
 
 /*
@@ -271,18 +273,19 @@ fs_status fs_get_diag(fs_ctx *ctx, fs_diag *d_h);
  * printed per step by profilers.cpp:46-65). */
 enum {
   FS_STAGE_SPREAD = 0,      /* binning + force distribution (FCMGauss + FCMForcD) */
-  FS_STAGE_FFT_FWD = 1,     /* cuFFT R2C x3 (FCMFFTFw) */
-  FS_STAGE_PROJECT = 2,     /* Stokes projection (FCMFlowS) */
-  FS_STAGE_FFT_INV = 3,     /* cuFFT C2R x3 (FCMFFTBk) */
+  FS_STAGE_FFT_FWD = 1,     /* forward real transform x3 (FCMFFTFw); FP32 power-of-two grids: z and y passes */
+  FS_STAGE_PROJECT = 2,     /* Stokes projection (FCMFlowS); FP32 power-of-two grids: with the x transforms */
+  FS_STAGE_FFT_INV = 3,     /* inverse real transform x3 (FCMFFTBk); FP32 power-of-two grids: y and z passes */
   FS_STAGE_INTERP = 4,      /* U and Omega interpolation (FCMParVR) */
   FS_STAGE_LINK = 5,        /* cell binning (ColBarri, link) */
   FS_STAGE_BARRIER = 6,     /* pair forces (ColBarri) */
   FS_STAGE_FORCES = 7,      /* unRobotArmify + filament forces + assign (Assign F) */
-  FS_STAGE_JACOBIAN = 8,    /* J build + LU (Bld Jinv) */
+  FS_STAGE_JACOBIAN = 8,    /* J build + Schur-complement inverse (Bld Jinv) */
   FS_STAGE_ERROR_CHECK = 9, /* ErrorChk */
   FS_STAGE_BROYDEN = 10,    /* J0^-1 applications + history (Slv Jinv) */
   FS_STAGE_UPDATE = 11,     /* state update + step */
   FS_STAGE_FRICTION = 12,   /* Stokes-drag mobility */
+  FS_STAGE_LEARN = 13,      /* warm-start features + MLP inference, and MLP training steps */
   FS_STAGE_COUNT = 16
 };
 typedef struct fs_profile {
@@ -296,6 +299,67 @@ fs_status fs_profile_get(fs_ctx *ctx, fs_profile *out_h);
 /* Number of kernels this library has launched in the process (cuFFT's own
  * kernels are not counted). */
 unsigned long long fs_kernel_launches(void);
+
+/* ---- learned Broyden warm start (no reference counterpart) --------------------
+ *
+ * A per-filament MLP (features -> 3 x [Linear(hidden) + SiLU] -> Linear) that
+ * predicts, for filaments of nw beads, the update from the extrapolated guess
+ * of Filament::initialGuess (Filament.hpp:227-237) to the converged state of
+ * the step, in the Broyden unknowns' layout [X0 (3) | U (3 nw) | lambda
+ * (3 nw - 3)], and a correction to the diagonal of the initial inverse
+ * Jacobian (6 nw). Trained and evaluated by this library's BF16 tensor-core
+ * GEMMs (FP32 accumulation, FP32 master weights, Adam).
+ *
+ * Features per filament (n_features = 19 nw + 9 (nw - 1) + 1), for bead i:
+ * X_i - centroid (3), q_i (4), (X_i - Xt_i)/dt (3), U_i/dt (3), Ut_i/dt (3),
+ * (X_i - 2 Xt_i + Xtt_i)/dt^2 (3; Xtt: positions two steps back, kept by the
+ * library from the steps it ran, zero after an upload that changes X or Xt);
+ * for link j: lambda_j, lambda1_j, lambda2_j (9); then log K_B. Targets per filament
+ * (n_targets = 12 nw): converged - guess (6 nw), then diag(sum_i C_i D_i^T) of
+ * the Broyden history at convergence (6 nw). Inputs and targets are normalised
+ * with the statistics given to fs_mlp_set_normalization. */
+
+/* Creates (or replaces) the context's model for filaments of nw beads; hidden is
+ * a multiple of 128; batch_capacity rows per GEMM pass (rounded up to 128);
+ * weights uniform in +-1/sqrt(fan_in) from seed. */
+fs_status fs_mlp_create(fs_ctx *ctx, int nw, int hidden, int batch_capacity, unsigned long long seed);
+/* dims_h[8] = {nw, n_features, k_in (padded), hidden, n_targets, k_out (padded),
+ * batch capacity, parameter count}. */
+fs_status fs_mlp_dims(const fs_ctx *ctx, int *dims_h);
+fs_status fs_mlp_set_normalization(fs_ctx *ctx, const float *in_mean_h, const float *in_std_h,
+                                   const float *out_mean_h, const float *out_std_h);
+/* Flat FP32 parameters [W1 b1 W2 b2 W3 b3 W4 b4], W_l row-major [out x in] with the
+ * padded widths. Setting them resets the Adam moments. */
+fs_status fs_mlp_get_params(fs_ctx *ctx, float *params_h, size_t count);
+fs_status fs_mlp_set_params(fs_ctx *ctx, const float *params_h, size_t count);
+/* Denormalised predictions [n x n_targets] of raw features [n x n_features] (device). */
+fs_status fs_mlp_forward(fs_ctx *ctx, const float *features_d, int n, float *out_d);
+/* Gradients of the mean-square loss of one batch (n <= capacity rows), in the
+ * flat parameter layout, without an update. */
+fs_status fs_mlp_gradients(fs_ctx *ctx, const float *features_d, const float *targets_d, int n, float *grads_h,
+                           size_t count, double *loss_h);
+/* One Adam step (beta 0.9, 0.999, eps 1e-8) on a batch; loss_h may be NULL (no sync). */
+fs_status fs_mlp_train_step(fs_ctx *ctx, const float *features_d, const float *targets_d, int n, float lr,
+                            double *loss_h);
+/* Features [nfil x n_features] of the uploaded state (filaments of another
+ * length get zeros). */
+fs_status fs_learn_features(fs_ctx *ctx, float *features_d);
+/* While on, every implicit step keeps its targets for fs_learn_targets. */
+fs_status fs_learn_record(fs_ctx *ctx, int on);
+/* Targets [nfil x n_targets] of the last recorded step. */
+fs_status fs_learn_targets(fs_ctx *ctx, float *targets_d);
+/* The next warm-started step uses pred_d [nfil x n_targets] (denormalised, as
+ * fs_mlp_forward returns) instead of the network's output: for checking the
+ * start and fallback logic with known predictions. */
+fs_status fs_learn_override(fs_ctx *ctx, const float *pred_d);
+/* 0: the reference's start; 1: learned iterate; 2: learned iterate and
+ * inverse-Jacobian diagonal. A filament whose first residual (max |Err| over its
+ * rows) from the learned start exceeds that of the plain start is put back to
+ * the plain start. */
+fs_status fs_set_warm_start(fs_ctx *ctx, int mode);
+/* D[M x N] (FP32) = A[M x K] B[N x K]^T with BF16 operands on the tensor cores;
+ * M, N multiples of 128, K of 64. */
+fs_status fs_gemm_bf16(fs_ctx *ctx, const void *A_d, const void *B_d, float *D_d, int M, int N, int K);
 
 /* ---- synthetic inputs (host only, no GPU needed) ------------------------------ */
 
