@@ -59,6 +59,10 @@ struct fs_mlp {
 namespace {
 
 constexpr int RND = 128;
+// normalised inputs and targets are clipped to +-NORM_CLIP standard deviations:
+// the targets are heavy-tailed (collision events) and the mean-square loss
+// would otherwise be set by a few outliers
+constexpr float NORM_CLIP = 10.f;
 int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
 // ---- small kernels ---------------------------------------------------------------
@@ -121,7 +125,8 @@ __global__ void k_prep_input(const float *__restrict__ raw, int n, int cap, int 
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (size_t)cap * k_in) return;
   const int row = (int)(idx % cap), col = (int)(idx / cap);
-  const float v = (row < n && col < nfeat) ? (raw[(size_t)row * nfeat + col] - mu[col]) / sd[col] : 0.f;
+  float v = (row < n && col < nfeat) ? (raw[(size_t)row * nfeat + col] - mu[col]) / sd[col] : 0.f;
+  v = isfinite(v) ? fminf(fmaxf(v, -NORM_CLIP), NORM_CLIP) : 0.f;
   const fs_bf16 h = __float2bfloat16_rn(v);
   X[(size_t)row * k_in + col] = h;
   if (XT) XT[idx] = h;
@@ -132,7 +137,8 @@ __global__ void k_prep_target(const float *__restrict__ raw, int n, int cap, int
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (size_t)cap * k_out) return;
   const int row = (int)(idx / k_out), col = (int)(idx % k_out);
-  T[idx] = (row < n && col < ntgt) ? (raw[(size_t)row * ntgt + col] - mu[col]) / sd[col] : 0.f;
+  const float v = (row < n && col < ntgt) ? (raw[(size_t)row * ntgt + col] - mu[col]) / sd[col] : 0.f;
+  T[idx] = isfinite(v) ? fminf(fmaxf(v, -NORM_CLIP), NORM_CLIP) : 0.f;
 }
 
 // mean-square loss over the valid rows and targets; dY = d loss / d Y in BF16 and transposed
@@ -177,7 +183,7 @@ __global__ void k_adam(float *__restrict__ P, const float *__restrict__ G, float
                        fs_bf16 *__restrict__ Pb, fs_bf16 *__restrict__ PTb) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const float g = G[i];
+  const float g = isfinite(G[i]) ? G[i] : 0.f;
   const float mi = b1 * m[i] + (1.f - b1) * g, vi = b2 * v[i] + (1.f - b2) * g * g;
   m[i] = mi;
   v[i] = vi;

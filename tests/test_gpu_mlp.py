@@ -61,10 +61,11 @@ def _model_case(ctx, n=200, seed=0):
     norm = (rng.normal(size=m.n_features).astype(np.float32), rng.uniform(0.5, 4, m.n_features).astype(np.float32),
             rng.normal(size=m.n_targets).astype(np.float32), rng.uniform(0.5, 2, m.n_targets).astype(np.float32))
     m.set_normalization(*norm)
+    # the kernels clip normalised values to +-10 standard deviations
     x = np.zeros((m.capacity, m.k_in), np.float32)
-    x[:n, :m.n_features] = (feats - norm[0]) / norm[1]
+    x[:n, :m.n_features] = np.clip((feats - norm[0]) / norm[1], -10, 10)
     t = np.zeros((m.capacity, m.k_out), np.float32)
-    t[:n, :m.n_targets] = (tgts - norm[2]) / norm[3]
+    t[:n, :m.n_targets] = np.clip((tgts - norm[2]) / norm[3], -10, 10)
     return m, feats, tgts, norm, x, t
 
 
