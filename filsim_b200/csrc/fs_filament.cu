@@ -8,8 +8,8 @@
 //                        applyExternalForcesTorques (Filament.hpp:271-402), one thread per bead
 //                        adding its links' terms in the reference's order
 //   k_jacobian_schur     buildApproximateJacobian with BlockC/D/E/F (Filament.hpp:803-1120) reduced
-//                        to the 3Nw x 3Nw Schur complement of its constraint block, inverted in
-//                        shared memory (one CTA per filament)
+//                        to the 3Nw x 3Nw Schur complement of its constraint block (one CTA per
+//                        filament); k_schur_gj inverts it in shared memory
 //   k_error_check        ErrorCheckFCM + dexpinv (MobilityConstraints.cpp:109-143, 447-770)
 //   k_schur_apply        filamentJsolver::solve (FilamentJacobianSolver.hpp:49-73): J0^-1 b from
 //                        the Schur inverse, then the bad-Broyden history corrections
@@ -437,8 +437,9 @@ __device__ void blockE_row(int k, int nw, const double *qs, const double *Us, co
 //         [ 0  E  F' ]    E  = BlockE,       F' = BlockF/dt (block bidiagonal)
 // Eliminating lambda = D'^-1 (b1 - C u) leaves S u = b2 - F' D'^-1 b1 with
 // S = E - F' D'^-1 C (3nw x 3nw). k_jacobian_schur builds S in shared memory and
-// inverts it (Gauss-Jordan, partial pivoting); k_schur_apply then applies J^-1
-// exactly, with the reference's 1/dt scaling of the lambda rows (:864).
+// stores it; k_schur_gj inverts it (Gauss-Jordan, partial pivoting) in a lean
+// kernel with more CTAs per SM; k_schur_apply then applies J^-1 exactly, with the
+// reference's 1/dt scaling of the lambda rows (:864).
 //
 // Per-filament auxiliary data (aux, nw >= 2): d[nw-1], e[nw-1] (D' blocks),
 // Fd[nw-1][9] = F'(k,k), Fl[nw-1][9] = F'(k+1,k), t[nw][3] tangents, pcoef.
@@ -458,10 +459,6 @@ __global__ void __launch_bounds__(256) k_jacobian_schur(
     double *__restrict__ Sinv_all, double *__restrict__ aux_all, int nt, FilConsts k, double a, double ah,
     int *__restrict__ flags) {
   extern __shared__ double S[];  // 3nw x 3nw, row-major
-  __shared__ int perm[3 * FS_MAX_NW];
-  __shared__ double fcol[3 * FS_MAX_NW];
-  __shared__ int s_piv;
-  __shared__ double s_inv;
   const int f = blockIdx.x;
   const int b0 = fil_start[f], nw = fil_start[f + 1] - b0, l0 = b0 - f;
   if (nw < 2) return;  // J0 is the identity
@@ -545,7 +542,35 @@ __global__ void __launch_bounds__(256) k_jacobian_schur(
     }
   }
   __syncthreads();
-  // Gauss-Jordan inversion in place with partial pivoting (first maximum wins)
+  double *Sout = Sinv_all + soff[f];
+  for (int e = tid; e < m * m; e += nthr) Sout[e] = S[e];
+}
+
+// Inverse of S (k_jacobian_schur's output, in place) by Gauss-Jordan with partial
+// pivoting (the first maximum wins); one CTA per filament with S in shared memory.
+__global__ void __launch_bounds__(384) k_schur_gj(const int *__restrict__ fil_start,
+                                                  const long long *__restrict__ soff, double *__restrict__ Sinv_all,
+                                                  int *__restrict__ flags) {
+  extern __shared__ double S[];
+  __shared__ int perm[3 * FS_MAX_NW];
+  __shared__ double fcol[3 * FS_MAX_NW];
+  __shared__ int colsrc[3 * FS_MAX_NW];
+  __shared__ int s_piv;
+  __shared__ double s_inv, s_diag;
+  const int f = blockIdx.x;
+  const int nw = fil_start[f + 1] - fil_start[f];
+  if (nw < 2) return;
+  const int m = 3 * nw;
+  const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  double *Sg = Sinv_all + soff[f];
+  for (int e = tid; e < m * m; e += nthr) S[e] = Sg[e];
+  __syncthreads();
+  // Gauss-Jordan inversion in place with partial pivoting (first maximum wins).
+  // Thread (g, c) owns column c for rows g, g + G, ...; per pivot: search (warp 0),
+  // swap + scale of the pivot row and a copy of column kc, elimination.
+  const int G = nthr / m;
+  const bool act = tid < G * m;
+  const int cj = tid % m, g0 = tid / m;
   for (int kc = 0; kc < m; ++kc) {
     if (warp == 0) {
       double best = -1.0;
@@ -561,47 +586,49 @@ __global__ void __launch_bounds__(256) k_jacobian_schur(
       }
       if (lane == 0) {
         s_piv = bi;
+        s_inv = 1.0 / S[bi * m + kc];
+        s_diag = S[kc * m + kc];
         perm[kc] = bi;
         if (!(best > 0.0)) atomicOr(&flags[FLAG_PIVOT], 1);
       }
     }
     __syncthreads();
     const int p = s_piv;
-    if (p != kc)
-      for (int c = tid; c < m; c += nthr) {
-        double t = S[kc * m + c];
-        S[kc * m + c] = S[p * m + c];
-        S[p * m + c] = t;
-      }
-    __syncthreads();
-    if (tid == 0) {
-      s_inv = 1.0 / S[kc * m + kc];
-      S[kc * m + kc] = 1.0;
+    const double inv = s_inv;
+    if (act && g0 == 0) {
+      const double a = S[kc * m + cj], b = S[p * m + cj];
+      if (p != kc) S[p * m + cj] = a;
+      S[kc * m + cj] = (cj == kc) ? inv : b * inv;  // in place: the pivot column turns into inv
     }
+    for (int r = tid; r < m; r += nthr) fcol[r] = (r == p && p != kc) ? s_diag : (r == kc ? 0.0 : S[r * m + kc]);
     __syncthreads();
-    for (int c = tid; c < m; c += nthr) S[kc * m + c] *= s_inv;
-    for (int r = tid; r < m; r += nthr) fcol[r] = S[r * m + kc];
-    __syncthreads();
-    for (int e = tid; e < m * m; e += nthr) {
-      const int r = e / m, c = e - r * m;
-      if (r == kc) continue;
-      const double base = (c == kc) ? 0.0 : S[e];
-      S[e] = base - fcol[r] * S[kc * m + c];
+    if (act) {
+      const double prow = S[kc * m + cj];
+      for (int r = g0; r < m; r += G) {
+        if (r == kc) continue;
+        const double base = (cj == kc) ? 0.0 : S[r * m + cj];
+        S[r * m + cj] = base - fcol[r] * prow;
+      }
     }
     __syncthreads();
   }
-  for (int kc = m - 1; kc >= 0; --kc) {  // undo the row interchanges on the columns
-    const int p = perm[kc];
-    if (p != kc)
-      for (int r = tid; r < m; r += nthr) {
-        double t = S[r * m + kc];
-        S[r * m + kc] = S[r * m + p];
-        S[r * m + p] = t;
+  // undo the row interchanges on the columns: column c of the inverse is column colsrc[c]
+  if (tid == 0) {
+    for (int c = 0; c < m; ++c) colsrc[c] = c;
+    for (int kc = m - 1; kc >= 0; --kc) {
+      const int p = perm[kc];
+      if (p != kc) {
+        const int t = colsrc[kc];
+        colsrc[kc] = colsrc[p];
+        colsrc[p] = t;
       }
-    __syncthreads();
+    }
   }
-  double *Sinv = Sinv_all + soff[f];
-  for (int e = tid; e < m * m; e += nthr) Sinv[e] = S[e];
+  __syncthreads();
+  for (int e = tid; e < m * m; e += nthr) {
+    const int r = e / m, c = e - r * m;
+    Sg[e] = S[r * m + colsrc[c]];
+  }
 }
 
 // x = J0^-1 b for one filament (shared-memory vectors; 128 threads)
@@ -941,6 +968,8 @@ fs_status fil_jacobian_build(fs_ctx *c, int nt) {
                                                       c->soff, c->aoff, c->Sinv, c->aux, nt, k, c->p.a, c->p.ah,
                                                       c->flags);
   FS_LAUNCH_CHECK();
+  k_schur_gj<<<c->nfil, 384, smem, c->stream>>>(c->fil_start, c->soff, c->Sinv, c->flags);
+  FS_LAUNCH_CHECK();
   return FS_OK;
 }
 
@@ -948,6 +977,7 @@ fs_status fil_jacobian_prepare(fs_ctx *c) {
   if (c->max_nw > FS_MAX_NW) return FS_ERR_INVALID_ARG;
   const size_t smem = sizeof(double) * 9 * (size_t)c->max_nw * c->max_nw;
   FS_CUDA(cudaFuncSetAttribute(k_jacobian_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  FS_CUDA(cudaFuncSetAttribute(k_schur_gj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   return FS_OK;
 }
 
