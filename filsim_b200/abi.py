@@ -183,6 +183,7 @@ def _declare(L):
         "fs_learn_record": (c_int, [c_void_p, c_int]),
         "fs_learn_targets": (c_int, [c_void_p, c_void_p]),
         "fs_set_warm_start": (c_int, [c_void_p, c_int]),
+        "fs_set_graph_mode": (c_int, [c_void_p, c_int]),
         "fs_learn_override": (c_int, [c_void_p, c_void_p]),
         "fs_gemm_bf16": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int]),
     }

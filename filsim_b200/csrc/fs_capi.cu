@@ -110,6 +110,12 @@ fs_status barrier_and_mobility(fs_ctx *c, int nt) {
   return FS_OK;
 }
 
+}  // namespace
+
+fs_status step_barrier_mobility(fs_ctx *c, int nt) { return barrier_and_mobility(c, nt); }
+
+namespace {
+
 // one implicit step (main.cpp:334-707)
 fs_status step_implicit(fs_ctx *c, int nt, int *iters_out) {
   FS_TRY(fil_initial_guess(c));
@@ -272,6 +278,7 @@ fs_status fs_destroy(fs_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->prof.created)
     for (int i = 0; i < 2 * FS_PROF_SLOTS; ++i) cudaEventDestroy(c->prof.ev[i]);
+  graph_free(c);
   mlp_free(c);
   fcm_free(c);
   cells_free(c);
@@ -430,7 +437,10 @@ fs_status fs_state_upload(fs_ctx *c, const fs_host_state *s) {
   const bool same_layout = c->have_state && c->fil_start_h && c->nfil == nf && c->np == np &&
                            memcmp(c->fil_start_h, s->fil_start, sizeof(int) * (nf + 1)) == 0;
   FS_TRY(learn_before_upload(c, same_layout));
-  if (!same_layout) FS_TRY(upload_layout(c, s));
+  if (!same_layout) {
+    graph_invalidate(c);
+    FS_TRY(upload_layout(c, s));
+  }
   struct F3 {
     double *d;
     const double *h;
@@ -612,11 +622,26 @@ static fs_status run_one(fs_ctx *c, int nt, int *iters_h) {
   return c->diag.not_converged_steps > before ? FS_ERR_NOT_CONVERGED : FS_OK;
 }
 
+static bool use_graph(const fs_ctx *c, int nt) {
+  return c->graph_mode && graph_steady(c, nt) && !learn_active(c) && !learn_recording(c);
+}
+
 fs_status fs_step_implicit(fs_ctx *c, int nt, int *iters_h) {
   if (!c) return FS_ERR_INVALID_ARG;
   if (!c->have_state) return FS_ERR_STATE;
   memset(&c->diag, 0, sizeof c->diag);
+  if (use_graph(c, nt)) {
+    FS_TRY(graph_launch_step(c, nt));
+    return graph_flush(c, iters_h);
+  }
   return run_one(c, nt, iters_h);
+}
+
+fs_status fs_set_graph_mode(fs_ctx *c, int on) {
+  if (!c) return FS_ERR_INVALID_ARG;
+  c->graph_mode = on ? 1 : 0;
+  if (!on) graph_invalidate(c);
+  return FS_OK;
 }
 
 fs_status fs_run_steps(fs_ctx *c, int nt_start, int nsteps, int *iters_h) {
@@ -624,12 +649,28 @@ fs_status fs_run_steps(fs_ctx *c, int nt_start, int nsteps, int *iters_h) {
   if (!c->have_state) return FS_ERR_STATE;
   memset(&c->diag, 0, sizeof c->diag);
   fs_status worst = FS_OK;
-  for (int k = 0; k < nsteps; ++k) {
+  int k = 0;
+  while (k < nsteps) {
+    if (use_graph(c, nt_start + k)) {
+      // a run of graph launches, one synchronisation at its end
+      const int k0 = k;
+      int n = 0;
+      while (k < nsteps && n < 4096 && use_graph(c, nt_start + k)) {
+        FS_TRY(graph_launch_step(c, nt_start + k));
+        ++k;
+        ++n;
+      }
+      fs_status s = graph_flush(c, iters_h ? iters_h + k0 : nullptr);
+      if (s != FS_OK && s != FS_ERR_NOT_CONVERGED) return s;
+      if (s != FS_OK) worst = s;
+      continue;
+    }
     int it = 0;
     fs_status s = run_one(c, nt_start + k, &it);
     if (iters_h) iters_h[k] = it;
     if (s != FS_OK && s != FS_ERR_NOT_CONVERGED) return s;
     if (s != FS_OK) worst = s;
+    ++k;
   }
   return worst;
 }

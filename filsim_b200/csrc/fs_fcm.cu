@@ -629,6 +629,15 @@ void fcm_free(fs_ctx *c) {
   c->bead_sw = nullptr;
 }
 
+fs_status fcm_set_stream(fs_ctx *c, cudaStream_t st) {
+  const int prec = c->precision;
+  if (prec == FS_PREC_FP32 && c->fft_tw) return FS_OK;  // the warp FFT uses no cuFFT plan
+  FS_TRY(ensure_plans(c, prec));
+  if (cufftSetStream(c->plan_fwd[prec], st) != CUFFT_SUCCESS) return FS_ERR_CUFFT;
+  if (cufftSetStream(c->plan_inv[prec], st) != CUFFT_SUCCESS) return FS_ERR_CUFFT;
+  return FS_OK;
+}
+
 fs_status fcm_mobility(fs_ctx *c, const double *Y, const double *F, const double *T, double *V, double *W, int np) {
   if (c->precision == FS_PREC_FP32) return mobility_t<float>(c, Y, F, T, V, W, np);
   return mobility_t<double>(c, Y, F, T, V, W, np);

@@ -708,7 +708,8 @@ __global__ void __launch_bounds__(128) k_schur_apply(const int *__restrict__ fil
                                                      const double *__restrict__ Sinv_all,
                                                      const double *__restrict__ aux_all, const double *__restrict__ b,
                                                      double *__restrict__ x, const double *__restrict__ C,
-                                                     const double *__restrict__ dots, int iter, size_t n6, double dt,
+                                                     const double *__restrict__ dots, int iter,
+                                                     const int *__restrict__ iter_d, size_t n6, double dt,
                                                      double fac) {
   __shared__ double bb[6 * FS_MAX_NW], xs[6 * FS_MAX_NW], y[3 * FS_MAX_NW], w[3 * FS_MAX_NW];
   const int f = blockIdx.x;
@@ -722,9 +723,10 @@ __global__ void __launch_bounds__(128) k_schur_apply(const int *__restrict__ fil
   } else {
     schur_apply_one(nw, Sinv_all + soff[f], aux_all + aoff[f], bb, xs, y, w, dt, fac);
   }
+  const int ncol = iter_d ? *iter_d : iter;
   for (int r = tid; r < n; r += nthr) {
     double v = xs[r];
-    for (int i = 0; i < iter; ++i) v += C[(size_t)i * n6 + s0 + r] * dots[i];
+    for (int i = 0; i < ncol; ++i) v += C[(size_t)i * n6 + s0 + r] * dots[i];
     x[s0 + r] = v;
   }
 }
@@ -792,31 +794,37 @@ __global__ void k_error_check(int np, const int *__restrict__ fil_id, const int 
 #define RED_THREADS 256
 #define RED_BLOCKS 296
 
-// partial dot products D_i . b, i < iter: grid (RED_BLOCKS, iter)
+// partial dot products D_i . b for i < iter (iter_d ? *iter_d : iter): each of the
+// RED_BLOCKS blocks sums a fixed strided slice of every column, so the partials
+// (and the fixed-order final sums) do not depend on how many columns there are
 __global__ void __launch_bounds__(RED_THREADS) k_dots(const double *__restrict__ D, const double *__restrict__ b,
-                                                       size_t n6, double *__restrict__ partial) {
+                                                       size_t n6, int iter, const int *__restrict__ iter_d,
+                                                       double *__restrict__ partial) {
   __shared__ double sh[RED_THREADS / 32];
-  const int i = blockIdx.y;
-  const double *d = D + (size_t)i * n6;
-  double acc = 0.0;
-  for (size_t k = (size_t)blockIdx.x * RED_THREADS + threadIdx.x; k < n6; k += (size_t)gridDim.x * RED_THREADS)
-    acc += d[k] * b[k];
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w = 0; w < RED_THREADS / 32; ++w) s += sh[w];
-    partial[(size_t)i * gridDim.x + blockIdx.x] = s;
+  const int ncol = iter_d ? *iter_d : iter;
+  for (int i = 0; i < ncol; ++i) {
+    const double *d = D + (size_t)i * n6;
+    double acc = 0.0;
+    for (size_t k = (size_t)blockIdx.x * RED_THREADS + threadIdx.x; k < n6; k += (size_t)gridDim.x * RED_THREADS)
+      acc += d[k] * b[k];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < RED_THREADS / 32; ++w) s += sh[w];
+      partial[(size_t)i * gridDim.x + blockIdx.x] = s;
+    }
+    __syncthreads();
   }
 }
 
 // fixed-order final sums: one warp per output
 __global__ void k_reduce_rows(const double *__restrict__ partial, int nparts, int nrows, double *__restrict__ out,
-                              int do_sqrt) {
+                              int do_sqrt, const int *__restrict__ nrows_d) {
   const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (row >= nrows) return;
+  if (row >= (nrows_d ? *nrows_d : nrows)) return;
   double acc = 0.0;
   for (int p = lane; p < nparts; p += 32) acc += partial[(size_t)row * nparts + p];
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -845,11 +853,16 @@ __global__ void __launch_bounds__(RED_THREADS) k_diff_sq(const double *__restric
 }
 
 // C_iter = -tmp/|dE| - upd/|dE|, D_iter = dE/|dE| (main.cpp:657-661)
+// column iter (iter_d ? *iter_d : iter) of the history
 __global__ void k_broyden_cols(const double *__restrict__ tmp, const double *__restrict__ upd,
                                const double *__restrict__ dE, const double *__restrict__ nrm, size_t n6,
-                               double *__restrict__ Ccol, double *__restrict__ Dcol) {
+                               double *__restrict__ Cmat, double *__restrict__ Dmat, int iter,
+                               const int *__restrict__ iter_d) {
   size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n6) return;
+  const size_t col = (size_t)(iter_d ? *iter_d : iter) * n6;
+  double *__restrict__ Ccol = Cmat + col;
+  double *__restrict__ Dcol = Dmat + col;
   const double n = nrm[0];
   double t = tmp[k] * (-1. / n);
   t -= upd[k] / n;
@@ -1009,38 +1022,38 @@ fs_status fil_error_check(fs_ctx *c, const double *V, const double *W, double *e
   return FS_OK;
 }
 
-fs_status fil_broyden_apply(fs_ctx *c, const double *b, double *x, int iter) {
+// iter_d (graph capture): the history length is read on the device
+fs_status fil_broyden_apply(fs_ctx *c, const double *b, double *x, int iter, const int *iter_d) {
   if (!c->have_state) return FS_ERR_STATE;
   ProfScope ps(c, FS_STAGE_BROYDEN);
   const size_t n6 = (size_t)6 * c->np;
-  if (iter > 0) {
-    dim3 g(RED_BLOCKS, iter);
-    k_dots<<<g, RED_THREADS, 0, c->stream>>>(c->Dmat, b, n6, c->partials);
+  if (iter > 0 || iter_d) {
+    const int rows = iter_d ? c->p.broyden_maxiter : iter;
+    k_dots<<<RED_BLOCKS, RED_THREADS, 0, c->stream>>>(c->Dmat, b, n6, iter, iter_d, c->partials);
     FS_LAUNCH_CHECK();
-    k_reduce_rows<<<fs_blocks(iter, 8), 256, 0, c->stream>>>(c->partials, RED_BLOCKS, iter, c->dots, 0);
+    k_reduce_rows<<<fs_blocks(rows, 8), 256, 0, c->stream>>>(c->partials, RED_BLOCKS, rows, c->dots, 0, iter_d);
     FS_LAUNCH_CHECK();
   }
   k_schur_apply<<<c->nfil, 128, 0, c->stream>>>(c->fil_start, c->soff, c->aoff, c->Sinv, c->aux, b, x, c->Cmat,
-                                                 c->dots, iter, n6, c->p.dt, 0.5 * c->p.dl);
+                                                 c->dots, iter, iter_d, n6, c->p.dt, 0.5 * c->p.dl);
   FS_LAUNCH_CHECK();
   return learn_diag_apply(c, b, x);  // learned initial inverse-Jacobian diagonal, when on
 }
 
 // main.cpp:641-663 with the current err/newerr/upd: history column `iter`
-fs_status fil_broyden_update(fs_ctx *c, int iter) {
+fs_status fil_broyden_update(fs_ctx *c, int iter, const int *iter_d) {
   const size_t n6 = (size_t)6 * c->np;
   {
     ProfScope ps(c, FS_STAGE_BROYDEN);
     k_diff_sq<<<RED_BLOCKS, RED_THREADS, 0, c->stream>>>(c->newerr, c->err, c->dE, n6, c->partials);
     FS_LAUNCH_CHECK();
-    k_reduce_rows<<<1, 32, 0, c->stream>>>(c->partials, RED_BLOCKS, 1, c->scalars, 1);
+    k_reduce_rows<<<1, 32, 0, c->stream>>>(c->partials, RED_BLOCKS, 1, c->scalars, 1, nullptr);
     FS_LAUNCH_CHECK();
   }
-  FS_TRY(fil_broyden_apply(c, c->dE, c->tmp, iter));
+  FS_TRY(fil_broyden_apply(c, c->dE, c->tmp, iter, iter_d));
   ProfScope ps(c, FS_STAGE_BROYDEN);
   k_broyden_cols<<<fs_blocks((long long)n6, 256), 256, 0, c->stream>>>(c->tmp, c->upd, c->dE, c->scalars, n6,
-                                                                       c->Cmat + (size_t)iter * n6,
-                                                                       c->Dmat + (size_t)iter * n6);
+                                                                       c->Cmat, c->Dmat, iter, iter_d);
   FS_LAUNCH_CHECK();
   return FS_OK;
 }

@@ -95,6 +95,8 @@ struct fs_ctx {
   fs_diag diag;
   size_t bytes;
   struct fs_mlp *mlp;    // learned warm start (fs_mlp.cu); null until fs_mlp_create
+  struct fs_graph *graph;  // captured steady step (fs_graph.cu); null until first used
+  int graph_mode;        // 1: steady steps run as CUDA graphs with the Broyden loop on the device
 };
 
 #define FS_CUDA(call)                                                         \
@@ -170,13 +172,24 @@ fs_status fil_jacobian_prepare(fs_ctx *c);  // after an upload: kernel attribute
 int fil_aux_size(int nw);
 fs_status fil_jacobian_inverse(fs_ctx *c, int f, double *out_d);
 fs_status fil_error_check(fs_ctx *c, const double *V, const double *W, double *err, int nt);
-fs_status fil_broyden_apply(fs_ctx *c, const double *b, double *x, int iter);
-fs_status fil_broyden_update(fs_ctx *c, int iter);
+fs_status fil_broyden_apply(fs_ctx *c, const double *b, double *x, int iter, const int *iter_d = nullptr);
+fs_status fil_broyden_update(fs_ctx *c, int iter, const int *iter_d = nullptr);
 fs_status fil_state_update(fs_ctx *c, const double *upd);
 fs_status fil_step(fs_ctx *c, int nt);
 fs_status fil_max_abs_err(fs_ctx *c, const double *err, double *out_h);
 
+fs_status fcm_set_stream(fs_ctx *c, cudaStream_t st);  // creates the cuFFT plans the precision needs, binds them
+fs_status step_barrier_mobility(fs_ctx *c, int nt);     // collision barrier + FCM (or friction) solve
+
+// ---- graph-captured steps (fs_graph.cu) ----
+bool graph_steady(const fs_ctx *c, int nt);
+fs_status graph_launch_step(fs_ctx *c, int nt);
+fs_status graph_flush(fs_ctx *c, int *iters_h);
+void graph_invalidate(fs_ctx *c);
+void graph_free(fs_ctx *c);
+
 // ---- learned warm start (fs_mlp.cu) ----
+fs_status learn_prepare_capture(fs_ctx *c);
 bool learn_active(const fs_ctx *c);
 bool learn_recording(const fs_ctx *c);
 fs_status learn_save_guess(fs_ctx *c);

@@ -586,6 +586,13 @@ fs_status learn_warm_start(fs_ctx *c, int nt, fs_status (*solve)(fs_ctx *, int))
   return fil_error_check(c, c->V, c->W, c->err, nt);
 }
 
+// before a graph capture: the learn module's per-step work must not allocate
+fs_status learn_prepare_capture(fs_ctx *c) {
+  if (!c->mlp) return FS_OK;
+  if (c->mlp->mode || c->mlp->record) return FS_ERR_STATE;
+  return ensure_step_buffers(c);
+}
+
 fs_status learn_diag_apply(fs_ctx *c, const double *b, double *x) {
   fs_mlp *m = c->mlp;
   if (!m || !m->jdiag_on) return FS_OK;

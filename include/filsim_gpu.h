@@ -265,6 +265,13 @@ fs_status fs_step_implicit(fs_ctx *ctx, int nt, int *iters_h);
  * Broyden iteration count of each step. */
 fs_status fs_run_steps(fs_ctx *ctx, int nt_start, int nsteps, int *iters_h);
 fs_status fs_get_diag(fs_ctx *ctx, fs_diag *d_h);
+/* 1: steps in the steady regime (nt above impl_euler_steps, initial_friction_steps
+ * and lambda_extrap_step) run as one CUDA graph each, with the Broyden loop on
+ * the device (a conditional WHILE node) and one host synchronisation per
+ * fs_run_steps call instead of one per iteration; results are bitwise those of
+ * the host-driven step. Not used while the learned warm start is on or
+ * recording. No reference counterpart. */
+fs_status fs_set_graph_mode(fs_ctx *ctx, int on);
 
 /* ---- stage profiling ---------------------------------------------------------- */
 
