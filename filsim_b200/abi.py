@@ -184,6 +184,9 @@ def _declare(L):
         "fs_learn_targets": (c_int, [c_void_p, c_void_p]),
         "fs_set_warm_start": (c_int, [c_void_p, c_int]),
         "fs_set_graph_mode": (c_int, [c_void_p, c_int]),
+        "fs_batch_create": (c_int, [c_void_p, c_int, ctypes.POINTER(c_void_p)]),
+        "fs_batch_destroy": (c_int, [c_void_p]),
+        "fs_batch_run": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p]),
         "fs_learn_override": (c_int, [c_void_p, c_void_p]),
         "fs_gemm_bf16": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int]),
     }

@@ -15,6 +15,7 @@
 // non-finite / explosion / pivot / capacity flags are kept on the device.
 // The arithmetic and its order are the host-driven step's, so trajectories are
 // bitwise identical.
+#include <vector>
 #include "fs_internal.cuh"
 
 enum { GD_ITER = 0, GD_STEPS, GD_NONFIN, GD_EXPLODE, GD_NOTCONV, GD_PIVOT, GD_CAPACITY, GD_HDR = 8 };
@@ -25,6 +26,7 @@ struct fs_graph {
   cudaStream_t body_stream = nullptr;
   int *dev = nullptr;  // GD_HDR header ints, then the iteration count of each launched step
   int *host = nullptr;  // pinned copy
+  unsigned long long *ts = nullptr;  // per launched step: device clock (ns) at its start and end (batches)
   unsigned long long kpre = 0, kbody = 0;  // kernels per launch outside / inside the loop
   int precision = -1, np = -1, nfil = -1, pending = 0;
 };
@@ -55,6 +57,13 @@ __global__ void k_step_done(int *__restrict__ gd, const int *__restrict__ flags,
   gd[GD_STEPS] = k + 1;
   if (flags[FLAG_CHECK]) gd[GD_NOTCONV] += 1;
   gd[GD_CAPACITY] |= flags[FLAG_CAPACITY];
+}
+
+__global__ void k_stamp(const int *__restrict__ gd, unsigned long long *__restrict__ ts, int which, int slots) {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  const int k = gd[GD_STEPS] - which;  // the end stamp follows k_step_done's increment
+  if (k >= 0 && k < slots) ts[2 * k + which] = t;
 }
 
 // the start, loop and end of one step, captured on c->stream
@@ -134,6 +143,7 @@ void graph_free(fs_ctx *c) {
   if (g->exec) cudaGraphExecDestroy(g->exec);
   if (g->body_stream) cudaStreamDestroy(g->body_stream);
   cudaFree(g->dev);
+  cudaFree(g->ts);
   if (g->host) cudaFreeHost(g->host);
   delete g;
   c->graph = nullptr;
@@ -146,7 +156,9 @@ void graph_invalidate(fs_ctx *c) {
   }
 }
 
-static fs_status graph_build(fs_ctx *c, int nt) {
+// buffers of the graph state, cuFFT plans and learn buffers: everything the
+// captured work touches must exist before a capture
+static fs_status graph_prepare(fs_ctx *c) {
   fs_graph *g = c->graph;
   if (!g) {
     g = new fs_graph();
@@ -154,12 +166,17 @@ static fs_status graph_build(fs_ctx *c, int nt) {
     FS_CUDA(cudaStreamCreateWithFlags(&g->body_stream, cudaStreamNonBlocking));
     FS_CUDA(cudaMalloc(&g->dev, sizeof(int) * (GD_HDR + GRAPH_STEP_SLOTS)));
     FS_CUDA(cudaMallocHost(&g->host, sizeof(int) * (GD_HDR + GRAPH_STEP_SLOTS)));
+    FS_CUDA(cudaMalloc(&g->ts, sizeof(unsigned long long) * 2 * GRAPH_STEP_SLOTS));
     FS_CUDA(cudaMemsetAsync(g->dev, 0, sizeof(int) * GD_HDR, c->stream));
   }
-  graph_invalidate(c);
-  // everything the captured work touches must exist before the capture
   FS_TRY(fcm_set_stream(c, c->stream));
-  FS_TRY(learn_prepare_capture(c));
+  return learn_prepare_capture(c);
+}
+
+static fs_status graph_build(fs_ctx *c, int nt) {
+  FS_TRY(graph_prepare(c));
+  fs_graph *g = c->graph;
+  graph_invalidate(c);
   const bool prof = c->prof.on;
   c->prof.on = false;
   const fs_diag diag = c->diag;  // the capture runs nothing; its host-side counters are undone
@@ -233,3 +250,160 @@ fs_status graph_launch_step(fs_ctx *c, int nt) {
   c->diag.last_nt = nt;
   return FS_OK;
 }
+
+// ---- ensembles: one graph launch advances every box by one step ------------------
+struct fs_batch {
+  int n = 0;
+  fs_ctx **ctx = nullptr;
+  cudaStream_t origin = nullptr;
+  cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+  cudaEvent_t *join = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+static fs_status batch_build(fs_batch *b, int nt) {
+  for (int i = 0; i < b->n; ++i) {
+    fs_ctx *c = b->ctx[i];
+    if (!c->have_state || !graph_steady(c, nt)) return FS_ERR_STATE;
+    FS_TRY(graph_prepare(c));
+    FS_TRY(graph_flush(c, nullptr));
+  }
+  std::vector<fs_diag> diag(b->n);
+  std::vector<bool> prof(b->n);
+  for (int i = 0; i < b->n; ++i) {
+    diag[i] = b->ctx[i]->diag;
+    prof[i] = b->ctx[i]->prof.on;
+    b->ctx[i]->prof.on = false;
+  }
+  FS_CUDA(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal));
+  fs_status st = FS_OK;
+  unsigned long long captured = 0;
+  // every box forks from the same point and joins at the end: the boxes' steps are
+  // independent branches of the graph
+  if (cudaEventRecord(b->fork, b->origin) != cudaSuccess) st = FS_ERR_CUDA;
+  for (int i = 0; i < b->n && st == FS_OK; ++i) {
+    fs_ctx *c = b->ctx[i];
+    fs_graph *g = c->graph;
+    const unsigned long long k0 = __atomic_load_n(&g_fs_kernel_launches, __ATOMIC_RELAXED);
+    if (cudaStreamWaitEvent(c->stream, b->fork, 0) != cudaSuccess) {
+      st = FS_ERR_CUDA;
+      break;
+    }
+    k_stamp<<<1, 1, 0, c->stream>>>(g->dev, g->ts, 0, GRAPH_STEP_SLOTS);
+    __atomic_fetch_add(&g_fs_kernel_launches, 1ull, __ATOMIC_RELAXED);
+    st = capture_step(c, nt, g, nullptr);
+    if (st != FS_OK) break;
+    k_stamp<<<1, 1, 0, c->stream>>>(g->dev, g->ts, 1, GRAPH_STEP_SLOTS);
+    __atomic_fetch_add(&g_fs_kernel_launches, 1ull, __ATOMIC_RELAXED);
+    if (cudaGetLastError() != cudaSuccess || cudaEventRecord(b->join[i], c->stream) != cudaSuccess) st = FS_ERR_CUDA;
+    const unsigned long long kb = __atomic_load_n(&g_fs_kernel_launches, __ATOMIC_RELAXED) - k0;
+    g->kpre = kb - g->kbody;
+    captured += kb;
+  }
+  for (int i = 0; i < b->n && st == FS_OK; ++i)
+    if (cudaStreamWaitEvent(b->origin, b->join[i], 0) != cudaSuccess) st = FS_ERR_CUDA;
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(b->origin, &graph);
+  __atomic_fetch_sub(&g_fs_kernel_launches, captured, __ATOMIC_RELAXED);
+  for (int i = 0; i < b->n; ++i) {
+    b->ctx[i]->diag = diag[i];
+    b->ctx[i]->prof.on = prof[i];
+  }
+  if (st != FS_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return st;
+  }
+  FS_CUDA(e);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  b->exec = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&b->exec, graph, 0);
+  cudaGraphDestroy(graph);
+  FS_CUDA(ei);
+  return FS_OK;
+}
+
+extern "C" {
+
+fs_status fs_batch_create(fs_ctx *const *ctxs, int n, fs_batch **out) {
+  if (!ctxs || n <= 0 || !out) return FS_ERR_INVALID_ARG;
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    if (!ctxs[i]) return FS_ERR_INVALID_ARG;
+    for (int j = 0; j < i; ++j)
+      if (ctxs[j] == ctxs[i] || ctxs[j]->stream == ctxs[i]->stream) return FS_ERR_INVALID_ARG;
+  }
+  fs_batch *b = new fs_batch();
+  b->n = n;
+  b->ctx = new fs_ctx *[n];
+  b->join = new cudaEvent_t[n]();
+  for (int i = 0; i < n; ++i) b->ctx[i] = ctxs[i];
+  fs_status st = FS_OK;
+  if (cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreate(&b->t0) != cudaSuccess || cudaEventCreate(&b->t1) != cudaSuccess)
+    st = FS_ERR_CUDA;
+  for (int i = 0; i < n && st == FS_OK; ++i)
+    if (cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) != cudaSuccess) st = FS_ERR_CUDA;
+  if (st != FS_OK) {
+    fs_batch_destroy(b);
+    return st;
+  }
+  *out = b;
+  return FS_OK;
+}
+
+fs_status fs_batch_destroy(fs_batch *b) {
+  if (!b) return FS_OK;
+  if (b->origin) cudaStreamSynchronize(b->origin);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  for (int i = 0; i < b->n; ++i)
+    if (b->join && b->join[i]) cudaEventDestroy(b->join[i]);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->t0) cudaEventDestroy(b->t0);
+  if (b->t1) cudaEventDestroy(b->t1);
+  if (b->origin) cudaStreamDestroy(b->origin);
+  delete[] b->join;
+  delete[] b->ctx;
+  delete b;
+  return FS_OK;
+}
+
+fs_status fs_batch_run(fs_batch *b, int nt_start, int nsteps, int *iters_h, float *box_ms_h, float *total_ms_h) {
+  if (!b || nsteps < 0 || nsteps > GRAPH_STEP_SLOTS) return FS_ERR_INVALID_ARG;
+  if (nsteps == 0) return FS_OK;
+  if (!b->exec) FS_TRY(batch_build(b, nt_start));
+  for (int i = 0; i < b->n; ++i) {
+    fs_ctx *c = b->ctx[i];
+    if (!graph_steady(c, nt_start)) return FS_ERR_STATE;
+    memset(&c->diag, 0, sizeof c->diag);
+    // the boxes' own streams finish their earlier work before the batch starts
+    FS_CUDA(cudaEventRecord(b->join[i], c->stream));
+    FS_CUDA(cudaStreamWaitEvent(b->origin, b->join[i], 0));
+  }
+  FS_CUDA(cudaEventRecord(b->t0, b->origin));
+  for (int k = 0; k < nsteps; ++k) FS_CUDA(cudaGraphLaunch(b->exec, b->origin));
+  FS_CUDA(cudaEventRecord(b->t1, b->origin));
+  FS_CUDA(cudaStreamSynchronize(b->origin));
+  if (total_ms_h) FS_CUDA(cudaEventElapsedTime(total_ms_h, b->t0, b->t1));
+  fs_status worst = FS_OK;
+  std::vector<int> its(nsteps);
+  std::vector<unsigned long long> ts(2 * (size_t)nsteps);
+  for (int i = 0; i < b->n; ++i) {
+    fs_ctx *c = b->ctx[i];
+    fs_graph *g = c->graph;
+    g->pending = nsteps;
+    if (box_ms_h) {
+      FS_CUDA(cudaMemcpy(ts.data(), g->ts, sizeof(unsigned long long) * 2 * nsteps, cudaMemcpyDeviceToHost));
+      for (int k = 0; k < nsteps; ++k) box_ms_h[(size_t)k * b->n + i] = (float)((ts[2 * k + 1] - ts[2 * k]) * 1e-6);
+    }
+    fs_status s = graph_flush(c, its.data());
+    c->diag.last_nt = nt_start + nsteps - 1;
+    if (iters_h)
+      for (int k = 0; k < nsteps; ++k) iters_h[(size_t)k * b->n + i] = its[k];
+    if (s != FS_OK && s != FS_ERR_NOT_CONVERGED) return s;
+    if (s != FS_OK) worst = s;
+  }
+  return worst;
+}
+
+}  // extern "C"

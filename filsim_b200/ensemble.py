@@ -1,0 +1,93 @@
+"""Ensembles of independent periodic boxes advanced together (fs_batch_*).
+
+Workload ensemble_64: 64 boxes with grids drawn uniformly from {48^3, 64^3, 96^3,
+128^3} and 8-256 filaments of 16 beads each, K_B log-uniform in [0.1, 10],
+gravity (0,0,-1) per bead, dt = 0.05, BDF2. Filament counts are capped at a bead
+volume fraction of 5% (48^3: 12, 64^3: 30, 96^3: 102, 128^3: 243): the uncapped
+draw is not placeable (256 filaments of 16 beads fill 99.8% of a 48^3 box).
+
+Each box is its own context (grid, parameters, suspension, stream). After the
+start-up steps every ensemble step is one CUDA graph launch holding every box's
+captured step, Broyden loops on the device (fs_graph.cu).
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import abi
+from .abi import check, lib
+from .configs import DX, sediment_params
+from .fcm import Context, Simulation
+from .suspension import random_suspension
+
+GRIDS = (48, 64, 96, 128)
+NW = 16
+PHI_MAX = 0.05
+
+
+def filament_cap(npts, nw=NW, phi=PHI_MAX, a=1.0):
+    """Most filaments of nw beads in an npts^3 box at bead volume fraction phi."""
+    L = npts * DX
+    return int(phi * L ** 3 / (nw * 4.0 / 3.0 * math.pi * a ** 3))
+
+
+def make_boxes(seed, nboxes=64, grids=GRIDS, nfil_range=(8, 256), nw=NW, kb_range=(0.1, 10.0),
+               broyden_maxiter=100):
+    """[(npts, params, suspension, K_B)] drawn as the workload states, seeded."""
+    rng = np.random.default_rng(seed)
+    boxes = []
+    for i in range(nboxes):
+        npts = int(rng.choice(grids))
+        nfil = min(int(rng.integers(nfil_range[0], nfil_range[1] + 1)), filament_cap(npts, nw))
+        kb = float(np.exp(rng.uniform(np.log(kb_range[0]), np.log(kb_range[1]))))
+        p = sediment_params(npts, broyden_maxiter=broyden_maxiter)
+        s = random_suspension(p, nfil, nw, seed=seed * 1000 + i, kap=kb)
+        boxes.append((npts, p, s, kb))
+    return boxes
+
+
+class Ensemble:
+    """One context per box, all advanced by fs_batch_run."""
+
+    def __init__(self, boxes, precision=abi.FS_PREC_FP32):
+        self.boxes = boxes
+        self.ctxs, self.sims = [], []
+        for npts, p, s, kb in boxes:
+            c = Context(p, max_beads=s.np, max_filaments=s.nfil)
+            c.set_precision(precision)
+            check(lib().fs_set_graph_mode(c.h, 1), "fs_set_graph_mode")
+            self.ctxs.append(c)
+            self.sims.append(Simulation(c, s))
+        self.n = len(boxes)
+        self.beads = np.array([s.np for _, _, s, _ in boxes])
+        arr = (ctypes.c_void_p * self.n)(*[c.h.value for c in self.ctxs])
+        h = ctypes.c_void_p()
+        check(lib().fs_batch_create(arr, self.n, ctypes.byref(h)), "fs_batch_create")
+        self.h = h
+
+    def startup(self, nsteps):
+        """The start-up steps (implicit Euler, constant/linear tension extrapolation), box by box."""
+        for sim in self.sims:
+            its, st = sim.run_steps(1, nsteps)
+            if st not in (abi.FS_OK, abi.FS_ERR_NOT_CONVERGED):
+                check(st, "fs_run_steps")
+
+    def run(self, nt_start, nsteps):
+        """(iterations [nsteps x n], per-box step ms [nsteps x n], total ms, status)."""
+        its = np.zeros((nsteps, self.n), np.int32)
+        ms = np.zeros((nsteps, self.n), np.float32)
+        tot = ctypes.c_float()
+        st = lib().fs_batch_run(self.h, nt_start, nsteps, its.ctypes.data_as(ctypes.c_void_p),
+                                ms.ctypes.data_as(ctypes.c_void_p), ctypes.byref(tot))
+        if st not in (abi.FS_OK, abi.FS_ERR_NOT_CONVERGED):
+            check(st, "fs_batch_run")
+        return its, ms, tot.value, st
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fs_batch_destroy(self.h)
+            self.h = None
+        for c in self.ctxs:
+            c.close()
+        self.ctxs = []

@@ -273,6 +273,21 @@ fs_status fs_get_diag(fs_ctx *ctx, fs_diag *d_h);
  * recording. No reference counterpart. */
 fs_status fs_set_graph_mode(fs_ctx *ctx, int on);
 
+/* ---- ensembles of independent boxes (no reference counterpart; the reference
+ * runs such sweeps one program at a time, batch_compile.py) ------------------- */
+typedef struct fs_batch fs_batch;
+/* n contexts with distinct streams, each holding its own box (grid, params,
+ * suspension); the batch does not own them. */
+fs_status fs_batch_create(fs_ctx *const *ctxs, int n, fs_batch **out);
+fs_status fs_batch_destroy(fs_batch *b);
+/* nsteps steady-regime steps (nt_start past every box's start-up steps) of every
+ * box. Each ensemble step is one CUDA graph launch holding every box's captured
+ * step on its own stream (fork/join), Broyden loops on the device; one host
+ * synchronisation for the whole call. iters_h, box_ms_h: [nsteps x n] iteration
+ * counts and per-box step device times (may be NULL); total_ms_h: the call's
+ * device time. The graph is captured at the first call. */
+fs_status fs_batch_run(fs_batch *b, int nt_start, int nsteps, int *iters_h, float *box_ms_h, float *total_ms_h);
+
 /* ---- stage profiling ---------------------------------------------------------- */
 
 /* Device time per stage, taken with CUDA events on the context's stream. The
