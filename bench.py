@@ -442,6 +442,7 @@ def run_ensemble(args, rank, world):
     t0 = time.time()
     ens.startup(PREP_STEPS)
     t_start = time.time() - t0
+    tuned = ens.autotune(reps=3)
     nt0 = PREP_STEPS + 1
     ens.run(nt0, W)                                    # captures the ensemble graph, warms up
     launches0 = abi.lib().fs_kernel_launches()
@@ -480,6 +481,9 @@ def run_ensemble(args, rank, world):
                            "max": float(ms.max())},
            "iters_per_step": float(its.mean()), "status": abi.STATUS_NAMES.get(st, st),
            "clocks": clk.summary(), "gpu_launches": int(launches), "graph_launches": K,
+           "autotuned": {str(g): {"spread_beads_per_pass": v[0], "interp_beads_per_cta": v[1],
+                                  "transform": "cuFFT" if v[2] else "warp FFT (or cuFFT if not a power of two)",
+                                  "ms_per_solve": v[3]} for g, v in tuned.items()},
            "sequential_host_driven": {"value": seq_value, "ms_per_ensemble_step": seq_ms / K2, "steps": K2},
            "speedup_vs_sequential": value / seq_value}
     ens.close()

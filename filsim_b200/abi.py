@@ -184,6 +184,8 @@ def _declare(L):
         "fs_learn_targets": (c_int, [c_void_p, c_void_p]),
         "fs_set_warm_start": (c_int, [c_void_p, c_int]),
         "fs_set_graph_mode": (c_int, [c_void_p, c_int]),
+        "fs_autotune": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
+        "fs_set_tuning": (c_int, [c_void_p, c_void_p]),
         "fs_batch_create": (c_int, [c_void_p, c_int, ctypes.POINTER(c_void_p)]),
         "fs_batch_destroy": (c_int, [c_void_p]),
         "fs_batch_run": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p]),

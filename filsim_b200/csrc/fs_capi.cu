@@ -298,6 +298,7 @@ fs_status fs_get_params(const fs_ctx *c, fs_params *p_h) {
 
 fs_status fs_set_precision(fs_ctx *c, int precision) {
   if (!c || (precision != FS_PREC_FP64 && precision != FS_PREC_FP32)) return FS_ERR_INVALID_ARG;
+  if (precision != c->precision) graph_invalidate(c);
   c->precision = precision;
   return FS_OK;
 }

@@ -74,12 +74,13 @@ struct W4 {
   R g, d, r, pad;
 };
 
-template <typename R>
+// CH beads are staged per pass (32 or 64, chosen per grid by fs_autotune)
+template <typename R, int CH>
 struct SpreadStage {
-  W4<R> w[FS_SPREAD_CHUNK][3][FS_TILE];  // weights by tile-local coordinate
-  R f[FS_SPREAD_CHUNK][4];                // force
-  R th[FS_SPREAD_CHUNK][4];               // half torque (GA_setup, :536-547)
-  unsigned mask[FS_SPREAD_CHUNK][3];      // per axis: tile-local coordinates covered
+  W4<R> w[CH][3][FS_TILE];  // weights by tile-local coordinate
+  R f[CH][4];                // force
+  R th[CH][4];               // half torque (GA_setup, :536-547)
+  unsigned mask[CH][3];      // per axis: tile-local coordinates covered
 };
 
 template <typename R>
@@ -111,13 +112,13 @@ __device__ inline double fs_exp<double>(double x) { return exp(x); }
 template <>
 __device__ inline float fs_exp<float>(float x) { return expf(x); }
 
-template <typename R>
+template <typename R, int CH>
 __global__ void __launch_bounds__(FS_SPREAD_THREADS)
     k_spread(const double *__restrict__ Y, const double *__restrict__ F, const double *__restrict__ T,
              const int *__restrict__ bin_start, const int *__restrict__ sorted, const int *__restrict__ bead_sw,
              FcmConsts c, R *__restrict__ fgrid) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  SpreadStage<R> &st = *reinterpret_cast<SpreadStage<R> *>(smem_raw);
+  SpreadStage<R, CH> &st = *reinterpret_cast<SpreadStage<R, CH> *>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int tile = blockIdx.x;
   const int tz = tile % c.nbin[2], ty = (tile / c.nbin[2]) % c.nbin[1], tx = tile / (c.nbin[2] * c.nbin[1]);
@@ -147,8 +148,8 @@ __global__ void __launch_bounds__(FS_SPREAD_THREADS)
   const int px = 2 * bx + (lane & 1), pyo = (lane >> 1) & 1, pz = 8 * bz + (lane >> 2);
   const size_t N = (size_t)c.N[0] * c.N[1] * c.N[2];
   const int ngd = c.ngd;
-  for (int base = 0; base < total; base += FS_SPREAD_CHUNK) {
-    const int nb = min(FS_SPREAD_CHUNK, total - base);
+  for (int base = 0; base < total; base += CH) {
+    const int nb = min(CH, total - base);
     __syncthreads();  // the previous chunk's tables are no longer read
     // stage: one half-warp per (bead slot, axis), lane l -> tile-local coordinate l
     const int nitems = nb * 3 * FS_TILE;
@@ -202,9 +203,9 @@ __global__ void __launch_bounds__(FS_SPREAD_THREADS)
     }
     __syncthreads();
     // beads reaching this warp's column, and per y-block those reaching the block
-    unsigned col[FS_SPREAD_CHUNK / 32], ym[8][FS_SPREAD_CHUNK / 32];
+    unsigned col[CH / 32], ym[8][CH / 32];
 #pragma unroll
-    for (int h = 0; h < FS_SPREAD_CHUNK / 32; ++h) {
+    for (int h = 0; h < CH / 32; ++h) {
       const int s = 32 * h + lane;
       unsigned mx = 0, my = 0, mz = 0;
       if (s < nb) {
@@ -226,7 +227,7 @@ __global__ void __launch_bounds__(FS_SPREAD_THREADS)
       a1.init();
       a2.init();
 #pragma unroll
-      for (int h = 0; h < FS_SPREAD_CHUNK / 32; ++h) {
+      for (int h = 0; h < CH / 32; ++h) {
         unsigned m = col[h] & ym[by][h];
         while (m) {
           const int s = 32 * h + __ffs(m) - 1;
@@ -396,13 +397,14 @@ struct InterpWarp {
   int ind[3][16];
 };
 
-template <typename R>
-__global__ void __launch_bounds__(256) k_interp(const R *__restrict__ u, const double *__restrict__ Y,
-                                                const int *__restrict__ order, const int *__restrict__ bead_sw,
-                                                int np, FcmConsts c, double *__restrict__ V, double *__restrict__ W) {
-  __shared__ InterpWarp<R> sw[8];
+template <typename R, int WPB>
+__global__ void __launch_bounds__(32 * WPB) k_interp(const R *__restrict__ u, const double *__restrict__ Y,
+                                                     const int *__restrict__ order, const int *__restrict__ bead_sw,
+                                                     int np, FcmConsts c, double *__restrict__ V,
+                                                     double *__restrict__ W) {
+  __shared__ InterpWarp<R> sw[WPB];
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-  const int wid = blockIdx.x * 8 + wl;
+  const int wid = blockIdx.x * WPB + wl;
   if (wid >= np) return;
   const int b = order[wid];
   InterpWarp<R> &s = sw[wl];
@@ -525,7 +527,7 @@ fs_status ensure_plans(fs_ctx *c, int prec) {
 template <typename R>
 fs_status flow_solve_t(fs_ctx *c) {
   const int prec = sizeof(R) == 8 ? FS_PREC_FP64 : FS_PREC_FP32;
-  if (prec == FS_PREC_FP32 && c->fft_tw) return fft32_flow_solve(c);
+  if (prec == FS_PREC_FP32 && c->fft_tw && c->tune_fft32 == 0) return fft32_flow_solve(c);
   FS_TRY(ensure_plans(c, prec));
   cufftResult r;
   {
@@ -572,16 +574,24 @@ fs_status mobility_t(fs_ctx *c, const double *Y, const double *F, const double *
       FS_LAUNCH_CHECK();
     }
     FS_TRY(fs_sort_run(&c->bins, np, c->stream));
-    const size_t smem = sizeof(SpreadStage<R>);
-    k_spread<R><<<c->nbins, FS_SPREAD_THREADS, smem, c->stream>>>(Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k,
-                                                              (R *)c->grid_real);
+    if (c->tune_spread_chunk == 32)
+      k_spread<R, 32><<<c->nbins, FS_SPREAD_THREADS, sizeof(SpreadStage<R, 32>), c->stream>>>(
+          Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k, (R *)c->grid_real);
+    else
+      k_spread<R, 64><<<c->nbins, FS_SPREAD_THREADS, sizeof(SpreadStage<R, 64>), c->stream>>>(
+          Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k, (R *)c->grid_real);
     FS_LAUNCH_CHECK();
   }
   FS_TRY(flow_solve_t<R>(c));
   if (np > 0) {
     ProfScope ps(c, FS_STAGE_INTERP);
-    k_interp<R><<<fs_blocks(np, 8), 256, 0, c->stream>>>((const R *)c->grid_real, Y, c->bins.sorted, c->bead_sw, np, k,
-                                                          V, W);
+    const R *ug = (const R *)c->grid_real;
+    if (c->tune_interp_wpb == 4)
+      k_interp<R, 4><<<fs_blocks(np, 4), 128, 0, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V, W);
+    else if (c->tune_interp_wpb == 16)
+      k_interp<R, 16><<<fs_blocks(np, 16), 512, 0, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V, W);
+    else
+      k_interp<R, 8><<<fs_blocks(np, 8), 256, 0, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V, W);
     FS_LAUNCH_CHECK();
   }
   c->last_grid_prec = sizeof(R) == 8 ? FS_PREC_FP64 : FS_PREC_FP32;
@@ -606,10 +616,17 @@ fs_status fcm_init(fs_ctx *c) {
   FS_TRY(fs_sort_alloc(&c->bins, c->nbins, c->max_beads, &c->bytes));
   FS_CUDA(cudaMalloc(&c->bead_sw, sizeof(int) * 3 * (size_t)(c->max_beads > 0 ? c->max_beads : 1)));
   c->bytes += sizeof(int) * 3 * (size_t)c->max_beads;
-  FS_CUDA(cudaFuncSetAttribute(k_spread<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)sizeof(SpreadStage<double>)));
-  FS_CUDA(cudaFuncSetAttribute(k_spread<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)sizeof(SpreadStage<float>)));
+  FS_CUDA(cudaFuncSetAttribute(k_spread<double, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(SpreadStage<double, 64>)));
+  FS_CUDA(cudaFuncSetAttribute(k_spread<float, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(SpreadStage<float, 64>)));
+  FS_CUDA(cudaFuncSetAttribute(k_spread<double, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(SpreadStage<double, 32>)));
+  FS_CUDA(cudaFuncSetAttribute(k_spread<float, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(SpreadStage<float, 32>)));
+  c->tune_spread_chunk = 64;
+  c->tune_interp_wpb = 8;
+  c->tune_fft32 = 0;
   return fft32_init(c);
 }
 
@@ -631,7 +648,7 @@ void fcm_free(fs_ctx *c) {
 
 fs_status fcm_set_stream(fs_ctx *c, cudaStream_t st) {
   const int prec = c->precision;
-  if (prec == FS_PREC_FP32 && c->fft_tw) return FS_OK;  // the warp FFT uses no cuFFT plan
+  if (prec == FS_PREC_FP32 && c->fft_tw && c->tune_fft32 == 0) return FS_OK;  // the warp FFT uses no cuFFT plan
   FS_TRY(ensure_plans(c, prec));
   if (cufftSetStream(c->plan_fwd[prec], st) != CUFFT_SUCCESS) return FS_ERR_CUFFT;
   if (cufftSetStream(c->plan_inv[prec], st) != CUFFT_SUCCESS) return FS_ERR_CUFFT;
@@ -662,7 +679,7 @@ fs_status fcm_spread_only(fs_ctx *c, const double *Y, const double *F, const dou
     FS_LAUNCH_CHECK();
   }
   FS_TRY(fs_sort_run(&c->bins, np, c->stream));
-  k_spread<double><<<c->nbins, FS_SPREAD_THREADS, sizeof(SpreadStage<double>), c->stream>>>(
+  k_spread<double, 64><<<c->nbins, FS_SPREAD_THREADS, sizeof(SpreadStage<double, 64>), c->stream>>>(
       Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k, (double *)c->grid_real);
   FS_LAUNCH_CHECK();
   FS_CUDA(cudaMemcpyAsync(f, c->grid_real, sizeof(double) * 3 * c->N, cudaMemcpyDeviceToDevice, c->stream));

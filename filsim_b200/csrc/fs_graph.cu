@@ -150,6 +150,7 @@ void graph_free(fs_ctx *c) {
 }
 
 void graph_invalidate(fs_ctx *c) {
+  c->graph_gen++;
   if (c->graph && c->graph->exec) {
     cudaGraphExecDestroy(c->graph->exec);
     c->graph->exec = nullptr;
@@ -255,6 +256,7 @@ fs_status graph_launch_step(fs_ctx *c, int nt) {
 struct fs_batch {
   int n = 0;
   fs_ctx **ctx = nullptr;
+  int *gen = nullptr;  // each box's graph_gen when the batch graph was captured
   cudaStream_t origin = nullptr;
   cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
   cudaEvent_t *join = nullptr;
@@ -305,6 +307,7 @@ static fs_status batch_build(fs_batch *b, int nt) {
   cudaGraph_t graph = nullptr;
   const cudaError_t e = cudaStreamEndCapture(b->origin, &graph);
   __atomic_fetch_sub(&g_fs_kernel_launches, captured, __ATOMIC_RELAXED);
+  for (int i = 0; i < b->n; ++i) b->gen[i] = b->ctx[i]->graph_gen;
   for (int i = 0; i < b->n; ++i) {
     b->ctx[i]->diag = diag[i];
     b->ctx[i]->prof.on = prof[i];
@@ -335,6 +338,7 @@ fs_status fs_batch_create(fs_ctx *const *ctxs, int n, fs_batch **out) {
   fs_batch *b = new fs_batch();
   b->n = n;
   b->ctx = new fs_ctx *[n];
+  b->gen = new int[n]();
   b->join = new cudaEvent_t[n]();
   for (int i = 0; i < n; ++i) b->ctx[i] = ctxs[i];
   fs_status st = FS_OK;
@@ -363,6 +367,7 @@ fs_status fs_batch_destroy(fs_batch *b) {
   if (b->t1) cudaEventDestroy(b->t1);
   if (b->origin) cudaStreamDestroy(b->origin);
   delete[] b->join;
+  delete[] b->gen;
   delete[] b->ctx;
   delete b;
   return FS_OK;
@@ -371,7 +376,9 @@ fs_status fs_batch_destroy(fs_batch *b) {
 fs_status fs_batch_run(fs_batch *b, int nt_start, int nsteps, int *iters_h, float *box_ms_h, float *total_ms_h) {
   if (!b || nsteps < 0 || nsteps > GRAPH_STEP_SLOTS) return FS_ERR_INVALID_ARG;
   if (nsteps == 0) return FS_OK;
-  if (!b->exec) FS_TRY(batch_build(b, nt_start));
+  bool stale = !b->exec;
+  for (int i = 0; i < b->n; ++i) stale = stale || b->gen[i] != b->ctx[i]->graph_gen;
+  if (stale) FS_TRY(batch_build(b, nt_start));
   for (int i = 0; i < b->n; ++i) {
     fs_ctx *c = b->ctx[i];
     if (!graph_steady(c, nt_start)) return FS_ERR_STATE;

@@ -61,6 +61,9 @@ struct fs_ctx {
   fs_sort bins;
   int *bead_sw;        // per bead, wrapped Gaussian stencil start per axis
   int last_grid_prec;  // precision of the grids from the last solve (-1: none)
+  int tune_spread_chunk;  // beads staged per spread pass: 32 or 64 (fs_autotune)
+  int tune_interp_wpb;    // beads (warps) per interpolation CTA: 4, 8 or 16
+  int tune_fft32;         // FP32 power-of-two grids: 0 warp FFT (fs_fft.cu), 1 cuFFT
   void *fft_tw;        // FP32 transform twiddle tables (null: grid not handled by fs_fft.cu, cuFFT is used)
 
   // collision cells
@@ -97,6 +100,7 @@ struct fs_ctx {
   struct fs_mlp *mlp;    // learned warm start (fs_mlp.cu); null until fs_mlp_create
   struct fs_graph *graph;  // captured steady step (fs_graph.cu); null until first used
   int graph_mode;        // 1: steady steps run as CUDA graphs with the Broyden loop on the device
+  int graph_gen;         // bumped whenever captured graphs of this context become stale
 };
 
 #define FS_CUDA(call)                                                         \

@@ -273,6 +273,14 @@ fs_status fs_get_diag(fs_ctx *ctx, fs_diag *d_h);
  * recording. No reference counterpart. */
 fs_status fs_set_graph_mode(fs_ctx *ctx, int on);
 
+/* ---- autotuner (no reference counterpart) -----------------------------------
+ * choice = {beads staged per spread pass (32 | 64), beads per interpolation CTA
+ * (4 | 8 | 16), FP32 power-of-two grids: 0 warp FFT | 1 cuFFT}. fs_autotune times
+ * every combination on the uploaded suspension (reps mobility solves each, after
+ * one warm-up) and keeps the fastest; best_ms_h: its time per solve. */
+fs_status fs_autotune(fs_ctx *ctx, int reps, int *choice_h, float *best_ms_h);
+fs_status fs_set_tuning(fs_ctx *ctx, const int *choice_h);
+
 /* ---- ensembles of independent boxes (no reference counterpart; the reference
  * runs such sweeps one program at a time, batch_compile.py) ------------------- */
 typedef struct fs_batch fs_batch;
