@@ -202,55 +202,71 @@ __global__ void __launch_bounds__(FS_SPREAD_THREADS)
       }
     }
     __syncthreads();
-    // beads reaching this warp's column, and per y-block those reaching the block
-    unsigned col[CH / 32], ym[8][CH / 32];
+    // beads reaching this warp's column (its x pair and z octet)
+    unsigned col[CH / 32];
 #pragma unroll
     for (int h = 0; h < CH / 32; ++h) {
       const int s = 32 * h + lane;
-      unsigned mx = 0, my = 0, mz = 0;
+      unsigned mx = 0, mz = 0;
       if (s < nb) {
         mx = st.mask[s][0];
-        my = st.mask[s][1];
         mz = st.mask[s][2];
       }
       col[h] = __ballot_sync(0xffffffffu, ((mx >> (2 * bx)) & 3u) && ((mz >> (8 * bz)) & 0xffu));
-#pragma unroll
-      for (int by = 0; by < 8; ++by) ym[by][h] = __ballot_sync(0xffffffffu, (my >> (2 * by)) & 3u);
     }
     const W4<R> *wxp = &st.w[0][0][px];
     const W4<R> *wzp = &st.w[0][2][pz];
+    // two passes of four y pairs; per bead the x and z factors and the rotlet cross
+    // terms are formed once per pass, each y row then needs one weight load:
+    //   f_a += F_a gx gy gz + (T/2 x grad)_a gdx gdy gdz, regrouped by y
 #pragma unroll 1
-    for (int by = 0; by < 8; ++by) {
-      const int py = 2 * by + pyo;
-      KAcc<R> a0, a1, a2;
-      a0.init();
-      a1.init();
-      a2.init();
+    for (int half = 0; half < 2; ++half) {
+      KAcc<R> acc[4][3];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        acc[q][0].init();
+        acc[q][1].init();
+        acc[q][2].init();
+      }
 #pragma unroll
       for (int h = 0; h < CH / 32; ++h) {
-        unsigned m = col[h] & ym[by][h];
+        unsigned m = col[h];
         while (m) {
           const int s = 32 * h + __ffs(m) - 1;
           m &= m - 1;
-          const W4<R> wx = wxp[s * 3 * FS_TILE], wy = st.w[s][1][py], wz = wzp[s * 3 * FS_TILE];
+          const unsigned my = (st.mask[s][1] >> (8 * half)) & 0xffu;  // y pairs 4 half .. 4 half + 3
+          if (my == 0) continue;
+          const W4<R> wx = wxp[s * 3 * FS_TILE], wz = wzp[s * 3 * FS_TILE];
           const R F0 = st.f[s][0], F1 = st.f[s][1], F2 = st.f[s][2];
           const R h0 = st.th[s][0], h1 = st.th[s][1], h2 = st.th[s][2];
-          const R temp = wx.g * wy.g * wz.g;
-          const R temp2 = wx.d * wy.d * wz.d;
-          a0.add(F0 * temp + (h2 * wy.r - h1 * wz.r) * temp2);
-          a1.add(F1 * temp + (-h2 * wx.r + h0 * wz.r) * temp2);
-          a2.add(F2 * temp + (h1 * wx.r - h0 * wy.r) * temp2);
+          const R gxz = wx.g * wz.g, dxz = wx.d * wz.d;
+          const R f0 = F0 * gxz, f1 = F1 * gxz, f2 = F2 * gxz;
+          const R h2d = h2 * dxz, h0d = h0 * dxz;
+          const R c0 = -h1 * wz.r * dxz, c1 = (-h2 * wx.r + h0 * wz.r) * dxz, c2 = h1 * wx.r * dxz;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            if ((my >> (2 * q)) & 3u) {
+              const W4<R> wy = st.w[s][1][2 * (4 * half + q) + pyo];
+              acc[q][0].add(f0 * wy.g + (h2d * wy.r + c0) * wy.d);
+              acc[q][1].add(f1 * wy.g + c1 * wy.d);
+              acc[q][2].add(f2 * wy.g + (c2 - h0d * wy.r) * wy.d);
+            }
+          }
         }
       }
-      const size_t m0 = ((size_t)(X0[0] + px) * c.N[1] + (X0[1] + py)) * c.N[2] + (X0[2] + pz);
-      if (base == 0) {
-        fgrid[m0] = a0.value();
-        fgrid[N + m0] = a1.value();
-        fgrid[2 * N + m0] = a2.value();
-      } else {  // more candidates than one chunk: add in chunk order
-        fgrid[m0] += a0.value();
-        fgrid[N + m0] += a1.value();
-        fgrid[2 * N + m0] += a2.value();
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int py = 2 * (4 * half + q) + pyo;
+        const size_t m0 = ((size_t)(X0[0] + px) * c.N[1] + (X0[1] + py)) * c.N[2] + (X0[2] + pz);
+        if (base == 0) {
+          fgrid[m0] = acc[q][0].value();
+          fgrid[N + m0] = acc[q][1].value();
+          fgrid[2 * N + m0] = acc[q][2].value();
+        } else {  // more candidates than one chunk: add in chunk order
+          fgrid[m0] += acc[q][0].value();
+          fgrid[N + m0] += acc[q][1].value();
+          fgrid[2 * N + m0] += acc[q][2].value();
+        }
       }
     }
   }
