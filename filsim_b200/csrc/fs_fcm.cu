@@ -14,7 +14,8 @@
 //      reduces U and Omega over the stencil (particle_velocities :740-770,
 //      particle_rotations :774-808) with warp shuffles.
 // FP64 mode follows the reference arithmetic; FP32 mode keeps grids, FFTs and
-// weights in float with Kahan-compensated tile and warp sums.
+// weights in float, with Kahan-compensated spread sums and FP64 accumulation of
+// the interpolation products.
 #include "fs_internal.cuh"
 
 namespace {
@@ -375,56 +376,42 @@ __global__ void k_project_planes(typename Cplx<R>::T *__restrict__ fh, size_t NH
 
 // ---- 6. interpolation -------------------------------------------------------
 template <typename R>
-struct KSum;
-template <>
-struct KSum<double> {
-  double s;
-  __device__ void init() { s = 0.0; }
-  __device__ void add(double v) { s += v; }
-  __device__ double value() const { return s; }
-  __device__ void warp_reduce() {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  }
-};
-template <>
-struct KSum<float> {  // Kahan per lane, TwoSum across lanes
-  float s, c;
-  __device__ void init() { s = 0.f; c = 0.f; }
-  __device__ void add(float v) {
-    float y = v - c;
-    float t = s + y;
-    c = (t - s) - y;
-    s = t;
-  }
-  __device__ double value() const { return (double)s - (double)c; }
-  __device__ void warp_reduce() {
-    double v = (double)s - (double)c;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    s = (float)v;
-    c = (float)((double)s - v);
-  }
-};
-
-template <typename R>
 struct InterpWarp {
   R g[3][16], gd[3][16], r[3][16];
   int ind[3][16];
 };
+template <typename R>
+struct __align__(4 * sizeof(R)) XY4 {
+  R gg, dd, rx, ry;  // gx gy, gdx gdy, rx, ry of one (i, j) of the x-y stencil
+};
+// dynamic shared memory per warp: the per-axis tables, then per (i, j) the
+// products and the grid offset of (x_i, y_j, 0)
+template <typename R>
+__host__ __device__ constexpr size_t interp_xy_offset() {
+  return (sizeof(InterpWarp<R>) + 4 * sizeof(R) - 1) / (4 * sizeof(R)) * (4 * sizeof(R));
+}
+template <typename R>
+__host__ __device__ constexpr size_t interp_warp_bytes(int ngd) {
+  return interp_xy_offset<R>() + (size_t)ngd * ngd * (sizeof(XY4<R>) + sizeof(long long));
+}
 
+// One warp per bead; lanes take the stencil points p = lane + 32 t (z fastest),
+// all 32 lanes busy. FP32 mode multiplies in FP32 and accumulates in FP64 per lane.
 template <typename R, int WPB>
 __global__ void __launch_bounds__(32 * WPB) k_interp(const R *__restrict__ u, const double *__restrict__ Y,
                                                      const int *__restrict__ order, const int *__restrict__ bead_sw,
                                                      int np, FcmConsts c, double *__restrict__ V,
                                                      double *__restrict__ W) {
-  __shared__ InterpWarp<R> sw[WPB];
+  extern __shared__ __align__(32) unsigned char interp_smem[];
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const int wid = blockIdx.x * WPB + wl;
   if (wid >= np) return;
   const int b = order[wid];
-  InterpWarp<R> &s = sw[wl];
-  const int ngd = c.ngd;
+  const int ngd = c.ngd, n2 = ngd * ngd, n3 = n2 * ngd;
+  unsigned char *base = interp_smem + (size_t)wl * interp_warp_bytes<R>(ngd);
+  InterpWarp<R> &s = *reinterpret_cast<InterpWarp<R> *>(base);
+  XY4<R> *xy = reinterpret_cast<XY4<R> *>(base + interp_xy_offset<R>());
+  long long *off = reinterpret_cast<long long *>(xy + n2);
   for (int it = lane; it < 3 * 16; it += 32) {
     const int a = it >> 4, i = it & 15;
     if (i >= ngd) continue;
@@ -446,43 +433,60 @@ __global__ void __launch_bounds__(32 * WPB) k_interp(const R *__restrict__ u, co
     }
   }
   __syncwarp();
+  for (int ij = lane; ij < n2; ij += 32) {
+    const int i = ij / ngd, j = ij - i * ngd;
+    XY4<R> e;
+    e.gg = s.g[0][i] * s.g[1][j];
+    e.dd = s.gd[0][i] * s.gd[1][j];
+    e.rx = s.r[0][i];
+    e.ry = s.r[1][j];
+    xy[ij] = e;
+    off[ij] = ((long long)s.ind[0][i] * c.N[1] + s.ind[1][j]) * c.N[2];
+  }
+  __syncwarp();
   const size_t N = (size_t)c.N[0] * c.N[1] * c.N[2];
   const R *ux = u, *uy = u + N, *uz = u + 2 * N;
-  KSum<R> v0, v1, v2, w0, w1, w2;
-  v0.init(); v1.init(); v2.init(); w0.init(); w1.init(); w2.init();
-  // lane -> (row parity, z index): two stencil rows (i, j) per pass, z contiguous
-  const int k = lane & 15, jsub = lane >> 4;
-  if (k < ngd) {
-    const R gzk = s.g[2][k], dzk = s.gd[2][k], zz = s.r[2][k];
-    const int iz = s.ind[2][k];
-    for (int i = 0; i < ngd; ++i) {
-      const R gx = s.g[0][i], dxv = s.gd[0][i], xx = s.r[0][i];
-      const size_t plane = (size_t)s.ind[0][i] * c.N[1];
-      for (int j = jsub; j < ngd; j += 2) {
-        const size_t m = (plane + s.ind[1][j]) * c.N[2] + iz;
-        const R a0 = ux[m], a1 = uy[m], a2 = uz[m];
-        const R temp = gx * s.g[1][j] * gzk;
-        const R tempd = dxv * s.gd[1][j] * dzk;
-        const R yy = s.r[1][j];
-        v0.add(a0 * temp);
-        v1.add(a1 * temp);
-        v2.add(a2 * temp);
-        w0.add((a2 * yy - a1 * zz) * tempd);
-        w1.add((a0 * zz - a2 * xx) * tempd);
-        w2.add((a1 * xx - a0 * yy) * tempd);
-      }
+  double v0 = 0, v1 = 0, v2 = 0, w0 = 0, w1 = 0, w2 = 0;
+  // point p = ij * ngd + k; a step of 32 points advances (ij, k) by (32 / ngd, 32 % ngd)
+  const int dij = 32 / ngd, dk = 32 - dij * ngd;
+  int ij = lane / ngd, k = lane - ij * ngd;
+  for (int p = lane; p < n3; p += 32) {
+    const XY4<R> e = xy[ij];
+    const long long m = off[ij] + s.ind[2][k];
+    const R temp = e.gg * s.g[2][k];    // (gx gy) gz, the reference's order
+    const R tempd = e.dd * s.gd[2][k];
+    const R zz = s.r[2][k];
+    const R a0 = ux[m], a1 = uy[m], a2 = uz[m];
+    v0 += (double)(a0 * temp);
+    v1 += (double)(a1 * temp);
+    v2 += (double)(a2 * temp);
+    w0 += (double)((a2 * e.ry - a1 * zz) * tempd);
+    w1 += (double)((a0 * zz - a2 * e.rx) * tempd);
+    w2 += (double)((a1 * e.rx - a0 * e.ry) * tempd);
+    k += dk;
+    ij += dij;
+    if (k >= ngd) {
+      k -= ngd;
+      ++ij;
     }
   }
-  v0.warp_reduce(); v1.warp_reduce(); v2.warp_reduce();
-  w0.warp_reduce(); w1.warp_reduce(); w2.warp_reduce();
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+    v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+    v2 += __shfl_xor_sync(0xffffffffu, v2, o);
+    w0 += __shfl_xor_sync(0xffffffffu, w0, o);
+    w1 += __shfl_xor_sync(0xffffffffu, w1, o);
+    w2 += __shfl_xor_sync(0xffffffffu, w2, o);
+  }
   if (lane == 0) {
     const double norm = c.dx * c.dx * c.dx;
-    V[3 * b + 0] = v0.value() * norm;
-    V[3 * b + 1] = v1.value() * norm;
-    V[3 * b + 2] = v2.value() * norm;
-    W[3 * b + 0] = -0.5 * w0.value() * norm;
-    W[3 * b + 1] = -0.5 * w1.value() * norm;
-    W[3 * b + 2] = -0.5 * w2.value() * norm;
+    V[3 * b + 0] = v0 * norm;
+    V[3 * b + 1] = v1 * norm;
+    V[3 * b + 2] = v2 * norm;
+    W[3 * b + 0] = -0.5 * w0 * norm;
+    W[3 * b + 1] = -0.5 * w1 * norm;
+    W[3 * b + 2] = -0.5 * w2 * norm;
   }
 }
 
@@ -602,12 +606,14 @@ fs_status mobility_t(fs_ctx *c, const double *Y, const double *F, const double *
   if (np > 0) {
     ProfScope ps(c, FS_STAGE_INTERP);
     const R *ug = (const R *)c->grid_real;
+    const size_t wb = interp_warp_bytes<R>(c->p.ngd);
     if (c->tune_interp_wpb == 4)
-      k_interp<R, 4><<<fs_blocks(np, 4), 128, 0, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V, W);
+      k_interp<R, 4><<<fs_blocks(np, 4), 128, 4 * wb, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V, W);
     else if (c->tune_interp_wpb == 16)
-      k_interp<R, 16><<<fs_blocks(np, 16), 512, 0, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V, W);
+      k_interp<R, 16><<<fs_blocks(np, 16), 512, 16 * wb, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V,
+                                                                      W);
     else
-      k_interp<R, 8><<<fs_blocks(np, 8), 256, 0, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V, W);
+      k_interp<R, 8><<<fs_blocks(np, 8), 256, 8 * wb, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V, W);
     FS_LAUNCH_CHECK();
   }
   c->last_grid_prec = sizeof(R) == 8 ? FS_PREC_FP64 : FS_PREC_FP32;
@@ -640,6 +646,21 @@ fs_status fcm_init(fs_ctx *c) {
                                (int)sizeof(SpreadStage<double, 32>)));
   FS_CUDA(cudaFuncSetAttribute(k_spread<float, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(SpreadStage<float, 32>)));
+  {
+    const int nd = 16;  // largest ngd
+    FS_CUDA(cudaFuncSetAttribute(k_interp<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(4 * interp_warp_bytes<double>(nd))));
+    FS_CUDA(cudaFuncSetAttribute(k_interp<double, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(8 * interp_warp_bytes<double>(nd))));
+    FS_CUDA(cudaFuncSetAttribute(k_interp<double, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(16 * interp_warp_bytes<double>(nd))));
+    FS_CUDA(cudaFuncSetAttribute(k_interp<float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(4 * interp_warp_bytes<float>(nd))));
+    FS_CUDA(cudaFuncSetAttribute(k_interp<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(8 * interp_warp_bytes<float>(nd))));
+    FS_CUDA(cudaFuncSetAttribute(k_interp<float, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(16 * interp_warp_bytes<float>(nd))));
+  }
   c->tune_spread_chunk = 64;
   c->tune_interp_wpb = 8;
   c->tune_fft32 = 0;
