@@ -62,8 +62,8 @@ ENSEMBLE_SEED = 3000
 # DRAM bytes per launch from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum);
 # the kernels and captures are listed in profiles/.
 NCU_TRAFFIC = {
-    # mobility_256 capture of k_spread<float>: 307.9 MB, scaled x8 to the 512^3 grid it writes
-    "spread": 2.463e9,
+    # mobility_256 capture of k_spread<float, 64>: 249.4 MB, scaled x8 to the 512^3 grid it writes
+    "spread": 1.995e9,
 }
 
 
@@ -78,6 +78,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-stride", type=int, default=64)
     ap.add_argument("--no-learned", action="store_true", help="skip training; time the reference's start only")
+    ap.add_argument("--no-graph", action="store_true", help="host-driven steps only (no CUDA graphs)")
     ap.add_argument("--train-seeds", type=int, default=20, help="plain-solver runs that generate training data")
     ap.add_argument("--workload", default="sediment_512", choices=["sediment_512", "mobility_256", "ensemble_64"],
                     help="sediment_512: implicit steps (the headline); mobility_256: FCM mobility solves, "
@@ -162,6 +163,7 @@ def run_ours(args, rank, world):
     from filsim_b200 import abi
     from filsim_b200.configs import make_sediment_case
     from filsim_b200.fcm import Context, Simulation
+    from filsim_b200 import replicas
     from filsim_b200.learn import WarmStartModel, generate, set_warm_start
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
@@ -173,23 +175,17 @@ def run_ours(args, rank, world):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", dev))
     K, W = args.steps, args.warmup
     nw = WORKLOAD["nw"]
-    p, susp = make_sediment_case(WORKLOAD["npts"], WORKLOAD["nfil"], nw, seed=WORKLOAD["seed"] + rank)
+    p, susp = make_sediment_case(WORKLOAD["npts"], WORKLOAD["nfil"], nw,
+                                 seed=replicas.replica_seed(WORKLOAD["seed"], rank))
     npb = susp.np
     stream = torch.cuda.Stream()
     ctx = Context(p, max_beads=npb, max_filaments=susp.nfil, stream=stream)
 
     def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
+        replicas.barrier(dist)
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, dist, device="cuda")
 
     # Start-up (untimed): the first PREP_STEPS steps use implicit Euler and the
     # constant / linear tension extrapolation; every timed step is in the
@@ -243,7 +239,8 @@ def run_ours(args, rank, world):
             set_warm_start(ctx, mode)
         # reference-start arms run each steady step as one CUDA graph (Broyden loop on
         # the device); the learned start decides on the host and runs host-driven
-        abi.check(abi.lib().fs_set_graph_mode(ctx.h, 0 if (learned and mode) else 1), "fs_set_graph_mode")
+        graph = 0 if (args.no_graph or (learned and mode)) else 1
+        abi.check(abi.lib().fs_set_graph_mode(ctx.h, graph), "fs_set_graph_mode")
         sim = Simulation(ctx, prep.copy())
         sim.run_steps(nt0, W)
         barrier()
@@ -282,7 +279,7 @@ def run_ours(args, rank, world):
     prof = ctx.profile()
     ctx.profile_enable(False)
     del simp
-    value = world * npb * K / (ms / 1e3)
+    value = replicas.job_throughput(npb, K, ms, world)
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -357,7 +354,8 @@ def run_ours(args, rank, world):
         ctx.set_precision(abi.FS_PREC_FP32)
         if learned:
             set_warm_start(ctx, mode)
-        abi.check(abi.lib().fs_set_graph_mode(ctx.h, 0 if (learned and mode) else 1), "fs_set_graph_mode")
+        abi.check(abi.lib().fs_set_graph_mode(ctx.h, 0 if (args.no_graph or (learned and mode)) else 1),
+                  "fs_set_graph_mode")
         host = prep.copy()
         pinned = {}
         for k, v in host.arrays.items():

@@ -41,9 +41,40 @@ class Context {
   fs_ctx *get() const { return ctx_; }
   void synchronize() { check(fs_synchronize(ctx_), "fs_synchronize"); }
   void set_precision(int prec) { check(fs_set_precision(ctx_, prec), "fs_set_precision"); }
+  // steady steps as CUDA graphs with the Broyden loop on the device
+  void set_graph_mode(bool on) { check(fs_set_graph_mode(ctx_, on ? 1 : 0), "fs_set_graph_mode"); }
+  // fastest launch variants for the uploaded suspension; returns ms per mobility solve
+  float autotune(int reps = 3, int *choice = nullptr) {
+    int c[3];
+    float ms = 0.f;
+    check(fs_autotune(ctx_, reps, choice ? choice : c, &ms), "fs_autotune");
+    return ms;
+  }
 
  private:
   fs_ctx *ctx_ = nullptr;
+};
+
+// independent boxes advanced together, one graph launch per ensemble step
+class Batch {
+ public:
+  Batch(fs_ctx *const *ctxs, int n) : n_(n) { check(fs_batch_create(ctxs, n, &b_), "fs_batch_create"); }
+  ~Batch() { fs_batch_destroy(b_); }
+  Batch(const Batch &) = delete;
+  Batch &operator=(const Batch &) = delete;
+  // iterations [nsteps x n]; box_ms (optional) per-box step times; returns the call's device ms
+  float run(int nt_start, int nsteps, std::vector<int> &iters, std::vector<float> *box_ms = nullptr) {
+    iters.assign((size_t)nsteps * n_, 0);
+    if (box_ms) box_ms->assign((size_t)nsteps * n_, 0.f);
+    float total = 0.f;
+    fs_status s = fs_batch_run(b_, nt_start, nsteps, iters.data(), box_ms ? box_ms->data() : nullptr, &total);
+    if (s != FS_OK && s != FS_ERR_NOT_CONVERGED) throw Error(s, "fs_batch_run");
+    return total;
+  }
+
+ private:
+  fs_batch *b_ = nullptr;
+  int n_;
 };
 
 // struct Fcm: the caller owns the Np x 3 device arrays (row-major doubles).
