@@ -196,6 +196,25 @@ def run_ours(args, rank, world):
     prep = susp.copy()
     sim0.download_into(prep)
     nt0 = PREP_STEPS + 1
+    # the FP32 chain's error against FP64: one mobility solve of the prepared state in each
+    from filsim_b200.fcm import Fcm
+    sim_e = Simulation(ctx, prep.copy())
+    sim_e.initial_guess()
+    sim_e.filament_forces(nt0)
+    fcm = Fcm(ctx, npb)
+    for name, buf in (("Y", fcm.Y), ("F", fcm.F), ("TAU", fcm.T)):
+        buf.copy_(sim_e.device_array(name, (npb, 3)))
+    torch.cuda.synchronize()
+    vel = {}
+    for prec in (abi.FS_PREC_FP64, abi.FS_PREC_FP32):
+        ctx.set_precision(prec)
+        fcm.mobility_solve()
+        vel[prec] = (fcm.V.cpu().numpy(), fcm.W.cpu().numpy())
+    rel = lambda a, b: float(np.abs(a - b).max() / np.abs(b).max())
+    fp32_err = {"U": rel(vel[abi.FS_PREC_FP32][0], vel[abi.FS_PREC_FP64][0]),
+                "Omega": rel(vel[abi.FS_PREC_FP32][1], vel[abi.FS_PREC_FP64][1])}
+    del fcm, sim_e
+    ctx.set_precision(abi.FS_PREC_FP32)
     # launch variants for this grid and suspension (untimed)
     choice = np.zeros(3, np.int32)
     tune_ms = ctypes.c_float()
@@ -294,6 +313,8 @@ def run_ours(args, rank, world):
         "iters_per_step": float(np.mean(its)), "status": abi.STATUS_NAMES.get(st, st),
         "mobility_solves_per_step": diag.mobility_solves / K,
         "clocks": clocks, "gpu_launches": int(launches),
+        "fp32_velocity_error_vs_fp64": dict(fp32_err, norm="max |FP32 - FP64| / max |FP64|, one solve of the "
+                                                          "prepared state"),
         "autotuned": {"spread_beads_per_pass": int(choice[0]), "interp_beads_per_cta": int(choice[1]),
                       "transform": "cuFFT" if choice[2] else "warp FFT", "ms_per_solve": tune_ms.value},
     }

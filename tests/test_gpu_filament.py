@@ -95,14 +95,15 @@ def test_error_check_apply_update_step(oracle, small):
 
 
 def test_implicit_steps_trajectory(oracle, gpu_lib):
-    """20 implicit steps with a tight tolerance: positions agree to 1e-8."""
+    """100 implicit steps (start-up and steady BDF2 regimes) with a tight
+    tolerance: positions agree to 1e-8 of the box, quaternions to 1e-8."""
     p = sediment_params(32, tol=1e-12, broyden_maxiter=100)
     s = random_suspension(p, 6, 8, seed=31, kap=1.0, c=1.0)
     sysw = oracle.System(p, s)
-    its0, st0 = sysw.run_steps(1, 20)
+    its0, st0 = sysw.run_steps(1, 100)
     ctx = Context(p, max_beads=s.np, max_filaments=s.nfil)
     sim = Simulation(ctx, s)
-    its1, st1 = sim.run_steps(1, 20)
+    its1, st1 = sim.run_steps(1, 100)
     g = sim.download()
     o = sysw.download()
     L = np.array([32 * p.dx] * 3)
