@@ -80,7 +80,8 @@ def parse():
     ap.add_argument("--no-learned", action="store_true", help="skip training; time the reference's start only")
     ap.add_argument("--no-graph", action="store_true", help="host-driven steps only (no CUDA graphs)")
     ap.add_argument("--train-seeds", type=int, default=20, help="plain-solver runs that generate training data")
-    ap.add_argument("--workload", default="sediment_512", choices=["sediment_512", "mobility_256", "ensemble_64"],
+    ap.add_argument("--workload", default="sediment_512",
+                    choices=["sediment_512", "mobility_256", "ensemble_64", "mlp"],
                     help="sediment_512: implicit steps (the headline); mobility_256: FCM mobility solves, "
                          "FP32 against FP64, on 256^3 with 1024 x 30 beads; ensemble_64: 64 independent "
                          "boxes advanced by one graph launch per step")
@@ -534,6 +535,91 @@ def run_ensemble(args, rank, world):
     return out
 
 
+def run_mlp(args, rank, world):
+    """Workload mlp: the tensor-core GEMM of the warm-start network (fs_gemm_bf16:
+    tcgen05.mma, BF16 operands, FP32 accumulators in tensor memory) on 8192^3
+    against the measured cuBLAS BF16 peak, and the network itself at the sizes of
+    sediment_512 (888 features -> 3 x 256 -> 384 outputs): inference for 4096
+    filaments and one Adam step on 4096 pairs."""
+    import numpy as np
+    import torch
+    from filsim_b200.configs import params_for
+    from filsim_b200.fcm import Context
+    from filsim_b200.learn import WarmStartModel
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    K, W = args.steps, args.warmup
+    ctx = Context(params_for(32), max_beads=64, max_filaments=8)
+    n = 8192
+    g = torch.Generator(device="cuda")
+    g.manual_seed(rank)
+    A = torch.randn((n, n), generator=g, device="cuda").to(torch.bfloat16)
+    B = torch.randn((n, n), generator=g, device="cuda").to(torch.bfloat16)
+    D = torch.empty((n, n), dtype=torch.float32, device="cuda")
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+    for _ in range(W):
+        ctx.call("fs_gemm_bf16", ptr(A), ptr(B), ptr(D), n, n, n)
+    # the context's stream is a blocking stream, so events on torch's default stream
+    # bracket its work; each call also waits for its own completion (error word)
+    times = []
+    stream = torch.cuda.current_stream()
+    with ClockSampler(dev) as clk:
+        for _ in range(K):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.call("fs_gemm_bf16", ptr(A), ptr(B), ptr(D), n, n, n)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+    gemm_ms = float(np.median(times))
+    gemm_tf = 2.0 * n ** 3 / (gemm_ms / 1e3) / 1e12
+    ref = (A[:256].double() @ B[:256].double().T)
+    gemm_err = float((D[:256, :256].double() - ref).abs().max() / ref.abs().max())
+    del A, B, D
+    peaks = {}
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        peaks = json.load(open(path))
+    peak = peaks.get("bf16_tflops", 1590.0)
+    # the network at the sizes of sediment_512
+    model = WarmStartModel(ctx, WORKLOAD["nw"], hidden=256, batch_capacity=4096, seed=rank)
+    rows = 4096
+    feats = torch.randn((rows, model.n_features), generator=g, device="cuda")
+    tgts = torch.randn((rows, model.n_targets), generator=g, device="cuda")
+    model.fit_normalization(feats, tgts)
+    d = model.dims
+    fwd_flops = 2.0 * rows * sum(d[i] * d[i + 1] for i in range(4))
+    for _ in range(W):
+        model.forward(feats)
+        model.train_step(feats, tgts, 1e-4)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        model.forward(feats)
+    torch.cuda.synchronize()
+    inf_ms = (time.perf_counter() - t0) / K * 1e3
+    t0 = time.perf_counter()
+    for _ in range(K):
+        model.train_step(feats, tgts, 1e-4)
+    torch.cuda.synchronize()
+    train_ms = (time.perf_counter() - t0) / K * 1e3
+    ctx.close()
+    return {"metric": "BF16 tensor-core GEMM TFLOP/s (8192^3, tcgen05, FP32 accumulation)", "value": gemm_tf,
+            "unit": "TFLOP/s", "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": gemm_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (fp32 accumulation)",
+            "data": "synthetic (N(0,1) operands)",
+            "config": {"workload": "mlp", "gemm": [n, n, n], "mlp_layers": d, "mlp_rows": rows},
+            "roofline": {"kernel": "k_gemm_bf16", "bound": "tensor", "achieved": gemm_tf, "peak": peak,
+                         "unit": "TFLOP/s", "frac": gemm_tf / peak,
+                         "peak_source": "measured cuBLAS burst (MEASURED_PEAKS.json bf16_tflops)"
+                         if "bf16_tflops" in peaks else "fallback"},
+            "gemm_rel_error_vs_fp64": gemm_err,
+            "mlp_inference": {"ms": inf_ms, "tflops": fwd_flops / (inf_ms / 1e3) / 1e12, "filaments": rows},
+            "mlp_train_step": {"ms": train_ms, "tflops": 3 * fwd_flops / (train_ms / 1e3) / 1e12, "pairs": rows},
+            "clocks": clk.summary()}
+
+
 def cpu_baseline(p, susp, iters_per_step, stride):
     """Oracle stage costs of one Broyden iteration of this workload, each stage
     run on 1/stride of its independent work units and scaled back; a step is
@@ -598,6 +684,8 @@ def main():
         out = run_mobility(args, rank, world) if rank == 0 else None
     elif args.workload == "ensemble_64":
         out = run_ensemble(args, rank, world)
+    elif args.workload == "mlp":
+        out = run_mlp(args, rank, world) if rank == 0 else None
     else:
         out = run_ours(args, rank, world)
     if rank == 0 and out is not None:

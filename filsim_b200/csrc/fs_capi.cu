@@ -280,6 +280,7 @@ fs_status fs_destroy(fs_ctx *c) {
     for (int i = 0; i < 2 * FS_PROF_SLOTS; ++i) cudaEventDestroy(c->prof.ev[i]);
   graph_free(c);
   mlp_free(c);
+  cudaFree(c->gemm_err);
   fcm_free(c);
   cells_free(c);
   free_state(c);

@@ -4,9 +4,10 @@
 //   D[m][n] = sum_k A[m][k] B[n][k]      A: M x K, B: N x K, both K contiguous (bf16)
 //
 // One CTA (4 warps) computes a 128 x BN tile. K advances in 64-element blocks
-// through a two-stage shared-memory ring filled by cp.async in the canonical
+// through a three-stage shared-memory ring filled by cp.async in the canonical
 // K-major 128-byte-swizzle layout (row r, 16-byte chunk j at r*128 + (j ^ (r & 7))*16,
-// atoms 1024-byte aligned). Thread 0 issues four K=16 MMAs per block and commits
+// atoms 1024-byte aligned); the loads of the next two blocks are in flight while a
+// block's MMAs run. Thread 0 issues four K=16 MMAs per block and commits
 // them to the stage's mbarrier; a stage is refilled only after that barrier's
 // phase completes. After the last commit each warp reads its 32 accumulator
 // lanes with tcgen05.ld and applies the epilogue. Every wait is bounded: on
@@ -40,16 +41,18 @@ struct GemmArgs {
 
 namespace fsg {
 
-constexpr int BM = 128, BK = 64, STAGES = 2, THREADS = 128;
+constexpr int BM = 128, BK = 64, STAGES = 3, THREADS = 128;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit_wait() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// all but the N most recent groups of this thread have landed
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
@@ -142,12 +145,10 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(GemmArgs g) {
   tc_fence_after();
   const uint32_t tmem = tmem_slot;
   const int nk = g.K / BK;
-  bool ok = true;
-  for (int kb = 0; kb < nk && ok; ++kb) {
-    const int s = kb % STAGES;
-    const uint32_t sA = base + s * STAGE_BYTES, sB = sA + A_BYTES;
-    if (kb >= STAGES) ok = mbar_wait(smem_u32(&mbar[s]), ((kb / STAGES) - 1) & 1);
-    if (!ok) break;
+  // K block kb -> stage kb % STAGES; its 128 x 64 A tile and BN x 64 B tile in the
+  // 128-byte-swizzle K-major layout
+  auto load_block = [&](int kb) {
+    const uint32_t sA = base + (kb % STAGES) * STAGE_BYTES, sB = sA + A_BYTES;
     const fs_bf16 *ga = g.A + (size_t)m0 * g.lda + kb * BK;
     const fs_bf16 *gb = g.B + (size_t)n0 * g.ldb + kb * BK;
     for (int c = tid; c < BM * 8; c += THREADS) {
@@ -158,9 +159,20 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(GemmArgs g) {
       const int r = c >> 3, j = c & 7;
       cp_async16(sB + r * 128 + ((j ^ (r & 7)) << 4), gb + (size_t)r * g.ldb + j * 8);
     }
-    cp_async_commit_wait();
+  };
+  // software pipeline: blocks kb+1 .. kb+STAGES-1 are loading while block kb's MMAs
+  // run; one commit group per block (possibly empty) keeps the group count uniform
+  for (int pb = 0; pb < STAGES - 1; ++pb) {
+    if (pb < nk) load_block(pb);
+    cp_async_commit();
+  }
+  bool ok = true;
+  for (int kb = 0; kb < nk; ++kb) {
+    const int s = kb % STAGES;
+    const uint32_t sA = base + s * STAGE_BYTES, sB = sA + A_BYTES;
+    cp_async_wait_group<STAGES - 2>();  // this thread's copies of block kb have landed
     fence_proxy_async();
-    __syncthreads();
+    __syncthreads();                    // everyone's have
     if (tid == 0) {
       tc_fence_after();
 #pragma unroll
@@ -168,7 +180,16 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(GemmArgs g) {
         mma_bf16(tmem, sw128_desc(sA + kk * 32), sw128_desc(sB + kk * 32), IDESC, (kb | kk) != 0);
       mma_commit(smem_u32(&mbar[s]));
     }
+    // block kb + STAGES - 1 refills the stage of block kb - 1 once its MMAs completed
+    const int nb = kb + STAGES - 1;
+    if (nb < nk) {
+      if (kb >= 1) ok = mbar_wait(smem_u32(&mbar[(kb - 1) % STAGES]), ((kb - 1) / STAGES) & 1);
+      if (!ok) break;
+      load_block(nb);
+    }
+    cp_async_commit();
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
   if (ok) ok = mbar_wait(smem_u32(&mbar[(nk - 1) % STAGES]), ((nk - 1) / STAGES) & 1);
   tc_fence_after();
   if (ok) {

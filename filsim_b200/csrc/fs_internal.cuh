@@ -101,6 +101,7 @@ struct fs_ctx {
   struct fs_graph *graph;  // captured steady step (fs_graph.cu); null until first used
   int graph_mode;        // 1: steady steps run as CUDA graphs with the Broyden loop on the device
   int graph_gen;         // bumped whenever captured graphs of this context become stale
+  int *gemm_err;         // error word of fs_gemm_bf16 (allocated at its first call)
 };
 
 #define FS_CUDA(call)                                                         \

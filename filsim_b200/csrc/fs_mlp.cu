@@ -937,10 +937,12 @@ fs_status fs_set_warm_start(fs_ctx *c, int mode) {
 fs_status fs_gemm_bf16(fs_ctx *c, const void *A, const void *B, float *D, int M, int N, int K) {
   if (!c || !A || !B || !D || M <= 0 || N <= 0 || K <= 0) return FS_ERR_INVALID_ARG;
   if (M % fsg::BM || N % 128 || K % fsg::BK) return FS_ERR_INVALID_ARG;
-  FS_TRY(gemm_attrs());
-  int *err_d = nullptr;
-  FS_CUDA(cudaMalloc(&err_d, sizeof(int)));
-  cudaMemsetAsync(err_d, 0, sizeof(int), c->stream);
+  if (!c->gemm_err) {  // first call: the error word and the kernels' shared-memory limits
+    FS_TRY(gemm_attrs());
+    FS_CUDA(cudaMalloc(&c->gemm_err, sizeof(int)));
+  }
+  int *err_d = c->gemm_err;
+  FS_CUDA(cudaMemsetAsync(err_d, 0, sizeof(int), c->stream));
   GemmArgs g = gargs((const fs_bf16 *)A, K, (const fs_bf16 *)B, K, M, N, K, err_d);
   g.outF = D;
   g.ldo = N;
@@ -949,7 +951,6 @@ fs_status fs_gemm_bf16(fs_ctx *c, const void *A, const void *B, float *D, int M,
   if (st == FS_OK && cudaMemcpyAsync(&e, err_d, sizeof(int), cudaMemcpyDeviceToHost, c->stream) == cudaSuccess &&
       cudaStreamSynchronize(c->stream) == cudaSuccess && e)
     st = FS_ERR_CUDA;
-  cudaFree(err_d);
   return st;
 }
 
