@@ -4,10 +4,11 @@
 //   1. k_fcm_bin_keys + counting sort: beads binned by the 16-point tile that
 //      holds the start of their Gaussian stencil (gaussian_setup's index rule,
 //      FCMfunctions.cpp:565-589).
-//   2. k_spread: one CTA per 16^3 grid tile gathers the monopole + rotlet
-//      Gaussians of every bead whose stencil reaches the tile
-//      (mono_and_dipole_force_distribution, :596-646); each lane owns grid
-//      points and sums in registers: no atomics, bit-reproducible.
+//   2. k_spread (FP64) / k_spread_records32 + k_spread32 (FP32 chain): CTAs over
+//      16^3 grid tiles gather the monopole + rotlet Gaussians of every bead whose
+//      stencil reaches the tile (mono_and_dipole_force_distribution, :596-646);
+//      each lane owns grid points and sums in registers (FP32: Kahan-compensated,
+//      on packed f32x2 pairs): no atomics, bit-reproducible.
 //   3. cuFFT R2C (batched x3), 4. k_project / k_project_planes: the Stokes
 //      projection of flow_solve (:648-736), 5. cuFFT C2R (batched x3).
 //   6. k_interp: one warp per bead (in spread-bin order for L2 locality)
@@ -17,6 +18,7 @@
 // weights in float, with Kahan-compensated spread sums and FP64 accumulation of
 // the interpolation products.
 #include "fs_internal.cuh"
+#include "fs_f32x2.cuh"
 
 namespace {
 
@@ -278,6 +280,259 @@ __global__ void __launch_bounds__(FS_SPREAD_THREADS)
       fgrid[N + m0] = (R)0;
       fgrid[2 * N + m0] = (R)0;
     }
+}
+
+// ---- 2b. FP32 spread on packed pairs -------------------------------------------
+// The FP32 chain's spread. k_spread_weights32 evaluates each bead's stencil
+// weights once per solve, (g, d, r, r d) per axis and stencil index, with the
+// FP32 arithmetic of k_spread<float> (gaussian_setup, FCMfunctions.cpp:565-589:
+// xx = xg dx - Y in double, then the float Gaussians). k_spread32 then runs one
+// CTA (8 warps) per half of a 16^3 tile: x in [8h, 8h+8) of the tile, all y and
+// z. Warp w owns the 4 x 16 x 4 column x in [4(w&1), +4), z in [4(w>>1), +4);
+// lane l owns x = 4(w&1) + (l&3), the z pair 4(w>>1) + 2((l>>2)&1) + {0, 1}
+// and y = (l>>3) + 4k, k < 4: eight points held as four packed pairs per
+// component. Per staged bead reaching the warp's column the lane forms the
+// x-z factors of its pair once, then each covered y row costs three packed
+// FMA chains and three packed Kahan updates:
+//   y = term + nc, t = s + y, nc = y - (t - s), s = t      (nc = -c of Kahan)
+// The sums run over the candidates in sorted bead order and are written once
+// per point (s + nc): no atomics, bit-reproducible.
+#define FS_SPREAD32_THREADS 256
+
+// Record of the bead in sorted slot q (float4 units): [0] stencil starts (int),
+// [1] F0, F1, F2, h0, [2] h1, h2, -, -, then (g, d, r, r d) for axis a and stencil
+// index i at 3 + a ngd + i.
+__host__ __device__ inline int spread_rec_len(int ngd) { return 3 + 3 * ngd; }
+
+__global__ void k_spread_records32(const double *__restrict__ Y, const double *__restrict__ F,
+                                   const double *__restrict__ T, const int *__restrict__ sorted,
+                                   const int *__restrict__ bead_sw, int np, FcmConsts c, float4 *__restrict__ rec) {
+  const int ngd = c.ngd, RL = spread_rec_len(ngd);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)np * RL) return;
+  const int q = (int)(t / RL), e = (int)(t - (long long)q * RL);
+  const int bead = sorted[q];
+  float4 v;
+  if (e == 0) {
+    v = make_float4(__int_as_float(bead_sw[3 * bead]), __int_as_float(bead_sw[3 * bead + 1]),
+                    __int_as_float(bead_sw[3 * bead + 2]), 0.f);
+  } else if (e == 1) {
+    v = make_float4((float)F[3 * bead], (float)F[3 * bead + 1], (float)F[3 * bead + 2], (float)(0.5 * T[3 * bead]));
+  } else if (e == 2) {
+    v = make_float4((float)(0.5 * T[3 * bead + 1]), (float)(0.5 * T[3 * bead + 2]), 0.f, 0.f);
+  } else {
+    const int a = (e - 3) / ngd, i = (e - 3) - a * ngd;
+    const double Yv = Y[3 * bead + a];
+    const int xc = (int)(Yv / c.dx);
+    const int xg = xc - c.ngdh + (i + 1);
+    const double xx = ((double)xg) * c.dx - Yv;
+    const float xf = (float)xx;
+    const float g = (float)c.anorm * expf(-xf * xf / (float)c.anorm2);
+    const float d = (float)c.anormdip * expf(-xf * xf / (float)c.anormdip2);
+    const float r = -xf / (float)c.sigmadipsq;
+    v = make_float4(g, d, r, r * d);
+  }
+  rec[t] = v;
+}
+
+constexpr int FS_SPREAD32_REC_MAX = 3 + 3 * 16;  // record length for the largest ngd
+
+template <int CH>
+struct SpreadStage32 {
+  float4 raw[CH * FS_SPREAD32_REC_MAX];      // the chunk's records (slot sl at sl RL), copied as they are
+  float4 xw[CH][8];                          // (g, d, r, -) by x of the half tile
+  float zg[CH][FS_TILE], zd[CH][FS_TILE], zr[CH][FS_TILE];  // by tile-local z
+  float4 yw[CH][FS_TILE];                    // (g, g, d, d) by tile-local y
+  float2 yrd[CH][FS_TILE];                   // (r d, r d)
+  unsigned xzm[CH];                          // x coverage (8 bits) | z coverage (16 bits) << 8
+  unsigned rows[CH];                         // y rows k with a covered y in [4k, 4k + 4)
+};
+
+template <int CH>
+__global__ void __launch_bounds__(FS_SPREAD32_THREADS, 3)
+    k_spread32(const int *__restrict__ bin_start, const float4 *__restrict__ rec, FcmConsts c,
+               float *__restrict__ fgrid) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SpreadStage32<CH> &st = *reinterpret_cast<SpreadStage32<CH> *>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tile = blockIdx.x >> 1, xh = blockIdx.x & 1;
+  const int tz = tile % c.nbin[2], ty = (tile / c.nbin[2]) % c.nbin[1], tx = tile / (c.nbin[2] * c.nbin[1]);
+  const int X0[3] = {tx * FS_TILE, ty * FS_TILE, tz * FS_TILE};
+  // candidate bins, the tile's own bin and the one before it per axis, in the
+  // order (x, y, z) of k_spread; thread r < 8 reads combination r (empty when an
+  // axis has a single bin and the combination repeats it)
+  __shared__ int cand_rs[8], cand_len[8];
+  if (tid < 8) {
+    const int tb[3] = {tx, ty, tz};
+    const int pick[3] = {tid >> 2, (tid >> 1) & 1, tid & 1};
+    int bin = 0;
+    bool valid = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      valid = valid && (pick[d] == 1 || c.nbin[d] > 1);
+      bin = bin * c.nbin[d] + (pick[d] == 1 ? tb[d] : wrap_int(tb[d] - 1, c.nbin[d]));
+    }
+    cand_rs[tid] = valid ? bin_start[bin] : 0;
+    cand_len[tid] = valid ? bin_start[bin + 1] - bin_start[bin] : 0;
+  }
+  __syncthreads();
+  int total = 0;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) total += cand_len[r];
+  const int cx = warp & 1, cz = warp >> 1;
+  const int xl = 4 * cx + (lane & 3), zl = 4 * cz + 2 * ((lane >> 2) & 1), ly = lane >> 3;
+  const int ngd = c.ngd;
+  f2p s[4][3], nc[4][3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) s[k][a] = nc[k][a] = 0ull;
+
+  for (int base = 0; base < total; base += CH) {
+    const int nb = min(CH, total - base);
+    __syncthreads();  // the previous chunk's tables are no longer read
+    // staging, phase 1: the chunk's records to shared memory (slot sl at sl RL) with
+    // 16-byte asynchronous copies, one contiguous run per candidate bin, all independent
+    const int RL = spread_rec_len(ngd);
+    {
+      int pre = 0;  // candidates before bin range r
+#pragma unroll 1
+      for (int r = 0; r < 8; ++r) {
+        const int lo = max(pre, base), hi = min(pre + cand_len[r], base + nb);
+        if (lo < hi) {
+          const float4 *src = rec + (size_t)(cand_rs[r] + lo - pre) * RL;
+          const unsigned dst = (unsigned)__cvta_generic_to_shared(&st.raw[(lo - base) * RL]);
+          for (int e = tid; e < (hi - lo) * RL; e += FS_SPREAD32_THREADS)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + 16 * e), "l"(src + e) : "memory");
+        }
+        pre += cand_len[r];
+      }
+    }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    // phase 2: tables by tile coordinate, eight threads per bead slot; thread j
+    // takes x = 8h + j, y in {j, j+8}, z in {j, j+8}
+    const int j = tid & 7;
+#pragma unroll 1
+    for (int s0 = 0; s0 < CH; s0 += FS_SPREAD32_THREADS / 8) {
+      const int sl = s0 + (tid >> 3);
+      const bool act = sl < nb;
+      bool cov[5] = {false, false, false, false, false};
+      if (act) {
+        const float4 *rw = st.raw + sl * RL;
+        const float4 hd = rw[0];
+        const int swv[3] = {__float_as_int(hd.x), __float_as_int(hd.y), __float_as_int(hd.z)};
+        const int la[5] = {8 * xh + j, j, j + 8, j, j + 8};
+        const int ax[5] = {0, 1, 1, 2, 2};
+        float4 w[5];
+#pragma unroll
+        for (int it = 0; it < 5; ++it) {
+          const int a = ax[it], Nn = c.N[a];
+          const int i = wrap_near(la[it] + wrap_near(X0[a] - swv[a], Nn), Nn);
+          cov[it] = i < ngd;
+          w[it] = cov[it] ? rw[3 + a * ngd + i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        st.xw[sl][j] = w[0];
+        st.yw[sl][j] = make_float4(w[1].x, w[1].x, w[1].y, w[1].y);
+        st.yrd[sl][j] = make_float2(w[1].w, w[1].w);
+        st.yw[sl][j + 8] = make_float4(w[2].x, w[2].x, w[2].y, w[2].y);
+        st.yrd[sl][j + 8] = make_float2(w[2].w, w[2].w);
+        st.zg[sl][j] = w[3].x;
+        st.zd[sl][j] = w[3].y;
+        st.zr[sl][j] = w[3].z;
+        st.zg[sl][j + 8] = w[4].x;
+        st.zd[sl][j + 8] = w[4].y;
+        st.zr[sl][j + 8] = w[4].z;
+      }
+      // coverage masks by ballot: lanes 8q .. 8q+7 of this warp hold slot s0 + 4 warp + q
+      const unsigned bx = __ballot_sync(0xffffffffu, cov[0]);
+      const unsigned by0 = __ballot_sync(0xffffffffu, cov[1]), by1 = __ballot_sync(0xffffffffu, cov[2]);
+      const unsigned bz0 = __ballot_sync(0xffffffffu, cov[3]), bz1 = __ballot_sync(0xffffffffu, cov[4]);
+      if (act && j == 0) {
+        const int sh = lane & 24;
+        const unsigned xm = (bx >> sh) & 0xffu;
+        const unsigned ym = ((by0 >> sh) & 0xffu) | (((by1 >> sh) & 0xffu) << 8);
+        const unsigned zm = ((bz0 >> sh) & 0xffu) | (((bz1 >> sh) & 0xffu) << 8);
+        st.xzm[sl] = xm | (zm << 8);
+        unsigned rows = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) rows |= ((ym >> (4 * k)) & 0xfu) ? (1u << k) : 0u;
+        st.rows[sl] = rows;
+      }
+    }
+    __syncthreads();
+    // staged beads reaching this warp's column
+    unsigned col[CH / 32];
+#pragma unroll
+    for (int h = 0; h < CH / 32; ++h) {
+      const int sl = 32 * h + lane;
+      bool hit = false;
+      if (sl < nb) {
+        const unsigned m = st.xzm[sl];
+        hit = ((m >> (4 * cx)) & 0xfu) && ((m >> (8 + 4 * cz)) & 0xfu) && st.rows[sl];
+      }
+      col[h] = __ballot_sync(0xffffffffu, hit);
+    }
+#pragma unroll
+    for (int h = 0; h < CH / 32; ++h) {
+      unsigned m = col[h];
+      while (m) {
+        const int sl = 32 * h + __ffs(m) - 1;
+        m &= m - 1;
+        const unsigned rows = st.rows[sl];
+        const float4 wx = st.xw[sl][xl];
+        const float2 gz = *reinterpret_cast<const float2 *>(&st.zg[sl][zl]);
+        const float2 dz = *reinterpret_cast<const float2 *>(&st.zd[sl][zl]);
+        const float2 rz = *reinterpret_cast<const float2 *>(&st.zr[sl][zl]);
+        const float4 fh = st.raw[sl * RL + 1];  // F0, F1, F2, h0 (h = T / 2, GA_setup :536-547)
+        const float4 hh = st.raw[sl * RL + 2];  // h1, h2
+        // per z of the pair: f_a = F_a gx gz, the rotlet factors of k_spread (d = gdx gdz)
+        const float gxz0 = wx.x * gz.x, gxz1 = wx.x * gz.y;
+        const float dxz0 = wx.y * dz.x, dxz1 = wx.y * dz.y;
+        const f2p f0 = f2_pack(fh.x * gxz0, fh.x * gxz1);
+        const f2p f1 = f2_pack(fh.y * gxz0, fh.y * gxz1);
+        const f2p f2v = f2_pack(fh.z * gxz0, fh.z * gxz1);
+        const f2p h2d = f2_pack(hh.y * dxz0, hh.y * dxz1);
+        const f2p mh0d = f2_pack(-fh.w * dxz0, -fh.w * dxz1);
+        const f2p c0 = f2_pack(-hh.x * rz.x * dxz0, -hh.x * rz.y * dxz1);
+        const f2p c1 = f2_pack((-hh.y * wx.z + fh.w * rz.x) * dxz0, (-hh.y * wx.z + fh.w * rz.y) * dxz1);
+        const f2p c2 = f2_pack(hh.x * wx.z * dxz0, hh.x * wx.z * dxz1);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          if (rows & (1u << k)) {
+            const ulonglong2 gd = *reinterpret_cast<const ulonglong2 *>(&st.yw[sl][ly + 4 * k]);
+            const f2p rd = *reinterpret_cast<const f2p *>(&st.yrd[sl][ly + 4 * k]);
+            f2p y, t;
+            // f0 g + h2d (r d) + c0 d
+            y = f2_fma(f0, gd.x, f2_fma(h2d, rd, f2_fma(c0, gd.y, nc[k][0])));
+            t = f2_add(s[k][0], y);
+            nc[k][0] = f2_sub(y, f2_sub(t, s[k][0]));
+            s[k][0] = t;
+            // f1 g + c1 d
+            y = f2_fma(f1, gd.x, f2_fma(c1, gd.y, nc[k][1]));
+            t = f2_add(s[k][1], y);
+            nc[k][1] = f2_sub(y, f2_sub(t, s[k][1]));
+            s[k][1] = t;
+            // f2 g + c2 d - h0d (r d)
+            y = f2_fma(f2v, gd.x, f2_fma(mh0d, rd, f2_fma(c2, gd.y, nc[k][2])));
+            t = f2_add(s[k][2], y);
+            nc[k][2] = f2_sub(y, f2_sub(t, s[k][2]));
+            s[k][2] = t;
+          }
+        }
+      }
+    }
+  }
+  // one write per point: s - c
+  const size_t N = (size_t)c.N[0] * c.N[1] * c.N[2];
+  const int gx = X0[0] + 8 * xh + xl, gz0 = X0[2] + zl;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const size_t m0 = ((size_t)gx * c.N[1] + (X0[1] + ly + 4 * k)) * c.N[2] + gz0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+      *reinterpret_cast<float2 *>(fgrid + a * N + m0) = f2_unpack(f2_add(s[k][a], nc[k][a]));
+  }
 }
 
 // ---- 4. Stokes projection -----------------------------------------------------
@@ -584,23 +839,44 @@ fs_status flow_solve_t(fs_ctx *c) {
   return FS_OK;
 }
 
+// binning, sort and the spread of the force grid into c->grid_real (R precision)
+template <typename R>
+fs_status spread_t(fs_ctx *c, const FcmConsts &k, const double *Y, const double *F, const double *T, int np) {
+  if (np > 0) {
+    k_fcm_bin_keys<<<fs_blocks(np, 256), 256, 0, c->stream>>>(Y, np, k, c->bins.key, c->bead_sw);
+    FS_LAUNCH_CHECK();
+  }
+  FS_TRY(fs_sort_run(&c->bins, np, c->stream));
+  if (sizeof(R) == 4) {
+    const float4 *rec = (const float4 *)c->spread_wb;
+    if (np > 0) {
+      k_spread_records32<<<fs_blocks((long long)np * spread_rec_len(k.ngd), 256), 256, 0, c->stream>>>(
+          Y, F, T, c->bins.sorted, c->bead_sw, np, k, c->spread_wb);
+      FS_LAUNCH_CHECK();
+    }
+    if (c->tune_spread_chunk == 32)
+      k_spread32<32><<<2 * c->nbins, FS_SPREAD32_THREADS, sizeof(SpreadStage32<32>), c->stream>>>(
+          c->bins.start, rec, k, (float *)c->grid_real);
+    else
+      k_spread32<64><<<2 * c->nbins, FS_SPREAD32_THREADS, sizeof(SpreadStage32<64>), c->stream>>>(
+          c->bins.start, rec, k, (float *)c->grid_real);
+  } else if (c->tune_spread_chunk == 32) {
+    k_spread<R, 32><<<c->nbins, FS_SPREAD_THREADS, sizeof(SpreadStage<R, 32>), c->stream>>>(
+        Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k, (R *)c->grid_real);
+  } else {
+    k_spread<R, 64><<<c->nbins, FS_SPREAD_THREADS, sizeof(SpreadStage<R, 64>), c->stream>>>(
+        Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k, (R *)c->grid_real);
+  }
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
 template <typename R>
 fs_status mobility_t(fs_ctx *c, const double *Y, const double *F, const double *T, double *V, double *W, int np) {
   FcmConsts k = make_consts(c);
   {
     ProfScope ps(c, FS_STAGE_SPREAD);
-    if (np > 0) {
-      k_fcm_bin_keys<<<fs_blocks(np, 256), 256, 0, c->stream>>>(Y, np, k, c->bins.key, c->bead_sw);
-      FS_LAUNCH_CHECK();
-    }
-    FS_TRY(fs_sort_run(&c->bins, np, c->stream));
-    if (c->tune_spread_chunk == 32)
-      k_spread<R, 32><<<c->nbins, FS_SPREAD_THREADS, sizeof(SpreadStage<R, 32>), c->stream>>>(
-          Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k, (R *)c->grid_real);
-    else
-      k_spread<R, 64><<<c->nbins, FS_SPREAD_THREADS, sizeof(SpreadStage<R, 64>), c->stream>>>(
-          Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k, (R *)c->grid_real);
-    FS_LAUNCH_CHECK();
+    FS_TRY(spread_t<R>(c, k, Y, F, T, np));
   }
   FS_TRY(flow_solve_t<R>(c));
   if (np > 0) {
@@ -638,6 +914,15 @@ fs_status fcm_init(fs_ctx *c) {
   FS_TRY(fs_sort_alloc(&c->bins, c->nbins, c->max_beads, &c->bytes));
   FS_CUDA(cudaMalloc(&c->bead_sw, sizeof(int) * 3 * (size_t)(c->max_beads > 0 ? c->max_beads : 1)));
   c->bytes += sizeof(int) * 3 * (size_t)c->max_beads;
+  {
+    const size_t nw = (size_t)(c->max_beads > 0 ? c->max_beads : 1) * spread_rec_len(c->p.ngd);
+    FS_CUDA(cudaMalloc(&c->spread_wb, sizeof(float4) * nw));
+    c->bytes += sizeof(float4) * nw;
+  }
+  FS_CUDA(cudaFuncSetAttribute(k_spread32<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(SpreadStage32<64>)));
+  FS_CUDA(cudaFuncSetAttribute(k_spread32<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(SpreadStage32<32>)));
   FS_CUDA(cudaFuncSetAttribute(k_spread<double, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(SpreadStage<double, 64>)));
   FS_CUDA(cudaFuncSetAttribute(k_spread<float, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -681,6 +966,8 @@ void fcm_free(fs_ctx *c) {
   fs_sort_free(&c->bins);
   cudaFree(c->bead_sw);
   c->bead_sw = nullptr;
+  cudaFree(c->spread_wb);
+  c->spread_wb = nullptr;
 }
 
 fs_status fcm_set_stream(fs_ctx *c, cudaStream_t st) {
@@ -711,15 +998,15 @@ fs_status fcm_friction(fs_ctx *c, const double *F, const double *T, double *V, d
 
 fs_status fcm_spread_only(fs_ctx *c, const double *Y, const double *F, const double *T, int np, double *f) {
   FcmConsts k = make_consts(c);
-  if (np > 0) {
-    k_fcm_bin_keys<<<fs_blocks(np, 256), 256, 0, c->stream>>>(Y, np, k, c->bins.key, c->bead_sw);
+  const size_t n = 3 * c->N;
+  if (c->precision == FS_PREC_FP32) {
+    FS_TRY(spread_t<float>(c, k, Y, F, T, np));
+    k_convert<float, double><<<fs_blocks((long long)n, 256), 256, 0, c->stream>>>((const float *)c->grid_real, f, n);
     FS_LAUNCH_CHECK();
+  } else {
+    FS_TRY(spread_t<double>(c, k, Y, F, T, np));
+    FS_CUDA(cudaMemcpyAsync(f, c->grid_real, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
   }
-  FS_TRY(fs_sort_run(&c->bins, np, c->stream));
-  k_spread<double, 64><<<c->nbins, FS_SPREAD_THREADS, sizeof(SpreadStage<double, 64>), c->stream>>>(
-      Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k, (double *)c->grid_real);
-  FS_LAUNCH_CHECK();
-  FS_CUDA(cudaMemcpyAsync(f, c->grid_real, sizeof(double) * 3 * c->N, cudaMemcpyDeviceToDevice, c->stream));
   c->last_grid_prec = -1;
   return FS_OK;
 }

@@ -60,6 +60,7 @@ struct fs_ctx {
   int nbin[3], nbins;  // spread bins (FS_TILE wide in stencil-start space)
   fs_sort bins;
   int *bead_sw;        // per bead, wrapped Gaussian stencil start per axis
+  float4 *spread_wb;   // FP32 chain: per sorted bead, stencil starts, F, T/2 and weights
   int last_grid_prec;  // precision of the grids from the last solve (-1: none)
   int tune_spread_chunk;  // beads staged per spread pass: 32 or 64 (fs_autotune)
   int tune_interp_wpb;    // beads (warps) per interpolation CTA: 4, 8 or 16

@@ -109,7 +109,8 @@ class Fcm:
         self.ctx.call("fs_fcm_friction", _dptr(self.F), _dptr(self.T), _dptr(self.V), _dptr(self.W), self.np)
 
     def spread(self):
-        """The force grid f (3, Nx, Ny, Nz) of the current Y, F, T (FP64)."""
+        """The force grid f (3, Nx, Ny, Nz, float64) of the current Y, F, T, spread in
+        the context's precision."""
         p = self.ctx.params
         f = torch.empty((3, p.npts_x, p.npts_y, p.npts_z), dtype=torch.float64, device="cuda")
         self.ctx.call("fs_fcm_spread", _dptr(self.Y), _dptr(self.F), _dptr(self.T), self.np, _dptr(f))

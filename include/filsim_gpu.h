@@ -165,9 +165,10 @@ fs_status fs_fcm_mobility_host(fs_ctx *ctx, const double *Y_h, const double *F_h
  * Replaces Fcm::friction_mobility_solve (FCMfunctions.cpp:865-880). */
 fs_status fs_fcm_friction(fs_ctx *ctx, const double *F, const double *T, double *V, double *W, int np);
 /* The force-distribution step alone (GA_setup + gaussian_setup +
- * mono_and_dipole_force_distribution, FCMfunctions.cpp:536-646) in FP64:
- * writes the spread force grid f (device, 3 x Nx x Ny x Nz doubles,
- * component-major, z fastest). */
+ * mono_and_dipole_force_distribution, FCMfunctions.cpp:536-646) in the
+ * context's precision (FP32: the FP32 chain's spread, widened): writes the
+ * spread force grid f (device, 3 x Nx x Ny x Nz doubles, component-major,
+ * z fastest). */
 fs_status fs_fcm_spread(fs_ctx *ctx, const double *Y, const double *F, const double *T, int np, double *f);
 /* Copies the velocity grid u of the last FP64 mobility solve (3 x Nx x Ny x Nz
  * doubles) to host; count is the number of doubles grid_h holds. */

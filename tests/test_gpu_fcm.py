@@ -66,6 +66,43 @@ def test_spread_grid_matches_oracle(oracle):
     assert np.abs(f - f0).max() / np.abs(f0).max() < 1e-13
 
 
+FP32_SPREAD_REL = 1e-6
+
+
+@pytest.mark.parametrize("shape,nb,seed,chunk", [
+    ((32, 32, 32), 40, 21, 32),
+    ((16, 32, 48), 30, 22, 32),     # a 16-point axis: one bin, stencils wrap inside the tile
+    ((48, 32, 16), 60, 23, 64),
+    ((32, 32, 32), 1500, 24, 32),   # ~1500 candidates per tile: many staging chunks
+    ((64, 32, 32), 1500, 25, 64),
+])
+def test_fp32_spread_grid_matches_oracle(oracle, shape, nb, seed, chunk):
+    """The FP32 chain's spread (k_spread_records32 + k_spread32: Kahan sums on packed
+    pairs) against the oracle's FP64 force grid, positions drawn over 1.5 box lengths
+    (negative and past the far face included), F, T ~ N(0,1); a repeat is bitwise equal."""
+    import ctypes
+    from filsim_b200.abi import check, lib
+    p = params_for(shape[0])
+    p.npts_x, p.npts_y, p.npts_z = shape
+    rng = np.random.default_rng(seed)
+    L = np.array(shape) * p.dx
+    Y = rng.uniform(-0.25, 1.25, (nb, 3)) * L
+    F = rng.standard_normal((nb, 3))
+    T = rng.standard_normal((nb, 3))
+    _, _, f0, _ = oracle.fcm_mobility(p, Y, F, T, return_grids=True)
+    ctx = Context(p, max_beads=nb)
+    ctx.set_precision(abi.FS_PREC_FP32)
+    tune = np.array([chunk, 8, 0], np.int32)
+    check(lib().fs_set_tuning(ctx.h, tune.ctypes.data_as(ctypes.c_void_p)), "fs_set_tuning")
+    fcm = Fcm(ctx, nb)
+    fcm.set(Y, F, T)
+    f = fcm.spread().cpu().numpy()
+    f2 = fcm.spread().cpu().numpy()
+    ctx.close()
+    assert rel_err(f, f0) < FP32_SPREAD_REL
+    assert np.array_equal(f, f2)
+
+
 def test_velocity_grid_matches_oracle(oracle):
     p, s, Y, F, T = make_mobility_case(32, 6, 5, seed=8)
     _, _, _, u0 = oracle.fcm_mobility(p, Y, F, T, return_grids=True)
