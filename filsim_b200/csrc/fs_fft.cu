@@ -20,6 +20,7 @@
 // along x and y, the semantics of the reference's multi-dimensional real
 // inverse transform.
 #include "fs_internal.cuh"
+#include "fs_f32x2.cuh"
 
 namespace {
 
@@ -55,8 +56,13 @@ __host__ __device__ constexpr int bitrev_c(int i, int n) {
   return r;
 }
 
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// complex add / subtract as one packed f32x2 instruction on the (re, im) pair
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+  return f2_unpack(f2_add(f2_pack(a.x, a.y), f2_pack(b.x, b.y)));
+}
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+  return f2_unpack(f2_sub(f2_pack(a.x, a.y), f2_pack(b.x, b.y)));
+}
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -189,7 +195,7 @@ __device__ __forceinline__ void stage2_twiddle(float2 (&v)[Fft<N>::M], const flo
 }
 
 __device__ __forceinline__ float2 add_signed(float2 o, float sgn, float2 v) {
-  return make_float2(fmaf(sgn, v.x, o.x), fmaf(sgn, v.y, o.y));
+  return f2_unpack(f2_fma(f2_pack(sgn, sgn), f2_pack(v.x, v.y), f2_pack(o.x, o.y)));
 }
 
 // index of register i of this lane after fft_n2p (and before fft_p2n)
