@@ -481,12 +481,13 @@ static fs_status upload_layout(fs_ctx *c, const fs_host_state *s) {
   const int nf = s->nfil, np = s->np;
   std::vector<int> fid(np > 0 ? np : 1), sid(np > 0 ? np : 1);
   std::vector<long long> soff(nf + 1), aoff(nf + 1);
-  int max_nw = 1;
+  int max_nw = 1, min_nw = nf > 0 ? 1 << 30 : 1;
   soff[0] = aoff[0] = 0;
   for (int f = 0; f < nf; ++f) {
     const int nw = s->fil_start[f + 1] - s->fil_start[f];
     if (nw < 1) return FS_ERR_INVALID_ARG;
     max_nw = std::max(max_nw, nw);
+    min_nw = std::min(min_nw, nw);
     for (int i = 0; i < nw; ++i) {
       fid[s->fil_start[f] + i] = f;
       sid[s->fil_start[f] + i] = i;
@@ -500,6 +501,7 @@ static fs_status upload_layout(fs_ctx *c, const fs_host_state *s) {
     c->max_nw = prev_max_nw;
     return FS_ERR_INVALID_ARG;
   }
+  c->min_nw = min_nw;
   c->nfil = nf;
   c->np = np;
   c->nlink = np - nf;

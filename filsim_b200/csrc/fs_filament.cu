@@ -631,6 +631,160 @@ __global__ void __launch_bounds__(384) k_schur_gj(const int *__restrict__ fil_st
   }
 }
 
+// The same inversion with the matrix in registers, for m = 3 nw <= 96: warp
+// w = cb RB + rb (RB = ceil(m / 32) row blocks, CB = ceil(m / 12) column blocks)
+// holds rows 32 rb .. 32 rb + 31 (one per lane) of columns 12 cb .. 12 cb + 11.
+// Per pivot kc (row p and 1 / S[p][kc], found by the previous step):
+//   A: the lane holding row p publishes it scaled (prow = row p / v, with
+//      1 / v in column kc), the lane holding row kc publishes its old row, the
+//      warps holding column kc publish it (fcol);
+//   B: row r := r - fcol[r] prow for every r != kc (row p, the old row kc,
+//      takes the old (kc, kc) entry as its factor), row kc := prow, column kc
+//      of the other rows := -fcol[r] / v; then the warps holding column kc + 1
+//      search it over rows > kc (first maximum, by shuffles, per row block).
+// Each element sees the operations and roundings of k_schur_gj; two barriers per
+// pivot, one register-blocked outer product per thread.
+constexpr int GJ_CW = 12;        // columns per warp
+constexpr int GJ_MAX_M = 96;     // m handled by the register kernel
+__global__ void __launch_bounds__(768) k_schur_gj_reg(const int *__restrict__ fil_start,
+                                                      const long long *__restrict__ soff,
+                                                      double *__restrict__ Sinv_all, int *__restrict__ flags) {
+  constexpr int CW = GJ_CW;
+  __shared__ double fcol[GJ_MAX_M], rowkc[GJ_MAX_M + CW];
+  __shared__ __align__(16) double prow_s[GJ_MAX_M + CW];
+  __shared__ double cand_v[3], cand_x[3], cand_inv[3];
+  __shared__ int cand_r[3];
+  __shared__ int perm[GJ_MAX_M], colsrc[GJ_MAX_M], dstcol[GJ_MAX_M];
+  const int f = blockIdx.x;
+  const int nw = fil_start[f + 1] - fil_start[f], m = 3 * nw;
+  if (nw < 2 || m > GJ_MAX_M) return;  // block-uniform
+  const int RB = (m + 31) >> 5, CB = (m + CW - 1) / CW;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const bool wact = w < RB * CB;  // warp-uniform; spare warps only take the barriers
+  const int cb = w / RB, rb = w - cb * RB;
+  const int r = 32 * rb + lane, c0 = CW * cb;
+  double *Sg = Sinv_all + soff[f];
+  double a[CW];
+#pragma unroll
+  for (int k = 0; k < CW; ++k) a[k] = (wact && r < m && c0 + k < m) ? Sg[(size_t)r * m + c0 + k] : 0.0;
+  // first maximum of |a[k]| (k a compile-time slot after unrolling) over rows >
+  // after in this row block -> cand[rb]
+  auto search = [&](int k, int after) {
+    double v = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < CW; ++kk)
+      if (kk == k) v = a[kk];
+    double best = (r > after && r < m) ? fabs(v) : -1.0, x = v;
+    int bi = r;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      const double ox = __shfl_xor_sync(0xffffffffu, x, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+        x = ox;
+      }
+    }
+    if (lane == 0) {
+      cand_v[rb] = best;
+      cand_r[rb] = bi;
+      cand_x[rb] = x;
+      cand_inv[rb] = best >= 0.0 ? 1.0 / x : 0.0;
+    }
+  };
+  if (wact && cb == 0) search(0, -1);
+  __syncthreads();
+  // pivots kc = CW kb + kk: kk unrolled, so column kc is register slot kk of the
+  // warps with cb == kb
+  for (int kb = 0; kb < CB; ++kb) {
+#pragma unroll
+    for (int kk = 0; kk < CW; ++kk) {
+      const int kc = CW * kb + kk;
+      if (kc >= m) break;  // block-uniform
+      // phase A
+      double best = -1.0, inv = 0.0;
+      int p = kc;
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+        if (q < RB && cand_v[q] > best) {
+          best = cand_v[q];
+          p = cand_r[q];
+          inv = cand_inv[q];
+        }
+      if (wact) {
+        if (r == p) {
+#pragma unroll
+          for (int k = 0; k < CW; ++k) prow_s[c0 + k] = (cb == kb && k == kk) ? inv : a[k] * inv;
+        }
+        if (r == kc) {
+#pragma unroll
+          for (int k = 0; k < CW; ++k) rowkc[c0 + k] = a[k];
+        }
+        if (cb == kb && r < m) fcol[r] = a[kk];
+      }
+      if (threadIdx.x == 0) {
+        perm[kc] = p;
+        if (!(best > 0.0)) atomicOr(&flags[FLAG_PIVOT], 1);
+      }
+      __syncthreads();
+      // phase B
+      if (wact) {
+        double pr[CW];
+#pragma unroll
+        for (int k = 0; k < CW; k += 2) {
+          const double2 q = *reinterpret_cast<const double2 *>(&prow_s[c0 + k]);
+          pr[k] = q.x;
+          pr[k + 1] = q.y;
+        }
+        if (r == kc) {
+#pragma unroll
+          for (int k = 0; k < CW; ++k) a[k] = pr[k];
+        } else {
+          const bool rp = (r == p);  // row p: the old row kc, factor = old (kc, kc)
+          const double fr = fcol[rp ? kc : (r < m ? r : 0)];
+          if (rp) {
+#pragma unroll
+            for (int k = 0; k < CW; ++k) a[k] = rowkc[c0 + k];
+          }
+          if (cb == kb) a[kk] = 0.0;
+#pragma unroll
+          for (int k = 0; k < CW; ++k) a[k] = a[k] - fr * pr[k];
+        }
+        if (kc + 1 < m) {
+          if (kk + 1 < CW) {
+            if (cb == kb) search(kk + 1, kc);
+          } else if (cb == kb + 1) {
+            search(0, kc);
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // undo the row interchanges on the columns: output column c is column colsrc[c]
+  if (threadIdx.x == 0) {
+    for (int c = 0; c < m; ++c) colsrc[c] = c;
+    for (int kc = m - 1; kc >= 0; --kc) {
+      const int p = perm[kc];
+      if (p != kc) {
+        const int t = colsrc[kc];
+        colsrc[kc] = colsrc[p];
+        colsrc[p] = t;
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < m) dstcol[colsrc[threadIdx.x]] = threadIdx.x;
+  __syncthreads();
+  if (wact && r < m) {
+#pragma unroll
+    for (int k = 0; k < CW; ++k)
+      if (c0 + k < m) Sg[(size_t)r * m + dstcol[c0 + k]] = a[k];
+  }
+}
+
 // x = J0^-1 b for one filament (shared-memory vectors; 128 threads)
 // b: 6nw entries [first-bead position rows | constraint rows | Lie rows]
 // x: 6nw entries [X0 | U | lambda/dt]
@@ -981,7 +1135,14 @@ fs_status fil_jacobian_build(fs_ctx *c, int nt) {
                                                       c->soff, c->aoff, c->Sinv, c->aux, nt, k, c->p.a, c->p.ah,
                                                       c->flags);
   FS_LAUNCH_CHECK();
-  k_schur_gj<<<c->nfil, 384, smem, c->stream>>>(c->fil_start, c->soff, c->Sinv, c->flags);
+  // all filaments of at most 32 beads: the register kernel; otherwise the
+  // shared-memory kernel for every filament
+  if (3 * c->max_nw <= GJ_MAX_M) {
+    const int m = 3 * c->max_nw, warps = ((m + 31) / 32) * ((m + GJ_CW - 1) / GJ_CW);
+    k_schur_gj_reg<<<c->nfil, 32 * warps, 0, c->stream>>>(c->fil_start, c->soff, c->Sinv, c->flags);
+  } else {
+    k_schur_gj<<<c->nfil, 384, smem, c->stream>>>(c->fil_start, c->soff, c->Sinv, c->flags);
+  }
   FS_LAUNCH_CHECK();
   return FS_OK;
 }

@@ -89,7 +89,7 @@ struct fs_ctx {
   double *Sinv;          // per-filament inverse Schur complement (3Nw x 3Nw row-major) at soff[f]
   double *aux;           // per-filament D', F' blocks, tangents, P coefficient at aoff[f]
   long long *soff, *aoff;
-  int max_nw;
+  int max_nw, min_nw;  // longest and shortest filament
   double *dots;          // broyden_maxiter partial dots
   double *partials;      // reduction scratch
   double *scalars;       // [0] = ||dE||

@@ -168,7 +168,8 @@ def flow_input(kind, dims, seed):
     raise ValueError(kind)
 
 
-@pytest.mark.parametrize("dims", [(64, 64, 64), (32, 128, 64), (128, 32, 256), (32, 32, 32)])
+@pytest.mark.parametrize("dims", [(64, 64, 64), (32, 128, 64), (128, 32, 256), (32, 32, 32),
+                                  (512, 32, 64), (256, 64, 128), (64, 512, 64), (32, 64, 512)])
 @pytest.mark.parametrize("kind", ["noise", "kz0", "kzN", "kxN"])
 def test_flow_solve_fp64_and_fp32_against_numpy(dims, kind):
     """Power-of-two grids with nz >= 64 run the FP32 five-pass transform
