@@ -788,10 +788,16 @@ __global__ void __launch_bounds__(768) k_schur_gj_reg(const int *__restrict__ fi
 // x = J0^-1 b for one filament (shared-memory vectors; 128 threads)
 // b: 6nw entries [first-bead position rows | constraint rows | Lie rows]
 // x: 6nw entries [X0 | U | lambda/dt]
-__device__ void schur_apply_one(int nw, const double *__restrict__ Sinv, const double *__restrict__ aux,
-                                const double *bb, double *x, double *y, double *w, double dt, double fac) {
+// aux_g: the filament's D', F', tangents and P coefficient in HBM; aux: shared
+// memory for their copy (the serial link recurrences then wait on shared, not
+// global, loads)
+__device__ void schur_apply_one(int nw, const double *__restrict__ Sinv, const double *__restrict__ aux_g,
+                                double *aux, const double *bb, double *x, double *y, double *w, double dt,
+                                double fac) {
   const int m = 3 * nw, nl = nw - 1;
   const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarp = nthr >> 5;
+  for (int i = tid; i < 20 * nl + 3 * nw + 1; i += nthr) aux[i] = aux_g[i];
+  __syncthreads();
   const double *dd = aux, *ee = aux + nl, *Fd = aux + 2 * nl, *Fl = Fd + 9 * nl, *tt = Fl + 9 * nl;
   const double pcoef = tt[3 * nw];
   const double *b1 = bb + 3, *b2 = bb + m;
@@ -815,14 +821,30 @@ __device__ void schur_apply_one(int nw, const double *__restrict__ Sinv, const d
     w[row] = b2[row] - g;
   }
   __syncthreads();
-  // u = S^-1 w: one warp per row, coalesced row reads
+  // u = S^-1 w: each warp takes eight rows at a time (coalesced row reads, all
+  // of their loads in flight together); per row the lane-strided sum and the
+  // shuffle tree of a one-row-per-warp product
   double *u = x + 3;
-  for (int row = warp; row < m; row += nwarp) {
-    const double *srow = Sinv + (size_t)row * m;
-    double acc = 0.0;
-    for (int c = lane; c < m; c += 32) acc += srow[c] * w[c];
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) u[row] = acc;
+  constexpr int RU = 8;
+  for (int row0 = warp * RU; row0 < m; row0 += nwarp * RU) {
+    double acc[RU];
+#pragma unroll
+    for (int q = 0; q < RU; ++q) acc[q] = 0.0;
+#pragma unroll 3
+    for (int c = lane; c < m; c += 32) {
+      const double wc = w[c];
+#pragma unroll
+      for (int q = 0; q < RU; ++q)
+        if (row0 + q < m) acc[q] += Sinv[(size_t)(row0 + q) * m + c] * wc;
+    }
+#pragma unroll
+    for (int q = 0; q < RU; ++q)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+    if (lane == 0)
+#pragma unroll
+      for (int q = 0; q < RU; ++q)
+        if (row0 + q < m) u[row0 + q] = acc[q];
   }
   __syncthreads();
   // z = b1 - C u, (C u)_r = fac c_0 + 2 fac sum_{1<=q<=r} c_q + fac c_{r+1}, c_q = cross(u_q, t_q)
@@ -866,6 +888,7 @@ __global__ void __launch_bounds__(128) k_schur_apply(const int *__restrict__ fil
                                                      const int *__restrict__ iter_d, size_t n6, double dt,
                                                      double fac) {
   __shared__ double bb[6 * FS_MAX_NW], xs[6 * FS_MAX_NW], y[3 * FS_MAX_NW], w[3 * FS_MAX_NW];
+  __shared__ double auxs[20 * (FS_MAX_NW - 1) + 3 * FS_MAX_NW + 1];
   const int f = blockIdx.x;
   const int b0 = fil_start[f], nw = fil_start[f + 1] - b0, s0 = 6 * b0, n = 6 * nw;
   const int tid = threadIdx.x, nthr = blockDim.x;
@@ -875,11 +898,12 @@ __global__ void __launch_bounds__(128) k_schur_apply(const int *__restrict__ fil
     for (int r = tid; r < n; r += nthr) xs[r] = bb[r];
     __syncthreads();
   } else {
-    schur_apply_one(nw, Sinv_all + soff[f], aux_all + aoff[f], bb, xs, y, w, dt, fac);
+    schur_apply_one(nw, Sinv_all + soff[f], aux_all + aoff[f], auxs, bb, xs, y, w, dt, fac);
   }
   const int ncol = iter_d ? *iter_d : iter;
   for (int r = tid; r < n; r += nthr) {
     double v = xs[r];
+#pragma unroll 4
     for (int i = 0; i < ncol; ++i) v += C[(size_t)i * n6 + s0 + r] * dots[i];
     x[s0 + r] = v;
   }
@@ -890,6 +914,7 @@ __global__ void __launch_bounds__(128) k_schur_inverse(int nw, const double *__r
                                                        const double *__restrict__ aux, double dt, double fac,
                                                        double *__restrict__ out) {
   __shared__ double bb[6 * FS_MAX_NW], xs[6 * FS_MAX_NW], y[3 * FS_MAX_NW], w[3 * FS_MAX_NW];
+  __shared__ double auxs[20 * (FS_MAX_NW - 1) + 3 * FS_MAX_NW + 1];
   const int n = 6 * nw, e = blockIdx.x, tid = threadIdx.x;
   for (int r = tid; r < n; r += blockDim.x) bb[r] = (r == e) ? 1.0 : 0.0;
   __syncthreads();
@@ -897,7 +922,7 @@ __global__ void __launch_bounds__(128) k_schur_inverse(int nw, const double *__r
     for (int r = tid; r < n; r += blockDim.x) xs[r] = bb[r];
     __syncthreads();
   } else {
-    schur_apply_one(nw, Sinv, aux, bb, xs, y, w, dt, fac);
+    schur_apply_one(nw, Sinv, aux, auxs, bb, xs, y, w, dt, fac);
   }
   for (int r = tid; r < n; r += blockDim.x) out[(size_t)r * n + e] = xs[r];
 }
