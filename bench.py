@@ -17,9 +17,14 @@ the 200 steps of the configured run. Every arm starts from that same state.
 value      mixed precision (FP32 spread/FFT/interpolation, FP64 Broyden and
            filament mechanics) with the learned warm start (trained untimed
            before the run by the library's own kernels on 20 seeded plain-solver
-           runs of this workload, K_B log-uniform in [0.1, 10]); inputs resident
-           in HBM, device-timed with CUDA events on the context's stream, max
-           over ranks; weak scaling (one independent replica per GPU).
+           runs of this workload, K_B log-uniform in [0.1, 10]) under its cost
+           gate (fs_warm_start_gate, period 8: each step takes the start with the
+           lower running mean of mobility solves per step, the other one every
+           8th step; learned.gate reports how many timed steps took each);
+           inputs resident in HBM, device-timed with CUDA events on the
+           context's stream, max over ranks; weak scaling (one independent
+           replica per GPU).
+learned_every_step the same steps with the learned start on every step.
 fp32_plain_start   the same steps from the reference's extrapolated start.
 plain_fp64 the same steps with the FCM chain in FP64 and the reference's start.
 e2e        the value arm through the C-ABI with HOST state: every step uploads
@@ -58,6 +63,7 @@ PREP_STEPS = 12
 # warm-start training data: seeds TRAIN_SEED0.. of this workload, K_B log-uniform in [0.1, 10]
 TRAIN_SEED0 = 7000
 TRAIN_EPOCHS = 40
+GATE_PERIOD = 8  # the learned start's cost gate probes the other start every 8th step
 ENSEMBLE_SEED = 3000
 # DRAM bytes per launch from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum);
 # the kernels and captures are listed in profiles/.
@@ -253,10 +259,19 @@ def run_ours(args, rank, world):
             learned_failed = learned
             learned = None
 
-    def timed_steps(prec, mode, profile=False):
+    def gate_stats():
+        steps = np.zeros(2, np.int64)
+        solves = np.zeros(2, np.float64)
+        abi.check(abi.lib().fs_warm_start_gate_stats(ctx.h, steps.ctypes.data_as(ctypes.c_void_p),
+                                                     solves.ctypes.data_as(ctypes.c_void_p)),
+                  "fs_warm_start_gate_stats")
+        return steps, solves
+
+    def timed_steps(prec, mode, profile=False, gate=0):
         ctx.set_precision(prec)
         if learned:
             set_warm_start(ctx, mode)
+            abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate if mode else 0), "fs_warm_start_gate")
         # reference-start arms run each steady step as one CUDA graph (Broyden loop on
         # the device); the learned start decides on the host and runs host-driven
         graph = 0 if (args.no_graph or (learned and mode)) else 1
@@ -264,6 +279,7 @@ def run_ours(args, rank, world):
         sim = Simulation(ctx, prep.copy())
         sim.run_steps(nt0, W)
         barrier()
+        g0 = gate_stats()[0] if learned else None
         if profile:
             ctx.profile_enable(True)
         launches0 = abi.lib().fs_kernel_launches()
@@ -282,16 +298,23 @@ def run_ours(args, rank, world):
         if profile:
             ctx.profile_enable(False)
         diag = sim.diag()
+        if learned:
+            g1, gs = gate_stats()
+            diag.gate = {"period": gate if mode else 0, "timed_plain_start_steps": int(g1[0] - g0[0]),
+                         "timed_learned_start_steps": int(g1[1] - g0[1]),
+                         "mean_solves_per_step": {"plain_start": float(gs[0]), "learned_start": float(gs[1])}}
         barrier()
         return max_over_ranks(ms), its, st, prof, clk.summary(), launches, diag
 
     mode = 1 if learned else 0
-    ms, its, st, _, clocks, launches, diag = timed_steps(abi.FS_PREC_FP32, mode)
+    gate = GATE_PERIOD if learned else 0
+    ms, its, st, _, clocks, launches, diag = timed_steps(abi.FS_PREC_FP32, mode, gate=gate)
     # stage breakdown: the same steps again, host-driven with CUDA-event stage timing
     # (graph-captured steps carry no events); not part of the timed value
     abi.check(abi.lib().fs_set_graph_mode(ctx.h, 0), "fs_set_graph_mode")
     if learned:
         set_warm_start(ctx, mode)
+        abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate), "fs_warm_start_gate")
     simp = Simulation(ctx, prep.copy())
     simp.run_steps(nt0, W)
     ctx.profile_enable(True)
@@ -322,6 +345,7 @@ def run_ours(args, rank, world):
     if learned:
         nlf = diag.learned_filaments + diag.fallback_filaments
         learned["learned_fraction"] = diag.learned_filaments / max(1, nlf)
+        learned["gate"] = diag.gate
         out["learned"] = learned
     elif learned_failed:
         out["learned"] = dict(learned_failed, error="training loss not finite; value is the reference's start")
@@ -358,8 +382,16 @@ def run_ours(args, rank, world):
     out["fcm_chain"] = {"ms_per_solve": fcm_ms / solves, "bytes_per_solve": b_fcm,
                         "GBps": b_fcm / (fcm_ms / solves / 1e3) / 1e9, "frac": b_fcm / (fcm_ms / solves / 1e3) / 1e9 / peak}
 
-    # the same steps from the reference's start (no learned iterate), FP32 chain
+    # the same steps from the reference's start (no learned iterate), FP32 chain,
+    # and with the learned start on every step (no cost gate)
     if learned:
+        msa, itsa, sta, _, _, _, da = timed_steps(abi.FS_PREC_FP32, mode, gate=0)
+        nla = da.learned_filaments + da.fallback_filaments
+        out["learned_every_step"] = {"value": world * npb * K / (msa / 1e3), "ms_per_step": msa / K,
+                                     "iters_per_step": float(np.mean(itsa)),
+                                     "status": abi.STATUS_NAMES.get(sta, sta),
+                                     "mobility_solves_per_step": da.mobility_solves / K,
+                                     "learned_fraction": da.learned_filaments / max(1, nla)}
         ms0, its0, st0, _, _, _, d0 = timed_steps(abi.FS_PREC_FP32, 0)
         out["fp32_plain_start"] = {"value": world * npb * K / (ms0 / 1e3), "ms_per_step": ms0 / K,
                                    "iters_per_step": float(np.mean(its0)), "status": abi.STATUS_NAMES.get(st0, st0),
@@ -376,6 +408,7 @@ def run_ours(args, rank, world):
         ctx.set_precision(abi.FS_PREC_FP32)
         if learned:
             set_warm_start(ctx, mode)
+            abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate), "fs_warm_start_gate")
         abi.check(abi.lib().fs_set_graph_mode(ctx.h, 0 if (args.no_graph or (learned and mode)) else 1),
                   "fs_set_graph_mode")
         host = prep.copy()

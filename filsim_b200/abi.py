@@ -183,6 +183,8 @@ def _declare(L):
         "fs_learn_record": (c_int, [c_void_p, c_int]),
         "fs_learn_targets": (c_int, [c_void_p, c_void_p]),
         "fs_set_warm_start": (c_int, [c_void_p, c_int]),
+        "fs_warm_start_gate": (c_int, [c_void_p, c_int]),
+        "fs_warm_start_gate_stats": (c_int, [c_void_p, c_void_p, c_void_p]),
         "fs_set_graph_mode": (c_int, [c_void_p, c_int]),
         "fs_autotune": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
         "fs_set_tuning": (c_int, [c_void_p, c_void_p]),

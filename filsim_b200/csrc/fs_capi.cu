@@ -119,7 +119,9 @@ namespace {
 // one implicit step (main.cpp:334-707)
 fs_status step_implicit(fs_ctx *c, int nt, int *iters_out) {
   FS_TRY(fil_initial_guess(c));
-  const bool learned = learn_active(c) && nt > c->p.initial_friction_steps;
+  const bool learn_on = learn_active(c) && nt > c->p.initial_friction_steps;
+  const bool learned = learn_on && learn_gate_choose(c);
+  const long long solves0 = c->diag.mobility_solves;
   if (learned || learn_recording(c)) FS_TRY(learn_save_guess(c));
   FS_TRY(fil_forces(c, nt));
   FS_TRY(fil_jacobian_build(c, nt));
@@ -147,6 +149,7 @@ fs_status step_implicit(fs_ctx *c, int nt, int *iters_out) {
     check = c->flags_h[FLAG_CHECK];
   }
   if (learn_recording(c)) FS_TRY(learn_capture_targets(c, iter));
+  if (learn_on) learn_gate_record(c, learned, c->diag.mobility_solves - solves0);
   FS_TRY(learn_end_step(c));
   FS_TRY(fil_step(c, nt));
   c->diag.last_nt = nt;

@@ -54,6 +54,14 @@ struct fs_mlp {
   bool have_targets;
   bool override_next;              // the next warm start uses pred as given (fs_learn_override)
   long long learned_total, fallback_total;
+  // cost gate of the learned start (fs_warm_start_gate): per start, the running
+  // mean of mobility solves per step; the cheaper start runs, the other every
+  // gate_period-th step so that its mean stays current
+  int gate_period;                 // 0: off (the learned start runs every step)
+  double gate_solves[2];           // [0] plain start, [1] learned start
+  int gate_have[2];
+  int gate_since;
+  long long gate_steps[2];
 };
 
 namespace {
@@ -510,6 +518,28 @@ fs_status ensure_step_buffers(fs_ctx *c) {
 
 // ---- internal entry points used by the step driver -----------------------------------
 bool learn_active(const fs_ctx *c) { return c->mlp && c->mlp->mode > 0; }
+
+// the start of this step under the cost gate (true: learned)
+bool learn_gate_choose(fs_ctx *c) {
+  fs_mlp *m = c->mlp;
+  if (!m->gate_period) return true;
+  if (!m->gate_have[0]) return false;
+  if (!m->gate_have[1]) return true;
+  const int best = m->gate_solves[1] < m->gate_solves[0] ? 1 : 0;
+  if (++m->gate_since >= m->gate_period) {
+    m->gate_since = 0;
+    return best == 0;
+  }
+  return best == 1;
+}
+
+void learn_gate_record(fs_ctx *c, bool learned, long long solves) {
+  fs_mlp *m = c->mlp;
+  const int i = learned ? 1 : 0;
+  m->gate_solves[i] = m->gate_have[i] ? 0.7 * m->gate_solves[i] + 0.3 * (double)solves : (double)solves;
+  m->gate_have[i] = 1;
+  m->gate_steps[i]++;
+}
 bool learn_recording(const fs_ctx *c) { return c->mlp && c->mlp->record; }
 
 // after fil_initial_guess: keep the plain guess (for the fallback and the targets)
@@ -931,6 +961,26 @@ fs_status fs_set_warm_start(fs_ctx *c, int mode) {
   if (!c || mode < 0 || mode > 2) return FS_ERR_INVALID_ARG;
   if (mode > 0 && !c->mlp) return FS_ERR_STATE;
   if (c->mlp) c->mlp->mode = mode;
+  return FS_OK;
+}
+
+fs_status fs_warm_start_gate(fs_ctx *c, int period) {
+  if (!c || period < 0) return FS_ERR_INVALID_ARG;
+  if (!c->mlp) return period ? FS_ERR_STATE : FS_OK;
+  fs_mlp *m = c->mlp;
+  m->gate_period = period;
+  m->gate_have[0] = m->gate_have[1] = 0;
+  m->gate_since = 0;
+  m->gate_steps[0] = m->gate_steps[1] = 0;
+  return FS_OK;
+}
+
+fs_status fs_warm_start_gate_stats(fs_ctx *c, long long *steps_h, double *solves_h) {
+  if (!c || !steps_h || !solves_h) return FS_ERR_INVALID_ARG;
+  for (int i = 0; i < 2; ++i) {
+    steps_h[i] = c->mlp ? c->mlp->gate_steps[i] : 0;
+    solves_h[i] = (c->mlp && c->mlp->gate_have[i]) ? c->mlp->gate_solves[i] : 0.0;
+  }
   return FS_OK;
 }
 

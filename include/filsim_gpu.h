@@ -388,6 +388,16 @@ fs_status fs_learn_override(fs_ctx *ctx, const float *pred_d);
  * rows) from the learned start exceeds that of the plain start is put back to
  * the plain start. */
 fs_status fs_set_warm_start(fs_ctx *ctx, int mode);
+/* Cost gate of the learned start (no reference counterpart): with period > 0,
+ * each step runs the start (learned or plain) whose running mean of mobility
+ * solves per step is lower, and the other one every period-th step so that its
+ * mean stays current; the learned start pays off only when it saves more
+ * Broyden iterations than its own extra solves. period 0 (the default) runs the
+ * learned start every step. Resets the statistics. */
+fs_status fs_warm_start_gate(fs_ctx *ctx, int period);
+/* steps_h[2], solves_h[2]: steps run and running mean solves per step, [0] plain
+ * start, [1] learned start, since the last fs_warm_start_gate. */
+fs_status fs_warm_start_gate_stats(fs_ctx *ctx, long long *steps_h, double *solves_h);
 /* D[M x N] (FP32) = A[M x K] B[N x K]^T with BF16 operands on the tensor cores;
  * M, N multiples of 128, K of 64. */
 fs_status fs_gemm_bf16(fs_ctx *ctx, const void *A_d, const void *B_d, float *D_d, int M, int N, int K);

@@ -168,3 +168,36 @@ def test_trained_network_gain(gpu_lib):
     print("held-out X0 correction rms %.3e, residual after prediction %.3e; iterations plain %s learned %s"
           % (x0_rms, x0_err, list(its_plain), list(its)))
     ctx.close()
+
+
+def test_cost_gate(gpu_lib):
+    """fs_warm_start_gate: each step takes the start with the lower running mean of
+    mobility solves per step and probes the other every period-th step; with the gate
+    off the learned start runs on every step."""
+    ctx, model, sim = prepared()
+    s0 = snapshot(sim)
+    set_warm_start(ctx, 1)
+
+    def stats():
+        steps = np.zeros(2, np.int64)
+        solves = np.zeros(2, np.float64)
+        ctx.call("fs_warm_start_gate_stats", ctypes.c_void_p(steps.ctypes.data),
+                 ctypes.c_void_p(solves.ctypes.data))
+        return steps, solves
+
+    ctx.call("fs_warm_start_gate", 3)
+    its, st = sim.run_steps(WARM + 1, 12)
+    assert st == abi.FS_OK
+    steps, solves = stats()
+    assert steps.sum() == 12
+    assert steps.min() >= 2                       # both starts measured and re-probed
+    major = int(np.argmax(steps))
+    assert solves[major] <= solves[1 - major]     # the start run most is the cheaper one
+    # gate off: the learned start on every step
+    sim.upload(s0)
+    ctx.call("fs_warm_start_gate", 0)
+    its, st = sim.run_steps(WARM + 1, 4)
+    d = sim.diag()  # counts of this call
+    assert st == abi.FS_OK
+    assert d.learned_filaments + d.fallback_filaments == 4 * NFIL
+    ctx.close()
