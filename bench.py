@@ -51,7 +51,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "bead-steps/s & Broyden iters/step: learned+FP32 vs plain FP64 GPU, resid<=1e-6"
 UNIT = "bead-steps/s"
-WORKLOAD = dict(npts=512, nfil=4096, nw=32, seed=1002)
+WORKLOAD = dict(npts=512, nfil=4096, nw=32, seed=1002, name="sediment_512")
 # Broyden iterations per steady-state step of sediment_512 (FP64 chain, the
 # reference's start; measured on B200) used to scale the CPU baseline's
 # per-iteration sample to whole steps in the reference arm, which runs without
@@ -68,8 +68,9 @@ ENSEMBLE_SEED = 3000
 # DRAM bytes per launch from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum);
 # the kernels and captures are listed in profiles/.
 NCU_TRAFFIC = {
-    # mobility_256 capture of k_spread<float, 64>: 249.4 MB, scaled x8 to the 512^3 grid it writes
-    "spread": 1.995e9,
+    # per grid point, from the ncu capture of the spread kernel in profiles/ (DRAM read +
+    # write), times the grid points of the workload
+    "spread": 1.995e9 / 512 ** 3,
 }
 
 
@@ -91,7 +92,22 @@ def parse():
                     help="sediment_512: implicit steps (the headline); mobility_256: FCM mobility solves, "
                          "FP32 against FP64, on 256^3 with 1024 x 30 beads; ensemble_64: 64 independent "
                          "boxes advanced by one graph launch per step")
-    return ap.parse_args()
+    ap.add_argument("--grid", type=int, default=None,
+                    help="sediment_512 / mobility_256 on another cubic grid (profiling cases; the "
+                         "workload name in config says so)")
+    ap.add_argument("--filaments", type=int, default=None, help="and another filament count")
+    args = ap.parse_args()
+    if args.grid or args.filaments:
+        w = WORKLOAD if args.workload == "sediment_512" else None
+        if args.workload == "mobility_256":
+            from filsim_b200.configs import WORKLOADS
+            w = WORKLOADS["mobility_256"]
+        if w is not None:
+            w["npts"] = args.grid or w["npts"]
+            w["nfil"] = args.filaments or w["nfil"]
+            base = "sediment" if args.workload == "sediment_512" else "mobility"
+            w["name"] = "%s_%d_%dx%d" % (base, w["npts"], w["nfil"], w["nw"])
+    return args
 
 
 def measured_peaks():
@@ -327,7 +343,7 @@ def run_ours(args, rank, world):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 FCM chain + f64 Broyden/mechanics", "data": "synthetic (seeded rejection-placed filaments)",
-        "config": {"workload": "sediment_512", "grid": [512, 512, 512], "filaments": WORKLOAD["nfil"],
+        "config": {"workload": WORKLOAD["name"], "grid": [WORKLOAD["npts"]] * 3, "filaments": WORKLOAD["nfil"],
                    "beads_per_filament": nw, "beads": npb, "dt": p.dt, "tol": p.tol,
                    "precision": "mixed", "learned_warm_start": bool(learned),
                    "timed_steps": [nt0 + W, nt0 + W + K - 1],
@@ -355,8 +371,9 @@ def run_ours(args, rank, world):
 
     # roofline of the dominant kernel stage of this library
     peak, peak_kind = measured_peaks()
-    N = 512 ** 3
-    NH = 512 * 512 * 257
+    npts = WORKLOAD["npts"]
+    N = npts ** 3
+    NH = npts * npts * (npts // 2 + 1)
     s_real = 4  # FP32 grids in the mixed path
     aux = 20 * (nw - 1) + 3 * nw + 1  # doubles of D', F', tangents and P per filament (fil_aux_size)
     alg_bytes = {
@@ -374,7 +391,8 @@ def run_ours(args, rank, world):
     achieved = alg_bytes[dom] / (per_launch_ms / 1e3) / 1e9
     out["roofline"] = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                        "frac": achieved / peak, "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind,
-                       "traffic": NCU_TRAFFIC.get(dom), "algorithmic_bytes": alg_bytes[dom],
+                       "traffic": NCU_TRAFFIC[dom] * N if dom in NCU_TRAFFIC else None,
+                       "algorithmic_bytes": alg_bytes[dom],
                        "launch_ms": per_launch_ms}
     fcm_ms = sum(stage_ms.get(k, 0) for k in ("spread", "fft_fwd", "project", "fft_inv", "interp"))
     solves = max(1, stage_calls.get("interp", 0))
@@ -492,7 +510,7 @@ def run_mobility(args, rank, world):
             "unit": "bead-solves/s", "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded rejection-placed filaments, F, T ~ N(0,1))",
-            "config": {"workload": "mobility_256", "grid": [256, 256, 256], "filaments": w["nfil"],
+            "config": {"workload": w.get("name", "mobility_256"), "grid": [w["npts"]] * 3, "filaments": w["nfil"],
                        "beads_per_filament": w["nw"], "beads": s.np, "l2": "grids (~0.4 GB) larger than L2"},
             "fp64": {"value": s.np * K / (res["fp64"]["ms"] / 1e3), "ms_per_step": res["fp64"]["ms"] / K},
             "fp32_error_vs_fp64": {"U": relerr(res["fp32"]["V"], res["fp64"]["V"]),
@@ -700,8 +718,8 @@ def run_reference(args, rank, world):
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded rejection-placed filaments)",
-            "config": {"workload": "sediment_512", "grid": [512, 512, 512], "filaments": WORKLOAD["nfil"],
-                       "beads_per_filament": WORKLOAD["nw"], "beads": susp.np},
+            "config": {"workload": WORKLOAD["name"], "grid": [WORKLOAD["npts"]] * 3,
+                       "filaments": WORKLOAD["nfil"], "beads_per_filament": WORKLOAD["nw"], "beads": susp.np},
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
