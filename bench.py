@@ -70,7 +70,7 @@ ENSEMBLE_SEED = 3000
 NCU_TRAFFIC = {
     # per grid point, from the ncu capture of the spread kernel in profiles/ (DRAM read +
     # write), times the grid points of the workload
-    "spread": 1.995e9 / 512 ** 3,
+    "spread": (11.94e6 + 147.48e6) / 256 ** 3,  # k_spread32, mobility_256 with 512 x 30 beads
 }
 
 
