@@ -15,6 +15,7 @@
 //                        the Schur inverse, then the bad-Broyden history corrections
 //   k_broyden_cols       history update of main.cpp:640-663
 //   k_update / k_step    Filament::update (Filament.hpp:425-452), Filament::step (:455-478)
+#include <algorithm>
 #include "fs_internal.cuh"
 
 namespace {
@@ -1156,7 +1157,9 @@ fs_status fil_jacobian_build(fs_ctx *c, int nt) {
   ProfScope ps(c, FS_STAGE_JACOBIAN);
   FilConsts k = make_fconsts(c);
   const size_t smem = sizeof(double) * 9 * (size_t)c->max_nw * c->max_nw;
-  k_jacobian_schur<<<c->nfil, 256, smem, c->stream>>>(c->fil_start, c->qs, c->Us, c->TAU, c->lam, c->kap, c->cc,
+  // one thread per Schur column (3 Nw, rounded to warps): three filaments share an SM
+  const int jthreads = std::min(256, 32 * ((3 * c->max_nw + 31) / 32));
+  k_jacobian_schur<<<c->nfil, jthreads, smem, c->stream>>>(c->fil_start, c->qs, c->Us, c->TAU, c->lam, c->kap, c->cc,
                                                       c->soff, c->aoff, c->Sinv, c->aux, nt, k, c->p.a, c->p.ah,
                                                       c->flags);
   FS_LAUNCH_CHECK();
