@@ -633,8 +633,9 @@ __global__ void __launch_bounds__(384) k_schur_gj(const int *__restrict__ fil_st
 }
 
 // The same inversion with the matrix in registers, for m = 3 nw <= 96: warp
-// w = cb RB + rb (RB = ceil(m / 32) row blocks, CB = ceil(m / 12) column blocks)
-// holds rows 32 rb .. 32 rb + 31 (one per lane) of columns 12 cb .. 12 cb + 11.
+// w = cb RB + rb (RB = ceil(m / 32) row blocks, CB = ceil(m / 24) column blocks)
+// holds rows 32 rb .. 32 rb + 31 (one per lane) of columns 24 cb .. 24 cb + 23:
+// 12 warps at m = 96, two matrices per SM.
 // Per pivot kc (row p and 1 / S[p][kc], found by the previous step):
 //   A: the lane holding row p publishes it scaled (prow = row p / v, with
 //      1 / v in column kc), the lane holding row kc publishes its old row, the
@@ -645,9 +646,9 @@ __global__ void __launch_bounds__(384) k_schur_gj(const int *__restrict__ fil_st
 //      search it over rows > kc (first maximum, by shuffles, per row block).
 // Each element sees the operations and roundings of k_schur_gj; two barriers per
 // pivot, one register-blocked outer product per thread.
-constexpr int GJ_CW = 12;        // columns per warp
+constexpr int GJ_CW = 24;        // columns per warp
 constexpr int GJ_MAX_M = 96;     // m handled by the register kernel
-__global__ void __launch_bounds__(768) k_schur_gj_reg(const int *__restrict__ fil_start,
+__global__ void __launch_bounds__(384, 2) k_schur_gj_reg(const int *__restrict__ fil_start,
                                                       const long long *__restrict__ soff,
                                                       double *__restrict__ Sinv_all, int *__restrict__ flags) {
   constexpr int CW = GJ_CW;
@@ -732,16 +733,13 @@ __global__ void __launch_bounds__(768) k_schur_gj_reg(const int *__restrict__ fi
       __syncthreads();
       // phase B
       if (wact) {
-        double pr[CW];
-#pragma unroll
-        for (int k = 0; k < CW; k += 2) {
-          const double2 q = *reinterpret_cast<const double2 *>(&prow_s[c0 + k]);
-          pr[k] = q.x;
-          pr[k + 1] = q.y;
-        }
         if (r == kc) {
 #pragma unroll
-          for (int k = 0; k < CW; ++k) a[k] = pr[k];
+          for (int k = 0; k < CW; k += 2) {
+            const double2 q = *reinterpret_cast<const double2 *>(&prow_s[c0 + k]);
+            a[k] = q.x;
+            a[k + 1] = q.y;
+          }
         } else {
           const bool rp = (r == p);  // row p: the old row kc, factor = old (kc, kc)
           const double fr = fcol[rp ? kc : (r < m ? r : 0)];
@@ -751,7 +749,11 @@ __global__ void __launch_bounds__(768) k_schur_gj_reg(const int *__restrict__ fi
           }
           if (cb == kb) a[kk] = 0.0;
 #pragma unroll
-          for (int k = 0; k < CW; ++k) a[k] = a[k] - fr * pr[k];
+          for (int k = 0; k < CW; k += 2) {
+            const double2 q = *reinterpret_cast<const double2 *>(&prow_s[c0 + k]);
+            a[k] = a[k] - fr * q.x;
+            a[k + 1] = a[k + 1] - fr * q.y;
+          }
         }
         if (kc + 1 < m) {
           if (kk + 1 < CW) {
