@@ -144,20 +144,20 @@ __global__ void __launch_bounds__(128) k_barrier(const double *__restrict__ Y, d
   int npairs_here = 0;
   int out_base = (mode == 2) ? pair_off[b] : 0;
   double f[3], rsq;
-  // ---- b as i: the rest of its own cell, then the 13 neighbour cells ----
+  // cell ranges of both halves loaded up front (independent loads in flight together)
+  int rs_i[14], re_i[14];
+#pragma unroll
   for (int slot = 0; slot < 14; ++slot) {
-    int qs, qe;
-    int cj;
-    if (slot == 0) {
-      cj = cb;
-      qs = s0;
-      qe = p_asc;  // ascending positions below b's: later in the list
-    } else {
-      cj = map[13 * cb + slot - 1];
-      qs = start[cj];
-      qe = start[cj + 1];
-    }
-    const int ej = start[cj + 1];
+    const int cj = slot == 0 ? cb : map[13 * cb + slot - 1];
+    rs_i[slot] = start[cj];
+    re_i[slot] = start[cj + 1];
+  }
+  // ---- b as i: the rest of its own cell, then the 13 neighbour cells ----
+#pragma unroll 1
+  for (int slot = 0; slot < 14; ++slot) {
+    const int qs = rs_i[slot];
+    const int qe = slot == 0 ? p_asc : re_i[slot];  // own cell: ascending positions below b's
+    const int ej = re_i[slot];
     for (int q = qe - 1; q >= qs; --q) {
       const int j = sorted[q];
       if (excluded(k, fil_id, seg_id, b, j)) continue;
@@ -193,18 +193,27 @@ __global__ void __launch_bounds__(128) k_barrier(const double *__restrict__ Y, d
   // ---- b as j: beads before it in its own cell, and the cells whose slot maps to b's cell ----
   const int Mx = k.M[0], My = k.M[1];
   const int cx = cb % Mx, cy = (cb / Mx) % My, cz = cb / (Mx * My);
+  int rs_j[14], re_j[14], ci_j[14];
+#pragma unroll
   for (int slot = 0; slot < 14; ++slot) {
-    int ci, qs, qe;
+    const int ci = slot == 0 ? cb
+                             : icell(k.M, cx - c_nb_off[slot - 1][0], cy - c_nb_off[slot - 1][1],
+                                     cz - c_nb_off[slot - 1][2]);
+    ci_j[slot] = ci;
+    rs_j[slot] = start[ci];
+    re_j[slot] = start[ci + 1];
+  }
+#pragma unroll 1
+  for (int slot = 0; slot < 14; ++slot) {
+    int qs, qe;
     if (slot == 0) {
-      ci = cb;
       qs = p_asc + 1;
       qe = e0;
     } else {
-      ci = icell(k.M, cx - c_nb_off[slot - 1][0], cy - c_nb_off[slot - 1][1], cz - c_nb_off[slot - 1][2]);
-      qs = start[ci];
-      qe = start[ci + 1];
+      qs = rs_j[slot];
+      qe = re_j[slot];
     }
-    const int ei = start[ci + 1];
+    const int ci = ci_j[slot], ei = re_j[slot];
     for (int q = qs; q < qe; ++q) {
       const int i = sorted[q];
       if (excluded(k, fil_id, seg_id, i, b)) continue;
