@@ -283,15 +283,16 @@ __global__ void __launch_bounds__(FS_SPREAD_THREADS)
 }
 
 // ---- 2b. FP32 spread on packed pairs -------------------------------------------
-// The FP32 chain's spread. k_spread_weights32 evaluates each bead's stencil
-// weights once per solve, (g, d, r, r d) per axis and stencil index, with the
-// FP32 arithmetic of k_spread<float> (gaussian_setup, FCMfunctions.cpp:565-589:
-// xx = xg dx - Y in double, then the float Gaussians). k_spread32 then runs one
-// CTA (8 warps) per half of a 16^3 tile: x in [8h, 8h+8) of the tile, all y and
-// z. Warp w owns the 4 x 16 x 4 column x in [4(w&1), +4), z in [4(w>>1), +4);
-// lane l owns x = 4(w&1) + (l&3), the z pair 4(w>>1) + 2((l>>2)&1) + {0, 1}
-// and y = (l>>3) + 4k, k < 4: eight points held as four packed pairs per
-// component. Per staged bead reaching the warp's column the lane forms the
+// The FP32 chain's spread. k_spread_records32 writes each bead's record once per
+// solve: stencil starts, F, T/2 and the weights (g, d, r, r d) per axis and
+// stencil index, with the FP32 arithmetic of k_spread<float> (gaussian_setup,
+// FCMfunctions.cpp:565-589: xx = xg dx - Y in double, then the float Gaussians).
+// k_spread32 then runs one CTA (8 warps) per 16^3 tile, which stages the tile's
+// candidate records once and covers its 16 columns of 4 x 16 x 4 points in two
+// passes: in pass p warp w owns x in [4(w&3), +4), z in [4cz, +4) with
+// cz = (w>>2) + 2p; lane l owns x = 4(w&3) + (l&3), the z pair 4cz + 2((l>>2)&1)
+// + {0, 1} and y = (l>>3) + 4k, k < 4: eight points held as four packed pairs per
+// component (two columns per warp even out the warps' bead counts). Per staged bead reaching the warp's column the lane forms the
 // x-z factors of its pair once, then each covered y row costs three packed
 // FMA chains and three packed Kahan updates:
 //   y = term + nc, t = s + y, nc = y - (t - s), s = t      (nc = -c of Kahan)
@@ -340,11 +341,11 @@ constexpr int FS_SPREAD32_REC_MAX = 3 + 3 * 16;  // record length for the larges
 template <int CH>
 struct SpreadStage32 {
   float4 raw[CH * FS_SPREAD32_REC_MAX];      // the chunk's records (slot sl at sl RL), copied as they are
-  float4 xw[CH][8];                          // (g, d, r, -) by x of the half tile
+  float4 xw[CH][FS_TILE];                    // (g, d, r, -) by tile-local x
   float zg[CH][FS_TILE], zd[CH][FS_TILE], zr[CH][FS_TILE];  // by tile-local z
   float4 yw[CH][FS_TILE];                    // (g, g, d, d) by tile-local y
   float2 yrd[CH][FS_TILE];                   // (r d, r d)
-  unsigned xzm[CH];                          // x coverage (8 bits) | z coverage (16 bits) << 8
+  unsigned xzm[CH];                          // x coverage (16 bits) | z coverage (16 bits) << 16
   unsigned rows[CH];                         // y rows k with a covered y in [4k, 4k + 4)
 };
 
@@ -355,7 +356,7 @@ __global__ void __launch_bounds__(FS_SPREAD32_THREADS, 3)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SpreadStage32<CH> &st = *reinterpret_cast<SpreadStage32<CH> *>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int tile = blockIdx.x >> 1, xh = blockIdx.x & 1;
+  const int tile = blockIdx.x;
   const int tz = tile % c.nbin[2], ty = (tile / c.nbin[2]) % c.nbin[1], tx = tile / (c.nbin[2] * c.nbin[1]);
   const int X0[3] = {tx * FS_TILE, ty * FS_TILE, tz * FS_TILE};
   // candidate bins, the tile's own bin and the one before it per axis, in the
@@ -379,21 +380,13 @@ __global__ void __launch_bounds__(FS_SPREAD32_THREADS, 3)
   int total = 0;
 #pragma unroll
   for (int r = 0; r < 8; ++r) total += cand_len[r];
-  const int cx = warp & 1, cz = warp >> 1;
-  const int xl = 4 * cx + (lane & 3), zl = 4 * cz + 2 * ((lane >> 2) & 1), ly = lane >> 3;
-  const int ngd = c.ngd;
-  f2p s[4][3], nc[4][3];
-#pragma unroll
-  for (int k = 0; k < 4; ++k)
-#pragma unroll
-    for (int a = 0; a < 3; ++a) s[k][a] = nc[k][a] = 0ull;
-
-  for (int base = 0; base < total; base += CH) {
-    const int nb = min(CH, total - base);
-    __syncthreads();  // the previous chunk's tables are no longer read
-    // staging, phase 1: the chunk's records to shared memory (slot sl at sl RL) with
-    // 16-byte asynchronous copies, one contiguous run per candidate bin, all independent
-    const int RL = spread_rec_len(ngd);
+  const int ngd = c.ngd, RL = spread_rec_len(ngd);
+  // staging of candidates [base, base + nb): records to shared memory (slot sl at
+  // sl RL) with 16-byte asynchronous copies, one contiguous run per candidate bin,
+  // then tables by tile coordinate, eight threads per bead slot (thread j takes
+  // x, y and z in {j, j + 8})
+  auto stage = [&](int base, int nb) {
+    __syncthreads();  // the previous tables are no longer read
     {
       int pre = 0;  // candidates before bin range r
 #pragma unroll 1
@@ -410,128 +403,145 @@ __global__ void __launch_bounds__(FS_SPREAD32_THREADS, 3)
     }
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
-    // phase 2: tables by tile coordinate, eight threads per bead slot; thread j
-    // takes x = 8h + j, y in {j, j+8}, z in {j, j+8}
     const int j = tid & 7;
 #pragma unroll 1
     for (int s0 = 0; s0 < CH; s0 += FS_SPREAD32_THREADS / 8) {
       const int sl = s0 + (tid >> 3);
       const bool act = sl < nb;
-      bool cov[5] = {false, false, false, false, false};
+      bool cov[6] = {false, false, false, false, false, false};
       if (act) {
         const float4 *rw = st.raw + sl * RL;
         const float4 hd = rw[0];
         const int swv[3] = {__float_as_int(hd.x), __float_as_int(hd.y), __float_as_int(hd.z)};
-        const int la[5] = {8 * xh + j, j, j + 8, j, j + 8};
-        const int ax[5] = {0, 1, 1, 2, 2};
-        float4 w[5];
+        float4 w[6];
 #pragma unroll
-        for (int it = 0; it < 5; ++it) {
-          const int a = ax[it], Nn = c.N[a];
-          const int i = wrap_near(la[it] + wrap_near(X0[a] - swv[a], Nn), Nn);
+        for (int it = 0; it < 6; ++it) {
+          const int a = it >> 1, l = j + 8 * (it & 1), Nn = c.N[a];
+          const int i = wrap_near(l + wrap_near(X0[a] - swv[a], Nn), Nn);
           cov[it] = i < ngd;
           w[it] = cov[it] ? rw[3 + a * ngd + i] : make_float4(0.f, 0.f, 0.f, 0.f);
         }
         st.xw[sl][j] = w[0];
-        st.yw[sl][j] = make_float4(w[1].x, w[1].x, w[1].y, w[1].y);
-        st.yrd[sl][j] = make_float2(w[1].w, w[1].w);
-        st.yw[sl][j + 8] = make_float4(w[2].x, w[2].x, w[2].y, w[2].y);
-        st.yrd[sl][j + 8] = make_float2(w[2].w, w[2].w);
-        st.zg[sl][j] = w[3].x;
-        st.zd[sl][j] = w[3].y;
-        st.zr[sl][j] = w[3].z;
-        st.zg[sl][j + 8] = w[4].x;
-        st.zd[sl][j + 8] = w[4].y;
-        st.zr[sl][j + 8] = w[4].z;
+        st.xw[sl][j + 8] = w[1];
+        st.yw[sl][j] = make_float4(w[2].x, w[2].x, w[2].y, w[2].y);
+        st.yrd[sl][j] = make_float2(w[2].w, w[2].w);
+        st.yw[sl][j + 8] = make_float4(w[3].x, w[3].x, w[3].y, w[3].y);
+        st.yrd[sl][j + 8] = make_float2(w[3].w, w[3].w);
+        st.zg[sl][j] = w[4].x;
+        st.zd[sl][j] = w[4].y;
+        st.zr[sl][j] = w[4].z;
+        st.zg[sl][j + 8] = w[5].x;
+        st.zd[sl][j + 8] = w[5].y;
+        st.zr[sl][j + 8] = w[5].z;
       }
       // coverage masks by ballot: lanes 8q .. 8q+7 of this warp hold slot s0 + 4 warp + q
-      const unsigned bx = __ballot_sync(0xffffffffu, cov[0]);
-      const unsigned by0 = __ballot_sync(0xffffffffu, cov[1]), by1 = __ballot_sync(0xffffffffu, cov[2]);
-      const unsigned bz0 = __ballot_sync(0xffffffffu, cov[3]), bz1 = __ballot_sync(0xffffffffu, cov[4]);
+      unsigned bal[6];
+#pragma unroll
+      for (int it = 0; it < 6; ++it) bal[it] = __ballot_sync(0xffffffffu, cov[it]);
       if (act && j == 0) {
         const int sh = lane & 24;
-        const unsigned xm = (bx >> sh) & 0xffu;
-        const unsigned ym = ((by0 >> sh) & 0xffu) | (((by1 >> sh) & 0xffu) << 8);
-        const unsigned zm = ((bz0 >> sh) & 0xffu) | (((bz1 >> sh) & 0xffu) << 8);
-        st.xzm[sl] = xm | (zm << 8);
+        unsigned m3[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) m3[a] = ((bal[2 * a] >> sh) & 0xffu) | (((bal[2 * a + 1] >> sh) & 0xffu) << 8);
+        st.xzm[sl] = m3[0] | (m3[2] << 16);
         unsigned rows = 0;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) rows |= ((ym >> (4 * k)) & 0xfu) ? (1u << k) : 0u;
+        for (int k = 0; k < 4; ++k) rows |= ((m3[1] >> (4 * k)) & 0xfu) ? (1u << k) : 0u;
         st.rows[sl] = rows;
       }
     }
     __syncthreads();
-    // staged beads reaching this warp's column
-    unsigned col[CH / 32];
+  };
+  const bool one_chunk = total <= CH;
+  if (one_chunk && total > 0) stage(0, total);  // both column passes read these tables
+  // two column passes: warp w owns x in [4 (w & 3), +4) and z in [4 cz, +4) with
+  // cz = (w >> 2) + 2 pass; lane roles as in the header
+  const int cx = warp & 3;
+  const int xl = 4 * cx + (lane & 3), ly = lane >> 3;
+#pragma unroll 1
+  for (int pass = 0; pass < 2; ++pass) {
+    const int cz = (warp >> 2) + 2 * pass;
+    const int zl = 4 * cz + 2 * ((lane >> 2) & 1);
+    f2p s[4][3], nc[4][3];
 #pragma unroll
-    for (int h = 0; h < CH / 32; ++h) {
-      const int sl = 32 * h + lane;
-      bool hit = false;
-      if (sl < nb) {
-        const unsigned m = st.xzm[sl];
-        hit = ((m >> (4 * cx)) & 0xfu) && ((m >> (8 + 4 * cz)) & 0xfu) && st.rows[sl];
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int a = 0; a < 3; ++a) s[k][a] = nc[k][a] = 0ull;
+    for (int base = 0; base < total; base += CH) {
+      const int nb = min(CH, total - base);
+      if (!one_chunk) stage(base, nb);  // block-uniform
+      // staged beads reaching this warp's column
+      unsigned col[CH / 32];
+#pragma unroll
+      for (int h = 0; h < CH / 32; ++h) {
+        const int sl = 32 * h + lane;
+        bool hit = false;
+        if (sl < nb) {
+          const unsigned m = st.xzm[sl];
+          hit = ((m >> (4 * cx)) & 0xfu) && ((m >> (16 + 4 * cz)) & 0xfu) && st.rows[sl];
+        }
+        col[h] = __ballot_sync(0xffffffffu, hit);
       }
-      col[h] = __ballot_sync(0xffffffffu, hit);
-    }
 #pragma unroll
-    for (int h = 0; h < CH / 32; ++h) {
-      unsigned m = col[h];
-      while (m) {
-        const int sl = 32 * h + __ffs(m) - 1;
-        m &= m - 1;
-        const unsigned rows = st.rows[sl];
-        const float4 wx = st.xw[sl][xl];
-        const float2 gz = *reinterpret_cast<const float2 *>(&st.zg[sl][zl]);
-        const float2 dz = *reinterpret_cast<const float2 *>(&st.zd[sl][zl]);
-        const float2 rz = *reinterpret_cast<const float2 *>(&st.zr[sl][zl]);
-        const float4 fh = st.raw[sl * RL + 1];  // F0, F1, F2, h0 (h = T / 2, GA_setup :536-547)
-        const float4 hh = st.raw[sl * RL + 2];  // h1, h2
-        // per z of the pair: f_a = F_a gx gz, the rotlet factors of k_spread (d = gdx gdz)
-        const float gxz0 = wx.x * gz.x, gxz1 = wx.x * gz.y;
-        const float dxz0 = wx.y * dz.x, dxz1 = wx.y * dz.y;
-        const f2p f0 = f2_pack(fh.x * gxz0, fh.x * gxz1);
-        const f2p f1 = f2_pack(fh.y * gxz0, fh.y * gxz1);
-        const f2p f2v = f2_pack(fh.z * gxz0, fh.z * gxz1);
-        const f2p h2d = f2_pack(hh.y * dxz0, hh.y * dxz1);
-        const f2p mh0d = f2_pack(-fh.w * dxz0, -fh.w * dxz1);
-        const f2p c0 = f2_pack(-hh.x * rz.x * dxz0, -hh.x * rz.y * dxz1);
-        const f2p c1 = f2_pack((-hh.y * wx.z + fh.w * rz.x) * dxz0, (-hh.y * wx.z + fh.w * rz.y) * dxz1);
-        const f2p c2 = f2_pack(hh.x * wx.z * dxz0, hh.x * wx.z * dxz1);
+      for (int h = 0; h < CH / 32; ++h) {
+        unsigned m = col[h];
+        while (m) {
+          const int sl = 32 * h + __ffs(m) - 1;
+          m &= m - 1;
+          const unsigned rows = st.rows[sl];
+          const float4 wx = st.xw[sl][xl];
+          const float2 gz = *reinterpret_cast<const float2 *>(&st.zg[sl][zl]);
+          const float2 dz = *reinterpret_cast<const float2 *>(&st.zd[sl][zl]);
+          const float2 rz = *reinterpret_cast<const float2 *>(&st.zr[sl][zl]);
+          const float4 fh = st.raw[sl * RL + 1];  // F0, F1, F2, h0 (h = T / 2, GA_setup :536-547)
+          const float4 hh = st.raw[sl * RL + 2];  // h1, h2
+          // per z of the pair: f_a = F_a gx gz, the rotlet factors of k_spread (d = gdx gdz)
+          const float gxz0 = wx.x * gz.x, gxz1 = wx.x * gz.y;
+          const float dxz0 = wx.y * dz.x, dxz1 = wx.y * dz.y;
+          const f2p f0 = f2_pack(fh.x * gxz0, fh.x * gxz1);
+          const f2p f1 = f2_pack(fh.y * gxz0, fh.y * gxz1);
+          const f2p f2v = f2_pack(fh.z * gxz0, fh.z * gxz1);
+          const f2p h2d = f2_pack(hh.y * dxz0, hh.y * dxz1);
+          const f2p mh0d = f2_pack(-fh.w * dxz0, -fh.w * dxz1);
+          const f2p c0 = f2_pack(-hh.x * rz.x * dxz0, -hh.x * rz.y * dxz1);
+          const f2p c1 = f2_pack((-hh.y * wx.z + fh.w * rz.x) * dxz0, (-hh.y * wx.z + fh.w * rz.y) * dxz1);
+          const f2p c2 = f2_pack(hh.x * wx.z * dxz0, hh.x * wx.z * dxz1);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          if (rows & (1u << k)) {
-            const ulonglong2 gd = *reinterpret_cast<const ulonglong2 *>(&st.yw[sl][ly + 4 * k]);
-            const f2p rd = *reinterpret_cast<const f2p *>(&st.yrd[sl][ly + 4 * k]);
-            f2p y, t;
-            // f0 g + h2d (r d) + c0 d
-            y = f2_fma(f0, gd.x, f2_fma(h2d, rd, f2_fma(c0, gd.y, nc[k][0])));
-            t = f2_add(s[k][0], y);
-            nc[k][0] = f2_sub(y, f2_sub(t, s[k][0]));
-            s[k][0] = t;
-            // f1 g + c1 d
-            y = f2_fma(f1, gd.x, f2_fma(c1, gd.y, nc[k][1]));
-            t = f2_add(s[k][1], y);
-            nc[k][1] = f2_sub(y, f2_sub(t, s[k][1]));
-            s[k][1] = t;
-            // f2 g + c2 d - h0d (r d)
-            y = f2_fma(f2v, gd.x, f2_fma(mh0d, rd, f2_fma(c2, gd.y, nc[k][2])));
-            t = f2_add(s[k][2], y);
-            nc[k][2] = f2_sub(y, f2_sub(t, s[k][2]));
-            s[k][2] = t;
+          for (int k = 0; k < 4; ++k) {
+            if (rows & (1u << k)) {
+              const ulonglong2 gd = *reinterpret_cast<const ulonglong2 *>(&st.yw[sl][ly + 4 * k]);
+              const f2p rd = *reinterpret_cast<const f2p *>(&st.yrd[sl][ly + 4 * k]);
+              f2p y, t;
+              // f0 g + h2d (r d) + c0 d
+              y = f2_fma(f0, gd.x, f2_fma(h2d, rd, f2_fma(c0, gd.y, nc[k][0])));
+              t = f2_add(s[k][0], y);
+              nc[k][0] = f2_sub(y, f2_sub(t, s[k][0]));
+              s[k][0] = t;
+              // f1 g + c1 d
+              y = f2_fma(f1, gd.x, f2_fma(c1, gd.y, nc[k][1]));
+              t = f2_add(s[k][1], y);
+              nc[k][1] = f2_sub(y, f2_sub(t, s[k][1]));
+              s[k][1] = t;
+              // f2 g + c2 d - h0d (r d)
+              y = f2_fma(f2v, gd.x, f2_fma(mh0d, rd, f2_fma(c2, gd.y, nc[k][2])));
+              t = f2_add(s[k][2], y);
+              nc[k][2] = f2_sub(y, f2_sub(t, s[k][2]));
+              s[k][2] = t;
+            }
           }
         }
       }
     }
-  }
-  // one write per point: s - c
-  const size_t N = (size_t)c.N[0] * c.N[1] * c.N[2];
-  const int gx = X0[0] + 8 * xh + xl, gz0 = X0[2] + zl;
+    // one write per point: s - c
+    const size_t N = (size_t)c.N[0] * c.N[1] * c.N[2];
+    const int gx = X0[0] + xl, gz0 = X0[2] + zl;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const size_t m0 = ((size_t)gx * c.N[1] + (X0[1] + ly + 4 * k)) * c.N[2] + gz0;
+    for (int k = 0; k < 4; ++k) {
+      const size_t m0 = ((size_t)gx * c.N[1] + (X0[1] + ly + 4 * k)) * c.N[2] + gz0;
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
-      *reinterpret_cast<float2 *>(fgrid + a * N + m0) = f2_unpack(f2_add(s[k][a], nc[k][a]));
+      for (int a = 0; a < 3; ++a)
+        *reinterpret_cast<float2 *>(fgrid + a * N + m0) = f2_unpack(f2_add(s[k][a], nc[k][a]));
+    }
   }
 }
 
@@ -855,10 +865,10 @@ fs_status spread_t(fs_ctx *c, const FcmConsts &k, const double *Y, const double 
       FS_LAUNCH_CHECK();
     }
     if (c->tune_spread_chunk == 32)
-      k_spread32<32><<<2 * c->nbins, FS_SPREAD32_THREADS, sizeof(SpreadStage32<32>), c->stream>>>(
+      k_spread32<32><<<c->nbins, FS_SPREAD32_THREADS, sizeof(SpreadStage32<32>), c->stream>>>(
           c->bins.start, rec, k, (float *)c->grid_real);
     else
-      k_spread32<64><<<2 * c->nbins, FS_SPREAD32_THREADS, sizeof(SpreadStage32<64>), c->stream>>>(
+      k_spread32<64><<<c->nbins, FS_SPREAD32_THREADS, sizeof(SpreadStage32<64>), c->stream>>>(
           c->bins.start, rec, k, (float *)c->grid_real);
   } else if (c->tune_spread_chunk == 32) {
     k_spread<R, 32><<<c->nbins, FS_SPREAD_THREADS, sizeof(SpreadStage<R, 32>), c->stream>>>(
