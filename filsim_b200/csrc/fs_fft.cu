@@ -4,6 +4,7 @@
 // over HBM, replacing cuFFT R2C + projection + C2R in the mixed-precision path.
 //
 //   f[c][x][y][z] (real)  --z_r2c-->    A[c][kz][x][y]   z lines, real-to-half-complex
+//                                                        (two real lines as one complex line)
 //                         --y_fwd-->    B[c][kz][ky][x]  y lines, written transposed
 //                         --x_project-> B (in place)     x lines: forward, Stokes
 //                                                        projection, inverse, with the
@@ -18,7 +19,8 @@
 // the reference does. The half-complex inverse along z takes only the real part
 // of the kz = 0 and kz = Nz/2 coefficients after the complex inverse transforms
 // along x and y, the semantics of the reference's multi-dimensional real
-// inverse transform.
+// inverse transform. Along z a warp transforms its two real lines a, b as one
+// complex line a + i b and separates (or assembles) their half spectra.
 #include "fs_internal.cuh"
 #include "fs_f32x2.cuh"
 
@@ -276,56 +278,6 @@ __device__ __forceinline__ void fft_p2n(float2 (&v)[Fft<N>::M], float2 *S, const
   dit_reg<M, D>(v);
 }
 
-// ---- pass 1: real-to-half-complex along z ------------------------------------
-// CTA: component c, plane x, 16 consecutive y lines; output rows of 16 y values.
-template <int NZ>
-__global__ void __launch_bounds__(FFT_THREADS) k_fft_z_r2c(const float *__restrict__ f, float2 *__restrict__ A,
-                                                           int nx, int ny, const float2 *__restrict__ tw) {
-  constexpr int H = NZ / 2, M = Fft<H>::M, SW = Fft<H>::SW;
-  extern __shared__ float2 fft_smem[];
-  float2 *T = fft_smem;  // (H + 1) x FFT_TS
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float2 *S = fft_smem + (H + 1) * FFT_TS + warp * SW;
-  const int nyt = ny / FFT_TILE;
-  const int yt = blockIdx.x % nyt;
-  const int x = (blockIdx.x / nyt) % nx;
-  const int c = blockIdx.x / (nyt * nx);
-#pragma unroll 1
-  for (int r = 0; r < FFT_TILE / FFT_WARPS; ++r) {
-    const int wy = warp + FFT_WARPS * r;
-    const float2 *line =
-        reinterpret_cast<const float2 *>(f + (((size_t)c * nx + x) * ny + (size_t)yt * FFT_TILE + wy) * NZ);
-    float2 v[M];
-#pragma unroll
-    for (int m = 0; m < M; ++m) v[m] = __ldg(line + lane + 32 * m);
-    fft_n2p<H, 1>(v, S, tw, lane);
-#pragma unroll
-    for (int i = 0; i < M; ++i) S[prow<H>(out_index<H>(lane, i))] = v[i];
-    __syncwarp();
-    // X_k = ((Z_k + conj Z_{H-k}) - i W_NZ^k (Z_k - conj Z_{H-k})) / 2
-#pragma unroll
-    for (int m = 0; m < M; ++m) {
-      const int k = lane + 32 * m;
-      const float2 zk = S[prow<H>(k)], zr = S[prow<H>((H - k) & (H - 1))];
-      const float2 d = make_float2(zk.x - zr.x, zk.y + zr.y);
-      const float2 e = cmul(d, twd<1>(tw, k * (TW_FULL / NZ)));
-      T[k * FFT_TS + wy] = make_float2(0.5f * (zk.x + zr.x + e.y), 0.5f * (zk.y - zr.y - e.x));
-    }
-    if (lane == 0) {
-      const float2 z0 = S[0];
-      T[H * FFT_TS + wy] = make_float2(z0.x - z0.y, 0.f);
-    }
-    __syncwarp();
-  }
-  __syncthreads();
-  float2 *out = A + ((size_t)c * (H + 1) * nx + x) * ny + (size_t)yt * FFT_TILE;
-  const size_t plane = (size_t)nx * ny;
-  for (int idx = threadIdx.x; idx < (H + 1) * FFT_TILE; idx += FFT_THREADS) {
-    const int k = idx / FFT_TILE, j = idx % FFT_TILE;
-    out[(size_t)k * plane + j] = T[k * FFT_TS + j];
-  }
-}
-
 // ---- pass 2: forward y, written transposed -----------------------------------
 // CTA: (c, kz) plane, 16 consecutive x lines; output rows of 16 x values per ky.
 template <int NY>
@@ -449,14 +401,59 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_y_inv(const float2 *__restr
   }
 }
 
-// ---- pass 5: half-complex-to-real along z ---------------------------------------
-// Z'_k = (X_k + conj X_{H-k}) + i W_NZ^{-k} (X_k - conj X_{H-k}), k < H, with the
-// imaginary parts of X_0 and X_H dropped; z = unnormalised inverse H-point DFT
-// of Z'; u[2n] = Re z_n, u[2n+1] = Im z_n.
+// ---- passes 1 and 5: z lines in pairs -------------------------------------------
+// Warp w transforms its two real z lines a = y-line w and b = y-line w + 8 as one
+// NZ-point complex line z = a + i b: forward, A_k = (Z_k + conj Z_{NZ-k}) / 2 and
+// B_k = (Z_k - conj Z_{NZ-k}) / (2i) for k <= NZ/2; inverse, Z_k = A_k + i B_k
+// (k <= NZ/2, the imaginary parts of A_0, A_{NZ/2}, B_0, B_{NZ/2} dropped) and
+// Z_{NZ-k} = conj A_k + i conj B_k, then a = Re z, b = Im z. One full-length
+// transform per line pair instead of two half-length ones.
+template <int NZ>
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_z_r2c(const float *__restrict__ f, float2 *__restrict__ A,
+                                                            int nx, int ny, const float2 *__restrict__ tw) {
+  static_assert(FFT_TILE == 2 * FFT_WARPS, "two lines per warp");
+  constexpr int H = NZ / 2, M = Fft<NZ>::M, SW = Fft<NZ>::SW;
+  extern __shared__ float2 fft_smem[];
+  float2 *T = fft_smem;  // (H + 1) x FFT_TS
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2 *S = fft_smem + (H + 1) * FFT_TS + warp * SW;
+  const int nyt = ny / FFT_TILE;
+  const int yt = blockIdx.x % nyt;
+  const int x = (blockIdx.x / nyt) % nx;
+  const int c = blockIdx.x / (nyt * nx);
+  const int wa = warp, wb = warp + FFT_WARPS;
+  const float *la = f + (((size_t)c * nx + x) * ny + (size_t)yt * FFT_TILE + wa) * NZ;
+  const float *lb = la + (size_t)FFT_WARPS * NZ;
+  float2 v[M];
+#pragma unroll
+  for (int m = 0; m < M; ++m) v[m] = make_float2(__ldg(la + lane + 32 * m), __ldg(lb + lane + 32 * m));
+  fft_n2p<NZ, 1>(v, S, tw, lane);
+#pragma unroll
+  for (int i = 0; i < M; ++i) S[prow<NZ>(out_index<NZ>(lane, i))] = v[i];
+  __syncwarp();
+#pragma unroll
+  for (int m = 0; m < (H + 32) / 32; ++m) {
+    const int k = lane + 32 * m;
+    if (k <= H) {
+      const float2 zk = S[prow<NZ>(k)], zr = S[prow<NZ>((NZ - k) & (NZ - 1))];
+      T[k * FFT_TS + wa] = make_float2(0.5f * (zk.x + zr.x), 0.5f * (zk.y - zr.y));
+      T[k * FFT_TS + wb] = make_float2(0.5f * (zk.y + zr.y), -0.5f * (zk.x - zr.x));
+    }
+  }
+  __syncthreads();
+  float2 *out = A + ((size_t)c * (H + 1) * nx + x) * ny + (size_t)yt * FFT_TILE;
+  const size_t plane = (size_t)nx * ny;
+  for (int idx = threadIdx.x; idx < (H + 1) * FFT_TILE; idx += FFT_THREADS) {
+    const int k = idx / FFT_TILE, j = idx % FFT_TILE;
+    out[(size_t)k * plane + j] = T[k * FFT_TS + j];
+  }
+}
+
 template <int NZ>
 __global__ void __launch_bounds__(FFT_THREADS) k_fft_z_c2r(const float2 *__restrict__ A, float *__restrict__ u,
-                                                           int nx, int ny, const float2 *__restrict__ tw) {
-  constexpr int H = NZ / 2, M = Fft<H>::M, SW = Fft<H>::SW;
+                                                            int nx, int ny, const float2 *__restrict__ tw) {
+  static_assert(FFT_TILE == 2 * FFT_WARPS, "two lines per warp");
+  constexpr int H = NZ / 2, M = Fft<NZ>::M, SW = Fft<NZ>::SW;
   extern __shared__ float2 fft_smem[];
   float2 *T = fft_smem;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -473,28 +470,35 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_z_c2r(const float2 *__restr
   }
   cp_async_wait_all();
   __syncthreads();
-#pragma unroll 1
-  for (int r = 0; r < FFT_TILE / FFT_WARPS; ++r) {
-    const int wy = warp + FFT_WARPS * r;
-    float2 v[M];
+  const int wa = warp, wb = warp + FFT_WARPS;
+  float2 v[M];
 #pragma unroll
-    for (int m = 0; m < M; ++m) {
-      const int k = lane + 32 * m;
-      float2 xk = T[k * FFT_TS + wy], xr = T[(H - k) * FFT_TS + wy];
-      if (k == 0) xk.y = xr.y = 0.f;
-      const float2 d = make_float2(xk.x - xr.x, xk.y + xr.y);
-      const float2 e = cmul(d, twd<-1>(tw, k * (TW_FULL / NZ)));
-      v[m] = make_float2(xk.x + xr.x - e.y, xk.y - xr.y + e.x);
+  for (int m = 0; m < M; ++m) {
+    const int k = lane + 32 * m;
+    if (k <= H) {
+      float2 a = T[k * FFT_TS + wa], b = T[k * FFT_TS + wb];
+      if (k == 0 || k == H) a.y = b.y = 0.f;
+      v[m] = make_float2(a.x - b.y, a.y + b.x);
+    } else {
+      const int kk = NZ - k;
+      const float2 a = T[kk * FFT_TS + wa], b = T[kk * FFT_TS + wb];
+      v[m] = make_float2(a.x + b.y, b.x - a.y);
     }
-    fft_n2p<H, -1>(v, S, tw, lane);
-    float2 *line = reinterpret_cast<float2 *>(u + (((size_t)c * nx + x) * ny + (size_t)yt * FFT_TILE + wy) * NZ);
+  }
+  fft_n2p<NZ, -1>(v, S, tw, lane);
+  float *oa = u + (((size_t)c * nx + x) * ny + (size_t)yt * FFT_TILE + wa) * NZ;
+  float *ob = oa + (size_t)FFT_WARPS * NZ;
 #pragma unroll
-    for (int i = 0; i < M; ++i) line[out_index<H>(lane, i)] = v[i];
+  for (int i = 0; i < M; ++i) {
+    const int o = out_index<NZ>(lane, i);
+    oa[o] = v[i].x;
+    ob[o] = v[i].y;
   }
 }
 
 template <int NZ>
-constexpr size_t smem_z() { return sizeof(float2) * ((NZ / 2 + 1) * FFT_TS + FFT_WARPS * Fft<NZ / 2>::SW); }
+constexpr size_t smem_z() { return sizeof(float2) * ((NZ / 2 + 1) * FFT_TS + FFT_WARPS * Fft<NZ>::SW); }
+
 template <int NY>
 constexpr size_t smem_y() { return sizeof(float2) * (Fft<NY>::PEXT * FFT_TS + FFT_WARPS * Fft<NY>::SW); }
 
