@@ -70,10 +70,10 @@ ENSEMBLE_SEED = 3000
 NCU_TRAFFIC = {
     # per grid point, from the ncu capture in profiles/fcm_kernels_mobility_256_512x30.md
     # (DRAM read + write of the stage's kernels on 256^3), times the grid points of the workload
-    "spread": (11.94e6 + 147.48e6) / 256 ** 3,                          # k_spread32
-    "fft_fwd": (201.37e6 + 158.19e6 + 202.96e6 + 156.25e6) / 256 ** 3,  # z_r2c + y_fwd
-    "project": (202.95e6 + 143.14e6) / 256 ** 3,                        # x_project
-    "fft_inv": (202.99e6 + 159.33e6 + 202.95e6 + 158.13e6) / 256 ** 3,  # y_inv + z_c2r
+    "spread": (17.40e6 + 152.87e6) / 256 ** 3,                          # k_spread32
+    "fft_fwd": (201.36e6 + 156.52e6 + 202.93e6 + 156.83e6) / 256 ** 3,  # z_r2c + y_fwd
+    "project": (202.97e6 + 143.17e6) / 256 ** 3,                        # x_project
+    "fft_inv": (202.93e6 + 159.50e6 + 203.01e6 + 160.35e6) / 256 ** 3,  # y_inv + z_c2r
 }
 
 
