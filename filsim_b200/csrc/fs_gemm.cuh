@@ -4,16 +4,18 @@
 //   D[m][n] = sum_k A[m][k] B[n][k]      A: M x K, B: N x K, both K contiguous (bf16)
 //
 // One CTA (4 warps) computes a 128 x BN tile. K advances in 64-element blocks
-// through a three-stage shared-memory ring filled by cp.async in the canonical
-// K-major 128-byte-swizzle layout (row r, 16-byte chunk j at r*128 + (j ^ (r & 7))*16,
-// atoms 1024-byte aligned); the loads of the next two blocks are in flight while a
-// block's MMAs run. Thread 0 issues four K=16 MMAs per block and commits
-// them to the stage's mbarrier; a stage is refilled only after that barrier's
-// phase completes. After the last commit each warp reads its 32 accumulator
-// lanes with tcgen05.ld and applies the epilogue. Every wait is bounded: on
-// timeout the kernel records an error, skips the epilogue, frees its tensor
-// memory and returns.
+// through a three-stage shared-memory ring filled by TMA (cp.async.bulk.tensor,
+// 128-byte swizzle: row r, 16-byte chunk j at r*128 + (j ^ (r & 7))*16, the
+// canonical K-major layout the MMA descriptors name). Thread 0 is the producer:
+// per block it waits until the stage's previous MMAs have drained ("empty"
+// barrier), announces the stage's bytes on its "full" barrier and issues the two
+// tile loads, which complete that barrier. Thread 32 issues the MMAs: it waits on
+// "full", issues four K=16 MMAs and commits them to "empty"; after the last block
+// it commits to "done". Then each warp reads its 32 accumulator lanes with
+// tcgen05.ld and applies the epilogue. Every wait is bounded: on timeout the
+// kernel records an error, skips the epilogue, frees its tensor memory and returns.
 #pragma once
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
 
@@ -45,14 +47,18 @@ constexpr int BM = 128, BK = 64, STAGES = 3, THREADS = 128;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+// the stage's bytes announced on its full barrier (this thread's arrival included)
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mbar), "r"(bytes) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-// all but the N most recent groups of this thread have landed
-template <int N>
-__device__ __forceinline__ void cp_async_wait_group() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+// one 2-D tile (x = innermost coordinate in elements, y = row) into shared memory,
+// completing on mbar; no multicast
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::
+          "r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
+      : "memory");
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
@@ -125,17 +131,25 @@ template <int BN>
 constexpr int smem_bytes() { return STAGES * (BM * 128 + BN * 128) + 1024; }
 
 template <int BN, int EPI>
-__global__ void __launch_bounds__(THREADS) k_gemm_bf16(GemmArgs g) {
+__global__ void __launch_bounds__(THREADS)
+    k_gemm_bf16(GemmArgs g, const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB) {
   constexpr uint32_t A_BYTES = BM * 128, B_BYTES = BN * 128, STAGE_BYTES = A_BYTES + B_BYTES;
   constexpr uint32_t IDESC = idesc_bf16(BN);
   extern __shared__ uint8_t gemm_smem_raw[];
-  __shared__ uint64_t mbar[STAGES];
+  __shared__ uint64_t full[STAGES], empty[STAGES], done;
   __shared__ uint32_t tmem_slot;
+  __shared__ int s_fail, s_issued;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t base = (smem_u32(gemm_smem_raw) + 1023u) & ~1023u;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   if (tid == 0) {
-    for (int s = 0; s < STAGES; ++s) mbar_init(smem_u32(&mbar[s]), 1);
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(smem_u32(&full[s]), 1);
+      mbar_init(smem_u32(&empty[s]), 1);
+    }
+    mbar_init(smem_u32(&done), 1);
+    s_fail = 0;
+    s_issued = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     fence_proxy_async();
   }
@@ -145,52 +159,42 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(GemmArgs g) {
   tc_fence_after();
   const uint32_t tmem = tmem_slot;
   const int nk = g.K / BK;
-  // K block kb -> stage kb % STAGES; its 128 x 64 A tile and BN x 64 B tile in the
-  // 128-byte-swizzle K-major layout
-  auto load_block = [&](int kb) {
-    const uint32_t sA = base + (kb % STAGES) * STAGE_BYTES, sB = sA + A_BYTES;
-    const fs_bf16 *ga = g.A + (size_t)m0 * g.lda + kb * BK;
-    const fs_bf16 *gb = g.B + (size_t)n0 * g.ldb + kb * BK;
-    for (int c = tid; c < BM * 8; c += THREADS) {
-      const int r = c >> 3, j = c & 7;
-      cp_async16(sA + r * 128 + ((j ^ (r & 7)) << 4), ga + (size_t)r * g.lda + j * 8);
+  if (tid == 0) {  // producer
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % STAGES;
+      if (kb >= STAGES && !mbar_wait(smem_u32(&empty[s]), ((kb / STAGES) - 1) & 1)) {
+        s_fail = 1;
+        break;
+      }
+      const uint32_t sA = base + s * STAGE_BYTES, sB = sA + A_BYTES;
+      mbar_expect_tx(smem_u32(&full[s]), STAGE_BYTES);
+      tma_load_2d(sA, &tmA, kb * BK, m0, smem_u32(&full[s]));
+      tma_load_2d(sB, &tmB, kb * BK, n0, smem_u32(&full[s]));
+      s_issued = kb + 1;
     }
-    for (int c = tid; c < BN * 8; c += THREADS) {
-      const int r = c >> 3, j = c & 7;
-      cp_async16(sB + r * 128 + ((j ^ (r & 7)) << 4), gb + (size_t)r * g.ldb + j * 8);
-    }
-  };
-  // software pipeline: blocks kb+1 .. kb+STAGES-1 are loading while block kb's MMAs
-  // run; one commit group per block (possibly empty) keeps the group count uniform
-  for (int pb = 0; pb < STAGES - 1; ++pb) {
-    if (pb < nk) load_block(pb);
-    cp_async_commit();
-  }
-  bool ok = true;
-  for (int kb = 0; kb < nk; ++kb) {
-    const int s = kb % STAGES;
-    const uint32_t sA = base + s * STAGE_BYTES, sB = sA + A_BYTES;
-    cp_async_wait_group<STAGES - 2>();  // this thread's copies of block kb have landed
-    fence_proxy_async();
-    __syncthreads();                    // everyone's have
-    if (tid == 0) {
+  } else if (tid == 32) {  // MMA issuer
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % STAGES;
+      if (!mbar_wait(smem_u32(&full[s]), (kb / STAGES) & 1)) {
+        s_fail = 1;
+        break;
+      }
       tc_fence_after();
+      const uint32_t sA = base + s * STAGE_BYTES, sB = sA + A_BYTES;
 #pragma unroll
       for (int kk = 0; kk < BK / 16; ++kk)
         mma_bf16(tmem, sw128_desc(sA + kk * 32), sw128_desc(sB + kk * 32), IDESC, (kb | kk) != 0);
-      mma_commit(smem_u32(&mbar[s]));
+      mma_commit(smem_u32(&empty[s]));
     }
-    // block kb + STAGES - 1 refills the stage of block kb - 1 once its MMAs completed
-    const int nb = kb + STAGES - 1;
-    if (nb < nk) {
-      if (kb >= 1) ok = mbar_wait(smem_u32(&mbar[(kb - 1) % STAGES]), ((kb - 1) / STAGES) & 1);
-      if (!ok) break;
-      load_block(nb);
-    }
-    cp_async_commit();
+    mma_commit(smem_u32(&done));  // arrives once every MMA issued above has completed
   }
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
-  if (ok) ok = mbar_wait(smem_u32(&mbar[(nk - 1) % STAGES]), ((nk - 1) / STAGES) & 1);
+  __syncwarp();
+  bool ok = mbar_wait(smem_u32(&done), 0);
+  __syncthreads();
+  ok = ok && !s_fail;
+  if (!ok && tid == 0)  // before leaving, the tile loads still in flight land (bounded)
+    for (int kb = max(0, s_issued - STAGES); kb < s_issued; ++kb)
+      mbar_wait(smem_u32(&full[kb % STAGES]), (kb / STAGES) & 1);
   tc_fence_after();
   if (ok) {
     const int row = m0 + warp * 32 + lane;

@@ -21,6 +21,7 @@
 #include <vector>
 #include "fs_internal.cuh"
 #include "fs_gemm.cuh"
+#include <cudaTypedefs.h>
 
 struct fs_mlp {
   int nw, nfeat, k_in, hidden, ntgt, k_out, cap;
@@ -323,11 +324,39 @@ fs_status dalloc(T **p, size_t n, size_t *bytes) {
   return FS_OK;
 }
 
+// TMA descriptor of a row-major BF16 matrix [rows x cols] (leading dimension ld
+// elements) read in 64-column x 128-row boxes with the 128-byte swizzle; the
+// encoder comes from the driver through the runtime (no link against libcuda)
+fs_status tma_map_bf16(CUtensorMap *map, const fs_bf16 *ptr, int rows, int cols, int ld) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q;
+    void *fn = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return FS_ERR_CUDA;
+    encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  }
+  if (((uintptr_t)ptr & 15) || ((size_t)ld * sizeof(fs_bf16)) % 16) return FS_ERR_INVALID_ARG;
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(fs_bf16)};
+  const cuuint32_t box[2] = {(cuuint32_t)fsg::BK, 128u};
+  const cuuint32_t estr[2] = {1u, 1u};
+  if (encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<fs_bf16 *>(ptr), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return FS_ERR_CUDA;
+  return FS_OK;
+}
+
 template <int EPI>
 fs_status gemm(cudaStream_t st, const GemmArgs &g) {
   if (g.M % fsg::BM || g.N % 128 || g.K % fsg::BK || g.K <= 0) return FS_ERR_INVALID_ARG;
+  CUtensorMap ta, tb;
+  FS_TRY(tma_map_bf16(&ta, g.A, g.M, g.K, g.lda));
+  FS_TRY(tma_map_bf16(&tb, g.B, g.N, g.K, g.ldb));
   dim3 grid(g.M / fsg::BM, g.N / 128);
-  fsg::k_gemm_bf16<128, EPI><<<grid, fsg::THREADS, fsg::smem_bytes<128>(), st>>>(g);
+  fsg::k_gemm_bf16<128, EPI><<<grid, fsg::THREADS, fsg::smem_bytes<128>(), st>>>(g, ta, tb);
   FS_LAUNCH_CHECK();
   return FS_OK;
 }
