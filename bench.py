@@ -19,8 +19,9 @@ value      mixed precision (FP32 spread/FFT/interpolation, FP64 Broyden and
            before the run by the library's own kernels on 20 seeded plain-solver
            runs of this workload, K_B log-uniform in [0.1, 10]) under its cost
            gate (fs_warm_start_gate, period 8: each step takes the start with the
-           lower running mean of mobility solves per step, the other one every
-           8th step; learned.gate reports how many timed steps took each);
+           lower running mean of mobility solves per step and probes the other one
+           after 8 steps, an interval that doubles up to 128 while the probes lose;
+           learned.gate reports how many timed steps took each);
            inputs resident in HBM, device-timed with CUDA events on the
            context's stream, max over ranks; weak scaling (one independent
            replica per GPU).
@@ -63,7 +64,7 @@ PREP_STEPS = 12
 # warm-start training data: seeds TRAIN_SEED0.. of this workload, K_B log-uniform in [0.1, 10]
 TRAIN_SEED0 = 7000
 TRAIN_EPOCHS = 40
-GATE_PERIOD = 8  # the learned start's cost gate probes the other start every 8th step
+GATE_PERIOD = 8  # the learned start's cost gate: first probe of the other start after 8 steps
 ENSEMBLE_SEED = 3000
 # DRAM bytes per launch from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum);
 # the kernels and captures are listed in profiles/.

@@ -18,6 +18,8 @@
 // its plain-start residual is put back to the plain start, and the residual is
 // recomputed when any filament was put back. The Broyden iteration then runs
 // unchanged to the reference's tolerance test.
+#include <algorithm>
+#include <mutex>
 #include <vector>
 #include "fs_internal.cuh"
 #include "fs_gemm.cuh"
@@ -56,12 +58,16 @@ struct fs_mlp {
   bool override_next;              // the next warm start uses pred as given (fs_learn_override)
   long long learned_total, fallback_total;
   // cost gate of the learned start (fs_warm_start_gate): per start, the running
-  // mean of mobility solves per step; the cheaper start runs, the other every
-  // gate_period-th step so that its mean stays current
+  // mean of mobility solves per step; the cheaper start runs and the other one is
+  // probed after gate_interval steps. The interval starts at gate_period and
+  // doubles (up to GATE_BACKOFF_MAX x gate_period) after each probe that leaves
+  // the choice unchanged; a probe that changes it restores gate_period.
   int gate_period;                 // 0: off (the learned start runs every step)
+  int gate_interval;
   double gate_solves[2];           // [0] plain start, [1] learned start
   int gate_have[2];
   int gate_since;
+  int gate_probe_best = -1;        // -1: no probe pending; else the best start when the probe was chosen
   long long gate_steps[2];
 };
 
@@ -326,9 +332,29 @@ fs_status dalloc(T **p, size_t n, size_t *bytes) {
 
 // TMA descriptor of a row-major BF16 matrix [rows x cols] (leading dimension ld
 // elements) read in 64-column x 128-row boxes with the 128-byte swizzle; the
-// encoder comes from the driver through the runtime (no link against libcuda)
+// encoder comes from the driver through the runtime (no link against libcuda).
+// A descriptor is a function of (address, rows, cols, ld) only, so encoded ones
+// are kept in a small process-wide cache (the MLP's GEMMs reuse the same
+// operands every call; encoding costs tens of microseconds on the host).
+struct TmaCacheEntry {
+  const void *ptr;
+  int rows, cols, ld;
+  CUtensorMap map;
+};
+constexpr int TMA_CACHE_SIZE = 128;
+
 fs_status tma_map_bf16(CUtensorMap *map, const fs_bf16 *ptr, int rows, int cols, int ld) {
+  static std::mutex mu;
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  static std::vector<TmaCacheEntry> cache;
+  static size_t next_slot = 0;
+  if (((uintptr_t)ptr & 15) || ((size_t)ld * sizeof(fs_bf16)) % 16) return FS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lock(mu);
+  for (const TmaCacheEntry &e : cache)
+    if (e.ptr == ptr && e.rows == rows && e.cols == cols && e.ld == ld) {
+      *map = e.map;
+      return FS_OK;
+    }
   if (!encode) {
     cudaDriverEntryPointQueryResult q;
     void *fn = nullptr;
@@ -337,7 +363,6 @@ fs_status tma_map_bf16(CUtensorMap *map, const fs_bf16 *ptr, int rows, int cols,
       return FS_ERR_CUDA;
     encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
   }
-  if (((uintptr_t)ptr & 15) || ((size_t)ld * sizeof(fs_bf16)) % 16) return FS_ERR_INVALID_ARG;
   const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(fs_bf16)};
   const cuuint32_t box[2] = {(cuuint32_t)fsg::BK, 128u};
@@ -346,6 +371,13 @@ fs_status tma_map_bf16(CUtensorMap *map, const fs_bf16 *ptr, int rows, int cols,
              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return FS_ERR_CUDA;
+  const TmaCacheEntry e{ptr, rows, cols, ld, *map};
+  if ((int)cache.size() < TMA_CACHE_SIZE) {
+    cache.push_back(e);
+  } else {
+    cache[next_slot] = e;
+    next_slot = (next_slot + 1) % TMA_CACHE_SIZE;
+  }
   return FS_OK;
 }
 
@@ -549,14 +581,23 @@ fs_status ensure_step_buffers(fs_ctx *c) {
 bool learn_active(const fs_ctx *c) { return c->mlp && c->mlp->mode > 0; }
 
 // the start of this step under the cost gate (true: learned)
+constexpr int GATE_BACKOFF_MAX = 16;
+
+int gate_best(const fs_mlp *m) { return m->gate_solves[1] < m->gate_solves[0] ? 1 : 0; }
+
 bool learn_gate_choose(fs_ctx *c) {
   fs_mlp *m = c->mlp;
   if (!m->gate_period) return true;
   if (!m->gate_have[0]) return false;
-  if (!m->gate_have[1]) return true;
-  const int best = m->gate_solves[1] < m->gate_solves[0] ? 1 : 0;
-  if (++m->gate_since >= m->gate_period) {
+  if (!m->gate_have[1]) {  // first learned step: a probe against the plain start
     m->gate_since = 0;
+    m->gate_probe_best = 0;
+    return true;
+  }
+  const int best = gate_best(m);
+  if (++m->gate_since >= m->gate_interval) {
+    m->gate_since = 0;
+    m->gate_probe_best = best;
     return best == 0;
   }
   return best == 1;
@@ -568,6 +609,11 @@ void learn_gate_record(fs_ctx *c, bool learned, long long solves) {
   m->gate_solves[i] = m->gate_have[i] ? 0.7 * m->gate_solves[i] + 0.3 * (double)solves : (double)solves;
   m->gate_have[i] = 1;
   m->gate_steps[i]++;
+  if (m->gate_probe_best >= 0) {
+    const bool kept = gate_best(m) == m->gate_probe_best;
+    m->gate_interval = kept ? std::min(2 * m->gate_interval, GATE_BACKOFF_MAX * m->gate_period) : m->gate_period;
+    m->gate_probe_best = -1;
+  }
 }
 bool learn_recording(const fs_ctx *c) { return c->mlp && c->mlp->record; }
 
@@ -998,8 +1044,10 @@ fs_status fs_warm_start_gate(fs_ctx *c, int period) {
   if (!c->mlp) return period ? FS_ERR_STATE : FS_OK;
   fs_mlp *m = c->mlp;
   m->gate_period = period;
+  m->gate_interval = period;
   m->gate_have[0] = m->gate_have[1] = 0;
   m->gate_since = 0;
+  m->gate_probe_best = -1;
   m->gate_steps[0] = m->gate_steps[1] = 0;
   return FS_OK;
 }

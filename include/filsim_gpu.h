@@ -390,8 +390,10 @@ fs_status fs_learn_override(fs_ctx *ctx, const float *pred_d);
 fs_status fs_set_warm_start(fs_ctx *ctx, int mode);
 /* Cost gate of the learned start (no reference counterpart): with period > 0,
  * each step runs the start (learned or plain) whose running mean of mobility
- * solves per step is lower, and the other one every period-th step so that its
- * mean stays current; the learned start pays off only when it saves more
+ * solves per step is lower, and probes the other one so that its mean stays
+ * current: after period steps, an interval that doubles (up to 16 x period)
+ * while the probes leave the choice unchanged and returns to period when one
+ * changes it; the learned start pays off only when it saves more
  * Broyden iterations than its own extra solves. period 0 (the default) runs the
  * learned start every step. Resets the statistics. */
 fs_status fs_warm_start_gate(fs_ctx *ctx, int period);

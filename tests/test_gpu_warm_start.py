@@ -172,8 +172,9 @@ def test_trained_network_gain(gpu_lib):
 
 def test_cost_gate(gpu_lib):
     """fs_warm_start_gate: each step takes the start with the lower running mean of
-    mobility solves per step and probes the other every period-th step; with the gate
-    off the learned start runs on every step."""
+    mobility solves per step and probes the other one (first after period steps, then
+    at doubling intervals while the choice holds); with the gate off the learned start
+    runs on every step."""
     ctx, model, sim = prepared()
     s0 = snapshot(sim)
     set_warm_start(ctx, 1)
