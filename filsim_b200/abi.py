@@ -154,6 +154,8 @@ def _declare(L):
         "fs_state_device_ptr": (c_int, [c_void_p, ctypes.c_char_p, ctypes.POINTER(c_void_p)]),
         "fs_initial_guess": (c_int, [c_void_p]),
         "fs_filament_forces": (c_int, [c_void_p, c_int]),
+        "fs_set_swimming": (c_int, [c_void_p, c_void_p, c_double, c_int]),
+        "fs_set_spring_links": (c_int, [c_void_p, c_int, c_void_p, c_double, c_double]),
         "fs_jacobian_build": (c_int, [c_void_p, c_int]),
         "fs_jacobian_get_inverse": (c_int, [c_void_p, c_int, c_void_p, c_int]),
         "fs_error_check": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),

@@ -4,6 +4,7 @@
 // launches; all arithmetic on bead and grid data runs in the sm_100a kernels.
 #include <stdlib.h>
 #include <algorithm>
+#include <cmath>
 #include <vector>
 #include "fs_internal.cuh"
 
@@ -85,7 +86,8 @@ void free_state(fs_ctx *c) {
   void *ptrs[] = {c->X, c->Xs, c->Xt, c->U, c->Us, c->Ut, c->F, c->TAU, c->Y, c->V, c->W, c->lam, c->lam1,
                   c->lam2, c->q, c->qs, c->qt, c->err, c->newerr, c->upd, c->tmp, c->dE, c->kap, c->cc,
                   c->fil_start, c->fil_id, c->seg_id, c->soff, c->aoff, c->Cmat, c->Dmat, c->dots, c->partials,
-                  c->scalars, c->flags, c->maxerr_bits, c->Sinv, c->aux};
+                  c->scalars, c->flags, c->maxerr_bits, c->Sinv, c->aux, c->swim, c->spring_beads,
+                  c->spring_off, c->spring_ent};
   for (void *p : ptrs) cudaFree(p);
   if (c->flags_h) cudaFreeHost(c->flags_h);
 }
@@ -430,6 +432,7 @@ fs_status fs_collision_pairs(fs_ctx *c, const double *Y, int np, int nt, const i
 }
 
 static fs_status upload_layout(fs_ctx *c, const fs_host_state *s);
+static void spring_free(fs_ctx *c);
 
 // state arrays always; the filament layout (ids, offsets, Schur buffers) only
 // when it differs from the previous upload's
@@ -444,6 +447,11 @@ fs_status fs_state_upload(fs_ctx *c, const fs_host_state *s) {
   FS_TRY(learn_before_upload(c, same_layout));
   if (!same_layout) {
     graph_invalidate(c);
+    FS_CUDA(cudaStreamSynchronize(st));
+    // a swimming drive and spring links refer to the previous layout's filaments and beads
+    cudaFree(c->swim);
+    c->swim = nullptr;
+    spring_free(c);
     FS_TRY(upload_layout(c, s));
   }
   struct F3 {
@@ -569,6 +577,79 @@ fs_status fs_state_device_ptr(fs_ctx *c, const char *which, double **ptr_h) {
 
 fs_status fs_initial_guess(fs_ctx *c) { return c ? fil_initial_guess(c) : FS_ERR_INVALID_ARG; }
 fs_status fs_filament_forces(fs_ctx *c, int nt) { return c ? fil_forces(c, nt) : FS_ERR_INVALID_ARG; }
+
+fs_status fs_set_swimming(fs_ctx *c, const double *swim_h, double curvature, int sperm_decay) {
+  if (!c) return FS_ERR_INVALID_ARG;
+  if (!c->have_state) return FS_ERR_STATE;
+  graph_invalidate(c);
+  FS_CUDA(cudaStreamSynchronize(c->stream));  // no queued step still reads the old parameters
+  if (!swim_h) {
+    cudaFree(c->swim);
+    c->swim = nullptr;
+    return FS_OK;
+  }
+  const size_t n = 5 * (size_t)c->nfil;
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(swim_h[i])) return FS_ERR_INVALID_ARG;
+  if (!std::isfinite(curvature)) return FS_ERR_INVALID_ARG;
+  if (!c->swim) {
+    FS_CUDA(cudaMalloc(&c->swim, sizeof(double) * (n > 0 ? n : 1)));
+    c->bytes += sizeof(double) * n;
+  }
+  FS_CUDA(cudaMemcpyAsync(c->swim, swim_h, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  FS_CUDA(cudaStreamSynchronize(c->stream));
+  c->swim_curvature = curvature;
+  c->swim_sperm_decay = sperm_decay ? 1 : 0;
+  return FS_OK;
+}
+
+static void spring_free(fs_ctx *c) {
+  cudaFree(c->spring_beads);
+  cudaFree(c->spring_off);
+  cudaFree(c->spring_ent);
+  c->spring_beads = c->spring_off = c->spring_ent = nullptr;
+  c->nspring = 0;
+}
+
+fs_status fs_set_spring_links(fs_ctx *c, int nlinks, const int *beads_h, double k, double l0) {
+  if (!c || nlinks < 0 || (nlinks > 0 && !beads_h)) return FS_ERR_INVALID_ARG;
+  if (!c->have_state) return FS_ERR_STATE;
+  if (!std::isfinite(k) || !std::isfinite(l0)) return FS_ERR_INVALID_ARG;
+  for (int l = 0; l < nlinks; ++l) {
+    const int a = beads_h[2 * l], b = beads_h[2 * l + 1];
+    if (a < 0 || b < 0 || a >= c->np || b >= c->np || a == b) return FS_ERR_INVALID_ARG;
+  }
+  graph_invalidate(c);
+  FS_CUDA(cudaStreamSynchronize(c->stream));
+  spring_free(c);
+  if (nlinks == 0) return FS_OK;
+  // per bead, its links in link order: entry 2 l (first bead of link l) or 2 l + 1 (second)
+  std::vector<int> off(c->np + 1, 0), ent(2 * (size_t)nlinks);
+  for (int l = 0; l < nlinks; ++l) {
+    off[beads_h[2 * l] + 1]++;
+    off[beads_h[2 * l + 1] + 1]++;
+  }
+  for (int b = 0; b < c->np; ++b) off[b + 1] += off[b];
+  std::vector<int> fill(off.begin(), off.end() - 1);
+  for (int l = 0; l < nlinks; ++l) {
+    ent[fill[beads_h[2 * l]]++] = 2 * l;
+    ent[fill[beads_h[2 * l + 1]]++] = 2 * l + 1;
+  }
+  FS_CUDA(cudaMalloc(&c->spring_beads, sizeof(int) * 2 * (size_t)nlinks));
+  FS_CUDA(cudaMalloc(&c->spring_off, sizeof(int) * (size_t)(c->np + 1)));
+  FS_CUDA(cudaMalloc(&c->spring_ent, sizeof(int) * 2 * (size_t)nlinks));
+  FS_CUDA(cudaMemcpyAsync(c->spring_beads, beads_h, sizeof(int) * 2 * (size_t)nlinks, cudaMemcpyHostToDevice,
+                          c->stream));
+  FS_CUDA(cudaMemcpyAsync(c->spring_off, off.data(), sizeof(int) * (size_t)(c->np + 1), cudaMemcpyHostToDevice,
+                          c->stream));
+  FS_CUDA(cudaMemcpyAsync(c->spring_ent, ent.data(), sizeof(int) * 2 * (size_t)nlinks, cudaMemcpyHostToDevice,
+                          c->stream));
+  FS_CUDA(cudaStreamSynchronize(c->stream));  // the host vectors go out of scope
+  c->nspring = nlinks;
+  c->spring_k = k;
+  c->spring_l0 = l0;
+  return FS_OK;
+}
 
 fs_status fs_jacobian_build(fs_ctx *c, int nt) {
   if (!c) return FS_ERR_INVALID_ARG;

@@ -156,7 +156,39 @@ struct FilConsts {
   double dt, dl, mu, tol;
   double gravity[3], st[3];
   int impl_euler_steps, lambda_extrap_step;
+  // swimming drive: time of the forces (nt dt), per-filament parameters or null
+  double tt, swim_curvature;
+  int swim_sperm_decay;
+  const double *swim;
 };
+
+// Strain twist of link i of filament f (nw beads) at time k.tt
+// (applyElasticTorques, Filament.hpp:297-326): component 0 is the constant
+// STRAINTWISTZ; components 1 and 2 are set on every link by the swimming drive,
+// Beta facPref cos(k s - w t + phase) and Alpha facPref sin(...), so they are
+// zero for a filament without a drive.
+__device__ void link_strain_twist(const FilConsts &k, int f, int nw, int i, double *st) {
+  st[0] = k.st[0];
+  st[1] = 0.0;
+  st[2] = 0.0;
+  if (!k.swim) return;
+  const double *sw = k.swim + 5 * f;
+  const double dL = k.dl, L_filament = (nw - 1) * dL, L_filament_long = nw * dL;
+  const double T0 = (k.swim_curvature / L_filament_long);
+  const double sarc = dL * i + .5 * dL;
+  double facPref;
+  if (k.swim_sperm_decay) {
+    if (sarc > L_filament / 2.0)
+      facPref = T0 * 2.0 * (L_filament - sarc) / L_filament;
+    else
+      facPref = T0;
+  } else {
+    facPref = T0 * (L_filament - sarc) / L_filament;
+  }
+  const double arg = sw[3] * sarc - sw[4] * k.tt + sw[2];
+  st[1] = sw[1] * facPref * cos(arg);
+  st[2] = sw[0] * facPref * sin(arg);
+}
 
 // ---- per-bead / per-filament kernels -----------------------------------------
 __global__ void k_initial_guess(int np, const int *__restrict__ seg_id, const double *__restrict__ X,
@@ -226,14 +258,16 @@ __global__ void k_forces(int np, const int *__restrict__ fil_id, const int *__re
   const int nw = fil_start[f + 1] - fil_start[f];
   const int l0 = fil_start[f] - f;
   const double oneOverDL = 1. / k.dl;
-  double tau[3] = {0.0, 0.0, 0.0}, fo[3] = {0.0, 0.0, 0.0}, v[3];
+  double tau[3] = {0.0, 0.0, 0.0}, fo[3] = {0.0, 0.0, 0.0}, v[3], st[3];
   // elastic: link i-1 subtracts, link i adds (link order of Filament.hpp:297)
   if (i >= 1) {
-    elastic_link(qs + 4 * (b - 1), qs + 4 * b, oneOverDL, kap[f], cmod[f], k.st, v);
+    link_strain_twist(k, f, nw, i - 1, st);
+    elastic_link(qs + 4 * (b - 1), qs + 4 * b, oneOverDL, kap[f], cmod[f], st, v);
     for (int d = 0; d < 3; ++d) tau[d] -= v[d];
   }
   if (i < nw - 1) {
-    elastic_link(qs + 4 * b, qs + 4 * (b + 1), oneOverDL, kap[f], cmod[f], k.st, v);
+    link_strain_twist(k, f, nw, i, st);
+    elastic_link(qs + 4 * b, qs + 4 * (b + 1), oneOverDL, kap[f], cmod[f], st, v);
     for (int d = 0; d < 3; ++d) tau[d] += v[d];
   }
   // constraint forces and torques (Filament.hpp:351-368)
@@ -256,6 +290,38 @@ __global__ void k_forces(int np, const int *__restrict__ fil_id, const int *__re
     F[3 * b + d] = fo[d] + k.gravity[d];
     TAU[3 * b + d] = tau[d];
   }
+}
+
+// Spring links (spring_links::apply_spring_link_forces, spring_link_functions.cpp:24-45),
+// after the filaments' own forces (main.cpp:354-357): per link, the minimum-image
+// displacement of its beads (VecPeriodicX, :139-145) and a Hookean force along it,
+// + on the first bead and - on the second. One thread per bead adds its links in
+// link order, the order of the reference's sequential loop.
+__global__ void k_spring_forces(int np, const int *__restrict__ off, const int *__restrict__ ent,
+                                const int *__restrict__ beads, const double *__restrict__ Xs, double ks, double l0,
+                                FilConsts k, double *__restrict__ F) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= np) return;
+  double f[3] = {F[3 * b], F[3 * b + 1], F[3 * b + 2]};
+  for (int e = off[b]; e < off[b + 1]; ++e) {
+    const int l = ent[e] >> 1, second = ent[e] & 1;
+    const int bn = beads[2 * l], bm = beads[2 * l + 1];
+    double disp[3];
+    for (int d = 0; d < 3; ++d) {
+      disp[d] = Xs[3 * bn + d] - Xs[3 * bm + d];
+      disp[d] = disp[d] - k.L[d] * floor(disp[d] / k.L[d] + 0.5);
+    }
+    const double dist = sqrt(disp[0] * disp[0] + disp[1] * disp[1] + disp[2] * disp[2]);
+    const double mag = ks * (dist - l0);
+    for (int d = 0; d < 3; ++d) {
+      const double sf = -mag * disp[d] / dist;
+      if (second)
+        f[d] -= sf;
+      else
+        f[d] += sf;
+    }
+  }
+  for (int d = 0; d < 3; ++d) F[3 * b + d] = f[d];
 }
 
 // ---- Jacobian ------------------------------------------------------------------
@@ -506,8 +572,11 @@ __global__ void __launch_bounds__(256) k_jacobian_schur(
   }
   if (tid == 0) *pcoef = (dt / (9 * PI * MU * RAD(0))) / dt;
   __syncthreads();
+  // this->myStrainTwist as applyElasticTorques(nt) left it: its last link (nw >= 2 here)
+  double stj[3];
+  link_strain_twist(k, f, nw, nw - 2, stj);
   for (int kk = tid; kk < nw; kk += nthr)
-    blockE_row(kk, nw, q_f, Us_f, TAU_f, lam_f, RAD(kk), cmod[f], kap[f], k.st, DL, dt, MU, S, m);
+    blockE_row(kk, nw, q_f, Us_f, TAU_f, lam_f, RAD(kk), cmod[f], kap[f], stj, DL, dt, MU, S, m);
 #undef RAD
   __syncthreads();
   for (int e = tid; e < m; e += nthr) S[e * m + e] += 1.;  // BlockE's identity (Filament.hpp:1092-1094)
@@ -1127,6 +1196,10 @@ FilConsts make_fconsts(const fs_ctx *c) {
   k.tol = c->p.tol;
   k.impl_euler_steps = c->p.impl_euler_steps;
   k.lambda_extrap_step = c->p.lambda_extrap_step;
+  k.tt = 0.0;
+  k.swim_curvature = c->swim_curvature;
+  k.swim_sperm_decay = c->swim_sperm_decay;
+  k.swim = c->swim;
   return k;
 }
 
@@ -1142,15 +1215,21 @@ fs_status fil_initial_guess(fs_ctx *c) {
 }
 
 fs_status fil_forces(fs_ctx *c, int nt) {
-  (void)nt;
   if (!c->have_state) return FS_ERR_STATE;
   ProfScope ps(c, FS_STAGE_FORCES);
   FilConsts k = make_fconsts(c);
+  k.tt = nt * c->p.dt;  // double tt = nt*dt (Filament.hpp:295)
   k_unrobot_assign<<<fs_blocks(c->nfil, 128), 128, 0, c->stream>>>(c->nfil, c->fil_start, c->qs, c->Xs, c->Y, k);
   FS_LAUNCH_CHECK();
   k_forces<<<fs_blocks(c->np, 256), 256, 0, c->stream>>>(c->np, c->fil_id, c->seg_id, c->fil_start, c->qs, c->lam,
                                                           c->kap, c->cc, c->F, c->TAU, k);
   FS_LAUNCH_CHECK();
+  if (c->nspring > 0) {
+    k_spring_forces<<<fs_blocks(c->np, 256), 256, 0, c->stream>>>(c->np, c->spring_off, c->spring_ent,
+                                                                   c->spring_beads, c->Xs, c->spring_k,
+                                                                   c->spring_l0, k, c->F);
+    FS_LAUNCH_CHECK();
+  }
   return FS_OK;
 }
 
@@ -1158,6 +1237,7 @@ fs_status fil_jacobian_build(fs_ctx *c, int nt) {
   if (!c->have_state) return FS_ERR_STATE;
   ProfScope ps(c, FS_STAGE_JACOBIAN);
   FilConsts k = make_fconsts(c);
+  k.tt = nt * c->p.dt;
   const size_t smem = sizeof(double) * 9 * (size_t)c->max_nw * c->max_nw;
   // one thread per Schur column (3 Nw, rounded to warps): three filaments share an SM
   const int jthreads = std::min(256, 32 * ((3 * c->max_nw + 31) / 32));

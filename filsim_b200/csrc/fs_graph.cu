@@ -3,7 +3,8 @@
 //
 // A step in the steady regime (nt above the implicit-Euler, friction and
 // lambda-extrapolation thresholds, where every nt-dependent branch of the
-// kernels is fixed) is captured once: the start of the step (initial guess,
+// kernels is fixed; no swimming drive, whose strain twist depends on nt) is
+// captured once: the start of the step (initial guess,
 // forces, Jacobian, cell link, first barrier + mobility solve and residual), a
 // conditional WHILE node whose body is one Broyden iteration (apply, update,
 // forces, barrier + mobility, residual, history column, err <- newerr), and the
@@ -134,7 +135,9 @@ fs_status capture_step(fs_ctx *c, int nt, fs_graph *g, cudaGraph_t *out) {
 }  // namespace
 
 bool graph_steady(const fs_ctx *c, int nt) {
-  return nt > c->p.impl_euler_steps && nt > c->p.initial_friction_steps && nt > c->p.lambda_extrap_step;
+  // a swimming drive makes the forces depend on nt, which a captured step bakes in
+  return nt > c->p.impl_euler_steps && nt > c->p.initial_friction_steps && nt > c->p.lambda_extrap_step &&
+         !c->swim;
 }
 
 void graph_free(fs_ctx *c) {

@@ -90,6 +90,15 @@ struct fs_ctx {
   double *aux;           // per-filament D', F' blocks, tangents, P coefficient at aoff[f]
   long long *soff, *aoff;
   int max_nw, min_nw;  // longest and shortest filament
+  // swimming drive (fs_set_swimming): per filament (alpha, beta, phase, wavenumber,
+  // angular frequency); null when off. Spring links (fs_set_spring_links): bead
+  // pairs and, per bead, its links in link order (entry 2 l + side).
+  double *swim;
+  double swim_curvature;
+  int swim_sperm_decay;
+  int nspring;
+  int *spring_beads, *spring_off, *spring_ent;
+  double spring_k, spring_l0;
   double *dots;          // broyden_maxiter partial dots
   double *partials;      // reduction scratch
   double *scalars;       // [0] = ||dE||

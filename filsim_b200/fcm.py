@@ -229,6 +229,25 @@ class Simulation:
     def filament_forces(self, nt):
         self.ctx.call("fs_filament_forces", nt)
 
+    def set_swimming(self, swim, curvature=0.0, sperm_decay=False):
+        """Swimming drive: swim = [nfil x 5] (Alpha, Beta, Phase, Wavenumber,
+        AngFrequency) per filament, or None to switch it off (fs_set_swimming)."""
+        if swim is None:
+            self.ctx.call("fs_set_swimming", None, 0.0, 0)
+            return
+        self._swim = np.ascontiguousarray(swim, dtype=np.float64).reshape(-1, 5)
+        if self._swim.shape[0] != self.susp.nfil:
+            raise ValueError("swim needs one row per filament")
+        self.ctx.call("fs_set_swimming", self._swim.ctypes.data_as(ctypes.c_void_p), float(curvature),
+                      int(bool(sperm_decay)))
+
+    def set_spring_links(self, beads, k, l0):
+        """Spring links: beads = [n x 2] global bead indices, in link order
+        (spring_links::apply_spring_link_forces; fs_set_spring_links)."""
+        self._springs = np.ascontiguousarray(beads, dtype=np.int32).reshape(-1, 2)
+        self.ctx.call("fs_set_spring_links", self._springs.shape[0], self._springs.ctypes.data_as(ctypes.c_void_p),
+                      float(k), float(l0))
+
     def build_jacobian(self, nt):
         self.ctx.call("fs_jacobian_build", nt)
 

@@ -129,3 +129,23 @@ def fcm_positions(p, X):
     """Fcm::assign_filament_data position rule: Y = fmod(X, L) (FCMfunctions.cpp:902-904)."""
     L = np.array(box_lengths(p))
     return np.fmod(X, L)
+
+
+def swim_parameters(fil_start, p, K0, Sp4, alpha, beta, phase=0.0, kap=None):
+    """Per-filament swimming-drive rows (Alpha, Beta, Phase, Wavenumber,
+    AngFrequency) for fs_set_swimming, with the Filament constructor's
+    Wavenumber = 2 K0 pi / (Nw dL) and AngFrequency = KAP Sp4 / (4 pi mu (Nw dL)^4)
+    (Filament.hpp:135-144); alpha, beta, phase and kap are scalars or per filament
+    (kap defaults to 1, the bending modulus the constructor sees)."""
+    fil_start = np.asarray(fil_start)
+    nfil = fil_start.size - 1
+    nw = np.diff(fil_start).astype(np.float64)
+    kap = np.ones(nfil) if kap is None else np.broadcast_to(np.asarray(kap, dtype=np.float64), (nfil,))
+    length = nw * p.dl
+    out = np.zeros((nfil, 5))
+    out[:, 0] = alpha
+    out[:, 1] = beta
+    out[:, 2] = phase
+    out[:, 3] = 2 * K0 * np.pi / length
+    out[:, 4] = kap * Sp4 / (4 * np.pi * p.mu * length ** 4.)
+    return out

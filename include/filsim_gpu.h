@@ -241,6 +241,29 @@ fs_status fs_initial_guess(fs_ctx *ctx);
  * (Filament.hpp:271-402, 489-505), then Fcm::assign_filament_data
  * (FCMfunctions.cpp:882-918): Y = fmod(Xs, L), F, T into the FCM arrays. */
 fs_status fs_filament_forces(fs_ctx *ctx, int nt);
+/* Swimming drive (applyElasticTorques, Filament.hpp:297-326; set up per
+ * filament as filament_initialisation_functions.cpp:806-833 does): swim_h is
+ * nfil x 5 host doubles (Alpha, Beta, Phase, Wavenumber, AngFrequency) of the
+ * uploaded suspension, or NULL to switch the drive off. On link i at time
+ * t = nt dt the strain twist's components 1 and 2 are Beta facPref cos(Wavenumber s
+ * - AngFrequency t + Phase) and Alpha facPref sin(...), s = dL (i + 1/2),
+ * T0 = curvature / (Nw dL) and facPref = T0 (L - s) / L, or with sperm_decay
+ * T0 for s <= L/2 and 2 T0 (L - s) / L beyond (L = (Nw - 1) dL); the Jacobian
+ * uses the last link's values as the reference's buildJacobian does. As in the
+ * reference, components 1 and 2 of fs_params.strain_twist are replaced on
+ * every link (zero without a drive); component 0 stays constant. Steps with a
+ * drive run host-driven (a captured step graph would bake nt in). An upload
+ * with another filament layout drops the drive. */
+fs_status fs_set_swimming(fs_ctx *ctx, const double *swim_h, double curvature, int sperm_decay);
+/* Spring links between beads (spring_links::apply_spring_link_forces,
+ * spring_link_functions.cpp:24-45, applied after the filaments' own forces as
+ * main.cpp:354-357): beads_h holds 2 global bead indices per link, in link
+ * order; each link adds k (|d| - l0) along the minimum-image displacement d of
+ * its beads (VecPeriodicX, :139-145), - on the first bead and + on the second
+ * (F -= k (|d| - l0) d / |d| on the first). nlinks 0 removes the links. The
+ * indices must be distinct beads of the uploaded suspension; an upload with
+ * another filament layout drops the links. */
+fs_status fs_set_spring_links(fs_ctx *ctx, int nlinks, const int *beads_h, double k, double l0);
 /* filamentJsolver::buildJacobian (FilamentJacobianSolver.hpp:36-47 and
  * Filament.hpp:803-1120): per filament the approximate Jacobian is built and
  * LU-factorised; Broyden history is cleared. */

@@ -123,6 +123,14 @@ class SuspensionGpu {
   void initialGuess() { check(fs_initial_guess(ctx_.get()), "initialGuess"); }
   // unRobotArmify + forces/torques + Fcm::assign_filament_data
   void forces(int nt) { check(fs_filament_forces(ctx_.get(), nt), "forces"); }
+  // swimming drive: per filament {Alpha, Beta, Phase, Wavenumber, AngFrequency}; nullptr switches it off
+  void setSwimming(const double *swim, double curvature, bool spermCurvatureDecay) {
+    check(fs_set_swimming(ctx_.get(), swim, curvature, spermCurvatureDecay ? 1 : 0), "setSwimming");
+  }
+  // spring_links: 2 global bead indices per link, NetworkSpringConstant, NetworkSpringNaturalLength
+  void setSpringLinks(int nlinks, const int *beads, double k, double l0) {
+    check(fs_set_spring_links(ctx_.get(), nlinks, beads, k, l0), "setSpringLinks");
+  }
   // filamentJsolver::buildJacobian
   void buildJacobian(int nt) { check(fs_jacobian_build(ctx_.get(), nt), "filamentJsolver::buildJacobian"); }
   // filamentJsolver::solve

@@ -722,6 +722,13 @@ struct or_system {
   int *head, *list, *map;
   double min_dist2;
   long long nsolves;
+  /* swimming drive: per filament (alpha, beta, phase, wavenumber, angular
+   * frequency), or NULL; spring links: bead pairs (global indices) */
+  double *swim, swim_curvature;
+  int swim_sperm_decay;
+  int nspring;
+  int *spring_beads;
+  double spring_k, spring_l0;
 };
 
 static double *dalloc(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
@@ -779,7 +786,7 @@ void or_system_destroy(or_system *s) {
   void *ptrs[] = {s->fil_start, s->fil_id, s->seg_id, s->radius, s->X, s->Xs, s->Xt, s->U, s->Us, s->Ut,
                   s->q, s->qs, s->qt, s->F, s->TAU, s->lam, s->lam1, s->lam2, s->kap, s->cc, s->Y, s->V,
                   s->W, s->Err, s->NewErr, s->Upd, s->tmp, s->dE, s->Cmat, s->Dmat, s->joff, s->Jinv,
-                  s->head, s->list, s->map};
+                  s->head, s->list, s->map, s->swim, s->spring_beads};
   for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); ++i) free(ptrs[i]);
   free(s);
 }
@@ -836,12 +843,64 @@ void or_initial_guess(or_system *s) {
   }
 }
 
+void or_set_swimming(or_system *s, const double *swim, double curvature, int sperm_decay) {
+  free(s->swim);
+  s->swim = NULL;
+  if (swim) {
+    s->swim = dalloc(5 * (size_t)s->nfil);
+    memcpy(s->swim, swim, sizeof(double) * 5 * (size_t)s->nfil);
+  }
+  s->swim_curvature = curvature;
+  s->swim_sperm_decay = sperm_decay;
+}
+
+void or_set_spring_links(or_system *s, int nlinks, const int *beads, double k, double l0) {
+  free(s->spring_beads);
+  s->spring_beads = NULL;
+  s->nspring = nlinks > 0 ? nlinks : 0;
+  if (s->nspring) {
+    s->spring_beads = (int *)malloc(sizeof(int) * 2 * (size_t)nlinks);
+    memcpy(s->spring_beads, beads, sizeof(int) * 2 * (size_t)nlinks);
+  }
+  s->spring_k = k;
+  s->spring_l0 = l0;
+}
+
+/* Strain twist of link i of filament f at time tt (Filament.hpp:297-326):
+ * component 0 is the constant STRAINTWISTZ; components 1 and 2 are set on every
+ * link by the swimming drive (zero for a filament without it, since Alpha and
+ * Beta are zero). */
+static void or_link_strain_twist(const or_system *s, int f, int nw, int i, double tt, double *st) {
+  const double dL = s->p.dl;
+  st[0] = s->p.strain_twist[0];
+  st[1] = 0.0;
+  st[2] = 0.0;
+  if (!s->swim) return;
+  const double *sw = s->swim + 5 * f;
+  const double L_filament = (nw - 1) * dL, L_filament_long = nw * dL;
+  const double T0 = (s->swim_curvature / L_filament_long);
+  const double sarc = dL * i + .5 * dL;
+  double facPref;
+  if (s->swim_sperm_decay) {
+    if (sarc > L_filament / 2.0)
+      facPref = T0 * 2.0 * (L_filament - sarc) / L_filament;
+    else
+      facPref = T0;
+  } else {
+    facPref = T0 * (L_filament - sarc) / L_filament;
+  }
+  const double arg = sw[3] * sarc - sw[4] * tt + sw[2];
+  st[1] = sw[1] * facPref * cos(arg);
+  st[2] = sw[0] * facPref * sin(arg);
+}
+
 /* unRobotArmify (Filament.hpp:489-505), setZeroForcesTorques (:271-277),
  * applyElasticTorques (:289-342), applyConstraintForcesTorques (:345-370),
- * applyExternalForcesTorques (:379-402), then assign_filament_data
- * (FCMfunctions.cpp:882-918). */
+ * applyExternalForcesTorques (:379-402), the spring links
+ * (spring_link_functions.cpp:24-45, main.cpp:354-357), then
+ * assign_filament_data (FCMfunctions.cpp:882-918). */
 void or_filament_forces(or_system *s, int nt) {
-  (void)nt;
+  const double tt = nt * s->p.dt;
   const fs_params *p = &s->p;
   const double dL = p->dl, oneOverDL = 1. / p->dl;
   for (int f = 0; f < s->nfil; ++f) {
@@ -864,8 +923,10 @@ void or_filament_forces(or_system *s, int nt) {
     /* setZeroForcesTorques */
     for (int i = 0; i < nw; ++i)
       for (int d = 0; d < 3; ++d) { s->F[3 * (b0 + i) + d] = 0.0; s->TAU[3 * (b0 + i) + d] = 0.0; }
-    /* applyElasticTorques (no swimming: the strain twist is the constant p->strain_twist) */
+    /* applyElasticTorques, with the swimming drive's strain twist per link */
     for (int i = 0; i < nw - 1; ++i) {
+      double st[3];
+      or_link_strain_twist(s, f, nw, i, tt, st);
       int j = i + 1;
       or_quat qi, qj, qm;
       q_load(&qi, s->qs + 4 * (b0 + i));
@@ -883,7 +944,7 @@ void or_filament_forces(or_system *s, int nt) {
       double nv[3];
       for (int d = 0; d < 3; ++d) nv[d] = -q2.s * qm.v[d] + qm.s * q2.v[d] + tt[d];
       double vtmp[3];
-      for (int d = 0; d < 3; ++d) vtmp[d] = 2. * nv[d] - p->strain_twist[d];
+      for (int d = 0; d < 3; ++d) vtmp[d] = 2. * nv[d] - st[d];
       (void)scal_tmp;
       vtmp[0] *= s->cc[f];
       vtmp[1] *= s->kap[f];
@@ -918,8 +979,25 @@ void or_filament_forces(or_system *s, int nt) {
     for (int i = 0; i < nw; ++i)
       for (int d = 0; d < 3; ++d) s->F[3 * (b0 + i) + d] += p->gravity[d];
   }
-  /* assign_filament_data: Y = fmod(Xs, L) */
   const double L[3] = {s->c.Lx, s->c.Ly, s->c.Lz};
+  /* apply_spring_link_forces, links in order: minimum-image displacement
+   * (VecPeriodicX, spring_link_functions.cpp:139-145), Hookean force along it */
+  for (int l = 0; l < s->nspring; ++l) {
+    const int bn = s->spring_beads[2 * l], bm = s->spring_beads[2 * l + 1];
+    double disp[3];
+    for (int d = 0; d < 3; ++d) {
+      disp[d] = s->Xs[3 * bn + d] - s->Xs[3 * bm + d];
+      disp[d] = disp[d] - L[d] * floor(disp[d] / L[d] + 0.5);
+    }
+    const double dist = sqrt(disp[0] * disp[0] + disp[1] * disp[1] + disp[2] * disp[2]);
+    const double spring_mag = s->spring_k * (dist - s->spring_l0);
+    for (int d = 0; d < 3; ++d) {
+      const double sf = -spring_mag * disp[d] / dist;
+      s->F[3 * bn + d] += sf;
+      s->F[3 * bm + d] -= sf;
+    }
+  }
+  /* assign_filament_data: Y = fmod(Xs, L) */
   for (int b = 0; b < s->np; ++b)
     for (int d = 0; d < 3; ++d) s->Y[3 * b + d] = fmod(s->Xs[3 * b + d], L[d]);
 }
@@ -997,7 +1075,12 @@ static void or_build_J(or_system *s, int f, int nt, double *J) {
   const int b0 = s->fil_start[f], nw = s->fil_start[f + 1] - b0, l0 = b0 - f;
   const int n = 6 * nw;
   const double myC = s->cc[f], myKAP = s->kap[f];
-  const double *ST = p->strain_twist;
+  /* this->myStrainTwist as applyElasticTorques(nt) left it: its last link */
+  double ST[3];
+  if (nw >= 2)
+    or_link_strain_twist(s, f, nw, nw - 2, nt * dt, ST);
+  else
+    for (int d = 0; d < 3; ++d) ST[d] = p->strain_twist[d];
   memset(J, 0, sizeof(double) * (size_t)n * n);
   const double *rad = s->radius + b0;
 #define QS(k) (s->qs + 4 * (b0 + (k)))

@@ -45,6 +45,10 @@ void or_system_get(or_system *sys, fs_host_state *s);
 void or_system_set(or_system *sys, const fs_host_state *s);
 double *or_system_array(or_system *sys, const char *which);
 void or_initial_guess(or_system *sys);
+/* swimming drive: swim = per filament (alpha, beta, phase, wavenumber, angular
+ * frequency) or NULL (off); spring links: nlinks bead pairs (global indices) */
+void or_set_swimming(or_system *sys, const double *swim, double curvature, int sperm_decay);
+void or_set_spring_links(or_system *sys, int nlinks, const int *beads, double k, double l0);
 void or_filament_forces(or_system *sys, int nt);
 void or_build_jacobian(or_system *sys, int nt);
 void or_get_jinv(or_system *sys, int f, double *out);

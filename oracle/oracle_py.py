@@ -47,6 +47,8 @@ def lib():
         L.or_system_array.argtypes = [vp, ctypes.c_char_p]
         for n in ("or_initial_guess",):
             getattr(L, n).argtypes = [vp]
+        L.or_set_swimming.argtypes = [vp, vp, ctypes.c_double, ctypes.c_int]
+        L.or_set_spring_links.argtypes = [vp, ctypes.c_int, vp, ctypes.c_double, ctypes.c_double]
         L.or_filament_forces.argtypes = [vp, ctypes.c_int]
         L.or_build_jacobian.argtypes = [vp, ctypes.c_int]
         L.or_get_jinv.argtypes = [vp, ctypes.c_int, vp]
@@ -198,6 +200,19 @@ class System:
 
     def initial_guess(self):
         lib().or_initial_guess(self.h)
+
+    def set_swimming(self, swim, curvature=0.0, sperm_decay=False):
+        """swim: [nfil x 5] (alpha, beta, phase, wavenumber, angular frequency), or None."""
+        if swim is None:
+            lib().or_set_swimming(self.h, None, 0.0, 0)
+            return
+        self._swim = _f64(swim).reshape(-1, 5)
+        lib().or_set_swimming(self.h, _ptr(self._swim), float(curvature), int(bool(sperm_decay)))
+
+    def set_spring_links(self, beads, k, l0):
+        """beads: [n x 2] global bead indices of the linked pairs, in link order."""
+        self._springs = np.ascontiguousarray(beads, dtype=np.int32).reshape(-1, 2)
+        lib().or_set_spring_links(self.h, self._springs.shape[0], _ptr(self._springs), float(k), float(l0))
 
     def filament_forces(self, nt):
         lib().or_filament_forces(self.h, nt)

@@ -167,3 +167,76 @@ def test_suspension_rejection_rule():
     fid = s.fil_id
     other = fid[:, None] != fid[None, :]
     assert r2[other].min() >= (2.2 - 1e-9) ** 2
+
+
+def _link_twist_norms(tau, nw):
+    """Per-link torque magnitudes |w_i| of a filament whose beads receive
+    +w_i (bead i) and -w_i (bead i+1): w_i is the prefix sum of the torques."""
+    w = np.cumsum(tau[: nw - 1], axis=0)
+    return np.linalg.norm(w, axis=1)
+
+
+@pytest.mark.parametrize("sperm_decay", [False, True])
+def test_swimming_drive_strain_twist(oracle, sperm_decay):
+    """applyElasticTorques with the swimming drive (Filament.hpp:297-326) on
+    straight filaments (q equal along each filament, lambda = 0): the elastic
+    term vanishes, so link i carries the rotated (-C st0, -K st1, -K st2) with
+    st1 = Beta facPref cos(k s - w t + phase), st2 = Alpha facPref sin(...)."""
+    from filsim_b200.suspension import swim_parameters
+    p = sediment_params(32)
+    nfil, nw, nt = 3, 8, 7
+    kap = np.array([0.7, 1.0, 1.6])
+    s = random_suspension(p, nfil, nw, seed=61, kap=kap, c=1.0)
+    sysw = oracle.System(p, s)
+    swim = swim_parameters(s.fil_start, p, K0=1.0, Sp4=12.0, alpha=[0.3, 0.0, 1.1], beta=[1.0, 0.5, 0.0],
+                           phase=[0.2, -1.0, 2.0], kap=kap)
+    curvature = 8.25
+    sysw.set_swimming(swim, curvature=curvature, sperm_decay=sperm_decay)
+    sysw.filament_forces(nt)
+    tau = sysw.download()["TAU"].reshape(nfil, nw, 3)
+    F_swim = sysw.download()["F"]
+    sysw.set_swimming(None)
+    sysw.filament_forces(nt)
+    assert np.array_equal(sysw.download()["F"], F_swim)  # the drive acts on torques only
+    tt = nt * p.dt
+    L, Llong = (nw - 1) * p.dl, nw * p.dl
+    T0 = curvature / Llong
+    for f in range(nfil):
+        sarc = p.dl * np.arange(nw - 1) + 0.5 * p.dl
+        if sperm_decay:
+            fac = np.where(sarc > L / 2.0, T0 * 2.0 * (L - sarc) / L, T0)
+        else:
+            fac = T0 * (L - sarc) / L
+        arg = swim[f, 3] * sarc - swim[f, 4] * tt + swim[f, 2]
+        st1 = swim[f, 1] * fac * np.cos(arg)
+        st2 = swim[f, 0] * fac * np.sin(arg)
+        want = kap[f] * np.sqrt(st1 ** 2 + st2 ** 2)
+        got = _link_twist_norms(tau[f], nw)
+        assert np.allclose(got, want, rtol=1e-12, atol=1e-14), f
+
+
+def test_spring_links_forces(oracle):
+    """apply_spring_link_forces (spring_link_functions.cpp:24-45): the change of
+    F from the links is -k (|d| - l0) d/|d| on the first bead and the opposite on
+    the second, d the minimum-image displacement; links sharing a bead add up."""
+    p = sediment_params(32)
+    s = random_suspension(p, 3, 8, seed=62)
+    sysw = oracle.System(p, s)
+    nt = 5
+    sysw.filament_forces(nt)
+    F0 = sysw.download()["F"].copy()
+    Xs = sysw.download()["Xs"]
+    links = np.array([[0, 9], [9, 20], [3, 23]])
+    k, l0 = 2.5, 3.0
+    sysw.set_spring_links(links, k, l0)
+    sysw.filament_forces(nt)
+    F1 = sysw.download()["F"]
+    Lb = np.array(box_lengths(p))
+    want = np.zeros_like(F0)
+    for a, b in links:
+        d = Xs[a] - Xs[b]
+        d = d - Lb * np.floor(d / Lb + 0.5)
+        sf = -k * (np.linalg.norm(d) - l0) * d / np.linalg.norm(d)
+        want[a] += sf
+        want[b] -= sf
+    assert np.abs((F1 - F0) - want).max() < 1e-12 * max(1.0, np.abs(want).max())
