@@ -22,10 +22,12 @@ FS_OK = 0
 STATUS_NAMES = {
     0: "FS_OK", 1: "FS_ERR_INVALID_ARG", 2: "FS_ERR_NO_DEVICE", 3: "FS_ERR_CUDA", 4: "FS_ERR_CUFFT",
     5: "FS_ERR_OOM", 6: "FS_ERR_NOT_CONVERGED", 7: "FS_ERR_NONFINITE", 8: "FS_ERR_CAPACITY", 9: "FS_ERR_STATE",
+    10: "FS_ERR_IO",
 }
 FS_ERR_INVALID_ARG = 1
 FS_ERR_NOT_CONVERGED = 6
 FS_ERR_STATE = 9
+FS_ERR_IO = 10
 FS_PREC_FP64 = 0
 FS_PREC_FP32 = 1
 
@@ -71,6 +73,23 @@ class FsHostState(ctypes.Structure):
         ("F", P_double), ("TAU", P_double),
         ("lam", P_double), ("lam1", P_double), ("lam2", P_double),
         ("kap", P_double), ("c", P_double),
+    ]
+
+
+class FsRunInfo(ctypes.Structure):
+    """fs_run_info: the columns of the reference's .par file."""
+    _fields_ = [
+        ("simulation_name", ctypes.c_char * 128), ("simulation_tag", ctypes.c_char * 128),
+        ("a", c_double), ("ah", c_double), ("dl", c_double), ("sp4", c_double), ("kap", c_double),
+        ("c", c_double), ("mu", c_double), ("curvature", c_double), ("k0", c_double),
+        ("time_steps", c_double), ("steps_per_period", c_double), ("tol", c_double),
+        ("broyden_maxiter", c_int), ("box", c_double * 3), ("plot_steps", c_int),
+        ("strain_twist", c_double * 3),
+        ("kap_network_filaments", c_double), ("bnumber", c_double), ("steps_per_settling_time", c_double),
+        ("dt", c_double), ("initial_friction_steps", c_int), ("enable_spring_links", c_int),
+        ("cn_num_swimming_filaments", c_double), ("cn_num_nodes", c_double), ("cn_connection_radius", c_double),
+        ("cn_min_node_spacing", c_double), ("cn_spacing_away_from_node", c_double),
+        ("network_spring_constant", c_double), ("network_spring_natural_length", c_double),
     ]
 
 
@@ -195,6 +214,13 @@ def _declare(L):
         "fs_batch_run": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p]),
         "fs_learn_override": (c_int, [c_void_p, c_void_p]),
         "fs_gemm_bf16": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int]),
+        "fs_par_write": (c_int, [ctypes.c_char_p, ctypes.POINTER(FsRunInfo), ctypes.POINTER(FsHostState)]),
+        "fs_par_read_layout": (c_int, [ctypes.c_char_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int), c_void_p,
+                                       c_int]),
+        "fs_backup_write": (c_int, [ctypes.c_char_p, ctypes.POINTER(FsHostState), c_int]),
+        "fs_backup_read": (c_int, [ctypes.c_char_p, ctypes.POINTER(FsHostState), ctypes.POINTER(c_int)]),
+        "fs_data_write_header": (c_int, [ctypes.c_char_p, ctypes.POINTER(FsHostState)]),
+        "fs_data_append": (c_int, [ctypes.c_char_p, ctypes.POINTER(FsHostState), c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -182,6 +182,7 @@ const char *fs_status_string(fs_status s) {
     case FS_ERR_NONFINITE: return "non-finite residual or singular Jacobian";
     case FS_ERR_CAPACITY: return "internal list capacity exceeded";
     case FS_ERR_STATE: return "call order violated";
+    case FS_ERR_IO: return "file could not be opened, written or parsed";
     default: return "unknown status";
   }
 }

@@ -50,7 +50,8 @@ enum {
   FS_ERR_NOT_CONVERGED = 6,   /* Broyden reached broyden_maxiter (state is still advanced, as the reference does) */
   FS_ERR_NONFINITE = 7,       /* NaN/Inf met in a residual */
   FS_ERR_CAPACITY = 8,        /* an internal fixed-size list overflowed (reported, never written out of bounds) */
-  FS_ERR_STATE = 9            /* call order violated (e.g. barrier before link) */
+  FS_ERR_STATE = 9,           /* call order violated (e.g. barrier before link) */
+  FS_ERR_IO = 10              /* a file could not be opened, written or parsed */
 };
 
 /* Precision of the FCM spread / FFT / interpolation chain. */
@@ -437,6 +438,57 @@ fs_status fs_gemm_bf16(fs_ctx *ctx, const void *A_d, const void *B_d, float *D_d
  * Returns FS_ERR_CAPACITY if a filament cannot be placed in max_tries. */
 fs_status fs_suspension_random(const fs_params *p, int nfil, int nw, unsigned long long seed, double min_sep,
                                int max_tries, double *X_h, double *q_h);
+
+/* ---- reference-compatible run files (host only, no GPU needed) ---------------
+ * Text files in the reference's formats, so runs resume each other's
+ * checkpoints and feed the reference's plotting scripts. Numbers in .bak and
+ * .dat files are written as C++ streams with precision(16) and ios::fixed
+ * print them (printf "%.16f"), each followed by one space; .par values use the
+ * stream default (printf "%g"). Quaternions are scalar first. Filaments are in
+ * fs_host_state order (fil_start). */
+
+/* Columns of the .par file (save_parameter_values_to_file,
+ * file_functions.cpp:6-80), in the reference's names. Only Nsw and the bead
+ * numbers are read back (continue_from_checkpoint); the rest documents the run. */
+typedef struct fs_run_info {
+  char simulation_name[128], simulation_tag[128];
+  double a, ah, dl, sp4, kap, c, mu, curvature, k0;
+  double time_steps, steps_per_period, tol;
+  int broyden_maxiter;
+  double box[3];            /* LfcmBox_x, LfcmBox_y, LfcmBox_z */
+  int plot_steps;
+  double strain_twist[3];   /* STRAINTWISTX, STRAINTWISTY, STRAINTWISTZ */
+  double kap_network_filaments, bnumber, steps_per_settling_time, dt;
+  int initial_friction_steps, enable_spring_links;
+  double cn_num_swimming_filaments, cn_num_nodes, cn_connection_radius, cn_min_node_spacing,
+      cn_spacing_away_from_node, network_spring_constant, network_spring_natural_length;
+} fs_run_info;
+
+/* .par (file_functions.cpp:6-80): the column names, the values, BeadNumbers
+ * from s->fil_start and the bending factors s->kap[f] / info->kap. */
+fs_status fs_par_write(const char *path, const fs_run_info *info, const fs_host_state *s);
+/* The layout continue_from_checkpoint reads from a .par (file_functions.cpp:236-272):
+ * the third item of the second line is the filament count, the fifth line holds
+ * the bead numbers. fil_start_h receives nfil + 1 offsets (capacity max_fil + 1);
+ * *np_out the bead count. FS_ERR_CAPACITY if the file holds more than max_fil. */
+fs_status fs_par_read_layout(const char *path, int *nfil_out, int *np_out, int *fil_start_h, int max_fil);
+/* .bak (save_backup_data_to_file, file_functions.cpp:210-221, and
+ * Filament::writeBackupData, Filament.hpp:650-679): nt, then per filament and
+ * bead X, Xt, qs (q when s->qs is NULL), qt, U, Ut, then per link lam, lam1,
+ * lam2; overwrites. */
+fs_status fs_backup_write(const char *path, const fs_host_state *s, int nt);
+/* Reads a .bak written for the layout s->fil_start / s->nfil / s->np
+ * (continue_from_checkpoint, file_functions.cpp:274-303, and
+ * Filament::continue_from_checkpoint, Filament.hpp:683-748): fills X, Xt, q,
+ * qt, U, Ut, lam, lam1, lam2 and sets Xs = X, qs = q, Us = U; *nt_next = the
+ * file's nt + 1, the step the reference resumes at. */
+fs_status fs_backup_read(const char *path, fs_host_state *s, int *nt_next);
+/* .dat (save_data_column_names_to_file, file_functions.cpp:84-97, and
+ * save_data_to_file, :150-161; Filament::writeDataNames / writeData,
+ * Filament.hpp:509-560): the header overwrites the file ("it", then X Y Z qr qi
+ * qj qk per bead); a row appends nt and per bead Xs, qs. */
+fs_status fs_data_write_header(const char *path, const fs_host_state *s);
+fs_status fs_data_append(const char *path, const fs_host_state *s, int nt);
 
 #ifdef __cplusplus
 }
