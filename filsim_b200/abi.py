@@ -28,6 +28,7 @@ FS_ERR_INVALID_ARG = 1
 FS_ERR_NOT_CONVERGED = 6
 FS_ERR_STATE = 9
 FS_ERR_IO = 10
+FS_BARRIER_ALL, FS_BARRIER_NOT_SWIMMER, FS_BARRIER_NOT_TEST_PARTICLES, FS_BARRIER_OFF = 0, 1, 2, 3
 FS_PREC_FP64 = 0
 FS_PREC_FP32 = 1
 
@@ -175,6 +176,8 @@ def _declare(L):
         "fs_filament_forces": (c_int, [c_void_p, c_int]),
         "fs_set_swimming": (c_int, [c_void_p, c_void_p, c_double, c_int]),
         "fs_set_spring_links": (c_int, [c_void_p, c_int, c_void_p, c_double, c_double]),
+        "fs_set_barrier_mode": (c_int, [c_void_p, c_int]),
+        "fs_step_gait_reset": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
         "fs_jacobian_build": (c_int, [c_void_p, c_int]),
         "fs_jacobian_get_inverse": (c_int, [c_void_p, c_int, c_void_p, c_int]),
         "fs_error_check": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),

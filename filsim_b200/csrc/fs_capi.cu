@@ -103,7 +103,8 @@ fs_status read_flags(fs_ctx *c) {
 }
 
 fs_status barrier_and_mobility(fs_ctx *c, int nt) {
-  FS_TRY(cells_barrier(c, c->Y, c->F, c->np, nt, c->fil_id, c->seg_id, nullptr, 0, nullptr));
+  if (c->barrier_mode != FS_BARRIER_OFF)
+    FS_TRY(cells_barrier(c, c->Y, c->F, c->np, nt, c->fil_id, c->seg_id, nullptr, 0, nullptr, c->barrier_mode));
   if (nt > c->p.initial_friction_steps)
     FS_TRY(fcm_mobility(c, c->Y, c->F, c->TAU, c->V, c->W, c->np));
   else
@@ -118,8 +119,9 @@ fs_status step_barrier_mobility(fs_ctx *c, int nt) { return barrier_and_mobility
 
 namespace {
 
-// one implicit step (main.cpp:334-707)
-fs_status step_implicit(fs_ctx *c, int nt, int *iters_out) {
+// one implicit step (main.cpp:334-707); commit = false leaves out Filament::step
+// (the gait-reset driver's trial solves)
+fs_status step_implicit(fs_ctx *c, int nt, int *iters_out, bool commit = true) {
   FS_TRY(fil_initial_guess(c));
   const bool learn_on = learn_active(c) && nt > c->p.initial_friction_steps;
   const bool learned = learn_on && learn_gate_choose(c);
@@ -153,7 +155,7 @@ fs_status step_implicit(fs_ctx *c, int nt, int *iters_out) {
   if (learn_recording(c)) FS_TRY(learn_capture_targets(c, iter));
   if (learn_on) learn_gate_record(c, learned, c->diag.mobility_solves - solves0);
   FS_TRY(learn_end_step(c));
-  FS_TRY(fil_step(c, nt));
+  if (commit) FS_TRY(fil_step(c, nt));
   c->diag.last_nt = nt;
   c->diag.last_iters = iter;
   c->diag.total_iters += iter;
@@ -602,6 +604,51 @@ fs_status fs_set_swimming(fs_ctx *c, const double *swim_h, double curvature, int
   c->swim_curvature = curvature;
   c->swim_sperm_decay = sperm_decay ? 1 : 0;
   return FS_OK;
+}
+
+fs_status fs_set_barrier_mode(fs_ctx *c, int mode) {
+  if (!c || mode < FS_BARRIER_ALL || mode > FS_BARRIER_OFF) return FS_ERR_INVALID_ARG;
+  if (mode != c->barrier_mode) graph_invalidate(c);
+  c->barrier_mode = mode;
+  return FS_OK;
+}
+
+fs_status fs_step_gait_reset(fs_ctx *c, int nt, int *iters_h, double *vwf_h) {
+  if (!c || !iters_h) return FS_ERR_INVALID_ARG;
+  if (!c->have_state) return FS_ERR_STATE;
+  memset(&c->diag, 0, sizeof c->diag);
+  const int saved = c->barrier_mode;
+  const int modes[3] = {FS_BARRIER_OFF, FS_BARRIER_NOT_SWIMMER, saved};
+  const int nw0 = c->nfil > 0 ? c->fil_start_h[1] - c->fil_start_h[0] : 0;
+  fs_status st = FS_OK;
+  for (int pass = 0; pass < 3 && st == FS_OK; ++pass) {
+    c->barrier_mode = modes[pass];
+    st = step_implicit(c, nt, iters_h + pass, pass == 2);
+    if (st == FS_OK && vwf_h && nw0 > 0) {
+      // filament 0's beads: V, W, F of the solve (save_swimmer_velocity_data_to_file)
+      std::vector<double> v(3 * (size_t)nw0), w(3 * (size_t)nw0), f(3 * (size_t)nw0);
+      cudaError_t e = cudaMemcpyAsync(v.data(), c->V, sizeof(double) * 3 * nw0, cudaMemcpyDeviceToHost, c->stream);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(w.data(), c->W, sizeof(double) * 3 * nw0, cudaMemcpyDeviceToHost, c->stream);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(f.data(), c->F, sizeof(double) * 3 * nw0, cudaMemcpyDeviceToHost, c->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+      if (e != cudaSuccess) {
+        st = FS_ERR_CUDA;
+        break;
+      }
+      for (int b = 0; b < nw0; ++b)
+        for (int d = 0; d < 3; ++d) {
+          vwf_h[((size_t)pass * nw0 + b) * 9 + d] = v[3 * b + d];
+          vwf_h[((size_t)pass * nw0 + b) * 9 + 3 + d] = w[3 * b + d];
+          vwf_h[((size_t)pass * nw0 + b) * 9 + 6 + d] = f[3 * b + d];
+        }
+    }
+  }
+  c->barrier_mode = saved;
+  FS_TRY(st);
+  if (c->diag.nonfinite) return FS_ERR_NONFINITE;
+  return c->diag.not_converged_steps ? FS_ERR_NOT_CONVERGED : FS_OK;
 }
 
 static void spring_free(fs_ctx *c) {

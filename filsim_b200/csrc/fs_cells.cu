@@ -27,6 +27,7 @@ struct BarrierConsts {
   int M[3];
   double chiRnm2, den, cap, cap2, fs;
   int nt, initial_friction_steps;
+  int mode, np;  // pair filter (FS_BARRIER_*) and bead count
 };
 
 // bulkmap neighbour offsets (CollisionBarrierFilament.cpp:326-338)
@@ -116,7 +117,12 @@ __device__ __forceinline__ unsigned long long ev_key(int cell, int pos_i, int sl
           4096ull) + (unsigned long long)pos_j;
 }
 
+// pairs the barrier skips: neighbours on one filament (CollisionBarrierFilament.cpp:57),
+// and per mode swimmer-network pairs (apply_collision_barrier_not_swimmer, :474-477)
+// or pairs with one of the last two beads (apply_collision_barrier_not_test_particles, :754)
 __device__ __forceinline__ bool excluded(const BarrierConsts &k, const int *fil_id, const int *seg_id, int i, int j) {
+  if (k.mode == FS_BARRIER_NOT_SWIMMER && ((fil_id[i] == 0) != (fil_id[j] == 0))) return true;
+  if (k.mode == FS_BARRIER_NOT_TEST_PARTICLES && (i >= k.np - 2 || j >= k.np - 2)) return true;
   return (fil_id[j] == fil_id[i] && abs(seg_id[j] - seg_id[i]) == 1) && !(k.nt < k.initial_friction_steps);
 }
 
@@ -294,6 +300,8 @@ BarrierConsts make_bconsts(const fs_ctx *c, int nt) {
   k.fs = c->p.barrier_fs_over_2a;
   k.nt = nt;
   k.initial_friction_steps = c->p.initial_friction_steps;
+  k.mode = FS_BARRIER_ALL;
+  k.np = 0;
   return k;
 }
 
@@ -351,10 +359,12 @@ fs_status cells_link(fs_ctx *c, const double *Xs, int np) {
 }
 
 fs_status cells_barrier(fs_ctx *c, const double *Y, double *F, int np, int nt, const int *fil_id,
-                        const int *seg_id, int *pairs_d, int max_pairs, int *npairs_h) {
+                        const int *seg_id, int *pairs_d, int max_pairs, int *npairs_h, int mode) {
   if (c->cells_np != np) return FS_ERR_STATE;
   ProfScope ps(c, FS_STAGE_BARRIER);
   BarrierConsts k = make_bconsts(c, nt);
+  k.mode = mode;
+  k.np = np;
   k_set_min_init<<<1, 1, 0, c->stream>>>(c->min_dist2_bits);
   FS_LAUNCH_CHECK();
   if (np == 0) return FS_OK;

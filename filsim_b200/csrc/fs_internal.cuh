@@ -99,6 +99,7 @@ struct fs_ctx {
   int nspring;
   int *spring_beads, *spring_off, *spring_ent;
   double spring_k, spring_l0;
+  int barrier_mode;      // pair filter of the step's barrier (fs_set_barrier_mode)
   double *dots;          // broyden_maxiter partial dots
   double *partials;      // reduction scratch
   double *scalars;       // [0] = ||dE||
@@ -178,7 +179,7 @@ fs_status cells_init(fs_ctx *c);
 void cells_free(fs_ctx *c);
 fs_status cells_link(fs_ctx *c, const double *Xs, int np);
 fs_status cells_barrier(fs_ctx *c, const double *Y, double *F, int np, int nt, const int *fil_id, const int *seg_id,
-                        int *pairs_d, int max_pairs, int *npairs_h);
+                        int *pairs_d, int max_pairs, int *npairs_h, int mode = FS_BARRIER_ALL);
 
 fs_status fil_initial_guess(fs_ctx *c);
 fs_status fil_forces(fs_ctx *c, int nt);

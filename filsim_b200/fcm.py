@@ -241,6 +241,22 @@ class Simulation:
         self.ctx.call("fs_set_swimming", self._swim.ctypes.data_as(ctypes.c_void_p), float(curvature),
                       int(bool(sperm_decay)))
 
+    def set_barrier_mode(self, mode):
+        """Pair filter of the step's collision barrier (abi.FS_BARRIER_*)."""
+        self.ctx.call("fs_set_barrier_mode", int(mode))
+
+    def step_gait_reset(self, nt):
+        """One gait-reset step (main_gaitreset.cpp:302-830): returns the three
+        solves' iterations, filament 0's V, W, F per solve [3, Nw0, 9] and the status."""
+        nw0 = int(self.susp.fil_start[1] - self.susp.fil_start[0])
+        its = np.zeros(3, dtype=np.int32)
+        vwf = np.zeros((3, nw0, 9))
+        st = lib().fs_step_gait_reset(self.ctx.h, nt, its.ctypes.data_as(ctypes.c_void_p),
+                                      vwf.ctypes.data_as(ctypes.c_void_p))
+        if st not in (abi.FS_OK, abi.FS_ERR_NOT_CONVERGED):
+            check(st, "fs_step_gait_reset")
+        return its, vwf, st
+
     def set_spring_links(self, beads, k, l0):
         """Spring links: beads = [n x 2] global bead indices, in link order
         (spring_links::apply_spring_link_forces; fs_set_spring_links)."""

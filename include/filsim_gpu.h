@@ -265,6 +265,28 @@ fs_status fs_set_swimming(fs_ctx *ctx, const double *swim_h, double curvature, i
  * indices must be distinct beads of the uploaded suspension; an upload with
  * another filament layout drops the links. */
 fs_status fs_set_spring_links(fs_ctx *ctx, int nlinks, const int *beads_h, double k, double l0);
+
+/* Pair filters of the collision barrier in the implicit step: the reference's
+ * LinkedList::apply_collision_barrier (CollisionBarrierFilament.cpp:24-271),
+ * apply_collision_barrier_not_swimmer (:441-697: no pairs between filament 0,
+ * the swimmer, and the other filaments), apply_collision_barrier_not_test_particles
+ * (:698-945: no pairs with either of the last two beads), or no barrier. */
+enum {
+  FS_BARRIER_ALL = 0,
+  FS_BARRIER_NOT_SWIMMER = 1,
+  FS_BARRIER_NOT_TEST_PARTICLES = 2,
+  FS_BARRIER_OFF = 3
+};
+fs_status fs_set_barrier_mode(fs_ctx *ctx, int mode);
+/* One time step of the gait-reset driver (main_gaitreset.cpp:302-830): three
+ * solves of the implicit step from the same committed state, (0) without the
+ * barrier, (1) without swimmer-network barrier pairs, (2) with the context's
+ * barrier mode, and only the last one commits (Filament::step); lambda carries
+ * from one solve to the next as in the reference. iters_h[3]: Broyden
+ * iterations of each solve. vwf_h (optional): per solve, filament 0's beads'
+ * V, W and F after the solve ([3][Nw0][9]), the rows the reference writes with
+ * save_swimmer_velocity_data_to_file. Host-driven (no step graph). */
+fs_status fs_step_gait_reset(fs_ctx *ctx, int nt, int *iters_h, double *vwf_h);
 /* filamentJsolver::buildJacobian (FilamentJacobianSolver.hpp:36-47 and
  * Filament.hpp:803-1120): per filament the approximate Jacobian is built and
  * LU-factorised; Broyden history is cleared. */

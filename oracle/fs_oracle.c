@@ -540,9 +540,28 @@ static int or_pair(const fs_params *p, const double *L, const double *Yi, const 
 /* LinkedList::apply_collision_barrier (CollisionBarrierFilament.cpp:24-271),
  * one rank: F_total = F_on_node, added into F. Returns the pair count; the
  * first max_pairs pairs (i, j) are written to pairs in visiting order. */
+/* pair filter of the barrier variants (CollisionBarrierFilament.cpp:57, :474-477, :754) */
+static int or_pair_on(int mode, int np, int nt, int ifs, int i, int i_fil, int i_seg, int j, int j_fil, int j_seg) {
+  const int base = !(j_fil == i_fil && abs(j_seg - i_seg) == 1) || nt < ifs;
+  if (mode == FS_BARRIER_NOT_SWIMMER) return ((i_fil == 0) == (j_fil == 0)) && base;
+  if (mode == FS_BARRIER_NOT_TEST_PARTICLES) return base && (i < np - 2 && j < np - 2);
+  return base;
+}
+
+static int or_collision_barrier_mode(const fs_params *p, int np, const int *fil_id, const int *seg_id,
+                                     const double *Y, const int *head, const int *list, const int *map, int nt,
+                                     double *F, double *min_dist2_out, int *pairs, int max_pairs, int mode);
+
 int or_collision_barrier(const fs_params *p, int np, const int *fil_id, const int *seg_id, const double *Y,
                          const int *head, const int *list, const int *map, int nt, double *F, double *min_dist2_out,
                          int *pairs, int max_pairs) {
+  return or_collision_barrier_mode(p, np, fil_id, seg_id, Y, head, list, map, nt, F, min_dist2_out, pairs,
+                                   max_pairs, FS_BARRIER_ALL);
+}
+
+static int or_collision_barrier_mode(const fs_params *p, int np, const int *fil_id, const int *seg_id,
+                                     const double *Y, const int *head, const int *list, const int *map, int nt,
+                                     double *F, double *min_dist2_out, int *pairs, int max_pairs, int mode) {
   int M[3];
   or_cells_dims(p, M);
   int ncell = M[0] * M[1] * M[2];
@@ -560,7 +579,7 @@ int or_collision_barrier(const fs_params *p, int np, const int *fil_id, const in
         int j = (nabor < 0) ? list[i] : head[map[13 * icell + nabor]];
         while (j > -1) {
           int j_fil = fil_id[j], j_seg = seg_id[j];
-          if (!(j_fil == i_fil && abs(j_seg - i_seg) == 1) || nt < p->initial_friction_steps) {
+          if (or_pair_on(mode, np, nt, p->initial_friction_steps, i, i_fil, i_seg, j, j_fil, j_seg)) {
             if (or_pair(p, L, Y + 3 * i, Y + 3 * j, Fij, &min_dist2)) {
               fxi += Fij[0];
               fyi += Fij[1];
@@ -729,6 +748,7 @@ struct or_system {
   int nspring;
   int *spring_beads;
   double spring_k, spring_l0;
+  int barrier_mode;
 };
 
 static double *dalloc(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
@@ -1449,8 +1469,9 @@ void or_step(or_system *s, int nt) {
 
 static void or_barrier_and_mobility(or_system *s, int nt) {
   int np = s->np;
-  or_collision_barrier(&s->p, np, s->fil_id, s->seg_id, s->Y, s->head, s->list, s->map, nt, s->F,
-                       &s->min_dist2, NULL, 0);
+  if (s->barrier_mode != FS_BARRIER_OFF)
+    or_collision_barrier_mode(&s->p, np, s->fil_id, s->seg_id, s->Y, s->head, s->list, s->map, nt, s->F,
+                              &s->min_dist2, NULL, 0, s->barrier_mode);
   if (nt > s->p.initial_friction_steps)
     or_fcm_mobility(&s->p, np, s->Y, s->F, s->TAU, s->V, s->W, NULL, NULL);
   else
@@ -1458,8 +1479,38 @@ static void or_barrier_and_mobility(or_system *s, int nt) {
   s->nsolves++;
 }
 
-/* one time step: the body of main.cpp:284-754 */
-int or_step_implicit(or_system *s, int nt, int *iters_out) {
+void or_set_barrier_mode(or_system *s, int mode) { s->barrier_mode = mode; }
+
+/* one time step: the body of main.cpp:284-754; commit = 0 leaves out
+ * Filament::step (the gait-reset driver's trial solves) */
+static int or_step_solve(or_system *s, int nt, int *iters_out, int commit);
+
+int or_step_implicit(or_system *s, int nt, int *iters_out) { return or_step_solve(s, nt, iters_out, 1); }
+
+/* main_gaitreset.cpp:302-830: solves without the barrier, without
+ * swimmer-network pairs, then with the system's mode, committing the last */
+int or_step_gait_reset(or_system *s, int nt, int *iters, double *vwf) {
+  const int saved = s->barrier_mode;
+  const int modes[3] = {FS_BARRIER_OFF, FS_BARRIER_NOT_SWIMMER, saved};
+  const int nw0 = s->nfil > 0 ? s->fil_start[1] - s->fil_start[0] : 0;
+  int st = FS_OK;
+  for (int pass = 0; pass < 3; ++pass) {
+    s->barrier_mode = modes[pass];
+    int r = or_step_solve(s, nt, iters ? iters + pass : NULL, pass == 2);
+    if (r && !st) st = r;
+    if (vwf)
+      for (int b = 0; b < nw0; ++b)
+        for (int d = 0; d < 3; ++d) {
+          vwf[(pass * nw0 + b) * 9 + d] = s->V[3 * b + d];
+          vwf[(pass * nw0 + b) * 9 + 3 + d] = s->W[3 * b + d];
+          vwf[(pass * nw0 + b) * 9 + 6 + d] = s->F[3 * b + d];
+        }
+  }
+  s->barrier_mode = saved;
+  return st;
+}
+
+static int or_step_solve(or_system *s, int nt, int *iters_out, int commit) {
   size_t n6 = (size_t)6 * s->np;
   or_initial_guess(s);
   or_filament_forces(s, nt);
@@ -1490,7 +1541,7 @@ int or_step_implicit(or_system *s, int nt, int *iters_out) {
     memcpy(s->Err, s->NewErr, sizeof(double) * n6);
     ++iter;
   }
-  or_step(s, nt);
+  if (commit) or_step(s, nt);
   if (iters_out) *iters_out = iter;
   return check ? FS_ERR_NOT_CONVERGED : FS_OK;
 }

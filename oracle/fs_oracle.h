@@ -50,6 +50,10 @@ void or_initial_guess(or_system *sys);
 void or_set_swimming(or_system *sys, const double *swim, double curvature, int sperm_decay);
 void or_set_spring_links(or_system *sys, int nlinks, const int *beads, double k, double l0);
 void or_filament_forces(or_system *sys, int nt);
+/* barrier pair filter (FS_BARRIER_*) used by the implicit step */
+void or_set_barrier_mode(or_system *sys, int mode);
+/* one step of the gait-reset driver: iters[3], vwf: [3][Nw0][9] (V, W, F of filament 0) or NULL */
+int or_step_gait_reset(or_system *sys, int nt, int *iters, double *vwf);
 void or_build_jacobian(or_system *sys, int nt);
 void or_get_jinv(or_system *sys, int f, double *out);
 int or_error_check(or_system *sys, const double *V, const double *W, double *err, int nt);

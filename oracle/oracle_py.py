@@ -50,6 +50,9 @@ def lib():
         L.or_set_swimming.argtypes = [vp, vp, ctypes.c_double, ctypes.c_int]
         L.or_set_spring_links.argtypes = [vp, ctypes.c_int, vp, ctypes.c_double, ctypes.c_double]
         L.or_filament_forces.argtypes = [vp, ctypes.c_int]
+        L.or_set_barrier_mode.argtypes = [vp, ctypes.c_int]
+        L.or_step_gait_reset.restype = ctypes.c_int
+        L.or_step_gait_reset.argtypes = [vp, ctypes.c_int, vp, vp]
         L.or_build_jacobian.argtypes = [vp, ctypes.c_int]
         L.or_get_jinv.argtypes = [vp, ctypes.c_int, vp]
         L.or_error_check.argtypes = [vp, vp, vp, vp, ctypes.c_int]
@@ -216,6 +219,17 @@ class System:
 
     def filament_forces(self, nt):
         lib().or_filament_forces(self.h, nt)
+
+    def set_barrier_mode(self, mode):
+        lib().or_set_barrier_mode(self.h, int(mode))
+
+    def step_gait_reset(self, nt):
+        """Returns (iterations [3], V W F of filament 0 per solve [3, Nw0, 9], status)."""
+        nw0 = int(self.susp.fil_start[1] - self.susp.fil_start[0])
+        its = np.zeros(3, dtype=np.int32)
+        vwf = np.zeros((3, nw0, 9))
+        st = lib().or_step_gait_reset(self.h, nt, _ptr(its), _ptr(vwf))
+        return its, vwf, st
 
     def build_jacobian(self, nt):
         lib().or_build_jacobian(self.h, nt)

@@ -240,3 +240,49 @@ def test_spring_links_forces(oracle):
         want[a] += sf
         want[b] -= sf
     assert np.abs((F1 - F0) - want).max() < 1e-12 * max(1.0, np.abs(want).max())
+
+
+def _dense_case(seed):
+    """A crowded box: filaments placed 2.0a apart, inside the barrier's 2.2a range."""
+    p = sediment_params(32, tol=1e-10, broyden_maxiter=100)
+    s = random_suspension(p, 10, 8, seed=seed, min_sep=2.0)
+    return p, s
+
+
+def test_barrier_modes_on_the_oracle(oracle):
+    """The barrier variants differ only by their pair filter: without contacts
+    between filament 0 and the others the not-swimmer barrier gives the plain
+    trajectory bitwise; switching the barrier off changes a crowded run."""
+    from filsim_b200 import abi
+    p, s = _dense_case(91)
+    runs = {}
+    for mode in (abi.FS_BARRIER_ALL, abi.FS_BARRIER_NOT_SWIMMER, abi.FS_BARRIER_NOT_TEST_PARTICLES,
+                 abi.FS_BARRIER_OFF):
+        sysw = oracle.System(p, s)
+        sysw.set_barrier_mode(mode)
+        its, st = sysw.run_steps(1, 4)
+        runs[mode] = sysw.download()["X"]
+    assert not np.array_equal(runs[abi.FS_BARRIER_ALL], runs[abi.FS_BARRIER_OFF])
+    # a filament far from every other: the swimmer filter changes nothing
+    p2 = sediment_params(32, tol=1e-10, broyden_maxiter=100)
+    s2 = random_suspension(p2, 2, 8, seed=92)
+    a, b = oracle.System(p2, s2), oracle.System(p2, s2)
+    b.set_barrier_mode(abi.FS_BARRIER_NOT_SWIMMER)
+    a.run_steps(1, 3)
+    b.run_steps(1, 3)
+    assert np.array_equal(a.download()["X"], b.download()["X"])
+
+
+def test_gait_reset_step_on_the_oracle(oracle):
+    """main_gaitreset.cpp:302-830: the committed state advances once per step
+    (the trial solves leave X, U, q alone) and the last solve is a full barrier
+    solve from the trial solves' lambda."""
+    p, s = _dense_case(93)
+    g = oracle.System(p, s)
+    g.run_steps(1, 2)
+    before = g.download()
+    its, vwf, st = g.step_gait_reset(3)
+    after = g.download()
+    assert its.min() >= 1 and vwf.shape == (3, 8, 9)
+    assert np.array_equal(after["Xt"], before["X"])  # one Filament::step
+    assert not np.array_equal(vwf[0], vwf[2])        # the three solves differ
