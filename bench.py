@@ -292,9 +292,10 @@ def run_ours(args, rank, world):
         if learned:
             set_warm_start(ctx, mode)
             abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate if mode else 0), "fs_warm_start_gate")
-        # reference-start arms run each steady step as one CUDA graph (Broyden loop on
-        # the device); the learned start decides on the host and runs host-driven
-        graph = 0 if (args.no_graph or (learned and mode)) else 1
+        # steady steps with the reference's start run as one CUDA graph each (Broyden
+        # loop on the device), also those the cost gate gives the plain start; steps
+        # with the learned start run host-driven
+        graph = 0 if args.no_graph else 1
         abi.check(abi.lib().fs_set_graph_mode(ctx.h, graph), "fs_set_graph_mode")
         sim = Simulation(ctx, prep.copy())
         sim.run_steps(nt0, W)

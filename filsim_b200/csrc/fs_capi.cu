@@ -120,11 +120,12 @@ fs_status step_barrier_mobility(fs_ctx *c, int nt) { return barrier_and_mobility
 namespace {
 
 // one implicit step (main.cpp:334-707); commit = false leaves out Filament::step
-// (the gait-reset driver's trial solves)
-fs_status step_implicit(fs_ctx *c, int nt, int *iters_out, bool commit = true) {
+// (the gait-reset driver's trial solves); choice: the cost gate's start when the
+// caller has already asked it (0 plain, 1 learned), -1 to ask here
+fs_status step_implicit(fs_ctx *c, int nt, int *iters_out, bool commit = true, int choice = -1) {
   FS_TRY(fil_initial_guess(c));
   const bool learn_on = learn_active(c) && nt > c->p.initial_friction_steps;
-  const bool learned = learn_on && learn_gate_choose(c);
+  const bool learned = learn_on && (choice >= 0 ? choice == 1 : learn_gate_choose(c));
   const long long solves0 = c->diag.mobility_solves;
   if (learned || learn_recording(c)) FS_TRY(learn_save_guess(c));
   FS_TRY(fil_forces(c, nt));
@@ -748,11 +749,11 @@ fs_status fs_state_update(fs_ctx *c, const double *update) {
 
 fs_status fs_step(fs_ctx *c, int nt) { return c ? fil_step(c, nt) : FS_ERR_INVALID_ARG; }
 
-static fs_status run_one(fs_ctx *c, int nt, int *iters_h) {
+static fs_status run_one(fs_ctx *c, int nt, int *iters_h, int choice = -1) {
   FS_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(int) * FLAG_COUNT, c->stream));
   const int before = c->diag.not_converged_steps;
   int it = 0;
-  FS_TRY(step_implicit(c, nt, &it));
+  FS_TRY(step_implicit(c, nt, &it, true, choice));
   if (iters_h) *iters_h = it;
   if (c->diag.nonfinite) return FS_ERR_NONFINITE;
   return c->diag.not_converged_steps > before ? FS_ERR_NOT_CONVERGED : FS_OK;
@@ -760,6 +761,24 @@ static fs_status run_one(fs_ctx *c, int nt, int *iters_h) {
 
 static bool use_graph(const fs_ctx *c, int nt) {
   return c->graph_mode && graph_steady(c, nt) && !learn_active(c) && !learn_recording(c);
+}
+
+// the learned start under its cost gate: a step the gate gives the plain start
+// runs as the captured graph (flushed at once, so the gate sees its solves
+// before its next choice); a learned-start step runs host-driven
+static bool use_gated_graph(const fs_ctx *c, int nt) {
+  return c->graph_mode && graph_steady(c, nt) && learn_active(c) && learn_gate_on(c) && !learn_recording(c);
+}
+
+static fs_status run_one_gated(fs_ctx *c, int nt, int *iters_h) {
+  if (learn_gate_choose(c)) return run_one(c, nt, iters_h, 1);
+  FS_TRY(learn_end_step(c));  // the graph ends with Filament::step
+  FS_TRY(graph_launch_step(c, nt));
+  int it = 0;
+  fs_status s = graph_flush(c, &it);
+  if (iters_h) *iters_h = it;
+  if (s == FS_OK || s == FS_ERR_NOT_CONVERGED) learn_gate_record(c, false, (long long)it + 1);
+  return s;
 }
 
 fs_status fs_step_implicit(fs_ctx *c, int nt, int *iters_h) {
@@ -770,6 +789,7 @@ fs_status fs_step_implicit(fs_ctx *c, int nt, int *iters_h) {
     FS_TRY(graph_launch_step(c, nt));
     return graph_flush(c, iters_h);
   }
+  if (use_gated_graph(c, nt)) return run_one_gated(c, nt, iters_h);
   return run_one(c, nt, iters_h);
 }
 
@@ -802,7 +822,8 @@ fs_status fs_run_steps(fs_ctx *c, int nt_start, int nsteps, int *iters_h) {
       continue;
     }
     int it = 0;
-    fs_status s = run_one(c, nt_start + k, &it);
+    fs_status s = use_gated_graph(c, nt_start + k) ? run_one_gated(c, nt_start + k, &it)
+                                                    : run_one(c, nt_start + k, &it);
     if (iters_h) iters_h[k] = it;
     if (s != FS_OK && s != FS_ERR_NOT_CONVERGED) return s;
     if (s != FS_OK) worst = s;

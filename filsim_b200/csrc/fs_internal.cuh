@@ -208,6 +208,7 @@ void graph_free(fs_ctx *c);
 fs_status learn_prepare_capture(fs_ctx *c);
 bool learn_active(const fs_ctx *c);
 bool learn_gate_choose(fs_ctx *c);
+bool learn_gate_on(const fs_ctx *c);
 void learn_gate_record(fs_ctx *c, bool learned, long long solves);
 bool learn_recording(const fs_ctx *c);
 fs_status learn_save_guess(fs_ctx *c);

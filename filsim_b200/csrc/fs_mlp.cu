@@ -58,8 +58,9 @@ struct fs_mlp {
   bool override_next;              // the next warm start uses pred as given (fs_learn_override)
   long long learned_total, fallback_total;
   // cost gate of the learned start (fs_warm_start_gate): per start, the running
-  // mean of mobility solves per step; the cheaper start runs and the other one is
-  // probed after gate_interval steps. The interval starts at gate_period and
+  // mean of mobility solves per step; the cheaper start (the learned one only
+  // when it saves a solve per step) runs and the other one is probed after
+  // gate_interval steps. The interval starts at gate_period and
   // doubles (up to GATE_BACKOFF_MAX x gate_period) after each probe that leaves
   // the choice unchanged; a probe that changes it restores gate_period.
   int gate_period;                 // 0: off (the learned start runs every step)
@@ -582,8 +583,14 @@ bool learn_active(const fs_ctx *c) { return c->mlp && c->mlp->mode > 0; }
 
 // the start of this step under the cost gate (true: learned)
 constexpr int GATE_BACKOFF_MAX = 16;
+// the learned start is chosen only when its running mean is at least this many
+// mobility solves per step below the plain start's: a tie goes to the reference's
+// start, which also runs as a captured step graph
+constexpr double GATE_MARGIN = 1.0;
 
-int gate_best(const fs_mlp *m) { return m->gate_solves[1] < m->gate_solves[0] ? 1 : 0; }
+int gate_best(const fs_mlp *m) { return m->gate_solves[1] + GATE_MARGIN <= m->gate_solves[0] ? 1 : 0; }
+
+bool learn_gate_on(const fs_ctx *c) { return c->mlp && c->mlp->gate_period > 0; }
 
 bool learn_gate_choose(fs_ctx *c) {
   fs_mlp *m = c->mlp;
@@ -691,10 +698,13 @@ fs_status learn_warm_start(fs_ctx *c, int nt, fs_status (*solve)(fs_ctx *, int))
   return fil_error_check(c, c->V, c->W, c->err, nt);
 }
 
-// before a graph capture: the learn module's per-step work must not allocate
+// before a graph capture: the learn module's per-step work must not allocate.
+// A captured step is a plain-start step (with the learned start on, the cost
+// gate's plain steps); it holds no learned-start work, and recording steps,
+// which capture targets per step, are never captured.
 fs_status learn_prepare_capture(fs_ctx *c) {
   if (!c->mlp) return FS_OK;
-  if (c->mlp->mode || c->mlp->record) return FS_ERR_STATE;
+  if (c->mlp->record || c->mlp->jdiag_on) return FS_ERR_STATE;
   return ensure_step_buffers(c);
 }
 
@@ -717,6 +727,8 @@ fs_status learn_capture_targets(fs_ctx *c, int iters) {
 }
 
 // before Filament::step moves X -> Xt: keep Xt as the positions two steps back
+// before Filament::step of every step (also before a captured plain-start step,
+// whose graph ends with it): Xtt <- Xt, the positions two steps back afterwards
 fs_status learn_end_step(fs_ctx *c) {
   fs_mlp *m = c->mlp;
   if (!m) return FS_OK;

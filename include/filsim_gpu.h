@@ -316,8 +316,9 @@ fs_status fs_get_diag(fs_ctx *ctx, fs_diag *d_h);
  * and lambda_extrap_step) run as one CUDA graph each, with the Broyden loop on
  * the device (a conditional WHILE node) and one host synchronisation per
  * fs_run_steps call instead of one per iteration; results are bitwise those of
- * the host-driven step. Not used while the learned warm start is on or
- * recording. No reference counterpart. */
+ * the host-driven step. With the learned warm start on, only the steps its cost
+ * gate gives the plain start run as graphs (one synchronisation per step);
+ * learned-start and recording steps run host-driven. No reference counterpart. */
 fs_status fs_set_graph_mode(fs_ctx *ctx, int on);
 
 /* ---- autotuner (no reference counterpart) -----------------------------------
@@ -435,8 +436,9 @@ fs_status fs_learn_override(fs_ctx *ctx, const float *pred_d);
  * the plain start. */
 fs_status fs_set_warm_start(fs_ctx *ctx, int mode);
 /* Cost gate of the learned start (no reference counterpart): with period > 0,
- * each step runs the start (learned or plain) whose running mean of mobility
- * solves per step is lower, and probes the other one so that its mean stays
+ * each step runs the start whose running mean of mobility solves per step is
+ * lower (the learned one only when it is lower by at least one solve: a tie
+ * goes to the reference's start), and probes the other one so that its mean stays
  * current: after period steps, an interval that doubles (up to 16 x period)
  * while the probes leave the choice unchanged and returns to period when one
  * changes it; the learned start pays off only when it saves more
