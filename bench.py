@@ -29,8 +29,9 @@ learned_every_step the same steps with the learned start on every step.
 fp32_plain_start   the same steps from the reference's extrapolated start.
 plain_fp64 the same steps with the FCM chain in FP64 and the reference's start.
 e2e        the value arm through the C-ABI with HOST state: every step uploads
-           the suspension from pinned host memory (fs_state_upload), steps, and
-           downloads it (fs_state_download).
+           the suspension's state from pinned host memory (fs_state_upload), steps,
+           and downloads it (fs_state_download); the state is what the reference
+           checkpoints (X, Xt, q, qt, U, Ut, lam, lam1, lam2) plus K_B and C.
 --impl reference times the CPU restatement of the reference (the reference
            itself, MPI + FFTW 2.1.5 + Armadillo, cannot be built here).
 
@@ -64,6 +65,7 @@ PREP_STEPS = 12
 # warm-start training data: seeds TRAIN_SEED0.. of this workload, K_B log-uniform in [0.1, 10]
 TRAIN_SEED0 = 7000
 TRAIN_EPOCHS = 40
+CHECKPOINT_FIELDS = ("X", "Xt", "q", "qt", "U", "Ut", "lam", "lam1", "lam2", "kap", "c")
 GATE_PERIOD = 8  # the learned start's cost gate: first probe of the other start after 8 steps
 ENSEMBLE_SEED = 3000
 # DRAM bytes per launch from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum);
@@ -432,9 +434,12 @@ def run_ours(args, rank, world):
         if learned:
             set_warm_start(ctx, mode)
             abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate), "fs_warm_start_gate")
-        abi.check(abi.lib().fs_set_graph_mode(ctx.h, 0 if (args.no_graph or (learned and mode)) else 1),
-                  "fs_set_graph_mode")
+        abi.check(abi.lib().fs_set_graph_mode(ctx.h, 0 if args.no_graph else 1), "fs_set_graph_mode")
         host = prep.copy()
+        # the state a step needs, as the reference checkpoints it (.bak: X, Xt, q, qt, U, Ut,
+        # lam, lam1, lam2) plus K_B and C; Xs, Us, qs, F and TAU are recomputed by every step
+        # (initial guess, forces), so their upload and download are left out (NULL)
+        host.arrays = {k: v for k, v in host.arrays.items() if k in CHECKPOINT_FIELDS}
         pinned = {}
         for k, v in host.arrays.items():
             t = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)

@@ -41,3 +41,29 @@ def test_resume_from_checkpoint(gpu_lib, tmp_path):
     row = (tmp_path / "run.dat").read_text().split("\n")[1].split(" ")
     vals = np.array([float(x) for x in row[1:-1]]).reshape(s.np, 7)
     assert np.abs(vals[:, :3] - s10.Xs).max() < 1e-13
+
+
+def test_checkpoint_fields_are_the_whole_state(gpu_lib):
+    """Stepping from uploads of only the checkpointed fields (X, Xt, q, qt, U, Ut,
+    lam, lam1, lam2; Xs, Us, qs, F, TAU left NULL) gives the trajectory of full
+    uploads bitwise: every step recomputes the rest."""
+    p = sediment_params(32)
+    s = random_suspension(p, 6, 8, seed=83)
+    keep = ("X", "Xt", "q", "qt", "U", "Ut", "lam", "lam1", "lam2", "kap", "c")
+    out = []
+    for fields in (None, keep):
+        ctx = Context(p, max_beads=s.np, max_filaments=s.nfil)
+        sim = Simulation(ctx, s)
+        sim.run_steps(1, 14)
+        host = s.copy()
+        sim.download_into(host)
+        if fields:
+            host.arrays = {k: v for k, v in host.arrays.items() if k in fields}
+        for nt in range(15, 19):
+            sim.upload(host)
+            sim.step_implicit(nt)
+            sim.download_into(host)
+        out.append(host.arrays)
+        ctx.close()
+    for k in ("X", "Xt", "q", "qt", "U", "Ut", "lam", "lam1", "lam2"):
+        assert np.array_equal(out[0][k], out[1][k]), k
