@@ -33,7 +33,7 @@ def ctx(gpu_lib):
 
 
 @pytest.mark.parametrize("M,N,K", [(128, 128, 64), (128, 128, 128), (256, 384, 192), (512, 256, 512),
-                                   (1024, 512, 1024)])
+                                   (1024, 512, 1024), (4096, 4864, 256), (8192, 2560, 576)])
 def test_gemm_bf16_matches_fp64(ctx, M, N, K):
     g = torch.Generator(device="cuda")
     g.manual_seed(M + N + K)
