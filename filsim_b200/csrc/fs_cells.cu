@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(128) k_barrier(const double *__restrict__ Y, d
   if (b >= np) return;
   const int cb = cell_of[b];
   const int pb = rank_desc[b];
-  const int s0 = start[cb], e0 = start[cb + 1];
+  const int e0 = start[cb + 1];
   const int p_asc = e0 - 1 - pb;
   const double Yb[3] = {Y[3 * b], Y[3 * b + 1], Y[3 * b + 2]};
   unsigned long long keys[FS_MAX_EVENTS];

@@ -530,7 +530,7 @@ __global__ void __launch_bounds__(256) k_jacobian_schur(
   const int b0 = fil_start[f], nw = fil_start[f + 1] - b0, l0 = b0 - f;
   if (nw < 2) return;  // J0 is the identity
   const int m = 3 * nw, nl = nw - 1;
-  const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x, nthr = blockDim.x;
   const double PI = FS_PI, dt = k.dt, DL = k.dl, MU = k.mu;
   const double *q_f = qs + 4 * b0, *Us_f = Us + 3 * b0, *TAU_f = TAU + 3 * b0, *lam_f = lam + 3 * l0;
   double *aux = aux_all + aoff[f];
@@ -723,7 +723,7 @@ __global__ void __launch_bounds__(384, 2) k_schur_gj_reg(const int *__restrict__
   constexpr int CW = GJ_CW;
   __shared__ double fcol[GJ_MAX_M], rowkc[GJ_MAX_M + CW];
   __shared__ __align__(16) double prow_s[GJ_MAX_M + CW];
-  __shared__ double cand_v[3], cand_x[3], cand_inv[3];
+  __shared__ double cand_v[3], cand_inv[3];
   __shared__ int cand_r[3];
   __shared__ int perm[GJ_MAX_M], colsrc[GJ_MAX_M], dstcol[GJ_MAX_M];
   const int f = blockIdx.x;
@@ -761,7 +761,6 @@ __global__ void __launch_bounds__(384, 2) k_schur_gj_reg(const int *__restrict__
     if (lane == 0) {
       cand_v[rb] = best;
       cand_r[rb] = bi;
-      cand_x[rb] = x;
       cand_inv[rb] = best >= 0.0 ? 1.0 / x : 0.0;
     }
   };
