@@ -131,6 +131,13 @@ class SuspensionGpu {
   void setSpringLinks(int nlinks, const int *beads, double k, double l0) {
     check(fs_set_spring_links(ctx_.get(), nlinks, beads, k, l0), "setSpringLinks");
   }
+  // LinkedList::apply_collision_barrier / _not_swimmer / _not_test_particles, or none (FS_BARRIER_*)
+  void setBarrierMode(int mode) { check(fs_set_barrier_mode(ctx_.get(), mode), "setBarrierMode"); }
+  // one step of main_gaitreset.cpp: iters[3]; vwf (optional) [3][Nw0][9] V, W, F of filament 0
+  void stepGaitReset(int nt, int iters[3], double *vwf = nullptr) {
+    fs_status s = fs_step_gait_reset(ctx_.get(), nt, iters, vwf);
+    if (s != FS_OK && s != FS_ERR_NOT_CONVERGED) throw Error(s, "fs_step_gait_reset");
+  }
   // filamentJsolver::buildJacobian
   void buildJacobian(int nt) { check(fs_jacobian_build(ctx_.get(), nt), "filamentJsolver::buildJacobian"); }
   // filamentJsolver::solve
