@@ -265,7 +265,20 @@ __global__ void __launch_bounds__(128) k_barrier(const double *__restrict__ Y, d
   F[3 * b] = __dadd_rn(F[3 * b], ax);
   F[3 * b + 1] = __dadd_rn(F[3 * b + 1], ay);
   F[3 * b + 2] = __dadd_rn(F[3 * b + 2], az);
-  atomicMin(min_bits, fs_dbits(local_min));
+  // the minimum squared distance: one atomic per full warp after a shuffle
+  // reduction (per bead, all beads would contend for one address); the last,
+  // partial warp of the grid keeps per-thread atomics
+  unsigned long long mb = fs_dbits(local_min);
+  if (__activemask() == 0xffffffffu) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long other = __shfl_xor_sync(0xffffffffu, mb, o);
+      mb = other < mb ? other : mb;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMin(min_bits, mb);
+  } else {
+    atomicMin(min_bits, mb);
+  }
 }
 
 __global__ void k_pair_pos(const int *__restrict__ cell_of, const int *__restrict__ start,

@@ -205,23 +205,38 @@ __global__ void k_initial_guess(int np, const int *__restrict__ seg_id, const do
   qstore(q_expm(qload(q + 4 * b), us), qs + 4 * b);
 }
 
+// One warp per filament, beads in chunks of 32: the lanes form their beads'
+// tangents in parallel, then every lane runs the running sum of
+// Filament::unRobotArmify (Filament.hpp:489-505) over the chunk in bead order
+// (tangents broadcast by shuffles; the same additions in the same order as one
+// thread walking the filament) and keeps its own bead's position; the
+// fmod(X, L) of assign_filament_data runs per lane.
 __global__ void k_unrobot_assign(int nfil, const int *__restrict__ fil_start, const double *__restrict__ qs,
                                  double *__restrict__ Xs, double *__restrict__ Y, FilConsts k) {
-  int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= nfil) return;
-  int b0 = fil_start[f], b1 = fil_start[f + 1];
-  double Xsum[3] = {Xs[3 * b0], Xs[3 * b0 + 1], Xs[3 * b0 + 2]};
-  double t1[3], t2[3];
-  q_tangent(qload(qs + 4 * b0), t1);
+  const int f = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (f >= nfil) return;  // warp-uniform
+  const int b0 = fil_start[f], b1 = fil_start[f + 1];
   const double half = 0.5 * k.dl;
-  for (int d = 0; d < 3; ++d) Y[3 * b0 + d] = fmod(Xsum[d], k.L[d]);
-  for (int b = b0 + 1; b < b1; ++b) {
-    q_tangent(qload(qs + 4 * b), t2);
-    for (int d = 0; d < 3; ++d) {
-      Xsum[d] += (t1[d] + t2[d]) * half;
-      Xs[3 * b + d] = Xsum[d];
-      Y[3 * b + d] = fmod(Xsum[d], k.L[d]);
-      t1[d] = t2[d];
+  double Xsum[3] = {Xs[3 * b0], Xs[3 * b0 + 1], Xs[3 * b0 + 2]};
+  double t1[3] = {0.0, 0.0, 0.0};
+  for (int c0 = b0; c0 < b1; c0 += 32) {
+    const int b = c0 + lane, nb = min(32, b1 - c0);
+    double t[3] = {0.0, 0.0, 0.0}, mine[3] = {0.0, 0.0, 0.0};
+    if (b < b1) q_tangent(qload(qs + 4 * b), t);
+    for (int i = 0; i < nb; ++i) {  // warp-uniform trip count
+      double t2[3];
+      for (int d = 0; d < 3; ++d) t2[d] = __shfl_sync(0xffffffffu, t[d], i);
+      if (c0 + i > b0)
+        for (int d = 0; d < 3; ++d) Xsum[d] += (t1[d] + t2[d]) * half;
+      for (int d = 0; d < 3; ++d) t1[d] = t2[d];
+      if (lane == i)
+        for (int d = 0; d < 3; ++d) mine[d] = Xsum[d];
+    }
+    if (b < b1) {
+      for (int d = 0; d < 3; ++d) {
+        if (b > b0) Xs[3 * b + d] = mine[d];
+        Y[3 * b + d] = fmod(mine[d], k.L[d]);
+      }
     }
   }
 }
@@ -1218,7 +1233,7 @@ fs_status fil_forces(fs_ctx *c, int nt) {
   ProfScope ps(c, FS_STAGE_FORCES);
   FilConsts k = make_fconsts(c);
   k.tt = nt * c->p.dt;  // double tt = nt*dt (Filament.hpp:295)
-  k_unrobot_assign<<<fs_blocks(c->nfil, 128), 128, 0, c->stream>>>(c->nfil, c->fil_start, c->qs, c->Xs, c->Y, k);
+  k_unrobot_assign<<<fs_blocks(c->nfil, 4), 128, 0, c->stream>>>(c->nfil, c->fil_start, c->qs, c->Xs, c->Y, k);
   FS_LAUNCH_CHECK();
   k_forces<<<fs_blocks(c->np, 256), 256, 0, c->stream>>>(c->np, c->fil_id, c->seg_id, c->fil_start, c->qs, c->lam,
                                                           c->kap, c->cc, c->F, c->TAU, k);
