@@ -1065,20 +1065,35 @@ __global__ void k_error_check(int np, const int *__restrict__ fil_id, const int 
 __global__ void __launch_bounds__(RED_THREADS) k_dots(const double *__restrict__ D, const double *__restrict__ b,
                                                        size_t n6, int iter, const int *__restrict__ iter_d,
                                                        double *__restrict__ partial) {
-  __shared__ double sh[RED_THREADS / 32];
+  // columns in groups of DOT_COLS: a thread reads b[k] once per group and keeps
+  // the group's loads in flight together; each column's sum runs in the same
+  // order as one column at a time (k ascending per thread, then the shuffle
+  // tree, then the warps in order), so the partials are bitwise those
+  constexpr int DOT_COLS = 16;
+  __shared__ double sh[DOT_COLS][RED_THREADS / 32];
   const int ncol = iter_d ? *iter_d : iter;
-  for (int i = 0; i < ncol; ++i) {
-    const double *d = D + (size_t)i * n6;
-    double acc = 0.0;
-    for (size_t k = (size_t)blockIdx.x * RED_THREADS + threadIdx.x; k < n6; k += (size_t)gridDim.x * RED_THREADS)
-      acc += d[k] * b[k];
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  for (int i0 = 0; i0 < ncol; i0 += DOT_COLS) {
+    double acc[DOT_COLS];
+#pragma unroll
+    for (int j = 0; j < DOT_COLS; ++j) acc[j] = 0.0;
+    for (size_t k = (size_t)blockIdx.x * RED_THREADS + threadIdx.x; k < n6; k += (size_t)gridDim.x * RED_THREADS) {
+      const double bk = b[k];
+#pragma unroll
+      for (int j = 0; j < DOT_COLS; ++j)
+        if (i0 + j < ncol) acc[j] += D[(size_t)(i0 + j) * n6 + k] * bk;
+    }
+#pragma unroll
+    for (int j = 0; j < DOT_COLS; ++j) {
+      double a = acc[j];
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+      if ((threadIdx.x & 31) == 0) sh[j][threadIdx.x >> 5] = a;
+    }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < DOT_COLS && i0 + (int)threadIdx.x < ncol) {
+      const int j = threadIdx.x;
       double s = 0.0;
-      for (int w = 0; w < RED_THREADS / 32; ++w) s += sh[w];
-      partial[(size_t)i * gridDim.x + blockIdx.x] = s;
+      for (int w = 0; w < RED_THREADS / 32; ++w) s += sh[j][w];
+      partial[(size_t)(i0 + j) * gridDim.x + blockIdx.x] = s;
     }
     __syncthreads();
   }
