@@ -60,8 +60,6 @@ fs_status alloc_state(fs_ctx *c) {
   for (double **pp : b4) FS_CUDA(cudaMalloc(pp, sizeof(double) * 4 * nb));
   double **b6[] = {&c->err, &c->newerr, &c->upd, &c->tmp, &c->dE};
   for (double **pp : b6) FS_CUDA(cudaMalloc(pp, sizeof(double) * 6 * nb));
-  FS_CUDA(cudaMalloc(&c->schur_w, sizeof(double) * 3 * nb));
-  FS_CUDA(cudaMalloc(&c->schur_u, sizeof(double) * 3 * nb));
   FS_CUDA(cudaMalloc(&c->kap, sizeof(double) * nf));
   FS_CUDA(cudaMalloc(&c->cc, sizeof(double) * nf));
   FS_CUDA(cudaMalloc(&c->fil_start, sizeof(int) * (nf + 1)));
@@ -79,7 +77,7 @@ fs_status alloc_state(fs_ctx *c) {
   FS_CUDA(cudaMemset(c->flags, 0, sizeof(int) * FLAG_COUNT));
   FS_CUDA(cudaMalloc(&c->maxerr_bits, sizeof(unsigned long long)));
   FS_CUDA(cudaHostAlloc(&c->flags_h, sizeof(int) * FLAG_COUNT, cudaHostAllocDefault));
-  c->bytes += sizeof(double) * nb * (3 * 16 + 4 * 3 + 6 * 5) + sizeof(double) * 2 * hist +
+  c->bytes += sizeof(double) * nb * (3 * 14 + 4 * 3 + 6 * 5) + sizeof(double) * 2 * hist +
               sizeof(int) * nb * 8 + sizeof(double) * (size_t)c->p.broyden_maxiter * 297;
   return FS_OK;
 }
@@ -88,8 +86,7 @@ void free_state(fs_ctx *c) {
   void *ptrs[] = {c->X, c->Xs, c->Xt, c->U, c->Us, c->Ut, c->F, c->TAU, c->Y, c->V, c->W, c->lam, c->lam1,
                   c->lam2, c->q, c->qs, c->qt, c->err, c->newerr, c->upd, c->tmp, c->dE, c->kap, c->cc,
                   c->fil_start, c->fil_id, c->seg_id, c->soff, c->aoff, c->Cmat, c->Dmat, c->dots, c->partials,
-                  c->scalars, c->flags, c->maxerr_bits, c->Sinv, c->aux, c->schur_w, c->schur_u, c->swim,
-                  c->spring_beads,
+                  c->scalars, c->flags, c->maxerr_bits, c->Sinv, c->aux, c->swim, c->spring_beads,
                   c->spring_off, c->spring_ent};
   for (void *p : ptrs) cudaFree(p);
   if (c->flags_h) cudaFreeHost(c->flags_h);

@@ -11,9 +11,8 @@
 //                        to the 3Nw x 3Nw Schur complement of its constraint block (one CTA per
 //                        filament); k_schur_gj inverts it in shared memory
 //   k_error_check        ErrorCheckFCM + dexpinv (MobilityConstraints.cpp:109-143, 447-770)
-//   k_schur_pre/rows/post  filamentJsolver::solve (FilamentJacobianSolver.hpp:49-73): J0^-1 b from
-//                        the Schur inverse (link recurrences, the S^-1 product, link recurrences),
-//                        then the bad-Broyden history corrections
+//   k_schur_apply        filamentJsolver::solve (FilamentJacobianSolver.hpp:49-73): J0^-1 b from
+//                        the Schur inverse, then the bad-Broyden history corrections
 //   k_broyden_cols       history update of main.cpp:640-663
 //   k_update / k_step    Filament::update (Filament.hpp:425-452), Filament::step (:455-478)
 #include <algorithm>
@@ -521,7 +520,7 @@ __device__ void blockE_row(int k, int nw, const double *qs, const double *Us, co
 // Eliminating lambda = D'^-1 (b1 - C u) leaves S u = b2 - F' D'^-1 b1 with
 // S = E - F' D'^-1 C (3nw x 3nw). k_jacobian_schur builds S in shared memory and
 // stores it; k_schur_gj inverts it (Gauss-Jordan, partial pivoting) in a lean
-// kernel with more CTAs per SM; k_schur_pre/rows/post then apply J^-1 exactly, with the
+// kernel with more CTAs per SM; k_schur_apply then applies J^-1 exactly, with the
 // reference's 1/dt scaling of the lambda rows (:864).
 //
 // Per-filament auxiliary data (aux, nw >= 2): d[nw-1], e[nw-1] (D' blocks),
@@ -878,21 +877,15 @@ __global__ void __launch_bounds__(384, 2) k_schur_gj_reg(const int *__restrict__
 // aux_g: the filament's D', F', tangents and P coefficient in HBM; aux: shared
 // memory for their copy (the serial link recurrences then wait on shared, not
 // global, loads)
-// J0^-1 b of one filament in three parts (all threads of the CTA take part):
-// schur_pre: y = D'^-1 b1 and w = b2 - F' y (aux in shared memory, loaded);
-// schur_rows: u = S^-1 w, RU rows per warp; schur_post: z = b1 - C u,
-// lambda = D'^-1 z, X0 = b0 - P lambda, lambda / dt. k_schur_inverse runs them
-// in one CTA (schur_apply_one); the step's apply runs them as three kernels so
-// that the S^-1 stream runs at full occupancy, with the same arithmetic.
-__device__ void schur_load_aux(int nw, const double *__restrict__ aux_g, double *aux) {
-  const int nl = nw - 1;
-  for (int i = threadIdx.x; i < 20 * nl + 3 * nw + 1; i += blockDim.x) aux[i] = aux_g[i];
-}
-
-__device__ void schur_pre(int nw, const double *aux, const double *bb, double *y, double *w) {
+__device__ void schur_apply_one(int nw, const double *__restrict__ Sinv, const double *__restrict__ aux_g,
+                                double *aux, const double *bb, double *x, double *y, double *w, double dt,
+                                double fac) {
   const int m = 3 * nw, nl = nw - 1;
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  const double *dd = aux, *ee = aux + nl, *Fd = aux + 2 * nl, *Fl = Fd + 9 * nl;
+  const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarp = nthr >> 5;
+  for (int i = tid; i < 20 * nl + 3 * nw + 1; i += nthr) aux[i] = aux_g[i];
+  __syncthreads();
+  const double *dd = aux, *ee = aux + nl, *Fd = aux + 2 * nl, *Fl = Fd + 9 * nl, *tt = Fl + 9 * nl;
+  const double pcoef = tt[3 * nw];
   const double *b1 = bb + 3, *b2 = bb + m;
   // y = D'^-1 b1
   if (tid < 3) {
@@ -913,13 +906,11 @@ __device__ void schur_pre(int nw, const double *aux, const double *bb, double *y
            Fl[9 * (kb - 1) + 3 * i2 + 2] * y[3 * (kb - 1) + 2];
     w[row] = b2[row] - g;
   }
-}
-
-// u = S^-1 w: each warp takes eight rows at a time (coalesced row reads, all of
-// their loads in flight together); per row the lane-strided sum and the shuffle
-// tree of a one-row-per-warp product
-__device__ void schur_rows(int m, const double *__restrict__ Sinv, const double *w, double *u) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  __syncthreads();
+  // u = S^-1 w: each warp takes eight rows at a time (coalesced row reads, all
+  // of their loads in flight together); per row the lane-strided sum and the
+  // shuffle tree of a one-row-per-warp product
+  double *u = x + 3;
   constexpr int RU = 8;
   for (int row0 = warp * RU; row0 < m; row0 += nwarp * RU) {
     double acc[RU];
@@ -941,17 +932,7 @@ __device__ void schur_rows(int m, const double *__restrict__ Sinv, const double 
       for (int q = 0; q < RU; ++q)
         if (row0 + q < m) u[row0 + q] = acc[q];
   }
-}
-
-// x + 3 holds u on entry
-__device__ void schur_post(int nw, const double *aux, const double *bb, double *x, double *y, double dt,
-                           double fac) {
-  const int m = 3 * nw, nl = nw - 1;
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  const double *dd = aux, *ee = aux + nl, *tt = aux + 20 * nl;
-  const double pcoef = tt[3 * nw];
-  const double *b1 = bb + 3;
-  const double *u = x + 3;
+  __syncthreads();
   // z = b1 - C u, (C u)_r = fac c_0 + 2 fac sum_{1<=q<=r} c_q + fac c_{r+1}, c_q = cross(u_q, t_q)
   // (y is reused for z, then for lambda)
   if (tid < 3) {
@@ -982,70 +963,28 @@ __device__ void schur_post(int nw, const double *aux, const double *bb, double *
   __syncthreads();
 }
 
-__device__ void schur_apply_one(int nw, const double *__restrict__ Sinv, const double *__restrict__ aux_g,
-                                double *aux, const double *bb, double *x, double *y, double *w, double dt,
-                                double fac) {
-  schur_load_aux(nw, aux_g, aux);
-  __syncthreads();
-  schur_pre(nw, aux, bb, y, w);
-  __syncthreads();
-  schur_rows(3 * nw, Sinv, w, x + 3);
-  __syncthreads();
-  schur_post(nw, aux, bb, x, y, dt, fac);
-}
-
-// The step's J0^-1 b (filamentJsolver::solve, FilamentJacobianSolver.hpp:49-73),
-// part 1: w per filament into wbuf (3 Np)
-__global__ void __launch_bounds__(128) k_schur_pre(const int *__restrict__ fil_start,
-                                                   const long long *__restrict__ aoff,
-                                                   const double *__restrict__ aux_all, const double *__restrict__ b,
-                                                   double *__restrict__ wbuf) {
-  __shared__ double bb[6 * FS_MAX_NW], y[3 * FS_MAX_NW], w[3 * FS_MAX_NW];
-  __shared__ double auxs[20 * (FS_MAX_NW - 1) + 3 * FS_MAX_NW + 1];
-  const int f = blockIdx.x;
-  const int b0 = fil_start[f], nw = fil_start[f + 1] - b0, n = 6 * nw;
-  if (nw < 2) return;  // block-uniform
-  for (int r = threadIdx.x; r < n; r += blockDim.x) bb[r] = b[6 * b0 + r];
-  schur_load_aux(nw, aux_all + aoff[f], auxs);
-  __syncthreads();
-  schur_pre(nw, auxs, bb, y, w);
-  __syncthreads();
-  for (int r = threadIdx.x; r < 3 * nw; r += blockDim.x) wbuf[3 * b0 + r] = w[r];
-}
-
-// part 2: u = S^-1 w per filament into ubuf (one warp per eight rows)
-__global__ void k_schur_rows(const int *__restrict__ fil_start, const long long *__restrict__ soff,
-                             const double *__restrict__ Sinv_all, const double *__restrict__ wbuf,
-                             double *__restrict__ ubuf) {
-  const int f = blockIdx.x;
-  const int b0 = fil_start[f], nw = fil_start[f + 1] - b0;
-  if (nw < 2) return;  // block-uniform
-  schur_rows(3 * nw, Sinv_all + soff[f], wbuf + 3 * b0, ubuf + 3 * b0);
-}
-
-// part 3: the rest of J0^-1 b, then x += sum_i C_i dots_i
-__global__ void __launch_bounds__(128) k_schur_post(const int *__restrict__ fil_start,
-                                                    const long long *__restrict__ aoff,
-                                                    const double *__restrict__ aux_all, const double *__restrict__ b,
-                                                    const double *__restrict__ ubuf, double *__restrict__ x,
-                                                    const double *__restrict__ C, const double *__restrict__ dots,
-                                                    int iter, const int *__restrict__ iter_d, size_t n6, double dt,
-                                                    double fac) {
-  __shared__ double bb[6 * FS_MAX_NW], xs[6 * FS_MAX_NW], y[3 * FS_MAX_NW];
+// x_f = J0_f^-1 b_f, then x += sum_i C_i dots_i (FilamentJacobianSolver.hpp:49-73)
+__global__ void __launch_bounds__(128) k_schur_apply(const int *__restrict__ fil_start,
+                                                     const long long *__restrict__ soff,
+                                                     const long long *__restrict__ aoff,
+                                                     const double *__restrict__ Sinv_all,
+                                                     const double *__restrict__ aux_all, const double *__restrict__ b,
+                                                     double *__restrict__ x, const double *__restrict__ C,
+                                                     const double *__restrict__ dots, int iter,
+                                                     const int *__restrict__ iter_d, size_t n6, double dt,
+                                                     double fac) {
+  __shared__ double bb[6 * FS_MAX_NW], xs[6 * FS_MAX_NW], y[3 * FS_MAX_NW], w[3 * FS_MAX_NW];
   __shared__ double auxs[20 * (FS_MAX_NW - 1) + 3 * FS_MAX_NW + 1];
   const int f = blockIdx.x;
   const int b0 = fil_start[f], nw = fil_start[f + 1] - b0, s0 = 6 * b0, n = 6 * nw;
   const int tid = threadIdx.x, nthr = blockDim.x;
   for (int r = tid; r < n; r += nthr) bb[r] = b[s0 + r];
+  __syncthreads();
   if (nw < 2) {
-    __syncthreads();
     for (int r = tid; r < n; r += nthr) xs[r] = bb[r];
     __syncthreads();
   } else {
-    schur_load_aux(nw, aux_all + aoff[f], auxs);
-    for (int r = tid; r < 3 * nw; r += nthr) xs[3 + r] = ubuf[3 * b0 + r];
-    __syncthreads();
-    schur_post(nw, auxs, bb, xs, y, dt, fac);
+    schur_apply_one(nw, Sinv_all + soff[f], aux_all + aoff[f], auxs, bb, xs, y, w, dt, fac);
   }
   const int ncol = iter_d ? *iter_d : iter;
   for (int r = tid; r < n; r += nthr) {
@@ -1395,14 +1334,8 @@ fs_status fil_broyden_apply(fs_ctx *c, const double *b, double *x, int iter, con
     k_reduce_rows<<<fs_blocks(rows, 8), 256, 0, c->stream>>>(c->partials, RED_BLOCKS, rows, c->dots, 0, iter_d);
     FS_LAUNCH_CHECK();
   }
-  // three kernels: the serial link recurrences around a full-occupancy S^-1 stream
-  k_schur_pre<<<c->nfil, 128, 0, c->stream>>>(c->fil_start, c->aoff, c->aux, b, c->schur_w);
-  FS_LAUNCH_CHECK();
-  const int rows_threads = 32 * ((3 * c->max_nw + 7) / 8);  // one warp per eight rows
-  k_schur_rows<<<c->nfil, rows_threads, 0, c->stream>>>(c->fil_start, c->soff, c->Sinv, c->schur_w, c->schur_u);
-  FS_LAUNCH_CHECK();
-  k_schur_post<<<c->nfil, 128, 0, c->stream>>>(c->fil_start, c->aoff, c->aux, b, c->schur_u, x, c->Cmat, c->dots,
-                                                iter, iter_d, n6, c->p.dt, 0.5 * c->p.dl);
+  k_schur_apply<<<c->nfil, 128, 0, c->stream>>>(c->fil_start, c->soff, c->aoff, c->Sinv, c->aux, b, x, c->Cmat,
+                                                 c->dots, iter, iter_d, n6, c->p.dt, 0.5 * c->p.dl);
   FS_LAUNCH_CHECK();
   return learn_diag_apply(c, b, x);  // learned initial inverse-Jacobian diagonal, when on
 }

@@ -88,7 +88,6 @@ struct fs_ctx {
   double *Cmat, *Dmat;   // broyden_maxiter x 6Np
   double *Sinv;          // per-filament inverse Schur complement (3Nw x 3Nw row-major) at soff[f]
   double *aux;           // per-filament D', F' blocks, tangents, P coefficient at aoff[f]
-  double *schur_w, *schur_u;  // J0^-1 b scratch between its kernels (3 Np each)
   long long *soff, *aoff;
   int max_nw, min_nw;  // longest and shortest filament
   // swimming drive (fs_set_swimming): per filament (alpha, beta, phase, wavenumber,
