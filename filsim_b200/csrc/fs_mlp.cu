@@ -587,8 +587,12 @@ constexpr int GATE_BACKOFF_MAX = 16;
 // mobility solves per step below the plain start's: a tie goes to the reference's
 // start, which also runs as a captured step graph
 constexpr double GATE_MARGIN = 1.0;
+// and only once its mean rests on at least this many steps (one early step says little)
+constexpr long long GATE_MIN_STEPS = 2;
 
-int gate_best(const fs_mlp *m) { return m->gate_solves[1] + GATE_MARGIN <= m->gate_solves[0] ? 1 : 0; }
+int gate_best(const fs_mlp *m) {
+  return m->gate_steps[1] >= GATE_MIN_STEPS && m->gate_solves[1] + GATE_MARGIN <= m->gate_solves[0] ? 1 : 0;
+}
 
 bool learn_gate_on(const fs_ctx *c) { return c->mlp && c->mlp->gate_period > 0; }
 

@@ -437,8 +437,9 @@ fs_status fs_learn_override(fs_ctx *ctx, const float *pred_d);
 fs_status fs_set_warm_start(fs_ctx *ctx, int mode);
 /* Cost gate of the learned start (no reference counterpart): with period > 0,
  * each step runs the start whose running mean of mobility solves per step is
- * lower (the learned one only when it is lower by at least one solve: a tie
- * goes to the reference's start), and probes the other one so that its mean stays
+ * lower (the learned one only when it is lower by at least one solve over at
+ * least two of its steps: a tie goes to the reference's start), and probes the
+ * other one so that its mean stays
  * current: after period steps, an interval that doubles (up to 16 x period)
  * while the probes leave the choice unchanged and returns to period when one
  * changes it; the learned start pays off only when it saves more

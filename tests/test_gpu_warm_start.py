@@ -193,8 +193,9 @@ def test_cost_gate(gpu_lib):
     assert steps.sum() == 12
     assert steps.min() >= 2                       # both starts measured and re-probed
     major = int(np.argmax(steps))
-    # the start run most is the cheaper one, up to the gate's one-solve margin for the learned start
-    assert solves[major] <= solves[1 - major] + (1.0 if major == 0 else 0.0) + 1e-9
+    # the learned start runs most only when it saves at least one solve per step
+    if major == 1:
+        assert solves[1] + 1.0 <= solves[0] + 1e-9
     # gate off: the learned start on every step
     sim.upload(s0)
     ctx.call("fs_warm_start_gate", 0)
