@@ -25,7 +25,13 @@ STATUS_NAMES = {
     10: "FS_ERR_IO",
 }
 FS_ERR_INVALID_ARG = 1
+FS_ERR_NO_DEVICE = 2
+FS_ERR_CUDA = 3
+FS_ERR_CUFFT = 4
+FS_ERR_OOM = 5
 FS_ERR_NOT_CONVERGED = 6
+FS_ERR_NONFINITE = 7
+FS_ERR_CAPACITY = 8
 FS_ERR_STATE = 9
 FS_ERR_IO = 10
 FS_BARRIER_ALL, FS_BARRIER_NOT_SWIMMER, FS_BARRIER_NOT_TEST_PARTICLES, FS_BARRIER_OFF = 0, 1, 2, 3

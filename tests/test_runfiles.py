@@ -146,3 +146,19 @@ def test_resume_from_checkpoint_on_the_oracle(oracle, tmp_path):
     a, b = resumed.download(), full.download()
     assert np.abs(a["X"] - b["X"]).max() < 1e-9
     assert np.abs(a["q"] - b["q"]).max() < 1e-9
+
+
+def test_layout_capacity_is_reported(tmp_path):
+    """A .par holding more filaments than the caller's capacity: FS_ERR_CAPACITY,
+    and read_layout retries with a larger array."""
+    import ctypes
+    from filsim_b200 import abi
+    s = filled_suspension([0, 2, 4, 6, 8, 10], 6)
+    path = tmp_path / "run.par"
+    runfiles.write_parameters(path, s, runfiles.run_info())
+    nfil, np_ = ctypes.c_int(), ctypes.c_int()
+    fs = np.zeros(3, dtype=np.int32)
+    st = abi.lib().fs_par_read_layout(str(path).encode(), ctypes.byref(nfil), ctypes.byref(np_),
+                                      fs.ctypes.data_as(ctypes.c_void_p), 2)
+    assert st == abi.FS_ERR_CAPACITY
+    assert np.array_equal(runfiles.read_layout(path), [0, 2, 4, 6, 8, 10])
