@@ -15,7 +15,7 @@ import ctypes
 
 import numpy as np
 
-from .abi import FsRunInfo, check, lib
+from .abi import FS_ERR_CAPACITY, FsRunInfo, check, lib
 from .suspension import Suspension
 
 RUN_INFO_DEFAULTS = dict(a=1.0, ah=1.0, dl=2.2, sp4=0.0, kap=1.0, c=1.0, mu=1.0, curvature=0.0, k0=0.0,
@@ -62,7 +62,7 @@ def read_layout(path, max_fil=1 << 24):
                                       fs.ctypes.data_as(ctypes.c_void_p), cap)
         if st == 0:
             return fs[: nfil.value + 1].copy()
-        if st != 8 or cap == max_fil:  # FS_ERR_CAPACITY: retry with the full capacity
+        if st != FS_ERR_CAPACITY or cap == max_fil:  # too many filaments: retry with the full capacity
             check(st, "fs_par_read_layout")
     raise AssertionError("unreachable")
 
