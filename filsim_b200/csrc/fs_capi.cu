@@ -437,6 +437,7 @@ fs_status fs_collision_pairs(fs_ctx *c, const double *Y, int np, int nt, const i
 
 static fs_status upload_layout(fs_ctx *c, const fs_host_state *s);
 static void spring_free(fs_ctx *c);
+static void swim_free(fs_ctx *c);
 
 // state arrays always; the filament layout (ids, offsets, Schur buffers) only
 // when it differs from the previous upload's
@@ -453,8 +454,7 @@ fs_status fs_state_upload(fs_ctx *c, const fs_host_state *s) {
     graph_invalidate(c);
     FS_CUDA(cudaStreamSynchronize(st));
     // a swimming drive and spring links refer to the previous layout's filaments and beads
-    cudaFree(c->swim);
-    c->swim = nullptr;
+    swim_free(c);
     spring_free(c);
     FS_TRY(upload_layout(c, s));
   }
@@ -588,8 +588,7 @@ fs_status fs_set_swimming(fs_ctx *c, const double *swim_h, double curvature, int
   graph_invalidate(c);
   FS_CUDA(cudaStreamSynchronize(c->stream));  // no queued step still reads the old parameters
   if (!swim_h) {
-    cudaFree(c->swim);
-    c->swim = nullptr;
+    swim_free(c);
     return FS_OK;
   }
   const size_t n = 5 * (size_t)c->nfil;
@@ -598,7 +597,8 @@ fs_status fs_set_swimming(fs_ctx *c, const double *swim_h, double curvature, int
   if (!std::isfinite(curvature)) return FS_ERR_INVALID_ARG;
   if (!c->swim) {
     FS_CUDA(cudaMalloc(&c->swim, sizeof(double) * (n > 0 ? n : 1)));
-    c->bytes += sizeof(double) * n;
+    c->swim_bytes = sizeof(double) * n;
+    c->bytes += c->swim_bytes;
   }
   FS_CUDA(cudaMemcpyAsync(c->swim, swim_h, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
   FS_CUDA(cudaStreamSynchronize(c->stream));
@@ -652,12 +652,21 @@ fs_status fs_step_gait_reset(fs_ctx *c, int nt, int *iters_h, double *vwf_h) {
   return c->diag.not_converged_steps ? FS_ERR_NOT_CONVERGED : FS_OK;
 }
 
+static void swim_free(fs_ctx *c) {
+  cudaFree(c->swim);
+  c->swim = nullptr;
+  c->bytes -= c->swim_bytes;
+  c->swim_bytes = 0;
+}
+
 static void spring_free(fs_ctx *c) {
   cudaFree(c->spring_beads);
   cudaFree(c->spring_off);
   cudaFree(c->spring_ent);
   c->spring_beads = c->spring_off = c->spring_ent = nullptr;
   c->nspring = 0;
+  c->bytes -= c->spring_bytes;
+  c->spring_bytes = 0;
 }
 
 fs_status fs_set_spring_links(fs_ctx *c, int nlinks, const int *beads_h, double k, double l0) {
@@ -697,6 +706,8 @@ fs_status fs_set_spring_links(fs_ctx *c, int nlinks, const int *beads_h, double 
   c->nspring = nlinks;
   c->spring_k = k;
   c->spring_l0 = l0;
+  c->spring_bytes = sizeof(int) * (4 * (size_t)nlinks + (size_t)(c->np + 1));
+  c->bytes += c->spring_bytes;
   return FS_OK;
 }
 

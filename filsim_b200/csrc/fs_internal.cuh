@@ -99,6 +99,7 @@ struct fs_ctx {
   int nspring;
   int *spring_beads, *spring_off, *spring_ent;
   double spring_k, spring_l0;
+  size_t spring_bytes, swim_bytes;  // device bytes of the spring-link arrays and the drive
   int barrier_mode;      // pair filter of the step's barrier (fs_set_barrier_mode)
   double *dots;          // broyden_maxiter partial dots
   double *partials;      // reduction scratch

@@ -123,7 +123,7 @@ fs_status fs_par_write(const char *path, const fs_run_info *info, const fs_host_
   for (int i = 0; i < s->nfil; ++i) fprintf(f, i + 1 < s->nfil ? "%d " : "%d", s->fil_start[i + 1] - s->fil_start[i]);
   fprintf(f, "\n\nBendingModuli are KAP*\n");
   for (int i = 0; i < s->nfil; ++i) {
-    const double factor = s->kap ? s->kap[i] / info->kap : 1.0;
+    const double factor = s->kap ? (info->kap != 0.0 ? s->kap[i] / info->kap : s->kap[i]) : 1.0;
     fprintf(f, i + 1 < s->nfil ? "%g " : "%g", factor);
   }
   fprintf(f, "\n");

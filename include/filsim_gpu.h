@@ -253,8 +253,9 @@ fs_status fs_filament_forces(fs_ctx *ctx, int nt);
  * uses the last link's values as the reference's buildJacobian does. As in the
  * reference, components 1 and 2 of fs_params.strain_twist are replaced on
  * every link (zero without a drive); component 0 stays constant. Steps with a
- * drive run host-driven (a captured step graph would bake nt in). An upload
- * with another filament layout drops the drive. */
+ * drive run host-driven (a captured step graph would bake nt in), so an
+ * ensemble batch, whose steps are captured, refuses a box with a drive
+ * (FS_ERR_STATE). An upload with another filament layout drops the drive. */
 fs_status fs_set_swimming(fs_ctx *ctx, const double *swim_h, double curvature, int sperm_decay);
 /* Spring links between beads (spring_links::apply_spring_link_forces,
  * spring_link_functions.cpp:24-45, applied after the filaments' own forces as
@@ -490,7 +491,8 @@ typedef struct fs_run_info {
 } fs_run_info;
 
 /* .par (file_functions.cpp:6-80): the column names, the values, BeadNumbers
- * from s->fil_start and the bending factors s->kap[f] / info->kap. */
+ * from s->fil_start and the bending factors s->kap[f] / info->kap (s->kap[f]
+ * itself when info->kap is 0). */
 fs_status fs_par_write(const char *path, const fs_run_info *info, const fs_host_state *s);
 /* The layout continue_from_checkpoint reads from a .par (file_functions.cpp:236-272):
  * the third item of the second line is the filament count, the fifth line holds
