@@ -19,9 +19,11 @@ value      mixed precision (FP32 spread/FFT/interpolation, FP64 Broyden and
            before the run by the library's own kernels on 20 seeded plain-solver
            runs of this workload, K_B log-uniform in [0.1, 10]) under its cost
            gate (fs_warm_start_gate, period 8: each step takes the start with the
-           lower running mean of mobility solves per step and probes the other one
-           after 8 steps, an interval that doubles up to 128 while the probes lose;
-           learned.gate reports how many timed steps took each);
+           lower running mean of mobility solves per step, the learned one only
+           when it saves a solve per step over at least two of its steps, and
+           probes the other one after 8 steps, an interval that doubles up to 128
+           while the probes lose; steps with the reference's start run as captured
+           step graphs; learned.gate reports how many timed steps took each);
            inputs resident in HBM, device-timed with CUDA events on the
            context's stream, max over ranks; weak scaling (one independent
            replica per GPU).
