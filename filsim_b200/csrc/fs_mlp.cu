@@ -333,7 +333,7 @@ fs_status dalloc(T **p, size_t n, size_t *bytes) {
 
 // TMA descriptor of a row-major BF16 matrix [rows x cols] (leading dimension ld
 // elements) read in 64-column x 128-row boxes with the 128-byte swizzle; the
-// encoder comes from the driver through the runtime (no link against libcuda).
+// encoder comes from the CUDA driver API through the runtime (no link against libcuda).
 // A descriptor is a function of (address, rows, cols, ld) only, so encoded ones
 // are kept in a small process-wide cache (the MLP's GEMMs reuse the same
 // operands every call; encoding costs tens of microseconds on the host).

@@ -1,8 +1,8 @@
 /*
  * fs_oracle.c -- CPU FP64 restatement of FilSim's FCM mobility solve, collision
  * barrier and implicit BDF2/Broyden step. TEST INFRASTRUCTURE ONLY: the tests,
- * __graft_entry__.smoke() and bench.py's CPU baseline load it as the checker;
- * nothing in the product links or calls it.
+ * __graft_entry__.smoke() and bench.py's CPU baseline load it to compare results
+ * with; nothing in the product links or calls it.
  *
  * Parity unpinned: the reference cannot be built here (it needs MPI, FFTW 2.1.5
  * and Armadillo) and ships no golden vectors. Each function below follows the

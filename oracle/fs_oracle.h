@@ -1,6 +1,6 @@
 /*
- * fs_oracle.h -- CPU FP64 restatement of FilSim's hot path, used ONLY as the
- * checker by the tests, by __graft_entry__.smoke() and by bench.py's CPU
+ * fs_oracle.h -- CPU FP64 restatement of FilSim's hot path, used ONLY to check
+ * results, by the tests, by __graft_entry__.smoke() and by bench.py's CPU
  * baseline. It is not part of the product and the product never calls it.
  *
  * Parity status: the reference (MPI + FFTW 2.1.5 + Armadillo) cannot be built

@@ -1,7 +1,7 @@
 """ctypes bindings of the CPU oracle (oracle/fs_oracle.c).
 
 Test infrastructure only: imported by tests/, __graft_entry__.smoke() and the
-CPU-baseline leg of bench.py, always as the checker.
+CPU-baseline leg of bench.py, always as the reference the results are compared with.
 """
 import ctypes
 import os
