@@ -13,6 +13,7 @@
 // The readers tokenise on whitespace, which accepts everything the
 // reference's getline(..., ' ') readers accept from these writers.
 #include <errno.h>
+#include <locale.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -22,6 +23,20 @@
 #include "filsim_gpu.h"
 
 namespace {
+
+// The files use the "C" number format whatever the caller's locale: each call
+// switches its own thread to the C numeric locale (uselocale, thread-local) and
+// restores the previous one on return, as C++ streams with the classic locale do.
+struct CNumericLocale {
+  locale_t prev = (locale_t)0;
+  CNumericLocale() {
+    static locale_t c_loc = newlocale(LC_NUMERIC_MASK, "C", (locale_t)0);
+    if (c_loc) prev = uselocale(c_loc);
+  }
+  ~CNumericLocale() {
+    if (prev) uselocale(prev);
+  }
+};
 
 struct File {
   FILE *f = nullptr;
@@ -94,6 +109,7 @@ bool to_int(const std::pair<const char *, const char *> &tok, int *v) {
 extern "C" {
 
 fs_status fs_par_write(const char *path, const fs_run_info *info, const fs_host_state *s) {
+  CNumericLocale c_numbers;
   if (!path || !info || !layout_ok(s)) return FS_ERR_INVALID_ARG;
   File out(path, "w");
   if (!out.f) return FS_ERR_IO;
@@ -131,6 +147,7 @@ fs_status fs_par_write(const char *path, const fs_run_info *info, const fs_host_
 }
 
 fs_status fs_par_read_layout(const char *path, int *nfil_out, int *np_out, int *fil_start_h, int max_fil) {
+  CNumericLocale c_numbers;
   if (!path || !nfil_out || !np_out || !fil_start_h || max_fil < 0) return FS_ERR_INVALID_ARG;
   std::string text;
   if (!read_all(path, &text)) return FS_ERR_IO;
@@ -159,6 +176,7 @@ fs_status fs_par_read_layout(const char *path, int *nfil_out, int *np_out, int *
 }
 
 fs_status fs_backup_write(const char *path, const fs_host_state *s, int nt) {
+  CNumericLocale c_numbers;
   if (!path || !layout_ok(s) || !s->X || !s->Xt || !s->q || !s->qt || !s->U || !s->Ut)
     return FS_ERR_INVALID_ARG;
   if (s->np > s->nfil && (!s->lam || !s->lam1 || !s->lam2)) return FS_ERR_INVALID_ARG;
@@ -188,6 +206,7 @@ fs_status fs_backup_write(const char *path, const fs_host_state *s, int nt) {
 }
 
 fs_status fs_backup_read(const char *path, fs_host_state *s, int *nt_next) {
+  CNumericLocale c_numbers;
   if (!path || !nt_next || !layout_ok(s) || !s->X || !s->Xt || !s->q || !s->qt || !s->U || !s->Ut)
     return FS_ERR_INVALID_ARG;
   const int nlink = s->np - s->nfil;
@@ -224,6 +243,7 @@ fs_status fs_backup_read(const char *path, fs_host_state *s, int *nt_next) {
 }
 
 fs_status fs_data_write_header(const char *path, const fs_host_state *s) {
+  CNumericLocale c_numbers;
   if (!path || !layout_ok(s)) return FS_ERR_INVALID_ARG;
   File out(path, "w");
   if (!out.f) return FS_ERR_IO;
@@ -234,6 +254,7 @@ fs_status fs_data_write_header(const char *path, const fs_host_state *s) {
 }
 
 fs_status fs_data_append(const char *path, const fs_host_state *s, int nt) {
+  CNumericLocale c_numbers;
   if (!path || !layout_ok(s) || !s->Xs || !s->qs) return FS_ERR_INVALID_ARG;
   File out(path, "a");
   if (!out.f) return FS_ERR_IO;

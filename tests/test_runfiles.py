@@ -162,3 +162,29 @@ def test_layout_capacity_is_reported(tmp_path):
                                       fs.ctypes.data_as(ctypes.c_void_p), 2)
     assert st == abi.FS_ERR_CAPACITY
     assert np.array_equal(runfiles.read_layout(path), [0, 2, 4, 6, 8, 10])
+
+
+def test_files_ignore_the_callers_numeric_locale(tmp_path):
+    """A caller under a comma-decimal locale still gets the reference's '.'
+    number format (C++ streams with the classic locale)."""
+    import locale
+    s = filled_suspension([0, 3], 7)
+    ref = tmp_path / "c.bak"
+    runfiles.save_backup(ref, s, 4)
+    old = locale.setlocale(locale.LC_NUMERIC)
+    for name in ("de_DE.UTF-8", "fr_FR.UTF-8", "de_DE.utf8"):
+        try:
+            locale.setlocale(locale.LC_NUMERIC, name)
+            break
+        except locale.Error:
+            continue
+    else:
+        pytest.skip("no comma-decimal locale installed")
+    try:
+        out = tmp_path / "l.bak"
+        runfiles.save_backup(out, s, 4)
+        r, nt = runfiles.read_backup(out, [0, 3])
+    finally:
+        locale.setlocale(locale.LC_NUMERIC, old)
+    assert out.read_text() == ref.read_text() and nt == 5
+    assert np.array_equal(r.X[np.abs(s.X) >= 1], s.X[np.abs(s.X) >= 1])
