@@ -66,6 +66,9 @@ def test_struct_layouts_match_c(tmp_path):
           printf("%zu %zu %zu %zu\\n", offsetof(fs_params, tol), offsetof(fs_params, barrier_fs_over_2a),
                  offsetof(fs_params, lambda_extrap_step), offsetof(fs_diag, min_dist2));
           printf("%zu %zu\\n", offsetof(fs_host_state, lam), offsetof(fs_host_state, c));
+          printf("%zu %zu %zu %zu %zu\\n", sizeof(fs_run_info), offsetof(fs_run_info, a),
+                 offsetof(fs_run_info, box), offsetof(fs_run_info, dt),
+                 offsetof(fs_run_info, network_spring_natural_length));
           return 0;
         }
     """))
@@ -78,6 +81,9 @@ def test_struct_layouts_match_c(tmp_path):
     assert vals[3] == P.tol.offset and vals[4] == P.barrier_fs_over_2a.offset
     assert vals[5] == P.lambda_extrap_step.offset and vals[6] == D.min_dist2.offset
     assert vals[7] == H.lam.offset and vals[8] == H.c.offset
+    R = abi.FsRunInfo
+    assert vals[9:] == [ctypes.sizeof(R), R.a.offset, R.box.offset, R.dt.offset,
+                        R.network_spring_natural_length.offset]
 
 
 def test_sources_have_no_cpu_fallback():
