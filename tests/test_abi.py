@@ -111,6 +111,13 @@ def test_cpp_mirror_header_compiles_and_links(libpath, tmp_path):
             filsim::FcmGpu fcm(ctx, 8);
             filsim::LinkedListGpu ll(ctx);
             std::printf("context %d %d %d\\n", ll.cells()[0], ll.cells()[1], ll.cells()[2]);
+            // the swimming, spring-link, barrier-mode and gait-reset wrappers compile and link
+            // (taken by address, not run)
+            auto sw = &filsim::SuspensionGpu::setSwimming;
+            auto sl = &filsim::SuspensionGpu::setSpringLinks;
+            auto bm = &filsim::SuspensionGpu::setBarrierMode;
+            auto gr = &filsim::SuspensionGpu::stepGaitReset;
+            std::printf("wrappers %d\\n", (sw != nullptr) + (sl != nullptr) + (bm != nullptr) + (gr != nullptr));
           } catch (const filsim::Error &e) {
             std::printf("error %d\\n", e.status);
           }
