@@ -380,7 +380,11 @@ fs_status fs_cells_link(fs_ctx *c, const double *Xs, int np) {
   if (!c || np < 0 || np > c->max_beads || (np > 0 && !Xs)) return FS_ERR_INVALID_ARG;
   FS_CUDA(cudaMemsetAsync(c->flags + FLAG_CAPACITY, 0, sizeof(int), c->stream));
   FS_TRY(cells_link(c, Xs, np));
-  return FS_OK;
+  // a cell of 4096 beads or more does not fit the barrier's visiting-order key
+  int cap = 0;
+  FS_CUDA(cudaMemcpyAsync(&cap, c->flags + FLAG_CAPACITY, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  FS_CUDA(cudaStreamSynchronize(c->stream));
+  return cap ? FS_ERR_CAPACITY : FS_OK;
 }
 
 fs_status fs_cells_get_lists(fs_ctx *c, int *head_h, int *list_h, int *map_h) {
@@ -408,14 +412,17 @@ fs_status fs_collision_barrier(fs_ctx *c, const double *Y, double *F_inout, int 
   if (!c || np < 0 || (np > 0 && (!Y || !F_inout))) return FS_ERR_INVALID_ARG;
   FS_TRY(resolve_ids(c, np, &fil_id, &seg_id));
   FS_TRY(cells_barrier(c, Y, F_inout, np, nt, fil_id, seg_id, nullptr, 0, nullptr));
-  if (min_dist2_h) {
-    unsigned long long bits;
+  int cap = 0;
+  unsigned long long bits;
+  FS_CUDA(cudaMemcpyAsync(&cap, c->flags + FLAG_CAPACITY, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  if (min_dist2_h)
     FS_CUDA(cudaMemcpyAsync(&bits, c->min_dist2_bits, sizeof bits, cudaMemcpyDeviceToHost, c->stream));
-    FS_CUDA(cudaStreamSynchronize(c->stream));
+  FS_CUDA(cudaStreamSynchronize(c->stream));
+  if (min_dist2_h) {
     memcpy(min_dist2_h, &bits, sizeof bits);
     c->diag.min_dist2 = *min_dist2_h;
   }
-  return FS_OK;
+  return cap ? FS_ERR_CAPACITY : FS_OK;
 }
 
 fs_status fs_collision_pairs(fs_ctx *c, const double *Y, int np, int nt, const int *fil_id, const int *seg_id,

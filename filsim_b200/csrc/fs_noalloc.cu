@@ -13,6 +13,7 @@
 // Every call uses the same array and leaves its contents behind; the call
 // clears what must start at zero. Two calls that overlap on the GPU (on
 // different streams, or from different host threads) race on the array.
+#include <cmath>
 #include <mutex>
 #include "fs_internal.cuh"
 
@@ -114,12 +115,16 @@ __global__ void k_na_scatter(const int *__restrict__ key, int np, const int *__r
   }
 }
 
-// per cell: ascending bead ids (shell sort) and each bead's list rank
+// per cell: ascending bead ids (shell sort) and each bead's list rank. The
+// visiting-order key of k_na_barrier holds a list position in 12 bits, so a
+// cell of 4096 beads or more sets bit 1 of the flag (the barrier then adds
+// nothing and the call returns FS_ERR_CAPACITY).
 __global__ void k_na_cells(const int *__restrict__ start, int ncell, int *__restrict__ sorted,
-                           int *__restrict__ rank_desc) {
+                           int *__restrict__ rank_desc, int *__restrict__ overflow_flag) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncell) return;
   const int s0 = start[c], n = start[c + 1] - s0;
+  if (n >= 4096) atomicOr(overflow_flag, 2);
   int *a = sorted + s0;
   int gap = 1;
   while (gap < n / 3) gap = 3 * gap + 1;
@@ -170,7 +175,7 @@ __global__ void __launch_bounds__(128) k_na_barrier(const double *__restrict__ Y
                                                     unsigned long long *__restrict__ min_bits,
                                                     int *__restrict__ overflow_flag) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= np) return;
+  if (b >= np || (*overflow_flag & 2)) return;  // a cell too full for the key: F is left as it was
   const int cb = cell_of[b], pb = rank_desc[b];
   const int s0 = start[cb], e0 = start[cb + 1], p_asc = e0 - 1 - pb;
   const int Mx = k.M[0], My = k.M[1];
@@ -256,7 +261,6 @@ __global__ void k_na_init(unsigned long long *min_bits, int *overflow) {
 // device address of the scratch array, looked up once per device
 std::mutex g_na_mutex;
 unsigned char *g_na_ptr[64];
-bool g_na_sm100[64];
 
 fs_status na_setup(int *dev_out, unsigned char **ptr_out) {
   int dev = 0;
@@ -276,7 +280,6 @@ fs_status na_setup(int *dev_out, unsigned char **ptr_out) {
       return FS_ERR_CUDA;
     }
     g_na_ptr[dev] = (unsigned char *)p;
-    g_na_sm100[dev] = true;
   }
   *dev_out = dev;
   *ptr_out = g_na_ptr[dev];
@@ -296,9 +299,16 @@ extern "C" fs_status fs_collision_barrier_noalloc(const fs_params *p, const doub
   NaConsts k;
   const double Lb[3] = {p->npts_x * p->dx, p->npts_y * p->dx, p->npts_z * p->dx};
   for (int d = 0; d < 3; ++d) {
+    // the cell count per axis is checked as a double before the conversion to int
+    const double m = Lb[d] / p->cell_width;
+    if (!std::isfinite(p->cell_width) || !(p->cell_width > 0) || !std::isfinite(Lb[d]) || !(Lb[d] > 0) ||
+        !(m >= 1.0) || m > (double)kMaxCells) {
+      fprintf(stderr, "filsim_gpu: fs_collision_barrier_noalloc: box %g / cell width %g gives no valid cell count\n",
+              Lb[d], p->cell_width);
+      return FS_ERR_INVALID_ARG;
+    }
     k.L[d] = Lb[d];
-    k.M[d] = (int)(Lb[d] / p->cell_width);  // LinkedList::initialise (CollisionBarrierFilament.cpp:277-281)
-    if (k.M[d] < 1) return FS_ERR_INVALID_ARG;
+    k.M[d] = (int)m;  // LinkedList::initialise (CollisionBarrierFilament.cpp:277-281)
   }
   const long long ncell = (long long)k.M[0] * k.M[1] * k.M[2];
   if (ncell > kMaxCells) {
@@ -336,7 +346,7 @@ extern "C" fs_status fs_collision_barrier_noalloc(const fs_params *p, const doub
   if (np > 0) {
     k_na_scatter<<<fs_blocks(np, 256), 256, 0, st>>>(key, np, start, cursor, sorted);
     FS_LAUNCH_CHECK();
-    k_na_cells<<<fs_blocks(k.ncell, 256), 256, 0, st>>>(start, k.ncell, sorted, rank);
+    k_na_cells<<<fs_blocks(k.ncell, 256), 256, 0, st>>>(start, k.ncell, sorted, rank, overflow);
     FS_LAUNCH_CHECK();
     k_na_barrier<<<fs_blocks(np, 128), 128, 0, st>>>(Y, F_inout, np, k, key, start, sorted, rank, fil_id, seg_id,
                                                       min_bits, overflow);

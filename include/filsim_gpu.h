@@ -184,7 +184,9 @@ fs_status fs_fcm_flow_solve(fs_ctx *ctx, const double *f, double *u);
 /* Cell grid sizes M_X, M_Y, M_Z (CollisionBarrierFilament.cpp:277-281). */
 fs_status fs_cells_dims(const fs_ctx *ctx, int *mxyz_h);
 /* Bins beads into cells from unwrapped positions Xs (np x 3) with a counting
- * sort; the result is the reference's head/list linked list.
+ * sort; the result is the reference's head/list linked list. Synchronises the
+ * context's stream; FS_ERR_CAPACITY if a cell holds 4096 beads or more (the
+ * barrier's visiting-order key keeps list positions in 12 bits).
  * Replaces LinkedList::link (CollisionBarrierFilament.cpp:370-433). */
 fs_status fs_cells_link(fs_ctx *ctx, const double *Xs, int np);
 /* Copies the linked list out: head (ncell), list (np), map (13*ncell); any may be NULL. */
@@ -193,7 +195,9 @@ fs_status fs_cells_get_lists(fs_ctx *ctx, int *head_h, int *list_h, int *map_h);
  * using the cells of the last fs_cells_link. min_dist2_h (may be NULL)
  * receives the minimum squared separation examined.
  * fil_id, seg_id: per-bead filament/segment number (device ints) or NULL to
- * use the uploaded suspension.
+ * use the uploaded suspension. Synchronises the context's stream;
+ * FS_ERR_CAPACITY (discard F_inout) if the last link overflowed a cell or a
+ * bead takes part in more than 64 barrier interactions.
  * Replaces LinkedList::apply_collision_barrier (CollisionBarrierFilament.cpp:24-271). */
 fs_status fs_collision_barrier(fs_ctx *ctx, const double *Y, double *F_inout, int np, int nt,
                                const int *fil_id, const int *seg_id, double *min_dist2_h);
@@ -214,11 +218,15 @@ fs_status fs_collision_pairs(fs_ctx *ctx, const double *Y, int np, int nt,
  * allocates nothing: its working memory is one static 4 MiB device array that
  * every GPU loading this library holds until the process exits, which limits
  * a call to FS_NOALLOC_MAX_BEADS beads and FS_NOALLOC_MAX_CELLS cells (larger
- * calls return FS_ERR_INVALID_ARG). The first call on a device looks up the
+ * calls, and a cell width that is not finite and positive, return
+ * FS_ERR_INVALID_ARG). The first call on a device looks up the
  * array's device address on that device, so make it before any stream capture.
  * All calls share the array: calls that overlap on the GPU (different streams or
  * host threads) race. stream: a cudaStream_t or NULL; the call synchronises it.
- * All array arguments are device pointers; min_dist2_h (may be NULL) is host. */
+ * All array arguments are device pointers; min_dist2_h (may be NULL) is host.
+ * FS_ERR_CAPACITY: a cell holds 4096 beads or more (F_inout is left unchanged),
+ * or a bead takes part in more than 64 barrier interactions (F_inout then
+ * holds the sums of the interactions that fitted and must be discarded). */
 #define FS_NOALLOC_MAX_BEADS 65536
 #define FS_NOALLOC_MAX_CELLS 262144
 fs_status fs_collision_barrier_noalloc(const fs_params *p, const double *Xs, const double *Y, double *F_inout,

@@ -75,3 +75,33 @@ def test_link_bit_exact_benchmark_suspension(oracle, gpu_lib):
     head, lst, _ = ll.lists()
     head0, lst0, _ = oracle.cells_link(p, s.X)
     assert np.array_equal(head, head0) and np.array_equal(lst, lst0)
+
+
+def test_full_cell_and_crowded_bead_report_capacity(gpu_lib):
+    """The visiting-order key keeps list positions in 12 bits and a bead's events
+    in a 64-entry list: a cell of 4096 or more beads makes fs_cells_link return
+    FS_ERR_CAPACITY, and a bead with more than 64 interactions makes
+    fs_collision_barrier return it."""
+    from filsim_b200.abi import FsError, FS_ERR_CAPACITY
+    p = params_for(32)
+    L = 32 * p.dx
+    p.cell_width = 0.99 * L  # one cell for the whole box
+    n = 4100
+    X = np.random.default_rng(5).uniform(0, L, (n, 3))
+    ctx = Context(p, max_beads=n, max_filaments=n)
+    with pytest.raises(FsError) as e:
+        LinkedList(ctx).link(X)
+    assert e.value.status == FS_ERR_CAPACITY
+    ctx.close()
+    p = params_for(32)
+    n = 80
+    X = 8.0 + 0.3 * np.random.default_rng(6).standard_normal((n, 3))
+    ctx = Context(p, max_beads=n, max_filaments=n)
+    ll = LinkedList(ctx)
+    ll.link(X)
+    Y = torch.as_tensor(X, device="cuda")
+    F = torch.zeros_like(Y)
+    with pytest.raises(FsError) as e:
+        ll.apply_collision_barrier(Y, F, 5, np.arange(n), np.zeros(n))
+    assert e.value.status == FS_ERR_CAPACITY
+    ctx.close()
