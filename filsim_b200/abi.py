@@ -63,8 +63,10 @@ class FsDiag(ctypes.Structure):
 
 
 STAGES = ["spread", "fft_fwd", "project", "fft_inv", "interp", "link", "barrier", "forces", "jacobian",
-          "error_check", "broyden", "update", "friction", "learn"]
-FS_STAGE_COUNT = 16
+          "error_check", "broyden", "update", "friction", "learn",
+          # single kernels inside the stages above
+          "k_spread", "k_fft_z_fwd", "k_fft_y_fwd", "k_fft_y_inv", "k_fft_z_inv"]
+FS_STAGE_COUNT = 32
 
 
 class FsProfile(ctypes.Structure):

@@ -853,10 +853,13 @@ fs_status fs_run_steps(fs_ctx *c, int nt_start, int nsteps, int *iters_h) {
 fs_status fs_get_diag(fs_ctx *c, fs_diag *d_h) {
   if (!c || !d_h) return FS_ERR_INVALID_ARG;
   *d_h = c->diag;
-  unsigned long long bits = 0;
+  unsigned long long bits = 0, mbits = 0;
   FS_CUDA(cudaMemcpyAsync(&bits, c->maxerr_bits, sizeof bits, cudaMemcpyDeviceToHost, c->stream));
+  if (c->min_dist2_valid)
+    FS_CUDA(cudaMemcpyAsync(&mbits, c->min_dist2_bits, sizeof mbits, cudaMemcpyDeviceToHost, c->stream));
   FS_CUDA(cudaStreamSynchronize(c->stream));
   memcpy(&d_h->last_max_abs_err, &bits, sizeof bits);
+  if (c->min_dist2_valid) memcpy(&d_h->min_dist2, &mbits, sizeof mbits);
   return FS_OK;
 }
 

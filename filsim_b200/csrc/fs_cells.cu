@@ -380,6 +380,7 @@ fs_status cells_barrier(fs_ctx *c, const double *Y, double *F, int np, int nt, c
   k.np = np;
   k_set_min_init<<<1, 1, 0, c->stream>>>(c->min_dist2_bits);
   FS_LAUNCH_CHECK();
+  c->min_dist2_valid = true;
   if (np == 0) return FS_OK;
   const int T = 128;
   if (npairs_h) {

@@ -864,6 +864,7 @@ fs_status spread_t(fs_ctx *c, const FcmConsts &k, const double *Y, const double 
           Y, F, T, c->bins.sorted, c->bead_sw, np, k, c->spread_wb);
       FS_LAUNCH_CHECK();
     }
+    ProfScope pk(c, FS_STAGE_K_SPREAD);
     if (c->tune_spread_chunk == 32)
       k_spread32<32><<<c->nbins, FS_SPREAD32_THREADS, sizeof(SpreadStage32<32>), c->stream>>>(
           c->bins.start, rec, k, (float *)c->grid_real);
@@ -871,9 +872,11 @@ fs_status spread_t(fs_ctx *c, const FcmConsts &k, const double *Y, const double 
       k_spread32<64><<<c->nbins, FS_SPREAD32_THREADS, sizeof(SpreadStage32<64>), c->stream>>>(
           c->bins.start, rec, k, (float *)c->grid_real);
   } else if (c->tune_spread_chunk == 32) {
+    ProfScope pk(c, FS_STAGE_K_SPREAD);
     k_spread<R, 32><<<c->nbins, FS_SPREAD_THREADS, sizeof(SpreadStage<R, 32>), c->stream>>>(
         Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k, (R *)c->grid_real);
   } else {
+    ProfScope pk(c, FS_STAGE_K_SPREAD);
     k_spread<R, 64><<<c->nbins, FS_SPREAD_THREADS, sizeof(SpreadStage<R, 64>), c->stream>>>(
         Y, F, T, c->bins.start, c->bins.sorted, c->bead_sw, k, (R *)c->grid_real);
   }

@@ -620,7 +620,11 @@ fs_status fft32_flow_solve(fs_ctx *c) {
   float2 *B = A + (size_t)3 * c->nzh * c->nx * c->ny;
   {
     ProfScope ps(c, FS_STAGE_FFT_FWD);
-    FS_FFT_SWITCH_Z(c->nz, z_fwd, c, g, A, tw);
+    {
+      ProfScope pk(c, FS_STAGE_K_FFT_Z_FWD);
+      FS_FFT_SWITCH_Z(c->nz, z_fwd, c, g, A, tw);
+    }
+    ProfScope pk(c, FS_STAGE_K_FFT_Y_FWD);
     FS_FFT_SWITCH(c->ny, y_fwd, c, A, B, tw);
   }
   {
@@ -629,7 +633,11 @@ fs_status fft32_flow_solve(fs_ctx *c) {
   }
   {
     ProfScope ps(c, FS_STAGE_FFT_INV);
-    FS_FFT_SWITCH(c->ny, y_inv, c, B, A, tw);
+    {
+      ProfScope pk(c, FS_STAGE_K_FFT_Y_INV);
+      FS_FFT_SWITCH(c->ny, y_inv, c, B, A, tw);
+    }
+    ProfScope pk(c, FS_STAGE_K_FFT_Z_INV);
     FS_FFT_SWITCH_Z(c->nz, z_inv, c, A, g, tw);
   }
   return FS_OK;

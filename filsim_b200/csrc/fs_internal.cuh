@@ -74,6 +74,7 @@ struct fs_ctx {
   int *cell_rank;      // descending-id rank of each bead inside its cell
   int *pair_count, *pair_off, *pair_scan_tmp;
   int cells_np;        // beads in the last link (-1: none)
+  bool min_dist2_valid;  // a barrier has written min_dist2_bits
   double *min_dist2;   // device scalar
   unsigned long long *min_dist2_bits;
 

@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define FS_ABI_VERSION 1
+#define FS_ABI_VERSION 2
 
 typedef int fs_status;
 enum {
@@ -373,7 +373,13 @@ enum {
   FS_STAGE_UPDATE = 11,     /* state update + step */
   FS_STAGE_FRICTION = 12,   /* Stokes-drag mobility */
   FS_STAGE_LEARN = 13,      /* warm-start features + MLP inference, and MLP training steps */
-  FS_STAGE_COUNT = 16
+  /* single kernels inside the stages above (their time also counts there) */
+  FS_STAGE_K_SPREAD = 14,   /* the force-distribution kernel alone (no binning or records) */
+  FS_STAGE_K_FFT_Z_FWD = 15, /* FP32 transform: the forward pass over z lines */
+  FS_STAGE_K_FFT_Y_FWD = 16, /* FP32 transform: the forward pass over y lines */
+  FS_STAGE_K_FFT_Y_INV = 17, /* FP32 transform: the inverse pass over y lines */
+  FS_STAGE_K_FFT_Z_INV = 18, /* FP32 transform: the inverse pass over z lines */
+  FS_STAGE_COUNT = 32
 };
 typedef struct fs_profile {
   double ms[FS_STAGE_COUNT];     /* summed device milliseconds */

@@ -119,6 +119,63 @@ static void or_fft_line(or_cpx *data, size_t stride, const or_fftplan *pl, int s
   for (int i = 0; i < n; ++i) data[(size_t)i * stride] = work_out[i];
 }
 
+/* Power-of-two lengths: OR_FB lines at once, interleaved (element e of line b at
+ * e * OR_FB + b), by an iterative radix-2 Stockham transform (decimation in
+ * frequency, self-sorting), so the inner loops run over the lines and the
+ * strided passes read and write OR_FB adjacent values per element. Other
+ * lengths use the recursive transform above, one line at a time. */
+#define OR_FB 8
+
+static int or_is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+/* x, y: n * OR_FB values; the result is left in *x (the buffers may swap) */
+static void or_fft_block_pow2(or_cpx **x, or_cpx **y, int n, const or_fftplan *pl, int sign) {
+  or_cpx *a = *x, *b = *y;
+  for (int len = n, s = 1; len > 1; len >>= 1, s <<= 1) {
+    const int m = len / 2, ts = n / len;
+    for (int pp = 0; pp < m; ++pp) {
+      or_cpx w = pl->tw[(size_t)pp * ts];
+      if (sign > 0) w.im = -w.im;
+      for (int q = 0; q < s; ++q) {
+        const or_cpx *a0 = a + ((size_t)q + (size_t)s * pp) * OR_FB;
+        const or_cpx *a1 = a + ((size_t)q + (size_t)s * (pp + m)) * OR_FB;
+        or_cpx *b0 = b + ((size_t)q + (size_t)s * (2 * pp)) * OR_FB;
+        or_cpx *b1 = b + ((size_t)q + (size_t)s * (2 * pp + 1)) * OR_FB;
+        for (int l = 0; l < OR_FB; ++l) {
+          const double dr = a0[l].re - a1[l].re, di = a0[l].im - a1[l].im;
+          b0[l].re = a0[l].re + a1[l].re;
+          b0[l].im = a0[l].im + a1[l].im;
+          b1[l].re = dr * w.re - di * w.im;
+          b1[l].im = dr * w.im + di * w.re;
+        }
+      }
+    }
+    or_cpx *t = a;
+    a = b;
+    b = t;
+  }
+  *x = a;
+  *y = b;
+}
+
+/* transforms lines [l0, l0 + nb) (nb <= OR_FB) whose element e sits at
+ * base[line * lstride + e * estride] (complex), in place */
+static void or_fft_lines(or_cpx *base, long l0, int nb, size_t lstride, size_t estride, const or_fftplan *pl,
+                         int sign, or_cpx *wa, or_cpx *wb) {
+  const int n = pl->n;
+  if (!or_is_pow2(n)) {
+    for (int l = 0; l < nb; ++l) or_fft_line(base + (size_t)(l0 + l) * lstride, estride, pl, sign, wa, wb);
+    return;
+  }
+  for (int e = 0; e < n; ++e)
+    for (int l = 0; l < OR_FB; ++l)
+      wa[(size_t)e * OR_FB + l] = l < nb ? base[(size_t)(l0 + l) * lstride + (size_t)e * estride] : wa[0];
+  or_cpx *x = wa, *y = wb;
+  or_fft_block_pow2(&x, &y, n, pl, sign);
+  for (int e = 0; e < n; ++e)
+    for (int l = 0; l < nb; ++l) base[(size_t)(l0 + l) * lstride + (size_t)e * estride] = x[(size_t)e * OR_FB + l];
+}
+
 /* Unnormalised 3-D real-to-complex transform; out is [nx][ny][nz/2+1].
  * stride > 1 transforms the first 1/stride of the lines of each pass only (timing samples). */
 static void fft_r2c_3d_s(const double *in, or_cpx *out, int nx, int ny, int nz, long stride) {
@@ -131,24 +188,48 @@ static void fft_r2c_3d_s(const double *in, or_cpx *out, int nx, int ny, int nz, 
   nmax = nmax > nz ? nmax : nz;
 #pragma omp parallel
   {
-    or_cpx *wa = (or_cpx *)malloc(sizeof(or_cpx) * (size_t)nmax);
-    or_cpx *wb = (or_cpx *)malloc(sizeof(or_cpx) * (size_t)nmax);
+    or_cpx *wa = (or_cpx *)malloc(sizeof(or_cpx) * (size_t)nmax * OR_FB);
+    or_cpx *wb = (or_cpx *)malloc(sizeof(or_cpx) * (size_t)nmax * OR_FB);
+    const long nzl = (long)nx * ny;
 #pragma omp for schedule(static)
-    for (long line = 0; line < (long)nx * ny / stride; ++line) {
-      const double *src = in + (size_t)line * nz;
-      for (int k = 0; k < nz; ++k) { wa[k].re = src[k]; wa[k].im = 0.0; }
-      or_fft_rec(wa, wb, nz, 1, &pz, 1, pz.fac, -1);
-      or_cpx *dst = out + (size_t)line * nzh;
-      for (int k = 0; k < nzh; ++k) dst[k] = wb[k];
+    for (long blk = 0; blk < (nzl + OR_FB - 1) / OR_FB / stride; ++blk) {
+      const long l0 = blk * OR_FB;
+      const int nb = (int)(nzl - l0 < OR_FB ? nzl - l0 : OR_FB);
+      if (or_is_pow2(nz)) {
+        for (int e = 0; e < nz; ++e)
+          for (int l = 0; l < OR_FB; ++l) {
+            wa[(size_t)e * OR_FB + l].re = l < nb ? in[(size_t)(l0 + l) * nz + e] : 0.0;
+            wa[(size_t)e * OR_FB + l].im = 0.0;
+          }
+        or_cpx *x = wa, *y = wb;
+        or_fft_block_pow2(&x, &y, nz, &pz, -1);
+        for (int l = 0; l < nb; ++l)
+          for (int k = 0; k < nzh; ++k) out[(size_t)(l0 + l) * nzh + k] = x[(size_t)k * OR_FB + l];
+        continue;
+      }
+      for (int l = 0; l < nb; ++l) {
+        const double *src = in + (size_t)(l0 + l) * nz;
+        for (int k = 0; k < nz; ++k) { wa[k].re = src[k]; wa[k].im = 0.0; }
+        or_fft_rec(wa, wb, nz, 1, &pz, 1, pz.fac, -1);
+        or_cpx *dst = out + (size_t)(l0 + l) * nzh;
+        for (int k = 0; k < nzh; ++k) dst[k] = wb[k];
+      }
     }
+    /* y lines: fixed x, blocks of adjacent kz */
+    const long nkb = (nzh + OR_FB - 1) / OR_FB;
 #pragma omp for schedule(static)
-    for (long line = 0; line < (long)nx * nzh / stride; ++line) {
-      long i = line / nzh, k = line % nzh;
-      or_fft_line(out + (size_t)i * ny * nzh + k, nzh, &py, -1, wa, wb);
+    for (long blk = 0; blk < (long)nx * nkb / stride; ++blk) {
+      const long i = blk / nkb, k0 = (blk % nkb) * OR_FB;
+      const int nb = (int)(nzh - k0 < OR_FB ? nzh - k0 : OR_FB);
+      or_fft_lines(out + (size_t)i * ny * nzh + k0, 0, nb, 1, nzh, &py, -1, wa, wb);
     }
+    /* x lines: blocks of adjacent (y, kz) */
+    const long nl = (long)ny * nzh;
 #pragma omp for schedule(static)
-    for (long line = 0; line < (long)ny * nzh / stride; ++line) {
-      or_fft_line(out + line, (size_t)ny * nzh, &px, -1, wa, wb);
+    for (long blk = 0; blk < (nl + OR_FB - 1) / OR_FB / stride; ++blk) {
+      const long l0 = blk * OR_FB;
+      const int nb = (int)(nl - l0 < OR_FB ? nl - l0 : OR_FB);
+      or_fft_lines(out, l0, nb, 1, (size_t)nl, &px, -1, wa, wb);
     }
     free(wa);
     free(wb);
@@ -171,30 +252,61 @@ static void fft_c2r_3d_s(or_cpx *in, double *out, int nx, int ny, int nz, long s
   nmax = nmax > nz ? nmax : nz;
 #pragma omp parallel
   {
-    or_cpx *wa = (or_cpx *)malloc(sizeof(or_cpx) * (size_t)nmax);
-    or_cpx *wb = (or_cpx *)malloc(sizeof(or_cpx) * (size_t)nmax);
+    or_cpx *wa = (or_cpx *)malloc(sizeof(or_cpx) * (size_t)nmax * OR_FB);
+    or_cpx *wb = (or_cpx *)malloc(sizeof(or_cpx) * (size_t)nmax * OR_FB);
+    const long nl = (long)ny * nzh;
 #pragma omp for schedule(static)
-    for (long line = 0; line < (long)ny * nzh / stride; ++line) {
-      or_fft_line(in + line, (size_t)ny * nzh, &px, +1, wa, wb);
+    for (long blk = 0; blk < (nl + OR_FB - 1) / OR_FB / stride; ++blk) {
+      const long l0 = blk * OR_FB;
+      const int nb = (int)(nl - l0 < OR_FB ? nl - l0 : OR_FB);
+      or_fft_lines(in, l0, nb, 1, (size_t)nl, &px, +1, wa, wb);
     }
+    const long nkb = (nzh + OR_FB - 1) / OR_FB;
 #pragma omp for schedule(static)
-    for (long line = 0; line < (long)nx * nzh / stride; ++line) {
-      long i = line / nzh, k = line % nzh;
-      or_fft_line(in + (size_t)i * ny * nzh + k, nzh, &py, +1, wa, wb);
+    for (long blk = 0; blk < (long)nx * nkb / stride; ++blk) {
+      const long i = blk / nkb, k0 = (blk % nkb) * OR_FB;
+      const int nb = (int)(nzh - k0 < OR_FB ? nzh - k0 : OR_FB);
+      or_fft_lines(in + (size_t)i * ny * nzh + k0, 0, nb, 1, nzh, &py, +1, wa, wb);
     }
+    const long nzl = (long)nx * ny;
 #pragma omp for schedule(static)
-    for (long line = 0; line < (long)nx * ny / stride; ++line) {
-      const or_cpx *src = in + (size_t)line * nzh;
-      wa[0].re = src[0].re;
-      wa[0].im = 0.0;
-      for (int k = 1; k < nzh; ++k) {
-        wa[k] = src[k];
-        if (2 * k == nz) wa[k].im = 0.0;
-        else { wa[nz - k].re = src[k].re; wa[nz - k].im = -src[k].im; }
+    for (long blk = 0; blk < (nzl + OR_FB - 1) / OR_FB / stride; ++blk) {
+      const long l0 = blk * OR_FB;
+      const int nb = (int)(nzl - l0 < OR_FB ? nzl - l0 : OR_FB);
+      if (or_is_pow2(nz)) {
+        for (int l = 0; l < OR_FB; ++l) {
+          const or_cpx *src = in + (size_t)(l0 + (l < nb ? l : 0)) * nzh;
+          wa[l].re = src[0].re;
+          wa[l].im = 0.0;
+          for (int k = 1; k < nzh; ++k) {
+            or_cpx v = src[k];
+            if (2 * k == nz) v.im = 0.0;
+            else {
+              wa[(size_t)(nz - k) * OR_FB + l].re = v.re;
+              wa[(size_t)(nz - k) * OR_FB + l].im = -v.im;
+            }
+            wa[(size_t)k * OR_FB + l] = v;
+          }
+        }
+        or_cpx *x = wa, *y = wb;
+        or_fft_block_pow2(&x, &y, nz, &pz, +1);
+        for (int l = 0; l < nb; ++l)
+          for (int k = 0; k < nz; ++k) out[(size_t)(l0 + l) * nz + k] = x[(size_t)k * OR_FB + l].re;
+        continue;
       }
-      or_fft_rec(wa, wb, nz, 1, &pz, 1, pz.fac, +1);
-      double *dst = out + (size_t)line * nz;
-      for (int k = 0; k < nz; ++k) dst[k] = wb[k].re;
+      for (int l = 0; l < nb; ++l) {
+        const or_cpx *src = in + (size_t)(l0 + l) * nzh;
+        wa[0].re = src[0].re;
+        wa[0].im = 0.0;
+        for (int k = 1; k < nzh; ++k) {
+          wa[k] = src[k];
+          if (2 * k == nz) wa[k].im = 0.0;
+          else { wa[nz - k].re = src[k].re; wa[nz - k].im = -src[k].im; }
+        }
+        or_fft_rec(wa, wb, nz, 1, &pz, 1, pz.fac, +1);
+        double *dst = out + (size_t)(l0 + l) * nz;
+        for (int k = 0; k < nz; ++k) dst[k] = wb[k].re;
+      }
     }
     free(wa);
     free(wb);
@@ -749,6 +861,11 @@ struct or_system {
   int *spring_beads;
   double spring_k, spring_l0;
   int barrier_mode;
+  /* CPU-baseline workspace (or_stage_costs): grids and Gaussian tables, kept
+   * across calls so their pages are touched once */
+  double *wf, *wu, *wg, *wgd, *wgr;
+  or_cpx *wfh;
+  int *wind;
 };
 
 static double *dalloc(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
@@ -806,7 +923,8 @@ void or_system_destroy(or_system *s) {
   void *ptrs[] = {s->fil_start, s->fil_id, s->seg_id, s->radius, s->X, s->Xs, s->Xt, s->U, s->Us, s->Ut,
                   s->q, s->qs, s->qt, s->F, s->TAU, s->lam, s->lam1, s->lam2, s->kap, s->cc, s->Y, s->V,
                   s->W, s->Err, s->NewErr, s->Upd, s->tmp, s->dE, s->Cmat, s->Dmat, s->joff, s->Jinv,
-                  s->head, s->list, s->map, s->swim, s->spring_beads};
+                  s->head, s->list, s->map, s->swim, s->spring_beads, s->wf, s->wu, s->wfh, s->wg, s->wgd,
+                  s->wgr, s->wind};
   for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); ++i) free(ptrs[i]);
   free(s);
 }
@@ -1577,26 +1695,40 @@ static double or_now(void) {
  * parts[0] spread, [1] forward FFTs, [2] projection, [3] inverse FFTs,
  * [4] interpolation, [5] Jacobian build + inversion (once per step),
  * [6] forces + error check + two J0^-1 applications with 10 history columns
- * (full, not sampled), [7] link + barrier (full). Returns the thread count. */
-int or_sample_costs(or_system *s, int stride, double *parts) {
+ * (full, not sampled), [7] link + barrier (full). Only the stages whose bit is
+ * set in mask run (the others' parts are left as they are); warm = 1 runs them
+ * once untimed first. stride = 1 runs every work unit: the full-size stage.
+ * The grids live in the system's workspace, allocated and touched on the first
+ * call. Returns the thread count, or -1 if the workspace cannot be allocated. */
+int or_stage_costs(or_system *s, int stride, unsigned mask, int warm, double *parts) {
   const fs_params *p = &s->p;
   or_consts c;
   or_consts_init(p, &c);
   const int nx = p->npts_x, ny = p->npts_y, nz = p->npts_z, nzh = nz / 2 + 1, ngd = p->ngd, np = s->np;
   const size_t N = (size_t)nx * ny * nz, NH = (size_t)nx * ny * nzh;
-  double *f = (double *)calloc(3 * N, sizeof(double));
-  double *u = (double *)calloc(3 * N, sizeof(double));
-  or_cpx *fh = (or_cpx *)calloc(3 * NH, sizeof(or_cpx));
-  double *g = (double *)malloc(sizeof(double) * (size_t)np * 3 * ngd);
-  double *gd = (double *)malloc(sizeof(double) * (size_t)np * 3 * ngd);
-  double *gr = (double *)malloc(sizeof(double) * (size_t)np * 3 * ngd);
-  int *ind = (int *)malloc(sizeof(int) * (size_t)np * 3 * ngd);
+  if (!s->wf) {
+    s->wf = (double *)malloc(sizeof(double) * 3 * N);
+    s->wu = (double *)malloc(sizeof(double) * 3 * N);
+    s->wfh = (or_cpx *)malloc(sizeof(or_cpx) * 3 * NH);
+    s->wg = dalloc((size_t)np * 3 * ngd);
+    s->wgd = dalloc((size_t)np * 3 * ngd);
+    s->wgr = dalloc((size_t)np * 3 * ngd);
+    s->wind = (int *)calloc((size_t)np * 3 * ngd + 1, sizeof(int));
+    if (!s->wf || !s->wu || !s->wfh || !s->wg || !s->wgd || !s->wgr || !s->wind) return -1;
+    /* first touch, in parallel, outside any timed region */
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)(3 * N); ++i) s->wf[i] = s->wu[i] = 0.0;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)(3 * NH); ++i) s->wfh[i].re = s->wfh[i].im = 0.0;
+  }
+  double *f = s->wf, *u = s->wu, *g = s->wg, *gd = s->wgd, *gr = s->wgr;
+  or_cpx *fh = s->wfh;
+  int *ind = s->wind;
   const double *Y = s->Y, *F = s->F, *T = s->TAU;
   double sink = 0.0;
-  /* pass 0 is an untimed warm-up (first-touch page faults are not part of a
-   * solve); pass 1 is timed. The samples touch about 1/stride of the grids. */
-  for (int rep = 0; rep < 2; ++rep) {
+  for (int rep = warm ? 0 : 1; rep < 2; ++rep) {
   double t0 = or_now();
+  if (mask & 1u) {
 #pragma omp parallel for schedule(static)
   for (int b = 0; b < np / stride; ++b)
     or_gauss_bead(p, &c, Y + 3 * b, g + (size_t)b * 3 * ngd, gd + (size_t)b * 3 * ngd, gr + (size_t)b * 3 * ngd,
@@ -1630,9 +1762,13 @@ int or_sample_costs(or_system *s, int stride, double *parts) {
     }
   }
   parts[0] = (or_now() - t0) * stride;
+  }
+  if (mask & 2u) {
   t0 = or_now();
   for (int cpt = 0; cpt < 3; ++cpt) fft_r2c_3d_s(f + cpt * N, fh + cpt * NH, nx, ny, nz, stride);
   parts[1] = (or_now() - t0) * stride;
+  }
+  if (mask & 4u) {
   t0 = or_now();
   {
     const double TwoPI = 2. * OR_PI;
@@ -1658,9 +1794,13 @@ int or_sample_costs(or_system *s, int stride, double *parts) {
     }
   }
   parts[2] = (or_now() - t0) * stride;
+  }
+  if (mask & 8u) {
   t0 = or_now();
   for (int cpt = 0; cpt < 3; ++cpt) fft_c2r_3d_s(fh + cpt * NH, u + cpt * N, nx, ny, nz, stride);
   parts[3] = (or_now() - t0) * stride;
+  }
+  if (mask & 16u) {
   t0 = or_now();
 #pragma omp parallel for schedule(static) reduction(+ : sink)
   for (int b = 0; b < np / stride; ++b) {
@@ -1684,6 +1824,8 @@ int or_sample_costs(or_system *s, int stride, double *parts) {
     sink += v[0] + v[1] + v[2] + w[0] + w[1] + w[2];
   }
   parts[4] = (or_now() - t0) * stride;
+  }
+  if (mask & 32u) {
   t0 = or_now();
 #pragma omp parallel for schedule(dynamic)
   for (int fl = 0; fl < s->nfil / stride; ++fl) {
@@ -1695,6 +1837,8 @@ int or_sample_costs(or_system *s, int stride, double *parts) {
     free(J);
   }
   parts[5] = (or_now() - t0) * stride;
+  }
+  if (mask & 64u) {
   t0 = or_now();
   or_filament_forces(s, 2);
   or_error_check(s, s->V, s->W, s->NewErr, 2);
@@ -1702,16 +1846,20 @@ int or_sample_costs(or_system *s, int stride, double *parts) {
   or_jsolve(s, s->Err, s->Upd, hist);
   or_jsolve(s, s->NewErr, s->tmp, hist);
   parts[6] = or_now() - t0;
+  }
+  if (mask & 128u) {
   t0 = or_now();
   or_cells_link(p, np, s->Xs, s->head, s->list);
   or_collision_barrier(p, np, s->fil_id, s->seg_id, s->Y, s->head, s->list, s->map, 2, s->F, &s->min_dist2, NULL, 0);
   parts[7] = or_now() - t0;
   }
+  }
   parts[8] = sink;
-  free(f); free(u); free(fh); free(g); free(gd); free(gr); free(ind);
   int nth = 1;
 #ifdef _OPENMP
   nth = omp_get_max_threads();
 #endif
   return nth;
 }
+
+int or_sample_costs(or_system *s, int stride, double *parts) { return or_stage_costs(s, stride, 0xffu, 1, parts); }

@@ -66,9 +66,17 @@ int or_run_steps(or_system *sys, int nt_start, int nsteps, int *iters);
 /* CPU-baseline timing sample: stage wall times of one iteration, each stage run
  * on every stride-th work unit and scaled back (parts: 9 doubles) */
 int or_sample_costs(or_system *sys, int stride, double *parts);
+/* the same for the stages selected by mask (bit i: parts[i]); stride 1 = full
+ * size; warm = 1 runs the stages once untimed first */
+int or_stage_costs(or_system *sys, int stride, unsigned mask, int warm, double *parts);
 /* last step's barrier minimum squared distance */
 double or_last_min_dist2(or_system *sys);
 long long or_mobility_solves(or_system *sys);
+
+/* the seeded suspension generator, restated (or_suspension.c): X (nfil*nw x 3),
+ * Q (nfil*nw x 4); 0 = placed, 8 = a filament could not be placed, 1 = bad args */
+int or_suspension_random(const fs_params *p, int nfil, int nw, unsigned long long seed, double min_sep,
+                         int max_tries, double *X, double *Q);
 
 #ifdef __cplusplus
 }

@@ -68,6 +68,11 @@ def lib():
         L.or_mobility_solves.argtypes = [vp]
         L.or_sample_costs.restype = ctypes.c_int
         L.or_sample_costs.argtypes = [vp, ctypes.c_int, vp]
+        L.or_stage_costs.restype = ctypes.c_int
+        L.or_stage_costs.argtypes = [vp, ctypes.c_int, ctypes.c_uint, ctypes.c_int, vp]
+        L.or_suspension_random.restype = ctypes.c_int
+        L.or_suspension_random.argtypes = [pp, ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong, ctypes.c_double,
+                                           ctypes.c_int, vp, vp]
         _lib = L
     return _lib
 
@@ -79,6 +84,20 @@ def _ptr(a):
 def _f64(a, n=None):
     a = np.ascontiguousarray(a, dtype=np.float64)
     return a
+
+
+def suspension_random(p, nfil, nw, seed, min_sep=None, max_tries=1000000):
+    """Bead positions X and quaternions Q of the seeded generator, restated on
+    the CPU (or_suspension.c), so a CPU-only caller builds the same inputs as
+    filsim_b200.suspension.random_suspension without the GPU library."""
+    if min_sep is None:
+        min_sep = 2.2 * p.a
+    X = np.zeros((nfil * nw, 3))
+    Q = np.zeros((nfil * nw, 4))
+    st = lib().or_suspension_random(ctypes.byref(p), nfil, nw, seed, min_sep, max_tries, _ptr(X), _ptr(Q))
+    if st != 0:
+        raise RuntimeError("or_suspension_random failed: %d" % st)
+    return X, Q
 
 
 def fft_r2c_3d(x):
@@ -275,6 +294,19 @@ class System:
         return lib().or_last_min_dist2(self.h)
 
     STAGE_NAMES = ("spread", "fft_fwd", "project", "fft_inv", "interp", "jacobian", "iteration_other", "barrier")
+
+    def stage_costs(self, stages, stride=1, warm=False):
+        """Wall seconds of the named stages (STAGE_NAMES) of one iteration, each
+        on every stride-th work unit and scaled back (stride 1: full size);
+        returns (dict of the stages run, threads)."""
+        parts = np.zeros(9)
+        mask = 0
+        for name in stages:
+            mask |= 1 << self.STAGE_NAMES.index(name)
+        nth = lib().or_stage_costs(self.h, stride, mask, int(bool(warm)), _ptr(parts))
+        if nth < 0:
+            raise MemoryError("or_stage_costs: workspace allocation failed")
+        return {n: float(parts[i]) for i, n in enumerate(self.STAGE_NAMES) if mask & (1 << i)}, int(nth)
 
     def sample_costs(self, stride):
         """Stage wall seconds of one iteration, sampled on 1/stride of the work

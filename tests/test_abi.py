@@ -36,7 +36,7 @@ def test_no_device_status_without_gpu(libpath):
     h = ctypes.c_void_p()
     assert L.fs_create(ctypes.byref(p), 10, 2, None, ctypes.byref(h)) == 2  # FS_ERR_NO_DEVICE
     assert L.fs_status_string(2) == b"no sm_100 CUDA device"
-    assert L.fs_abi_version() == 1
+    assert L.fs_abi_version() == 2
 
 
 def test_params_default_matches_reference_constants(libpath):

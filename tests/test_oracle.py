@@ -169,6 +169,28 @@ def test_suspension_rejection_rule():
     assert r2[other].min() >= (2.2 - 1e-9) ** 2
 
 
+@pytest.mark.parametrize("npts,nfil,nw,seed,sep", [(64, 32, 15, 1000, 2.2), (32, 40, 6, 11, 1.2),
+                                                    ((96, 64, 48), 20, 16, 7, 2.2)])
+def test_cpu_generator_reproduces_the_library_bit_for_bit(oracle, npts, nfil, nw, seed, sep):
+    """The CPU baseline builds its inputs with the oracle's restatement of the
+    generator (no GPU library); both must give the same bits. The library's
+    generator is host code, so this runs without a GPU."""
+    p = params_for(npts)
+    s = random_suspension(p, nfil, nw, seed, min_sep=sep)
+    X, Q = oracle.suspension_random(p, nfil, nw, seed, min_sep=sep)
+    assert np.array_equal(X, s.X)
+    assert np.array_equal(Q, s.q)
+
+
+def test_cpu_generator_at_the_512_cube_benchmark(oracle):
+    """The 512^3 / 4096 x 32 benchmark suspension (seed 1002) from both generators."""
+    from filsim_b200.configs import make_sediment_case
+    p, s = make_sediment_case(512, 4096, 32, seed=1002)
+    X, Q = oracle.suspension_random(p, 4096, 32, 1002)
+    assert np.array_equal(X, s.X)
+    assert np.array_equal(Q, s.q)
+
+
 def _link_twist_norms(tau, nw):
     """Per-link torque magnitudes |w_i| of a filament whose beads receive
     +w_i (bead i) and -w_i (bead i+1): w_i is the prefix sum of the torques."""
