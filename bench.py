@@ -35,7 +35,10 @@ e2e        the value arm through the C-ABI with HOST state: every step uploads
            and downloads it (fs_state_download); the state is what the reference
            checkpoints (X, Xt, q, qt, U, Ut, lam, lam1, lam2) plus K_B and C.
 --impl reference times the CPU restatement of the reference (the reference
-           itself, MPI + FFTW 2.1.5 + Armadillo, cannot be built here).
+           itself, MPI + FFTW 2.1.5 + Armadillo, cannot be built here) on this
+           host's cores, without the GPU library: the inputs come from the
+           restated generator in oracle/, and each of its steps is one full-size
+           stage of a Broyden iteration (see run_reference).
 
 Grids (3 x 512^3 reals + 3 x 512^2 x 257 complex, several GB) exceed the 126 MB
 L2, so no flush is needed between steps.
@@ -56,11 +59,6 @@ sys.path.insert(0, ROOT)
 METRIC = "bead-steps/s & Broyden iters/step: learned+FP32 vs plain FP64 GPU, resid<=1e-6"
 UNIT = "bead-steps/s"
 WORKLOAD = dict(npts=512, nfil=4096, nw=32, seed=1002, name="sediment_512")
-# Broyden iterations per steady-state step of sediment_512 (FP64 chain, the
-# reference's start; measured on B200) used to scale the CPU baseline's
-# per-iteration sample to whole steps in the reference arm, which runs without
-# a GPU; the GPU FP64 path matches the oracle's iteration counts.
-REFERENCE_ITERS_PER_STEP = 12.7
 # untimed start-up steps before the measured window (the tension extrapolation
 # becomes quadratic after step 12, Filament::step, Filament.hpp:455-478)
 PREP_STEPS = 12
@@ -70,16 +68,18 @@ TRAIN_EPOCHS = 40
 CHECKPOINT_FIELDS = ("X", "Xt", "q", "qt", "U", "Ut", "lam", "lam1", "lam2", "kap", "c")
 GATE_PERIOD = 8  # the learned start's cost gate: first probe of the other start after 8 steps
 ENSEMBLE_SEED = 3000
-# DRAM bytes per launch from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum);
-# the kernels and captures are listed in profiles/.
-NCU_TRAFFIC = {
-    # per grid point, from the ncu capture in profiles/fcm_kernels_mobility_256_512x30.md
-    # (DRAM read + write of the stage's kernels on 256^3), times the grid points of the workload
-    "spread": (17.40e6 + 152.87e6) / 256 ** 3,                          # k_spread32
-    "fft_fwd": (201.36e6 + 156.52e6 + 202.93e6 + 156.83e6) / 256 ** 3,  # z_r2c + y_fwd
-    "project": (202.97e6 + 143.17e6) / 256 ** 3,                        # x_project
-    "fft_inv": (202.93e6 + 159.50e6 + 203.01e6 + 160.35e6) / 256 ** 3,  # y_inv + z_c2r
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the FCM
+# kernels, per grid point, from an ncu capture of the FP32 chain on 256^3 with
+# 15,360 beads (the 512^3 bead density); scaled to the workload by its grid points.
+NCU_TRAFFIC_PER_POINT = {
+    "k_spread": (17.40e6 + 152.87e6) / 256 ** 3,
+    "k_fft_z_fwd": (201.36e6 + 156.52e6) / 256 ** 3,
+    "k_fft_y_fwd": (202.93e6 + 156.83e6) / 256 ** 3,
+    "project": (202.97e6 + 143.17e6) / 256 ** 3,
+    "k_fft_y_inv": (202.93e6 + 159.50e6) / 256 ** 3,
+    "k_fft_z_inv": (203.01e6 + 160.35e6) / 256 ** 3,
 }
+NCU_TRAFFIC_SOURCE = "ncu capture at 256^3 / 15,360 beads, scaled by grid points"
 
 
 def parse():
@@ -91,15 +91,16 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--cpu-stride", type=int, default=64)
     ap.add_argument("--no-learned", action="store_true", help="skip training; time the reference's start only")
     ap.add_argument("--no-graph", action="store_true", help="host-driven steps only (no CUDA graphs)")
     ap.add_argument("--train-seeds", type=int, default=20, help="plain-solver runs that generate training data")
     ap.add_argument("--workload", default="sediment_512",
-                    choices=["sediment_512", "mobility_256", "ensemble_64", "mlp"],
+                    choices=["sediment_512", "mobility_256", "ensemble_64", "mlp", "trajectory_200"],
                     help="sediment_512: implicit steps (the headline); mobility_256: FCM mobility solves, "
                          "FP32 against FP64, on 256^3 with 1024 x 30 beads; ensemble_64: 64 independent "
-                         "boxes advanced by one graph launch per step")
+                         "boxes advanced by one graph launch per step; trajectory_200: the configured run "
+                         "of sediment_512, steps 1-200 from the placed suspension, mixed precision and FP64, "
+                         "with per-step iterations (a record, not a throughput benchmark)")
     ap.add_argument("--grid", type=int, default=None,
                     help="sediment_512 / mobility_256 on another cubic grid (profiling cases; the "
                          "workload name in config says so)")
@@ -378,21 +379,23 @@ def run_ours(args, rank, world):
     stage_calls = {k: v[1] for k, v in prof.items()}
     out["stage_ms_per_step"] = {k: v / K for k, v in stage_ms.items() if v > 0}
 
-    # roofline of the dominant kernel stage of this library
+    # roofline of the dominant single kernel of this library (CUDA events around
+    # each launch on the context's stream, host-driven steps); algorithmic bytes
+    # per launch: each grid pass reads and writes the grid once
     peak, peak_kind = measured_peaks()
     npts = WORKLOAD["npts"]
     N = npts ** 3
     NH = npts * npts * (npts // 2 + 1)
     s_real = 4  # FP32 grids in the mixed path
-    aux = 20 * (nw - 1) + 3 * nw + 1  # doubles of D', F', tangents and P per filament (fil_aux_size)
+    half = 3 * NH * 2 * s_real                         # the three half spectra, complex FP32
     alg_bytes = {
-        "spread": 3 * s_real * N + npb * 9 * 8,          # write f once, read bead Y, F, T
-        "fft_fwd": 2 * 2 * 3 * NH * 2 * s_real,          # two passes, each reads and writes 3 half spectra
-        "project": 2 * 3 * NH * 2 * s_real,              # x pass: read and write 3 half spectra
-        "fft_inv": 2 * 2 * 3 * NH * 2 * s_real,
-        "interp": 3 * s_real * N + npb * 9 * 8,          # read u once, bead Y in, V, W out
-        "jacobian": susp.nfil * ((3 * nw) ** 2 + aux) * 8,  # write the Schur inverse and the D', F' blocks
-        "broyden": susp.nfil * ((3 * nw) ** 2 + aux) * 8 + 2 * 6 * npb * 8,  # read them, read b, write x
+        "k_spread": 3 * s_real * N + npb * 9 * 8,      # write f once; read bead Y, F, T
+        "k_fft_z_fwd": 3 * s_real * N + half,          # read f, write the half spectra
+        "k_fft_y_fwd": 2 * half,
+        "project": 2 * half,                           # the x pass with the projection
+        "k_fft_y_inv": 2 * half,
+        "k_fft_z_inv": half + 3 * s_real * N,
+        "interp": 3 * s_real * N + npb * 9 * 8,        # read u once; bead Y in, V, W out
     }
     cands = {k: stage_ms[k] for k in alg_bytes if stage_ms.get(k, 0) > 0}
     dom = max(cands, key=cands.get)
@@ -400,9 +403,15 @@ def run_ours(args, rank, world):
     achieved = alg_bytes[dom] / (per_launch_ms / 1e3) / 1e9
     out["roofline"] = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                        "frac": achieved / peak, "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind,
-                       "traffic": NCU_TRAFFIC[dom] * N if dom in NCU_TRAFFIC else None,
-                       "algorithmic_bytes": alg_bytes[dom],
-                       "launch_ms": per_launch_ms}
+                       "traffic": NCU_TRAFFIC_PER_POINT[dom] * N if dom in NCU_TRAFFIC_PER_POINT else None,
+                       "traffic_source": NCU_TRAFFIC_SOURCE, "algorithmic_bytes": alg_bytes[dom],
+                       "launch_ms": per_launch_ms,
+                       "kernels": {k: {"ms_per_launch": stage_ms[k] / max(1, stage_calls[k]),
+                                       "share_of_step": stage_ms[k] / max(1e-9, sum(stage_ms[x] for x in (
+                                           "spread", "fft_fwd", "project", "fft_inv", "interp", "link", "barrier",
+                                           "forces", "jacobian", "error_check", "broyden", "update", "learn"))),
+                                       "frac": alg_bytes[k] / (stage_ms[k] / max(1, stage_calls[k]) / 1e3) / 1e9
+                                       / peak} for k in cands}}
     fcm_ms = sum(stage_ms.get(k, 0) for k in ("spread", "fft_fwd", "project", "fft_inv", "interp"))
     solves = max(1, stage_calls.get("interp", 0))
     b_fcm = 24 * s_real * N
@@ -469,12 +478,53 @@ def run_ours(args, rank, world):
     # CPU baseline: the oracle on this host's cores, sampled
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(p, susp, out.get("plain_fp64", {}).get("iters_per_step",
-                                                                                   out["iters_per_step"]),
-                                           args.cpu_stride)
+                                                                                   out["iters_per_step"]))
     ctx.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+    return out
+
+
+def run_trajectory(args, rank, world):
+    """Workload trajectory_200: the configured run of sediment_512, steps 1-200
+    from the placed suspension (start-up steps included), once with the mixed-
+    precision chain (FP32 spread/FFT/interpolation, FP64 Broyden and mechanics)
+    and once in FP64, both from the reference's start with graph-captured steady
+    steps. Records per-step Broyden iterations, the status, the final barrier
+    minimum squared distance and the wall time of each run."""
+    import numpy as np
+    import torch
+    from filsim_b200 import abi
+    from filsim_b200.configs import make_sediment_case
+    from filsim_b200.fcm import Context, Simulation
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    nsteps = args.steps if args.steps > 8 else 200
+    p, susp = make_sediment_case(WORKLOAD["npts"], WORKLOAD["nfil"], WORKLOAD["nw"], seed=WORKLOAD["seed"])
+    stream = torch.cuda.Stream()
+    ctx = Context(p, max_beads=susp.np, max_filaments=susp.nfil, stream=stream)
+    abi.check(abi.lib().fs_set_graph_mode(ctx.h, 1), "fs_set_graph_mode")
+    out = {"workload": "trajectory_%d" % nsteps, "grid": [WORKLOAD["npts"]] * 3, "filaments": WORKLOAD["nfil"],
+           "beads_per_filament": WORKLOAD["nw"], "beads": susp.np, "dt": p.dt, "tol": p.tol, "steps": nsteps}
+    for name, prec in (("mixed", abi.FS_PREC_FP32), ("fp64", abi.FS_PREC_FP64)):
+        ctx.set_precision(prec)
+        sim = Simulation(ctx, susp.copy())
+        torch.cuda.synchronize()
+        t0 = time.time()
+        with ClockSampler(dev) as clk:
+            its, st = sim.run_steps(1, nsteps)
+        wall = time.time() - t0
+        d = sim.diag()
+        X = sim.download()["X"]
+        out[name] = {"status": abi.STATUS_NAMES.get(st, st), "iters": [int(v) for v in its],
+                     "iters_mean_steps_13_on": float(np.mean(its[12:])), "iters_max": int(its.max()),
+                     "not_converged_steps": int(d.not_converged_steps), "nonfinite": int(d.nonfinite),
+                     "final_min_dist2": d.min_dist2, "final_max_abs_err": d.last_max_abs_err,
+                     "wall_s": wall, "mobility_solves": int(d.mobility_solves), "clocks": clk.summary(),
+                     "final_mean_z": float(X[:, 2].mean())}
+    ctx.close()
     return out
 
 
@@ -683,56 +733,132 @@ def run_mlp(args, rank, world):
             "clocks": clk.summary()}
 
 
-def cpu_baseline(p, susp, iters_per_step, stride):
-    """Oracle stage costs of one Broyden iteration of this workload, each stage
-    run on 1/stride of its independent work units and scaled back; a step is
-    the Jacobian build plus (iters+1) iterations."""
+# The CPU arms time the oracle's stages of one Broyden iteration at full size
+# (every work unit): per iteration the collision barrier, the FCM mobility solve
+# (spread, forward FFTs, projection, inverse FFTs, interpolation) and the rest
+# (forces, error check, two J0^-1 applications with 10 history columns); once
+# per step the Jacobian build and inversion. A step costs
+# jacobian + (iterations + 1) x iteration.
+ITERATION_STAGES = ("barrier", "spread", "fft_fwd", "project", "fft_inv", "interp", "iteration_other")
+STAGE_CYCLE = ITERATION_STAGES + ("jacobian",)
+# Broyden iterations per step of sediment_512 (seed 1002) in FP64, steps 1-200,
+# measured on a B200 by `python bench.py --workload trajectory_200` (the FP64
+# GPU path takes the oracle's iteration counts, tests/test_gpu_configs.py);
+# the reference arm, which runs without a GPU, averages the entries of the
+# steps its window covers.
+FP64_ITERS_BY_STEP = (
+    85, 28, 28, 26, 26, 26, 26, 26, 26, 26, 26, 26, 12, 12, 14, 12, 12, 12, 12, 16,
+    19, 14, 16, 22, 15, 23, 14, 23, 17, 23, 16, 23, 23, 22, 24, 14, 23, 21, 23, 23,
+    23, 14, 23, 15, 23, 23, 23, 12, 23, 16, 23, 17, 23, 23, 23, 12, 23, 17, 23, 23,
+    23, 23, 16, 23, 15, 23, 23, 23, 14, 23, 23, 23, 22, 24, 22, 24, 19, 23, 14, 24,
+    23, 23, 22, 16, 23, 22, 23, 17, 23, 15, 24, 23, 26, 24, 18, 24, 19, 24, 19, 26,
+    21, 27, 21, 27, 23, 22, 22, 14, 28, 20, 26, 21, 29, 23, 23, 24, 18, 22, 24, 19,
+    23, 19, 26, 23, 20, 17, 22, 14, 22, 20, 21, 22, 22, 22, 22, 22, 23, 23, 22, 23,
+    23, 23, 24, 22, 23, 23, 24, 15, 29, 22, 26, 22, 24, 22, 28, 23, 24, 24, 24, 23,
+    25, 23, 24, 23, 24, 23, 28, 23, 24, 24, 24, 24, 14, 29, 20, 26, 12, 29, 20, 26,
+    22, 24, 24, 24, 24, 12, 30, 14, 26, 12, 29, 21, 24, 22, 23, 24, 22, 24, 20, 27,
+)
+
+
+def oracle_step_seconds(stage_s, iters):
+    per_iter = sum(stage_s[k] for k in ITERATION_STAGES)
+    return stage_s["jacobian"] + (iters + 1) * per_iter, per_iter
+
+
+def cpu_baseline(p, susp, iters_per_step):
+    """One complete full-size Broyden iteration and Jacobian build of the oracle
+    on this host's cores (the workspace is allocated and touched first, untimed)."""
     from oracle import oracle_py
     sysw = oracle_py.System(p, susp)
     sysw.initial_guess()
     sysw.filament_forces(1)
+    sysw.stage_costs(["project"], 1)  # allocates and touches the grids
     t0 = time.time()
-    parts, nth = sysw.sample_costs(stride)
+    parts, nth = sysw.stage_costs(STAGE_CYCLE, 1)
     wall = time.time() - t0
-    per_iter = sum(v for k, v in parts.items() if k != "jacobian")
-    step_s = parts["jacobian"] + (iters_per_step + 1) * per_iter
+    step_s, per_iter = oracle_step_seconds(parts, iters_per_step)
     sysw.close()
     return {"value": susp.np / step_s, "unit": UNIT, "cores": nth, "kind": "port",
-            "sample": "oracle stage costs of one Broyden iteration of sediment_512 on 1/%d of each stage's work "
-                      "units (lines, beads, modes, filaments), scaled by %d; step = Jacobian + (%.1f+1) "
-                      "iterations; %.1f s wall" % (stride, stride, iters_per_step, wall),
-            "seconds_per_step": step_s, "stage_seconds": parts}
+            "sample": "one full-size Broyden iteration (barrier, FCM solve, forces, error check, J0^-1 "
+                      "applications) and one Jacobian build of sediment_512 by the oracle, every work unit, "
+                      "%.1f s wall; step = Jacobian + (%.2f+1) iterations, the FP64 GPU arm's mean in this run "
+                      "(the oracle takes the same counts)" % (wall, iters_per_step),
+            "seconds_per_step": step_s, "seconds_per_iteration": per_iter, "stage_seconds": parts}
+
+
+def reference_case():
+    """The workload's parameters and suspension, built on the CPU without the GPU
+    library (the oracle's restatement of the generator reproduces its bits)."""
+    import numpy as np
+    from filsim_b200.configs import sediment_params
+    from filsim_b200.suspension import Suspension
+    from oracle import oracle_py
+    p = sediment_params(WORKLOAD["npts"])
+    X, Q = oracle_py.suspension_random(p, WORKLOAD["nfil"], WORKLOAD["nw"], WORKLOAD["seed"])
+    fil_start = np.arange(WORKLOAD["nfil"] + 1, dtype=np.int32) * WORKLOAD["nw"]
+    return p, Suspension(fil_start, X, Q, kap=1.0, c=1.0)
 
 
 def run_reference(args, rank, world):
+    """The CPU restatement of the reference on this host's cores. Each step (warm-up
+    and timed) runs ONE stage of a Broyden iteration at full size, cycling through
+    barrier, spread, forward FFTs, projection, inverse FFTs, interpolation, the rest
+    of the iteration and the Jacobian build, so ms_per_step is what each step
+    really took and every 8 steps cover one complete iteration and Jacobian build.
+    value = beads / (jacobian + (iterations + 1) x iteration), with the stage times
+    averaged over the timed steps (warm-up times for stages the timed window does
+    not reach) and the iteration count of FP64_ITERS_BY_STEP over the window the GPU
+    arms time."""
     if rank != 0:
         return None
-    from filsim_b200.configs import make_sediment_case
-    p, susp = make_sediment_case(WORKLOAD["npts"], WORKLOAD["nfil"], WORKLOAD["nw"], seed=WORKLOAD["seed"])
+    import numpy as np
     from oracle import oracle_py
+    p, susp = reference_case()
     sysw = oracle_py.System(p, susp)
     sysw.initial_guess()
     sysw.filament_forces(1)
-    for _ in range(args.warmup):
-        sysw.sample_costs(args.cpu_stride)
-    times = []
+    K, W = args.steps, args.warmup
+    seen = {k: [] for k in STAGE_CYCLE}
+    warm = {k: [] for k in STAGE_CYCLE}
+    timed = []
     nth = 1
-    for _ in range(args.steps):
-        parts, nth = sysw.sample_costs(args.cpu_stride)
-        per_iter = sum(v for k, v in parts.items() if k != "jacobian")
-        times.append(parts["jacobian"] + (REFERENCE_ITERS_PER_STEP + 1) * per_iter)
-    step_s = statistics.mean(times)
+    for i in range(W + K):
+        st = STAGE_CYCLE[i % len(STAGE_CYCLE)]
+        t0 = time.perf_counter()
+        parts, nth = sysw.stage_costs([st], 1)
+        dt = time.perf_counter() - t0
+        (seen if i >= W else warm)[st].append(parts[st])
+        if i >= W:
+            timed.append(dt)
+    # fewer than one cycle of steps: the stages not reached run once more, untimed
+    for st in STAGE_CYCLE:
+        if not seen[st] and not warm[st]:
+            parts, nth = sysw.stage_costs([st], 1)
+            warm[st].append(parts[st])
+    sysw.close()
+    stage_s = {k: float(np.mean(seen[k] if seen[k] else warm[k])) for k in STAGE_CYCLE}
+    nt0 = PREP_STEPS + 1
+    window = list(range(nt0 + W, nt0 + W + K))
+    iters = float(np.mean([FP64_ITERS_BY_STEP[min(nt, len(FP64_ITERS_BY_STEP)) - 1] for nt in window]))
+    step_s, per_iter = oracle_step_seconds(stage_s, iters)
     value = susp.np / step_s
-    sample = ("CPU restatement of the reference (oracle/fs_oracle.c, OpenMP, %d threads): stage costs of one "
-              "Broyden iteration of sediment_512 on 1/%d of each stage's work units scaled back; step = Jacobian "
-              "+ (%.0f+1) iterations. The reference binary (MPI + FFTW 2.1.5 + Armadillo) is not buildable here."
-              % (nth, args.cpu_stride, REFERENCE_ITERS_PER_STEP))
-    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+    sample = ("CPU restatement of the reference (oracle/fs_oracle.c, OpenMP, %d threads; the reference binary, "
+              "MPI + FFTW 2.1.5 + Armadillo, is not buildable here), inputs from the restated generator "
+              "(oracle/or_suspension.c), no GPU library loaded. Each step is one full-size stage of a Broyden "
+              "iteration of sediment_512, cycling through %s; a simulated step costs jacobian + (%.2f+1) "
+              "iterations = %.1f s, %.2f the FP64 iteration count of steps %d-%d (bench.py FP64_ITERS_BY_STEP)"
+              % (nth, ", ".join(STAGE_CYCLE), iters, step_s, iters, window[0], window[-1]))
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": float(np.mean(timed)) * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded rejection-placed filaments)",
             "config": {"workload": WORKLOAD["name"], "grid": [WORKLOAD["npts"]] * 3,
-                       "filaments": WORKLOAD["nfil"], "beads_per_filament": WORKLOAD["nw"], "beads": susp.np},
+                       "filaments": WORKLOAD["nfil"], "beads_per_filament": WORKLOAD["nw"], "beads": susp.np,
+                       "timed_steps": [window[0], window[-1]]},
             "impl": "reference",
+            "steps_are": "one full-size oracle stage per step (cycle of %d: %s)" % (len(STAGE_CYCLE),
+                                                                                    ", ".join(STAGE_CYCLE)),
+            "seconds_per_simulated_step": step_s, "seconds_per_iteration": per_iter,
+            "iters_per_step": iters, "stage_seconds": stage_s,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
@@ -749,6 +875,8 @@ def main():
         out = run_ensemble(args, rank, world)
     elif args.workload == "mlp":
         out = run_mlp(args, rank, world) if rank == 0 else None
+    elif args.workload == "trajectory_200":
+        out = run_trajectory(args, rank, world) if rank == 0 else None
     else:
         out = run_ours(args, rank, world)
     if rank == 0 and out is not None:

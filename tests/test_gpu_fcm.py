@@ -263,3 +263,36 @@ def test_too_many_beads_rejected():
     fcm = Fcm(ctx, 3)
     with pytest.raises(abi.FsError):
         fcm.mobility_solve()
+
+
+@pytest.mark.parametrize("shape,nfil,nw,seed", [((32, 32, 32), 6, 3, 41), ((48, 32, 64), 8, 4, 42)])
+def test_reference_default_stencil_ngd20(oracle, gpu_lib, shape, nfil, nw, seed):
+    """The reference's own stencil: ngd = 20 points per axis with dx = sigma_dip / 1.5
+    (config_template.hpp:76, multi_filament_header.hpp:48), where a stencil reaches
+    three 16-point tiles per axis. FP64 within 1e-10 of the oracle, FP32 within 1e-5
+    of FP64, including beads outside the box."""
+    from filsim_b200.abi import make_params
+    from filsim_b200.suspension import random_forces, random_suspension, fcm_positions
+    p = make_params(shape, ngd=20)
+    assert abs(p.dx - p.sigma_dip / 1.5) < 1e-15
+    s = random_suspension(p, nfil, nw, seed, min_sep=1.5)
+    F, T = random_forces(s.np, seed + 1)
+    X = s.X.copy()
+    X[::3] -= np.array(shape) * p.dx  # negative coordinates
+    Y = fcm_positions(p, X)
+    V0, W0 = oracle.fcm_mobility(p, Y, F, T)
+    V, W = gpu_mobility(p, Y, F, T)
+    assert rel_err(V, V0) < FP64_REL
+    assert rel_err(W, W0) < FP64_REL
+    V32, W32 = gpu_mobility(p, Y, F, T, abi.FS_PREC_FP32)
+    assert rel_err(V32, V) < FP32_REL
+    assert rel_err(W32, W) < FP32_REL
+
+
+def test_stencil_limits_are_checked(gpu_lib):
+    """ngd above 20, or above a grid dimension, is rejected at context creation."""
+    from filsim_b200.abi import FsError, make_params
+    for shape, ngd in (((32, 32, 32), 21), ((16, 32, 32), 20)):
+        with pytest.raises(FsError) as e:
+            Context(make_params(shape, ngd=ngd), max_beads=4)
+        assert e.value.status == abi.FS_ERR_INVALID_ARG

@@ -73,7 +73,10 @@ def test_error_check_apply_update_step(oracle, small):
     e0, c0 = sysw.error_check(V, W, nt)
     e1, c1 = sim.error_check(V, W, nt)
     assert c0 == c1
-    assert rel(e1.cpu().numpy(), e0) < 1e-12
+    # Err = Xs - 4/3 X + 1/3 Xt - 2/3 dt V cancels positions of size L (17 here)
+    # down to ~1e-3: a rounding difference of the GPU's contracted arithmetic
+    # (~1e-16 L) shows as ~1e-12 of max |Err|
+    assert rel(e1.cpu().numpy(), e0) < 1e-11
     # history columns then the bad-Broyden apply
     n6 = 6 * s2.np
     C = rng.standard_normal((2, n6))
