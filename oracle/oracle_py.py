@@ -16,8 +16,83 @@ _SO = os.path.join(_DIR, "_build", "libfs_oracle.so")
 _lib = None
 
 
+_REF_DIR = os.path.join(_DIR, "_ref")
+REFERENCE_TREE = "/root/reference"
+
+
 def build():
     subprocess.run(["make", "-s", "-C", _DIR], check=True)
+    # the reference's own FCM and barrier sources, where the FilSim tree is present
+    if os.path.isdir(REFERENCE_TREE):
+        subprocess.run(["make", "-s", "-C", os.path.join(_DIR, "refshim"), "REF=" + REFERENCE_TREE], check=True)
+
+
+# ---- the reference pin: the reference's own sources built by oracle/refshim ----
+REF_FCM_CASES = {  # library tag -> (grid, ngd, dx rule)
+    "fcm_64_ngd12": ((64, 64, 64), 12, "a/1.86"),
+    "fcm_32_ngd20": ((32, 32, 32), 20, "sigma_dip/1.5"),
+    "fcm_48x32x64_ngd20": ((48, 32, 64), 20, "sigma_dip/1.5"),
+}
+_ref_libs = {}
+
+
+def ref_available(tag):
+    return os.path.exists(os.path.join(_REF_DIR, "libref_%s.so" % tag))
+
+
+def _ref_lib(tag):
+    if tag not in _ref_libs:
+        path = os.path.join(_REF_DIR, "libref_%s.so" % tag)
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        L = ctypes.CDLL(path)
+        vp = ctypes.c_void_p
+        L.ref_fcm_config.argtypes = [vp, vp]
+        L.ref_fcm_mobility.restype = ctypes.c_int
+        L.ref_fcm_mobility.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp]
+        if hasattr(L, "ref_barrier"):
+            L.ref_barrier.restype = ctypes.c_int
+            L.ref_barrier.argtypes = [ctypes.c_int, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp, vp]
+        _ref_libs[tag] = L
+    return _ref_libs[tag]
+
+
+def ref_config(tag):
+    """(grid, ngd, dx) the reference library was compiled for."""
+    L = _ref_lib(tag)
+    cfg = np.zeros(4, dtype=np.int32)
+    dx = ctypes.c_double()
+    L.ref_fcm_config(_ptr(cfg), ctypes.byref(dx))
+    return tuple(int(v) for v in cfg[:3]), int(cfg[3]), dx.value
+
+
+def ref_fcm_mobility(tag, Y, F, T):
+    """Fcm::initialise + Fcm::mobility_solve of the reference's own code."""
+    L = _ref_lib(tag)
+    Y, F, T = _f64(Y), _f64(F), _f64(T)
+    V = np.zeros_like(Y)
+    W = np.zeros_like(Y)
+    st = L.ref_fcm_mobility(Y.shape[0], _ptr(Y), _ptr(F), _ptr(T), _ptr(V), _ptr(W))
+    assert st == 0
+    return V, W
+
+
+def ref_barrier(tag, fil_start, Xs, Y, F, nt):
+    """LinkedList::initialise, link and apply_collision_barrier of the reference's
+    own code; returns (F after, head, list, min_dist2)."""
+    L = _ref_lib(tag)
+    fil_start = np.ascontiguousarray(fil_start, dtype=np.int32)
+    Xs, Y = _f64(Xs), _f64(Y)
+    F = _f64(F).copy()
+    np_ = int(fil_start[-1])
+    head = np.zeros(1 << 20, dtype=np.int32)
+    lst = np.zeros(max(np_, 1), dtype=np.int32)
+    nc = ctypes.c_int()
+    md = ctypes.c_double()
+    st = L.ref_barrier(len(fil_start) - 1, _ptr(fil_start), _ptr(Xs), _ptr(Y), _ptr(F), nt, _ptr(head), _ptr(lst),
+                       ctypes.byref(nc), ctypes.byref(md))
+    assert st == 0, st
+    return F, head[: nc.value].copy(), lst[:np_].copy(), md.value
 
 
 def lib():
