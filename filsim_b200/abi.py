@@ -65,7 +65,7 @@ class FsDiag(ctypes.Structure):
 STAGES = ["spread", "fft_fwd", "project", "fft_inv", "interp", "link", "barrier", "forces", "jacobian",
           "error_check", "broyden", "update", "friction", "learn",
           # single kernels inside the stages above
-          "k_spread", "k_fft_z_fwd", "k_fft_y_fwd", "k_fft_y_inv", "k_fft_z_inv"]
+          "k_spread", "k_fft_z_fwd", "k_fft_y_fwd", "k_fft_y_inv", "k_fft_z_inv", "k_interp"]
 FS_STAGE_COUNT = 32
 
 
@@ -216,6 +216,12 @@ def _declare(L):
         "fs_learn_targets": (c_int, [c_void_p, c_void_p]),
         "fs_set_warm_start": (c_int, [c_void_p, c_int]),
         "fs_warm_start_gate": (c_int, [c_void_p, c_int]),
+        "fs_warm_start_bound": (c_int, [c_void_p, c_int]),
+        "fs_set_slab": (c_int, [c_void_p, c_int, c_int]),
+        "fs_fcm_interpolate": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+        "fs_slab_forward_yz": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
+        "fs_slab_solve_x": (c_int, [c_void_p, c_void_p, c_int, c_int]),
+        "fs_slab_inverse_yz": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
         "fs_warm_start_gate_stats": (c_int, [c_void_p, c_void_p, c_void_p]),
         "fs_set_graph_mode": (c_int, [c_void_p, c_int]),
         "fs_autotune": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),

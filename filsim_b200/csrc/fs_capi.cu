@@ -42,7 +42,9 @@ fs_status validate_params(const fs_params *p) {
   const int n[3] = {p->npts_x, p->npts_y, p->npts_z};
   for (int d = 0; d < 3; ++d)
     if (n[d] < FS_TILE || n[d] % FS_TILE != 0) return FS_ERR_INVALID_ARG;  // grids are whole 16^3 tiles
-  if (p->ngd < 2 || p->ngd > 16) return FS_ERR_INVALID_ARG;                // stencil fits a staged tile row
+  if (p->ngd < 2 || p->ngd > FS_NGD_MAX) return FS_ERR_INVALID_ARG;
+  for (int d = 0; d < 3; ++d)
+    if (n[d] < p->ngd) return FS_ERR_INVALID_ARG;  // a stencil never wraps onto itself
   if (!(p->dx > 0) || !(p->a > 0) || !(p->mu > 0) || !(p->sigma > 0) || !(p->sigma_dip > 0)) return FS_ERR_INVALID_ARG;
   if (!(p->cell_width > 0) || !(p->dt > 0) || !(p->dl > 0)) return FS_ERR_INVALID_ARG;
   if (p->broyden_maxiter < 1 || p->broyden_maxiter > 100000) return FS_ERR_INVALID_ARG;
@@ -233,6 +235,7 @@ fs_status fs_create(const fs_params *p, int max_beads, int max_filaments, void *
   if (!c) return FS_ERR_OOM;
   c->p = *p;
   c->device = dev;
+  c->num_sms = prop.multiProcessorCount;
   c->max_beads = max_beads;
   c->max_fil = max_filaments;
   c->precision = p->precision;
@@ -291,6 +294,7 @@ fs_status fs_destroy(fs_ctx *c) {
   mlp_free(c);
   cudaFree(c->gemm_err);
   fcm_free(c);
+  slab_free(c);
   cells_free(c);
   free_state(c);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);

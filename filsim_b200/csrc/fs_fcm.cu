@@ -24,6 +24,7 @@ namespace {
 
 struct FcmConsts {
   int N[3];
+  int gnx, x0;  // x extent of the whole box and the grid's first plane in it (a slab window; else N[0], 0)
   int ngd, ngdh;
   int nbin[3];
   double dx;
@@ -52,7 +53,10 @@ __global__ void k_fcm_bin_keys(const double *__restrict__ Y, int np, FcmConsts c
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     int xc = (int)(Y[3 * b + d] / c.dx);
-    int sw = wrap_int(xc - c.ngdh + 1, c.N[d]);
+    // the stencil start in the whole box, then in this grid (a slab window holds the
+    // beads whose x start lies in its own planes; others are clamped, never out of range)
+    int sw = wrap_int(xc - c.ngdh + 1, d == 0 ? c.gnx : c.N[d]) - (d == 0 ? c.x0 : 0);
+    sw = sw < 0 ? 0 : (sw >= c.N[d] ? c.N[d] - 1 : sw);
     sw_out[3 * b + d] = sw;
     bi[d] = sw / FS_TILE;
   }
@@ -126,17 +130,17 @@ __global__ void __launch_bounds__(FS_SPREAD_THREADS)
   const int tile = blockIdx.x;
   const int tz = tile % c.nbin[2], ty = (tile / c.nbin[2]) % c.nbin[1], tx = tile / (c.nbin[2] * c.nbin[1]);
   const int X0[3] = {tx * FS_TILE, ty * FS_TILE, tz * FS_TILE};
-  // candidate bins per axis: the tile's own bin and the one before it
-  int cb[3][2], ncb[3];
+  // candidate bins per axis: the tile's own bin and the ones before it that a
+  // stencil reaches (fs_cand_bins), each bin once on an axis with fewer bins
+  int cb[3][3], ncb[3];
   const int tb[3] = {tx, ty, tz};
+  const int K = fs_cand_bins(c.ngd);
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    cb[d][0] = wrap_int(tb[d] - 1, c.nbin[d]);
-    cb[d][1] = tb[d];
-    ncb[d] = (c.nbin[d] > 1) ? 2 : 1;
-    if (ncb[d] == 1) cb[d][0] = tb[d];
+    ncb[d] = min(K, c.nbin[d]);
+    for (int j = 0; j < ncb[d]; ++j) cb[d][j] = wrap_int(tb[d] - (ncb[d] - 1 - j), c.nbin[d]);
   }
-  int rs[8], re[8], nr = 0, total = 0;
+  int rs[27], re[27], nr = 0, total = 0;
   for (int a = 0; a < ncb[0]; ++a)
     for (int b2 = 0; b2 < ncb[1]; ++b2)
       for (int e = 0; e < ncb[2]; ++e) {
@@ -336,11 +340,11 @@ __global__ void k_spread_records32(const double *__restrict__ Y, const double *_
   rec[t] = v;
 }
 
-constexpr int FS_SPREAD32_REC_MAX = 3 + 3 * 16;  // record length for the largest ngd
 
+// the chunk's records (slot sl at sl RL, copied as they are) follow the tables
+// in dynamic shared memory: spread32_smem(ngd) bytes in all
 template <int CH>
 struct SpreadStage32 {
-  float4 raw[CH * FS_SPREAD32_REC_MAX];      // the chunk's records (slot sl at sl RL), copied as they are
   float4 xw[CH][FS_TILE];                    // (g, d, r, -) by tile-local x
   float zg[CH][FS_TILE], zd[CH][FS_TILE], zr[CH][FS_TILE];  // by tile-local z
   float4 yw[CH][FS_TILE];                    // (g, g, d, d) by tile-local y
@@ -350,36 +354,45 @@ struct SpreadStage32 {
 };
 
 template <int CH>
+__host__ __device__ constexpr size_t spread32_smem(int ngd) {
+  return (sizeof(SpreadStage32<CH>) + 15) / 16 * 16 + sizeof(float4) * CH * (size_t)spread_rec_len(ngd);
+}
+
+template <int CH>
 __global__ void __launch_bounds__(FS_SPREAD32_THREADS, 3)
     k_spread32(const int *__restrict__ bin_start, const float4 *__restrict__ rec, FcmConsts c,
                float *__restrict__ fgrid) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SpreadStage32<CH> &st = *reinterpret_cast<SpreadStage32<CH> *>(smem_raw);
+  float4 *const raw = reinterpret_cast<float4 *>(smem_raw + (sizeof(SpreadStage32<CH>) + 15) / 16 * 16);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int tile = blockIdx.x;
   const int tz = tile % c.nbin[2], ty = (tile / c.nbin[2]) % c.nbin[1], tx = tile / (c.nbin[2] * c.nbin[1]);
   const int X0[3] = {tx * FS_TILE, ty * FS_TILE, tz * FS_TILE};
-  // candidate bins, the tile's own bin and the one before it per axis, in the
-  // order (x, y, z) of k_spread; thread r < 8 reads combination r (empty when an
-  // axis has a single bin and the combination repeats it)
-  __shared__ int cand_rs[8], cand_len[8];
-  if (tid < 8) {
+  // candidate bins, the tile's own bin and the ones before it that a stencil
+  // reaches (fs_cand_bins: K per axis), in the order (x, y, z) of k_spread;
+  // thread r < K^3 reads combination r: per axis digit p in [0, K) names the bin
+  // K - 1 - p before the tile's own (empty when it would repeat a bin on an axis
+  // with fewer than K bins)
+  __shared__ int cand_rs[27], cand_len[27];
+  const int K = fs_cand_bins(c.ngd), nr = K * K * K;
+  if (tid < nr) {
     const int tb[3] = {tx, ty, tz};
-    const int pick[3] = {tid >> 2, (tid >> 1) & 1, tid & 1};
+    const int pick[3] = {tid / (K * K), (tid / K) % K, tid % K};
     int bin = 0;
     bool valid = true;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      valid = valid && (pick[d] == 1 || c.nbin[d] > 1);
-      bin = bin * c.nbin[d] + (pick[d] == 1 ? tb[d] : wrap_int(tb[d] - 1, c.nbin[d]));
+      const int back = K - 1 - pick[d];
+      valid = valid && back < c.nbin[d];
+      bin = bin * c.nbin[d] + wrap_int(tb[d] - back, c.nbin[d]);
     }
     cand_rs[tid] = valid ? bin_start[bin] : 0;
     cand_len[tid] = valid ? bin_start[bin + 1] - bin_start[bin] : 0;
   }
   __syncthreads();
   int total = 0;
-#pragma unroll
-  for (int r = 0; r < 8; ++r) total += cand_len[r];
+  for (int r = 0; r < nr; ++r) total += cand_len[r];
   const int ngd = c.ngd, RL = spread_rec_len(ngd);
   // staging of candidates [base, base + nb): records to shared memory (slot sl at
   // sl RL) with 16-byte asynchronous copies, one contiguous run per candidate bin,
@@ -390,11 +403,11 @@ __global__ void __launch_bounds__(FS_SPREAD32_THREADS, 3)
     {
       int pre = 0;  // candidates before bin range r
 #pragma unroll 1
-      for (int r = 0; r < 8; ++r) {
+      for (int r = 0; r < nr; ++r) {
         const int lo = max(pre, base), hi = min(pre + cand_len[r], base + nb);
         if (lo < hi) {
           const float4 *src = rec + (size_t)(cand_rs[r] + lo - pre) * RL;
-          const unsigned dst = (unsigned)__cvta_generic_to_shared(&st.raw[(lo - base) * RL]);
+          const unsigned dst = (unsigned)__cvta_generic_to_shared(&raw[(lo - base) * RL]);
           for (int e = tid; e < (hi - lo) * RL; e += FS_SPREAD32_THREADS)
             asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + 16 * e), "l"(src + e) : "memory");
         }
@@ -410,7 +423,7 @@ __global__ void __launch_bounds__(FS_SPREAD32_THREADS, 3)
       const bool act = sl < nb;
       bool cov[6] = {false, false, false, false, false, false};
       if (act) {
-        const float4 *rw = st.raw + sl * RL;
+        const float4 *rw = raw + sl * RL;
         const float4 hd = rw[0];
         const int swv[3] = {__float_as_int(hd.x), __float_as_int(hd.y), __float_as_int(hd.z)};
         float4 w[6];
@@ -493,8 +506,8 @@ __global__ void __launch_bounds__(FS_SPREAD32_THREADS, 3)
           const float2 gz = *reinterpret_cast<const float2 *>(&st.zg[sl][zl]);
           const float2 dz = *reinterpret_cast<const float2 *>(&st.zd[sl][zl]);
           const float2 rz = *reinterpret_cast<const float2 *>(&st.zr[sl][zl]);
-          const float4 fh = st.raw[sl * RL + 1];  // F0, F1, F2, h0 (h = T / 2, GA_setup :536-547)
-          const float4 hh = st.raw[sl * RL + 2];  // h1, h2
+          const float4 fh = raw[sl * RL + 1];  // F0, F1, F2, h0 (h = T / 2, GA_setup :536-547)
+          const float4 hh = raw[sl * RL + 2];  // h1, h2
           // per z of the pair: f_a = F_a gx gz, the rotlet factors of k_spread (d = gdx gdz)
           const float gxz0 = wx.x * gz.x, gxz1 = wx.x * gz.y;
           const float dxz0 = wx.y * dz.x, dxz1 = wx.y * dz.y;
@@ -642,8 +655,8 @@ __global__ void k_project_planes(typename Cplx<R>::T *__restrict__ fh, size_t NH
 // ---- 6. interpolation -------------------------------------------------------
 template <typename R>
 struct InterpWarp {
-  R g[3][16], gd[3][16], r[3][16];
-  int ind[3][16];
+  R g[3][FS_NGD_MAX], gd[3][FS_NGD_MAX], r[3][FS_NGD_MAX];
+  int ind[3][FS_NGD_MAX];
 };
 template <typename R>
 struct __align__(4 * sizeof(R)) XY4 {
@@ -677,8 +690,8 @@ __global__ void __launch_bounds__(32 * WPB) k_interp(const R *__restrict__ u, co
   InterpWarp<R> &s = *reinterpret_cast<InterpWarp<R> *>(base);
   XY4<R> *xy = reinterpret_cast<XY4<R> *>(base + interp_xy_offset<R>());
   long long *off = reinterpret_cast<long long *>(xy + n2);
-  for (int it = lane; it < 3 * 16; it += 32) {
-    const int a = it >> 4, i = it & 15;
+  for (int a = 0; a < 3; ++a) {  // lane i < ngd <= 20 takes stencil index i of each axis
+    const int i = lane;
     if (i >= ngd) continue;
     const double Yv = Y[3 * b + a];
     const int xc = (int)(Yv / c.dx);
@@ -755,6 +768,7 @@ __global__ void __launch_bounds__(32 * WPB) k_interp(const R *__restrict__ u, co
   }
 }
 
+
 template <typename A, typename B>
 __global__ void k_convert(const A *__restrict__ in, B *__restrict__ out, size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -775,6 +789,8 @@ FcmConsts make_consts(const fs_ctx *c) {
   k.N[0] = c->nx;
   k.N[1] = c->ny;
   k.N[2] = c->nz;
+  k.gnx = c->slab_nx > 0 ? c->slab_nx : c->nx;
+  k.x0 = c->slab_nx > 0 ? c->slab_x0 : 0;
   k.ngd = c->p.ngd;
   k.ngdh = c->p.ngd / 2;
   for (int d = 0; d < 3; ++d) k.nbin[d] = c->nbin[d];
@@ -866,10 +882,10 @@ fs_status spread_t(fs_ctx *c, const FcmConsts &k, const double *Y, const double 
     }
     ProfScope pk(c, FS_STAGE_K_SPREAD);
     if (c->tune_spread_chunk == 32)
-      k_spread32<32><<<c->nbins, FS_SPREAD32_THREADS, sizeof(SpreadStage32<32>), c->stream>>>(
+      k_spread32<32><<<c->nbins, FS_SPREAD32_THREADS, spread32_smem<32>(k.ngd), c->stream>>>(
           c->bins.start, rec, k, (float *)c->grid_real);
     else
-      k_spread32<64><<<c->nbins, FS_SPREAD32_THREADS, sizeof(SpreadStage32<64>), c->stream>>>(
+      k_spread32<64><<<c->nbins, FS_SPREAD32_THREADS, spread32_smem<64>(k.ngd), c->stream>>>(
           c->bins.start, rec, k, (float *)c->grid_real);
   } else if (c->tune_spread_chunk == 32) {
     ProfScope pk(c, FS_STAGE_K_SPREAD);
@@ -884,6 +900,26 @@ fs_status spread_t(fs_ctx *c, const FcmConsts &k, const double *Y, const double 
   return FS_OK;
 }
 
+// interpolation of U, Omega from the velocity grid in c->grid_real (R precision); the
+// beads must have been binned (k_fcm_bin_keys + sort) for this Y
+template <typename R>
+fs_status interp_t(fs_ctx *c, const FcmConsts &k, const double *Y, double *V, double *W, int np) {
+  if (np <= 0) return FS_OK;
+  ProfScope ps(c, FS_STAGE_INTERP);
+  ProfScope pk(c, FS_STAGE_K_INTERP);
+  const R *ug = (const R *)c->grid_real;
+  const size_t wb = interp_warp_bytes<R>(c->p.ngd);
+  const int wpb = (c->tune_interp_wpb == 16 && 16 * wb > FS_SMEM_MAX) ? 8 : c->tune_interp_wpb;
+  if (wpb == 4)
+    k_interp<R, 4><<<fs_blocks(np, 4), 128, 4 * wb, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V, W);
+  else if (wpb == 16)
+    k_interp<R, 16><<<fs_blocks(np, 16), 512, 16 * wb, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V, W);
+  else
+    k_interp<R, 8><<<fs_blocks(np, 8), 256, 8 * wb, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V, W);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
 template <typename R>
 fs_status mobility_t(fs_ctx *c, const double *Y, const double *F, const double *T, double *V, double *W, int np) {
   FcmConsts k = make_consts(c);
@@ -892,19 +928,7 @@ fs_status mobility_t(fs_ctx *c, const double *Y, const double *F, const double *
     FS_TRY(spread_t<R>(c, k, Y, F, T, np));
   }
   FS_TRY(flow_solve_t<R>(c));
-  if (np > 0) {
-    ProfScope ps(c, FS_STAGE_INTERP);
-    const R *ug = (const R *)c->grid_real;
-    const size_t wb = interp_warp_bytes<R>(c->p.ngd);
-    if (c->tune_interp_wpb == 4)
-      k_interp<R, 4><<<fs_blocks(np, 4), 128, 4 * wb, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V, W);
-    else if (c->tune_interp_wpb == 16)
-      k_interp<R, 16><<<fs_blocks(np, 16), 512, 16 * wb, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V,
-                                                                      W);
-    else
-      k_interp<R, 8><<<fs_blocks(np, 8), 256, 8 * wb, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V, W);
-    FS_LAUNCH_CHECK();
-  }
+  FS_TRY(interp_t<R>(c, k, Y, V, W, np));
   c->last_grid_prec = sizeof(R) == 8 ? FS_PREC_FP64 : FS_PREC_FP32;
   return FS_OK;
 }
@@ -928,14 +952,15 @@ fs_status fcm_init(fs_ctx *c) {
   FS_CUDA(cudaMalloc(&c->bead_sw, sizeof(int) * 3 * (size_t)(c->max_beads > 0 ? c->max_beads : 1)));
   c->bytes += sizeof(int) * 3 * (size_t)c->max_beads;
   {
-    const size_t nw = (size_t)(c->max_beads > 0 ? c->max_beads : 1) * spread_rec_len(c->p.ngd);
+    const size_t nb = (size_t)(c->max_beads > 0 ? c->max_beads : 1);
+    const size_t nw = nb * spread_rec_len(c->p.ngd);
     FS_CUDA(cudaMalloc(&c->spread_wb, sizeof(float4) * nw));
     c->bytes += sizeof(float4) * nw;
   }
   FS_CUDA(cudaFuncSetAttribute(k_spread32<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)sizeof(SpreadStage32<64>)));
+                               (int)spread32_smem<64>(FS_NGD_MAX)));
   FS_CUDA(cudaFuncSetAttribute(k_spread32<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)sizeof(SpreadStage32<32>)));
+                               (int)spread32_smem<32>(FS_NGD_MAX)));
   FS_CUDA(cudaFuncSetAttribute(k_spread<double, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(SpreadStage<double, 64>)));
   FS_CUDA(cudaFuncSetAttribute(k_spread<float, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -945,19 +970,16 @@ fs_status fcm_init(fs_ctx *c) {
   FS_CUDA(cudaFuncSetAttribute(k_spread<float, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(SpreadStage<float, 32>)));
   {
-    const int nd = 16;  // largest ngd
-    FS_CUDA(cudaFuncSetAttribute(k_interp<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(4 * interp_warp_bytes<double>(nd))));
-    FS_CUDA(cudaFuncSetAttribute(k_interp<double, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(8 * interp_warp_bytes<double>(nd))));
-    FS_CUDA(cudaFuncSetAttribute(k_interp<double, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(16 * interp_warp_bytes<double>(nd))));
-    FS_CUDA(cudaFuncSetAttribute(k_interp<float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(4 * interp_warp_bytes<float>(nd))));
-    FS_CUDA(cudaFuncSetAttribute(k_interp<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(8 * interp_warp_bytes<float>(nd))));
-    FS_CUDA(cudaFuncSetAttribute(k_interp<float, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(16 * interp_warp_bytes<float>(nd))));
+    // the attribute is per kernel, shared by every context: set for the largest
+    // ngd (capped at what a CTA may ask for; larger launches take 8 warps per CTA)
+    const size_t wd = interp_warp_bytes<double>(FS_NGD_MAX), wf = interp_warp_bytes<float>(FS_NGD_MAX);
+    auto cap = [](size_t b) { return (int)(b < (size_t)FS_SMEM_MAX ? b : (size_t)FS_SMEM_MAX); };
+    FS_CUDA(cudaFuncSetAttribute(k_interp<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap(4 * wd)));
+    FS_CUDA(cudaFuncSetAttribute(k_interp<double, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap(8 * wd)));
+    FS_CUDA(cudaFuncSetAttribute(k_interp<double, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap(16 * wd)));
+    FS_CUDA(cudaFuncSetAttribute(k_interp<float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap(4 * wf)));
+    FS_CUDA(cudaFuncSetAttribute(k_interp<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap(8 * wf)));
+    FS_CUDA(cudaFuncSetAttribute(k_interp<float, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap(16 * wf)));
   }
   c->tune_spread_chunk = 64;
   c->tune_interp_wpb = 8;
@@ -1006,6 +1028,26 @@ fs_status fcm_friction(fs_ctx *c, const double *F, const double *T, double *V, d
     k_friction<<<fs_blocks(3 * np, 256), 256, 0, c->stream>>>(F, T, V, W, 3 * np, a1, a2);
     FS_LAUNCH_CHECK();
   }
+  return FS_OK;
+}
+
+fs_status fcm_interpolate_only(fs_ctx *c, const double *u, const double *Y, int np, double *V, double *W) {
+  FcmConsts k = make_consts(c);
+  const size_t n = 3 * c->N;
+  if (np > 0) {
+    k_fcm_bin_keys<<<fs_blocks(np, 256), 256, 0, c->stream>>>(Y, np, k, c->bins.key, c->bead_sw);
+    FS_LAUNCH_CHECK();
+  }
+  FS_TRY(fs_sort_run(&c->bins, np, c->stream));
+  if (c->precision == FS_PREC_FP32) {
+    k_convert<double, float><<<fs_blocks((long long)n, 256), 256, 0, c->stream>>>(u, (float *)c->grid_real, n);
+    FS_LAUNCH_CHECK();
+    FS_TRY(interp_t<float>(c, k, Y, V, W, np));
+  } else {
+    FS_CUDA(cudaMemcpyAsync(c->grid_real, u, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    FS_TRY(interp_t<double>(c, k, Y, V, W, np));
+  }
+  c->last_grid_prec = -1;
   return FS_OK;
 }
 

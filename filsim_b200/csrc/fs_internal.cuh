@@ -12,6 +12,13 @@
 
 // Spread tile edge (grid points); spread bins have the same width.
 #define FS_TILE 16
+// largest Gaussian support per axis (the reference's default, config_template.hpp:76)
+#define FS_NGD_MAX 20
+// dynamic shared memory a CTA may ask for on sm_100 (227 KB)
+#define FS_SMEM_MAX (227 * 1024)
+// spread bins per axis whose beads can reach a tile: a stencil of ngd points
+// starting in bin t - k reaches tile t when 16 k <= ngd + 14
+__host__ __device__ inline int fs_cand_bins(int ngd) { return (ngd + 14) / FS_TILE + 1; }
 // Beads staged in shared memory per spread pass (a multiple of 32).
 #define FS_SPREAD_CHUNK 64
 // Collision events kept per bead (pairs inside the barrier range).
@@ -75,6 +82,9 @@ struct fs_ctx {
   int *pair_count, *pair_off, *pair_scan_tmp;
   int cells_np;        // beads in the last link (-1: none)
   bool min_dist2_valid;  // a barrier has written min_dist2_bits
+  int num_sms;           // streaming multiprocessors of the context's device
+  int slab_x0, slab_nx;  // slab window: first plane and x extent of the whole box (0: not a window)
+  struct fs_slab_plans *slab;  // cuFFT plans and scratch of the slab transforms (fs_slab.cu)
   double *min_dist2;   // device scalar
   unsigned long long *min_dist2_bits;
 
@@ -171,6 +181,8 @@ fs_status fcm_mobility(fs_ctx *c, const double *Y, const double *F, const double
 fs_status fcm_friction(fs_ctx *c, const double *F, const double *T, double *V, double *W, int np);
 fs_status fcm_flow_solve_only(fs_ctx *c, const double *f, double *u);
 fs_status fcm_spread_only(fs_ctx *c, const double *Y, const double *F, const double *T, int np, double *f);
+fs_status fcm_interpolate_only(fs_ctx *c, const double *u, const double *Y, int np, double *V, double *W);
+void slab_free(fs_ctx *c);
 
 bool fft32_supported(const fs_ctx *c);
 fs_status fft32_init(fs_ctx *c);

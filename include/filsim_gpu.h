@@ -65,7 +65,7 @@ enum { FS_PREC_FP64 = 0, FS_PREC_FP32 = 1 };
  */
 typedef struct fs_params {
   int npts_x, npts_y, npts_z;   /* NPTS_X/Y/Z: periodic FCM grid */
-  int ngd;                      /* Gaussian support points per axis (reference `ngd`) */
+  int ngd;                      /* Gaussian support points per axis (reference `ngd`), 2..20, at most the grid size */
   double a;                     /* bead radius (FCM kernels, drag) */
   double ah;                    /* radius of bead 0 of each filament (Jacobian, `ah`) */
   double mu;                    /* viscosity MU */
@@ -206,6 +206,34 @@ fs_status fs_collision_barrier(fs_ctx *ctx, const double *Y, double *F_inout, in
 fs_status fs_collision_pairs(fs_ctx *ctx, const double *Y, int np, int nt,
                              const int *fil_id, const int *seg_id,
                              int *pairs_h, int max_pairs, int *npairs_h);
+
+/* ---- one box over several ranks: x slabs ------------------------------------ */
+
+/* The pieces of an FCM mobility solve split over ranks by x slabs, as the
+ * reference splits it with FFTW-MPI (FCMfunctions.cpp:16-23, 360-406, 460-461);
+ * filsim_b200/slab.py drives them and makes the exchanges between ranks.
+ * A rank owning planes [x0, x0 + nxs) of an nx_box-plane box creates its context
+ * for a WINDOW of nxs + H planes (H >= ngd - 1) and calls fs_set_slab(ctx, x0,
+ * nx_box): fs_fcm_spread and fs_fcm_interpolate then take the beads whose
+ * stencil starts in the rank's planes (others are clamped into the window, not
+ * spread correctly: the caller passes only its own beads). nx_box = 0 ends
+ * slab mode. */
+fs_status fs_set_slab(fs_ctx *ctx, int x0, int nx_box);
+/* particle_velocities + particle_rotations (FCMfunctions.cpp:740-808) from a
+ * given velocity grid u (device, 3 x the context's grid, component-major, z
+ * fastest) in the context's precision. */
+fs_status fs_fcm_interpolate(fs_ctx *ctx, const double *u, const double *Y, int np, double *V, double *W);
+/* Slab transforms (FP64; complex values as (re, im) double pairs):
+ * forward: f [3][nxs][Ny][Nz] real -> spec [3][nxs][Nz/2+1][Ny], z real-to-complex
+ * then y; solve_x: spec_t [3][nkz][Ny][Nx] (the rank's kz range [kz0, kz0 + nkz),
+ * every x) -> forward x, the projection of flow_solve (FCMfunctions.cpp:648-736),
+ * inverse x, in place; inverse: spec (consumed) -> u [3][nxs][Ny][Nz], inverse
+ * y, the imaginary parts of kz = 0 and kz = Nz/2 dropped (the reference's
+ * halfcomplex inverse), real inverse z. Unnormalised but for the projection's
+ * 1/(Nx Ny Nz), as the reference. Require fs_set_slab. */
+fs_status fs_slab_forward_yz(fs_ctx *ctx, const double *f, int nxs, double *spec);
+fs_status fs_slab_solve_x(fs_ctx *ctx, double *spec_t, int kz0, int nkz);
+fs_status fs_slab_inverse_yz(fs_ctx *ctx, double *spec, int nxs, double *u);
 
 /* ---- collision barrier without device allocation --------------------------- */
 
@@ -379,6 +407,7 @@ enum {
   FS_STAGE_K_FFT_Y_FWD = 16, /* FP32 transform: the forward pass over y lines */
   FS_STAGE_K_FFT_Y_INV = 17, /* FP32 transform: the inverse pass over y lines */
   FS_STAGE_K_FFT_Z_INV = 18, /* FP32 transform: the inverse pass over z lines */
+  FS_STAGE_K_INTERP = 19,   /* the interpolation kernel alone (FP32: the tile pass, not the per-bead sums) */
   FS_STAGE_COUNT = 32
 };
 typedef struct fs_profile {
@@ -461,6 +490,16 @@ fs_status fs_set_warm_start(fs_ctx *ctx, int mode);
  * Broyden iterations than its own extra solves. period 0 (the default) runs the
  * learned start every step. Resets the statistics. */
 fs_status fs_warm_start_gate(fs_ctx *ctx, int period);
+/* Carried bound of the learned start's fallback (no reference counterpart):
+ * with refresh > 0, only every refresh-th learned step solves both starts (and
+ * puts back, in that step, each filament whose learned first residual is
+ * worse); it keeps each filament's plain-start first residual. The learned
+ * steps in between cost one mobility solve: they solve the learned start
+ * alone, and a filament whose first residual exceeds its carried plain one
+ * takes the plain start from the next step until the next comparison. The
+ * Broyden loop and its convergence test are unchanged. refresh 0 (the
+ * default) compares with the plain start on every learned step. */
+fs_status fs_warm_start_bound(fs_ctx *ctx, int refresh);
 /* steps_h[2], solves_h[2]: steps run and running mean solves per step, [0] plain
  * start, [1] learned start, since the last fs_warm_start_gate. */
 fs_status fs_warm_start_gate_stats(fs_ctx *ctx, long long *steps_h, double *solves_h);
