@@ -47,6 +47,12 @@ struct fs_mlp {
   double *updl, *jdiag;            // 6 Np
   float *feat, *pred, *tgt;        // [nfil x nfeat], [nfil x ntgt], [nfil x ntgt]
   float *rP, *rL;                  // per filament residuals
+  int *plain_next;                 // per filament: take the plain start until the next comparison step
+  // carried bound (fs_warm_start_bound): between comparison steps the learned
+  // start alone is solved and judged against rP of the last comparison step
+  int bound_refresh;               // 0: compare with the plain start every step
+  int bound_age;                   // learned steps since rP was measured
+  bool bound_ok;                   // rP holds a comparison step's plain residuals
   int *count;                      // [0] filaments put back to the plain start
   int *count_h;
   int nfil_alloc, np_alloc;
@@ -231,11 +237,13 @@ __global__ void k_denorm(const float *__restrict__ Y, int n, int ntgt, int k_out
 }
 
 // learned start: upd = -delta (state -= upd), jdiag = diagonal correction
+// (plain: per filament, nonzero = keep the plain start this step, or NULL)
 __global__ void k_learn_apply(int nfil, const int *__restrict__ fil_start, int nw_model, int ntgt,
-                              const float *__restrict__ pred, double *__restrict__ upd, double *__restrict__ jdiag) {
+                              const float *__restrict__ pred, const int *__restrict__ plain,
+                              double *__restrict__ upd, double *__restrict__ jdiag) {
   const int f = blockIdx.x;
   const int b0 = fil_start[f], nw = fil_start[f + 1] - b0;
-  const bool model = nw == nw_model;
+  const bool model = nw == nw_model && !(plain && plain[f]);
   for (int t = threadIdx.x; t < 6 * nw; t += blockDim.x) {
     const float u = model ? pred[(size_t)f * ntgt + t] : 0.f;
     upd[6 * (size_t)b0 + t] = isfinite(u) ? -(double)u : 0.0;  // a non-finite output is no update
@@ -259,6 +267,17 @@ __global__ void k_fil_maxabs(int nfil, const int *__restrict__ fil_start, const 
   }
   for (int m = 16; m >= 1; m >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, m));
   if (lane == 0) r[f] = (float)mx;
+}
+
+// carried steps: a filament whose learned first residual exceeds the carried
+// plain one takes the plain start from the next step on; counts those that
+// started plain this step
+__global__ void k_flag_worse(int nfil, const int *__restrict__ fil_start, int nw_model, const float *__restrict__ rP,
+                             const float *__restrict__ rL, int *__restrict__ plain, int *__restrict__ count) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nfil || fil_start[f + 1] - fil_start[f] != nw_model) return;
+  if (plain[f]) atomicAdd(count, 1);
+  else if (rL[f] > rP[f]) plain[f] = 1;
 }
 
 // filaments whose learned start is worse go back to the plain guess
@@ -550,6 +569,7 @@ fs_status ensure_step_buffers(fs_ctx *c) {
   cudaFree(m->tgt);
   cudaFree(m->rP);
   cudaFree(m->rL);
+  cudaFree(m->plain_next);
   cudaFree(m->Xtt);
   cudaFree(m->pX);
   cudaFree(m->pXt);
@@ -570,6 +590,8 @@ fs_status ensure_step_buffers(fs_ctx *c) {
   FS_TRY(dalloc(&m->tgt, nf * m->ntgt, &b));
   FS_TRY(dalloc(&m->rP, nf, &b));
   FS_TRY(dalloc(&m->rL, nf, &b));
+  FS_TRY(dalloc(&m->plain_next, nf, &b));
+  m->bound_ok = false;
   m->nfil_alloc = (int)nf;
   m->np_alloc = (int)np;
   c->bytes += b;
@@ -662,16 +684,55 @@ fs_status learn_warm_start(fs_ctx *c, int nt, fs_status (*solve)(fs_ctx *, int))
       FS_TRY(learn_features(c, m->feat));
       FS_TRY(predict(c, m->feat, c->nfil, m->pred));
     }
-    k_learn_apply<<<c->nfil, 128, 0, c->stream>>>(c->nfil, c->fil_start, m->nw, m->ntgt, m->pred, m->updl,
+  }
+  const bool carried = m->bound_refresh > 0 && m->bound_ok && m->bound_age < m->bound_refresh;
+  {
+    ProfScope ps(c, FS_STAGE_LEARN);
+    k_learn_apply<<<c->nfil, 128, 0, c->stream>>>(c->nfil, c->fil_start, m->nw, m->ntgt, m->pred,
+                                                  carried ? m->plain_next : nullptr, m->updl,
                                                   m->mode == 2 ? m->jdiag : nullptr);
     FS_LAUNCH_CHECK();
     m->jdiag_on = m->mode == 2;
   }
-  // plain start
-  FS_TRY(solve(c, nt));
-  FS_TRY(fil_error_check(c, c->V, c->W, c->err, nt));
-  k_fil_maxabs<<<fs_blocks(c->nfil, 8), 256, 0, c->stream>>>(c->nfil, c->fil_start, c->err, m->rP);
-  FS_LAUNCH_CHECK();
+  if (carried) {
+    // one solve: the learned start (the plain guess for the flagged filaments),
+    // judged per filament against rP, the plain start's residual of the last
+    // comparison step; a filament found worse takes the plain start from the
+    // next step on, and its residual stands for this step
+    ++m->bound_age;
+    FS_TRY(fil_state_update(c, m->updl));
+    FS_TRY(fil_forces(c, nt));
+    FS_TRY(solve(c, nt));
+    FS_TRY(fil_error_check(c, c->V, c->W, c->err, nt));
+    k_fil_maxabs<<<fs_blocks(c->nfil, 8), 256, 0, c->stream>>>(c->nfil, c->fil_start, c->err, m->rL);
+    FS_LAUNCH_CHECK();
+    FS_CUDA(cudaMemsetAsync(m->count, 0, sizeof(int), c->stream));
+    k_flag_worse<<<fs_blocks(c->nfil, 128), 128, 0, c->stream>>>(c->nfil, c->fil_start, m->nw, m->rP, m->rL,
+                                                                 m->plain_next, m->count);
+    FS_LAUNCH_CHECK();
+    FS_CUDA(cudaMemcpyAsync(m->count_h, m->count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    FS_CUDA(cudaStreamSynchronize(c->stream));
+    int nmodel = 0;
+    for (int f = 0; f < c->nfil; ++f) nmodel += (c->fil_start_h[f + 1] - c->fil_start_h[f]) == m->nw;
+    const int back = *m->count_h;
+    m->fallback_total += back;
+    m->learned_total += nmodel - back;
+    c->diag.learned_filaments += nmodel - back;
+    c->diag.fallback_filaments += back;
+    return FS_OK;
+  }
+  {
+    // plain start, measured: the comparison of this step and the bound of the next ones
+    FS_TRY(solve(c, nt));
+    FS_TRY(fil_error_check(c, c->V, c->W, c->err, nt));
+    k_fil_maxabs<<<fs_blocks(c->nfil, 8), 256, 0, c->stream>>>(c->nfil, c->fil_start, c->err, m->rP);
+    FS_LAUNCH_CHECK();
+    if (m->bound_refresh > 0) {
+      m->bound_ok = true;
+      m->bound_age = 0;
+      FS_CUDA(cudaMemsetAsync(m->plain_next, 0, sizeof(int) * c->nfil, c->stream));
+    }
+  }
   // learned start
   FS_TRY(fil_state_update(c, m->updl));
   FS_TRY(fil_forces(c, nt));
@@ -750,6 +811,7 @@ fs_status learn_before_upload(fs_ctx *c, bool same_layout) {
   if (!m) return FS_OK;
   m->cmp_pending = false;
   if (!same_layout || !m->Xtt || m->np_alloc < c->np) {
+    m->bound_ok = false;  // other filaments: the carried residuals no longer apply
     if (m->xtt_ok) FS_CUDA(cudaMemsetAsync(m->xtt_ok, 0, sizeof(int), c->stream));
     return FS_OK;
   }
@@ -1052,6 +1114,15 @@ fs_status fs_set_warm_start(fs_ctx *c, int mode) {
   if (!c || mode < 0 || mode > 2) return FS_ERR_INVALID_ARG;
   if (mode > 0 && !c->mlp) return FS_ERR_STATE;
   if (c->mlp) c->mlp->mode = mode;
+  return FS_OK;
+}
+
+fs_status fs_warm_start_bound(fs_ctx *c, int refresh) {
+  if (!c || refresh < 0) return FS_ERR_INVALID_ARG;
+  if (!c->mlp) return refresh ? FS_ERR_STATE : FS_OK;
+  c->mlp->bound_refresh = refresh;
+  c->mlp->bound_ok = false;
+  c->mlp->bound_age = 0;
   return FS_OK;
 }
 

@@ -159,14 +159,27 @@ def test_trained_network_gain(gpu_lib):
     x0_err = (ph[:, :3] - th[:, :3]).pow(2).mean().sqrt().item()
     x0_rms = th[:, :3].pow(2).mean().sqrt().item()
     assert x0_err < 0.9 * x0_rms
+    # the same six steps from the same state: plain start, then the learned start
+    # with its fallback judged against a carried plain residual (refreshed every 8
+    # learned steps), so that it costs one solve on all steps but the first
+    nsteps = 6
+    sim.upload(s0)
+    set_warm_start(ctx, 0)
+    its_plain, st = sim.run_steps(14, nsteps)
+    solves_plain = sim.diag().mobility_solves
+    assert st == abi.FS_OK
     sim.upload(s0)
     set_warm_start(ctx, 1)
-    its, st = sim.run_steps(14, 4)
+    abi.check(abi.lib().fs_warm_start_bound(ctx.h, 8), "fs_warm_start_bound")
+    its, st = sim.run_steps(14, nsteps)
     d = sim.diag()
     assert st == abi.FS_OK
     assert d.learned_filaments > d.fallback_filaments
-    print("held-out X0 correction rms %.3e, residual after prediction %.3e; iterations plain %s learned %s"
-          % (x0_rms, x0_err, list(its_plain), list(its)))
+    print("held-out X0 correction rms %.3e, residual after prediction %.3e; iterations plain %s learned %s; "
+          "mobility solves plain %d learned %d" % (x0_rms, x0_err, list(its_plain), list(its), solves_plain,
+                                                   d.mobility_solves))
+    assert sum(its) < sum(its_plain)
+    assert d.mobility_solves < solves_plain
     ctx.close()
 
 
