@@ -23,7 +23,10 @@ value      mixed precision (FP32 spread/FFT/interpolation, FP64 Broyden and
            when it saves a solve per step over at least two of its steps, and
            probes the other one after 8 steps, an interval that doubles up to 128
            while the probes lose; steps with the reference's start run as captured
-           step graphs; learned.gate reports how many timed steps took each);
+           step graphs; learned.gate reports how many timed steps took each); a
+           learned step compares both starts only every 8th learned step and in
+           between judges each filament's learned start against the carried
+           plain-start residual (fs_warm_start_bound);
            inputs resident in HBM, device-timed with CUDA events on the
            context's stream, max over ranks; weak scaling (one independent
            replica per GPU).
@@ -67,19 +70,21 @@ TRAIN_SEED0 = 7000
 TRAIN_EPOCHS = 40
 CHECKPOINT_FIELDS = ("X", "Xt", "q", "qt", "U", "Ut", "lam", "lam1", "lam2", "kap", "c")
 GATE_PERIOD = 8  # the learned start's cost gate: first probe of the other start after 8 steps
+BOUND_REFRESH = 8  # learned steps between comparisons with the plain start (fs_warm_start_bound)
 ENSEMBLE_SEED = 3000
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the FCM
-# kernels, per grid point, from an ncu capture of the FP32 chain on 256^3 with
-# 15,360 beads (the 512^3 bead density); scaled to the workload by its grid points.
+# kernels, per grid point: the mean over the 13 launches of each in one timed step
+# of the 512^3 workload under ncu (a one-pass metric set), FP32 chain, plain start.
 NCU_TRAFFIC_PER_POINT = {
-    "k_spread": (17.40e6 + 152.87e6) / 256 ** 3,
-    "k_fft_z_fwd": (201.36e6 + 156.52e6) / 256 ** 3,
-    "k_fft_y_fwd": (202.93e6 + 156.83e6) / 256 ** 3,
-    "project": (202.97e6 + 143.17e6) / 256 ** 3,
-    "k_fft_y_inv": (202.93e6 + 159.50e6) / 256 ** 3,
-    "k_fft_z_inv": (203.01e6 + 160.35e6) / 256 ** 3,
+    "k_spread": (163.39e6 + 1600.56e6) / 512 ** 3,
+    "k_fft_z_fwd": (1610.73e6 + 1566.82e6) / 512 ** 3,
+    "k_fft_y_fwd": (1616.95e6 + 1565.75e6) / 512 ** 3,
+    "project": (1617.04e6 + 1553.08e6) / 512 ** 3,
+    "k_fft_y_inv": (1617.00e6 + 1565.84e6) / 512 ** 3,
+    "k_fft_z_inv": (1616.98e6 + 1562.83e6) / 512 ** 3,
+    "k_interp": (1553.40e6 + 6.13e6) / 512 ** 3,
 }
-NCU_TRAFFIC_SOURCE = "ncu capture at 256^3 / 15,360 beads, scaled by grid points"
+NCU_TRAFFIC_SOURCE = "ncu capture of one timed step at 512^3 (13 launches per kernel), per grid point"
 
 
 def parse():
@@ -248,7 +253,7 @@ def run_ours(args, rank, world):
     del fcm, sim_e
     ctx.set_precision(abi.FS_PREC_FP32)
     # launch variants for this grid and suspension (untimed)
-    choice = np.zeros(3, np.int32)
+    choice = np.zeros(4, np.int32)
     tune_ms = ctypes.c_float()
     abi.check(abi.lib().fs_autotune(ctx.h, 2, choice.ctypes.data_as(ctypes.c_void_p), ctypes.byref(tune_ms)),
               "fs_autotune")
@@ -297,6 +302,7 @@ def run_ours(args, rank, world):
         if learned:
             set_warm_start(ctx, mode)
             abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate if mode else 0), "fs_warm_start_gate")
+            abi.check(abi.lib().fs_warm_start_bound(ctx.h, BOUND_REFRESH if mode else 0), "fs_warm_start_bound")
         # steady steps with the reference's start run as one CUDA graph each (Broyden
         # loop on the device), also those the cost gate gives the plain start; steps
         # with the learned start run host-driven
@@ -341,6 +347,7 @@ def run_ours(args, rank, world):
     if learned:
         set_warm_start(ctx, mode)
         abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate), "fs_warm_start_gate")
+        abi.check(abi.lib().fs_warm_start_bound(ctx.h, BOUND_REFRESH), "fs_warm_start_bound")
     simp = Simulation(ctx, prep.copy())
     simp.run_steps(nt0, W)
     ctx.profile_enable(True)
@@ -366,7 +373,9 @@ def run_ours(args, rank, world):
         "fp32_velocity_error_vs_fp64": dict(fp32_err, norm="max |FP32 - FP64| / max |FP64|, one solve of the "
                                                           "prepared state"),
         "autotuned": {"spread_beads_per_pass": int(choice[0]), "interp_beads_per_cta": int(choice[1]),
-                      "transform": "cuFFT" if choice[2] else "warp FFT", "ms_per_solve": tune_ms.value},
+                      "transform": "cuFFT" if choice[2] else "warp FFT",
+                      "spread_column_block": "%d x 16 x %d" % (choice[3], 16 // choice[3]),
+                      "ms_per_solve": tune_ms.value},
     }
     if learned:
         nlf = diag.learned_filaments + diag.fallback_filaments
@@ -395,7 +404,7 @@ def run_ours(args, rank, world):
         "project": 2 * half,                           # the x pass with the projection
         "k_fft_y_inv": 2 * half,
         "k_fft_z_inv": half + 3 * s_real * N,
-        "interp": 3 * s_real * N + npb * 9 * 8,        # read u once; bead Y in, V, W out
+        "k_interp": 3 * s_real * N + npb * 9 * 8,      # read u once; bead Y in, V, W out
     }
     cands = {k: stage_ms[k] for k in alg_bytes if stage_ms.get(k, 0) > 0}
     dom = max(cands, key=cands.get)
@@ -445,6 +454,7 @@ def run_ours(args, rank, world):
         if learned:
             set_warm_start(ctx, mode)
             abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate), "fs_warm_start_gate")
+            abi.check(abi.lib().fs_warm_start_bound(ctx.h, BOUND_REFRESH), "fs_warm_start_bound")
         abi.check(abi.lib().fs_set_graph_mode(ctx.h, 0 if args.no_graph else 1), "fs_set_graph_mode")
         host = prep.copy()
         # the state a step needs, as the reference checkpoints it (.bak: X, Xt, q, qt, U, Ut,
@@ -641,7 +651,8 @@ def run_ensemble(args, rank, world):
            "clocks": clk.summary(), "gpu_launches": int(launches), "graph_launches": K,
            "autotuned": {str(g): {"spread_beads_per_pass": v[0], "interp_beads_per_cta": v[1],
                                   "transform": "cuFFT" if v[2] else "warp FFT (or cuFFT if not a power of two)",
-                                  "ms_per_solve": v[3]} for g, v in tuned.items()},
+                                  "spread_column_block": "%d x 16 x %d" % (v[3], 16 // v[3]),
+                                  "ms_per_solve": v[4]} for g, v in tuned.items()},
            "sequential_host_driven": {"value": seq_value, "ms_per_ensemble_step": seq_ms / K2, "steps": K2},
            "speedup_vs_sequential": value / seq_value}
     ens.close()

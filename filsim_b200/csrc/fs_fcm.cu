@@ -358,10 +358,14 @@ __host__ __device__ constexpr size_t spread32_smem(int ngd) {
   return (sizeof(SpreadStage32<CH>) + 15) / 16 * 16 + sizeof(float4) * CH * (size_t)spread_rec_len(ngd);
 }
 
-template <int CH>
+// CX: the shape of a warp's column block, CX x 16 x (16 / CX) points (x, y, z),
+// an autotuner knob (2, 4 or 8); a lane owns one x, one z pair and four y rows
+template <int CH, int CX>
 __global__ void __launch_bounds__(FS_SPREAD32_THREADS, 3)
     k_spread32(const int *__restrict__ bin_start, const float4 *__restrict__ rec, FcmConsts c,
                float *__restrict__ fgrid) {
+  static_assert(CX == 2 || CX == 4 || CX == 8, "column widths");
+  constexpr int CZ = FS_TILE / CX, NCX = FS_TILE / CX;  // z width; columns across x
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SpreadStage32<CH> &st = *reinterpret_cast<SpreadStage32<CH> *>(smem_raw);
   float4 *const raw = reinterpret_cast<float4 *>(smem_raw + (sizeof(SpreadStage32<CH>) + 15) / 16 * 16);
@@ -467,14 +471,17 @@ __global__ void __launch_bounds__(FS_SPREAD32_THREADS, 3)
   };
   const bool one_chunk = total <= CH;
   if (one_chunk && total > 0) stage(0, total);  // both column passes read these tables
-  // two column passes: warp w owns x in [4 (w & 3), +4) and z in [4 cz, +4) with
-  // cz = (w >> 2) + 2 pass; lane roles as in the header
-  const int cx = warp & 3;
-  const int xl = 4 * cx + (lane & 3), ly = lane >> 3;
+  // two column passes over the tile's 16 column blocks: in pass p warp w owns block
+  // w + 8 p, x in [CX cx, +CX) and z in [CZ cz, +CZ) (CX = 4: the lane roles of the
+  // header); a lane owns x = CX cx + lane % CX, the z pair (lane / CX) % (CZ / 2)
+  // and the four y rows ly + 4 k, ly = lane / 8
+  // (8 is a multiple of NCX, so a warp keeps its x columns in both passes)
+  const int ly = lane >> 3, cx = warp % NCX;
+  const int xl = CX * cx + (lane % CX);
 #pragma unroll 1
   for (int pass = 0; pass < 2; ++pass) {
-    const int cz = (warp >> 2) + 2 * pass;
-    const int zl = 4 * cz + 2 * ((lane >> 2) & 1);
+    const int cz = warp / NCX + (8 / NCX) * pass;
+    const int zl = CZ * cz + 2 * ((lane / CX) % (CZ / 2));
     f2p s[4][3], nc[4][3];
 #pragma unroll
     for (int k = 0; k < 4; ++k)
@@ -491,7 +498,7 @@ __global__ void __launch_bounds__(FS_SPREAD32_THREADS, 3)
         bool hit = false;
         if (sl < nb) {
           const unsigned m = st.xzm[sl];
-          hit = ((m >> (4 * cx)) & 0xfu) && ((m >> (16 + 4 * cz)) & 0xfu) && st.rows[sl];
+          hit = ((m >> (CX * cx)) & ((1u << CX) - 1u)) && ((m >> (16 + CZ * cz)) & ((1u << CZ) - 1u)) && st.rows[sl];
         }
         col[h] = __ballot_sync(0xffffffffu, hit);
       }
@@ -881,12 +888,17 @@ fs_status spread_t(fs_ctx *c, const FcmConsts &k, const double *Y, const double 
       FS_LAUNCH_CHECK();
     }
     ProfScope pk(c, FS_STAGE_K_SPREAD);
-    if (c->tune_spread_chunk == 32)
-      k_spread32<32><<<c->nbins, FS_SPREAD32_THREADS, spread32_smem<32>(k.ngd), c->stream>>>(
-          c->bins.start, rec, k, (float *)c->grid_real);
-    else
-      k_spread32<64><<<c->nbins, FS_SPREAD32_THREADS, spread32_smem<64>(k.ngd), c->stream>>>(
-          c->bins.start, rec, k, (float *)c->grid_real);
+    const int ch = c->tune_spread_chunk, cx = c->tune_spread_cols;
+#define FS_SPREAD32_LAUNCH(CHV, CXV)                                                                             \
+  k_spread32<CHV, CXV><<<c->nbins, FS_SPREAD32_THREADS, spread32_smem<CHV>(k.ngd), c->stream>>>(c->bins.start, rec, \
+                                                                                                 k, (float *)c->grid_real)
+    if (ch == 32 && cx == 2) FS_SPREAD32_LAUNCH(32, 2);
+    else if (ch == 32 && cx == 8) FS_SPREAD32_LAUNCH(32, 8);
+    else if (ch == 32) FS_SPREAD32_LAUNCH(32, 4);
+    else if (cx == 2) FS_SPREAD32_LAUNCH(64, 2);
+    else if (cx == 8) FS_SPREAD32_LAUNCH(64, 8);
+    else FS_SPREAD32_LAUNCH(64, 4);
+#undef FS_SPREAD32_LAUNCH
   } else if (c->tune_spread_chunk == 32) {
     ProfScope pk(c, FS_STAGE_K_SPREAD);
     k_spread<R, 32><<<c->nbins, FS_SPREAD_THREADS, sizeof(SpreadStage<R, 32>), c->stream>>>(
@@ -957,9 +969,17 @@ fs_status fcm_init(fs_ctx *c) {
     FS_CUDA(cudaMalloc(&c->spread_wb, sizeof(float4) * nw));
     c->bytes += sizeof(float4) * nw;
   }
-  FS_CUDA(cudaFuncSetAttribute(k_spread32<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  FS_CUDA(cudaFuncSetAttribute(k_spread32<64, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)spread32_smem<64>(FS_NGD_MAX)));
-  FS_CUDA(cudaFuncSetAttribute(k_spread32<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  FS_CUDA(cudaFuncSetAttribute(k_spread32<64, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)spread32_smem<64>(FS_NGD_MAX)));
+  FS_CUDA(cudaFuncSetAttribute(k_spread32<64, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)spread32_smem<64>(FS_NGD_MAX)));
+  FS_CUDA(cudaFuncSetAttribute(k_spread32<32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)spread32_smem<32>(FS_NGD_MAX)));
+  FS_CUDA(cudaFuncSetAttribute(k_spread32<32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)spread32_smem<32>(FS_NGD_MAX)));
+  FS_CUDA(cudaFuncSetAttribute(k_spread32<32, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)spread32_smem<32>(FS_NGD_MAX)));
   FS_CUDA(cudaFuncSetAttribute(k_spread<double, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(SpreadStage<double, 64>)));
@@ -982,6 +1002,7 @@ fs_status fcm_init(fs_ctx *c) {
     FS_CUDA(cudaFuncSetAttribute(k_interp<float, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap(16 * wf)));
   }
   c->tune_spread_chunk = 64;
+  c->tune_spread_cols = 4;
   c->tune_interp_wpb = 8;
   c->tune_fft32 = 0;
   return fft32_init(c);

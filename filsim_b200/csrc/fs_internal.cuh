@@ -70,6 +70,7 @@ struct fs_ctx {
   float4 *spread_wb;   // FP32 chain: per sorted bead, stencil starts, F, T/2 and weights
   int last_grid_prec;  // precision of the grids from the last solve (-1: none)
   int tune_spread_chunk;  // beads staged per spread pass: 32 or 64 (fs_autotune)
+  int tune_spread_cols;   // FP32 spread: x width of a warp's column block (2, 4 or 8)
   int tune_interp_wpb;    // beads (warps) per interpolation CTA: 4, 8 or 16
   int tune_fft32;         // FP32 power-of-two grids: 0 warp FFT (fs_fft.cu), 1 cuFFT
   void *fft_tw;        // FP32 transform twiddle tables (null: grid not handled by fs_fft.cu, cuFFT is used)

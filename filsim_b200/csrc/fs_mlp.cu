@@ -65,12 +65,13 @@ struct fs_mlp {
   long long learned_total, fallback_total;
   // cost gate of the learned start (fs_warm_start_gate): per start, the running
   // mean of mobility solves per step; the cheaper start (the learned one only
-  // when it saves a solve per step) runs and the other one is probed after
+  // when it saves gate_margin solves per step) runs and the other one is probed after
   // gate_interval steps. The interval starts at gate_period and
   // doubles (up to GATE_BACKOFF_MAX x gate_period) after each probe that leaves
   // the choice unchanged; a probe that changes it restores gate_period.
   int gate_period;                 // 0: off (the learned start runs every step)
   int gate_interval;
+  double gate_margin = 0.25;       // solves per step the learned start must save (fs_warm_start_gate_margin)
   double gate_solves[2];           // [0] plain start, [1] learned start
   int gate_have[2];
   int gate_since;
@@ -605,15 +606,15 @@ bool learn_active(const fs_ctx *c) { return c->mlp && c->mlp->mode > 0; }
 
 // the start of this step under the cost gate (true: learned)
 constexpr int GATE_BACKOFF_MAX = 16;
-// the learned start is chosen only when its running mean is at least this many
-// mobility solves per step below the plain start's: a tie goes to the reference's
-// start, which also runs as a captured step graph
-constexpr double GATE_MARGIN = 1.0;
-// and only once its mean rests on at least this many steps (one early step says little)
+// the learned start is chosen only when its running mean is at least gate_margin
+// mobility solves per step below the plain start's (its inference and its
+// host-driven step cost about a quarter of a 512^3 solve): a tie goes to the
+// reference's start, which also runs as a captured step graph; and only once
+// its mean rests on at least this many steps (one early step says little)
 constexpr long long GATE_MIN_STEPS = 2;
 
 int gate_best(const fs_mlp *m) {
-  return m->gate_steps[1] >= GATE_MIN_STEPS && m->gate_solves[1] + GATE_MARGIN <= m->gate_solves[0] ? 1 : 0;
+  return m->gate_steps[1] >= GATE_MIN_STEPS && m->gate_solves[1] + m->gate_margin <= m->gate_solves[0] ? 1 : 0;
 }
 
 bool learn_gate_on(const fs_ctx *c) { return c->mlp && c->mlp->gate_period > 0; }
@@ -1136,6 +1137,13 @@ fs_status fs_warm_start_gate(fs_ctx *c, int period) {
   m->gate_since = 0;
   m->gate_probe_best = -1;
   m->gate_steps[0] = m->gate_steps[1] = 0;
+  return FS_OK;
+}
+
+fs_status fs_warm_start_gate_margin(fs_ctx *c, double margin) {
+  if (!c || !(margin >= 0.0) || margin > 1e6) return FS_ERR_INVALID_ARG;
+  if (!c->mlp) return FS_ERR_STATE;
+  c->mlp->gate_margin = margin;
   return FS_OK;
 }
 

@@ -75,18 +75,19 @@ class Ensemble:
 
     def autotune(self, reps=3):
         """fs_autotune on the first box of each grid size; the other boxes of that size
-        take its choice. Returns {grid: (spread chunk, interp beads per CTA, fft, ms)}."""
+        take its choice. Returns {grid: (spread chunk, interp beads per CTA, fft, spread
+        column width, ms)}."""
         chosen = {}
         for (npts, p, s, kb), c in zip(self.boxes, self.ctxs):
             if npts not in chosen:
-                ch = np.zeros(3, np.int32)
+                ch = np.zeros(4, np.int32)
                 ms = ctypes.c_float()
                 check(lib().fs_autotune(c.h, reps, ch.ctypes.data_as(ctypes.c_void_p), ctypes.byref(ms)),
                       "fs_autotune")
                 chosen[npts] = (ch, ms.value)
             else:
                 check(lib().fs_set_tuning(c.h, chosen[npts][0].ctypes.data_as(ctypes.c_void_p)), "fs_set_tuning")
-        return {g: (int(v[0][0]), int(v[0][1]), int(v[0][2]), v[1]) for g, v in chosen.items()}
+        return {g: (int(v[0][0]), int(v[0][1]), int(v[0][2]), int(v[0][3]), v[1]) for g, v in chosen.items()}
 
     def run(self, nt_start, nsteps):
         """(iterations [nsteps x n], per-box step ms [nsteps x n], total ms, status)."""

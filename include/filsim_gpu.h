@@ -360,9 +360,11 @@ fs_status fs_set_graph_mode(fs_ctx *ctx, int on);
 
 /* ---- autotuner (no reference counterpart) -----------------------------------
  * choice = {beads staged per spread pass (32 | 64), beads per interpolation CTA
- * (4 | 8 | 16), FP32 power-of-two grids: 0 warp FFT | 1 cuFFT}. fs_autotune times
- * every combination on the uploaded suspension (reps mobility solves each, after
- * one warm-up) and keeps the fastest; best_ms_h: its time per solve. */
+ * (4 | 8 | 16), FP32 power-of-two grids: 0 warp FFT | 1 cuFFT, FP32 spread: x
+ * width of a warp's column block in the 16^3 tile (2 | 4 | 8; the block is
+ * w x 16 x 16/w points)}: four ints. fs_autotune times every combination on the
+ * uploaded suspension (reps mobility solves each, after one warm-up) and keeps
+ * the fastest; best_ms_h: its time per solve. */
 fs_status fs_autotune(fs_ctx *ctx, int reps, int *choice_h, float *best_ms_h);
 fs_status fs_set_tuning(fs_ctx *ctx, const int *choice_h);
 
@@ -481,8 +483,9 @@ fs_status fs_learn_override(fs_ctx *ctx, const float *pred_d);
 fs_status fs_set_warm_start(fs_ctx *ctx, int mode);
 /* Cost gate of the learned start (no reference counterpart): with period > 0,
  * each step runs the start whose running mean of mobility solves per step is
- * lower (the learned one only when it is lower by at least one solve over at
- * least two of its steps: a tie goes to the reference's start), and probes the
+ * lower (the learned one only when it is lower by at least the margin of
+ * fs_warm_start_gate_margin over at least two of its steps: a tie goes to the
+ * reference's start), and probes the
  * other one so that its mean stays
  * current: after period steps, an interval that doubles (up to 16 x period)
  * while the probes leave the choice unchanged and returns to period when one
@@ -490,6 +493,10 @@ fs_status fs_set_warm_start(fs_ctx *ctx, int mode);
  * Broyden iterations than its own extra solves. period 0 (the default) runs the
  * learned start every step. Resets the statistics. */
 fs_status fs_warm_start_gate(fs_ctx *ctx, int period);
+/* The gate's margin: mobility solves per step the learned start must save to be
+ * chosen, standing for its own cost (inference, a host-driven step); default
+ * 0.25, about that cost at 512^3. Kept across fs_warm_start_gate calls. */
+fs_status fs_warm_start_gate_margin(fs_ctx *ctx, double margin);
 /* Carried bound of the learned start's fallback (no reference counterpart):
  * with refresh > 0, only every refresh-th learned step solves both starts (and
  * puts back, in that step, each filament whose learned first residual is

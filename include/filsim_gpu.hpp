@@ -45,7 +45,7 @@ class Context {
   void set_graph_mode(bool on) { check(fs_set_graph_mode(ctx_, on ? 1 : 0), "fs_set_graph_mode"); }
   // fastest launch variants for the uploaded suspension; returns ms per mobility solve
   float autotune(int reps = 3, int *choice = nullptr) {
-    int c[3];
+    int c[4];
     float ms = 0.f;
     check(fs_autotune(ctx_, reps, choice ? choice : c, &ms), "fs_autotune");
     return ms;

@@ -69,17 +69,20 @@ def test_spread_grid_matches_oracle(oracle):
 FP32_SPREAD_REL = 1e-6
 
 
-@pytest.mark.parametrize("shape,nb,seed,chunk", [
-    ((32, 32, 32), 40, 21, 32),
-    ((16, 32, 48), 30, 22, 32),     # a 16-point axis: one bin, stencils wrap inside the tile
-    ((48, 32, 16), 60, 23, 64),
-    ((32, 32, 32), 1500, 24, 32),   # ~1500 candidates per tile: many staging chunks
-    ((64, 32, 32), 1500, 25, 64),
+@pytest.mark.parametrize("shape,nb,seed,chunk,cols", [
+    ((32, 32, 32), 40, 21, 32, 4),
+    ((16, 32, 48), 30, 22, 32, 2),  # a 16-point axis: one bin, stencils wrap inside the tile
+    ((48, 32, 16), 60, 23, 64, 8),
+    ((32, 32, 32), 1500, 24, 32, 8),  # ~1500 candidates per tile: many staging chunks
+    ((64, 32, 32), 1500, 25, 64, 2),
+    ((64, 32, 32), 1500, 25, 64, 4),
 ])
-def test_fp32_spread_grid_matches_oracle(oracle, shape, nb, seed, chunk):
+def test_fp32_spread_grid_matches_oracle(oracle, shape, nb, seed, chunk, cols):
     """The FP32 chain's spread (k_spread_records32 + k_spread32: Kahan sums on packed
     pairs) against the oracle's FP64 force grid, positions drawn over 1.5 box lengths
-    (negative and past the far face included), F, T ~ N(0,1); a repeat is bitwise equal."""
+    (negative and past the far face included), F, T ~ N(0,1), for both staging chunks
+    and the three warp column blocks (2 x 16 x 8, 4 x 16 x 4, 8 x 16 x 2); a repeat is
+    bitwise equal."""
     import ctypes
     from filsim_b200.abi import check, lib
     p = params_for(shape[0])
@@ -92,7 +95,7 @@ def test_fp32_spread_grid_matches_oracle(oracle, shape, nb, seed, chunk):
     _, _, f0, _ = oracle.fcm_mobility(p, Y, F, T, return_grids=True)
     ctx = Context(p, max_beads=nb)
     ctx.set_precision(abi.FS_PREC_FP32)
-    tune = np.array([chunk, 8, 0], np.int32)
+    tune = np.array([chunk, 8, 0, cols], np.int32)
     check(lib().fs_set_tuning(ctx.h, tune.ctypes.data_as(ctypes.c_void_p)), "fs_set_tuning")
     fcm = Fcm(ctx, nb)
     fcm.set(Y, F, T)

@@ -1,8 +1,8 @@
 """The x-slab decomposition of one box's FCM mobility solve on the GPU: each
 rank's spread, transforms, projection and interpolation are the library's
 (fs_set_slab, fs_fcm_spread, fs_slab_forward_yz, fs_slab_solve_x,
-fs_slab_inverse_yz, fs_fcm_interpolate). One rank, and two ranks emulated by
-two host threads on this one GPU (each with its own context; the exchanges
+fs_slab_inverse_yz, fs_fcm_interpolate). One rank, and two or four ranks
+emulated by host threads on this one GPU (each with its own context; the exchanges
 are host-side tensor copies, so no kernel waits for another), give the
 library's one-box FP64 solve to 1e-10."""
 import threading
@@ -72,7 +72,8 @@ class ThreadExchange:
         t.copy_(acc)
 
 
-@pytest.mark.parametrize("shape,ngd,world", [((64, 32, 48), 12, 1), ((64, 32, 48), 12, 2), ((64, 32, 32), 20, 1)])
+@pytest.mark.parametrize("shape,ngd,world", [((64, 32, 48), 12, 1), ((64, 32, 48), 12, 2), ((64, 32, 48), 12, 4),
+                                             ((64, 32, 32), 20, 1), ((64, 32, 32), 20, 2)])
 def test_slab_solve_matches_the_one_box_solve(gpu_lib, shape, ngd, world):
     p, Y, F, T = case(shape, 60, 7, ngd)
     V0, W0 = one_box(p, Y, F, T)

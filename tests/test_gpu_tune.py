@@ -36,14 +36,18 @@ def test_all_variants_and_autotune(gpu_lib, npts):
     for ch in (32, 64):
         for wpb in (4, 8, 16):
             for fft in (0, 1):
-                abi.check(abi.lib().fs_set_tuning(ctx.h, _vp(np.array([ch, wpb, fft], np.int32))), "fs_set_tuning")
-                fcm.mobility_solve()
-                V, W = fcm.V.cpu().numpy(), fcm.W.cpu().numpy()
-                assert np.abs(V - V64).max() / np.abs(V64).max() < 1e-5, (ch, wpb, fft)
-                assert np.abs(W - W64).max() / np.abs(W64).max() < 1e-5, (ch, wpb, fft)
-    choice = np.zeros(3, np.int32)
+                for cx in (2, 4, 8):
+                    abi.check(abi.lib().fs_set_tuning(ctx.h, _vp(np.array([ch, wpb, fft, cx], np.int32))),
+                              "fs_set_tuning")
+                    fcm.mobility_solve()
+                    V, W = fcm.V.cpu().numpy(), fcm.W.cpu().numpy()
+                    assert np.abs(V - V64).max() / np.abs(V64).max() < 1e-5, (ch, wpb, fft, cx)
+                    assert np.abs(W - W64).max() / np.abs(W64).max() < 1e-5, (ch, wpb, fft, cx)
+    choice = np.zeros(4, np.int32)
     ms = ctypes.c_float()
     abi.check(abi.lib().fs_autotune(ctx.h, 2, _vp(choice), ctypes.byref(ms)), "fs_autotune")
     assert choice[0] in (32, 64) and choice[1] in (4, 8, 16) and choice[2] in (0, 1) and ms.value > 0
-    assert abi.lib().fs_set_tuning(ctx.h, _vp(np.array([48, 8, 0], np.int32))) == abi.FS_ERR_INVALID_ARG
+    assert choice[3] in (2, 4, 8)
+    for bad in ([48, 8, 0, 4], [64, 8, 0, 3], [64, 8, 0, 16]):
+        assert abi.lib().fs_set_tuning(ctx.h, _vp(np.array(bad, np.int32))) == abi.FS_ERR_INVALID_ARG
     ctx.close()

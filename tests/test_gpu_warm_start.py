@@ -186,8 +186,9 @@ def test_trained_network_gain(gpu_lib):
 def test_cost_gate(gpu_lib):
     """fs_warm_start_gate: each step takes the start with the lower running mean of
     mobility solves per step and probes the other one (first after period steps, then
-    at doubling intervals while the choice holds); with the gate off the learned start
-    runs on every step."""
+    at doubling intervals while the choice holds); the learned start must save the
+    margin (fs_warm_start_gate_margin); with the gate off the learned start runs on
+    every step."""
     ctx, model, sim = prepared()
     s0 = snapshot(sim)
     set_warm_start(ctx, 1)
@@ -199,6 +200,8 @@ def test_cost_gate(gpu_lib):
                  ctypes.c_void_p(solves.ctypes.data))
         return steps, solves
 
+    margin = 1.0
+    ctx.call("fs_warm_start_gate_margin", ctypes.c_double(margin))
     ctx.call("fs_warm_start_gate", 3)
     its, st = sim.run_steps(WARM + 1, 12)
     assert st == abi.FS_OK
@@ -206,9 +209,11 @@ def test_cost_gate(gpu_lib):
     assert steps.sum() == 12
     assert steps.min() >= 2                       # both starts measured and re-probed
     major = int(np.argmax(steps))
-    # the learned start runs most only when it saves at least one solve per step
+    # the learned start runs most only when it saves the margin
     if major == 1:
-        assert solves[1] + 1.0 <= solves[0] + 1e-9
+        assert solves[1] + margin <= solves[0] + 1e-9
+    assert abi.lib().fs_warm_start_gate_margin(ctx.h, ctypes.c_double(-1.0)) == abi.FS_ERR_INVALID_ARG
+    assert abi.lib().fs_warm_start_gate_margin(ctx.h, ctypes.c_double(float("nan"))) == abi.FS_ERR_INVALID_ARG
     # gate off: the learned start on every step
     sim.upload(s0)
     ctx.call("fs_warm_start_gate", 0)
