@@ -733,6 +733,9 @@ __global__ void __launch_bounds__(32 * WPB) k_interp(const R *__restrict__ u, co
   const R *ux = u, *uy = u + N, *uz = u + 2 * N;
   double v0 = 0, v1 = 0, v2 = 0, w0 = 0, w1 = 0, w2 = 0;
   // point p = ij * ngd + k; a step of 32 points advances (ij, k) by (32 / ngd, 32 % ngd)
+  // (loads one point at a time: four points in flight per lane, at 64 registers,
+  // ran 0.97 ms at 512^3 against 0.72 ms for this loop; the gathers are bound by
+  // the load units, not by latency)
   const int dij = 32 / ngd, dk = 32 - dij * ngd;
   int ij = lane / ngd, k = lane - ij * ngd;
   for (int p = lane; p < n3; p += 32) {
