@@ -87,6 +87,12 @@ NCU_TRAFFIC_PER_POINT = {
 NCU_TRAFFIC_SOURCE = "ncu capture of one timed step at 512^3 (13 launches per kernel), per grid point"
 
 
+def warp_fft_length(n):
+    """Grid lengths the FP32 warp transform covers on every axis (fs_fft.cu): 2^p in
+    [64, 512] or 96, 192, 384; other grids run cuFFT."""
+    return (64 <= n <= 512 and n & (n - 1) == 0) or n in (96, 192, 384)
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -373,7 +379,7 @@ def run_ours(args, rank, world):
         "fp32_velocity_error_vs_fp64": dict(fp32_err, norm="max |FP32 - FP64| / max |FP64|, one solve of the "
                                                           "prepared state"),
         "autotuned": {"spread_beads_per_pass": int(choice[0]), "interp_beads_per_cta": int(choice[1]),
-                      "transform": "cuFFT" if choice[2] else "warp FFT",
+                      "transform": "warp FFT" if (choice[2] == 0 and warp_fft_length(WORKLOAD["npts"])) else "cuFFT",
                       "spread_column_block": "%d x 16 x %d" % (choice[3], 16 // choice[3]),
                       "ms_per_solve": tune_ms.value},
     }
@@ -650,7 +656,7 @@ def run_ensemble(args, rank, world):
            "iters_per_step": float(its.mean()), "status": abi.STATUS_NAMES.get(st, st),
            "clocks": clk.summary(), "gpu_launches": int(launches), "graph_launches": K,
            "autotuned": {str(g): {"spread_beads_per_pass": v[0], "interp_beads_per_cta": v[1],
-                                  "transform": "cuFFT" if v[2] else "warp FFT (or cuFFT if not a power of two)",
+                                  "transform": "warp FFT" if (v[2] == 0 and warp_fft_length(g)) else "cuFFT",
                                   "spread_column_block": "%d x 16 x %d" % (v[3], 16 // v[3]),
                                   "ms_per_solve": v[4]} for g, v in tuned.items()},
            "sequential_host_driven": {"value": seq_value, "ms_per_ensemble_step": seq_ms / K2, "steps": K2},

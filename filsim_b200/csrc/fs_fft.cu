@@ -278,16 +278,131 @@ __device__ __forceinline__ void fft_p2n(float2 (&v)[Fft<N>::M], float2 *S, const
   dit_reg<M, D>(v);
 }
 
+// ---- lines of any supported length --------------------------------------------
+// N = 2^p (32..512) runs the pipelines above. N = 3P, P = 2^p (96, 192, 384) adds a
+// radix-3 step: a lane's registers m, m + P/32, m + 2P/32 hold the points n, n + P,
+// n + 2P (n = lane + 32 m); one 3-point DFT across them, the twiddles
+// exp(-D 2 pi i n k3 / N) (k3 = 1, 2), then the three P-point warp transforms, so
+// that register k3 P/32 + i holds X[3 index_P(i) + k3] (decimation in frequency;
+// the adjoint runs the steps backwards). The twiddles come from a per-N table of
+// exp(-2 pi i j / N), j < 2P, after the power-of-two tables.
+constexpr int TW3_BASE = TW_FULL + 512 - 32 + 512;
+constexpr int TW3_LEN = 64 + 128 + 256;  // 2P for N = 96, 192, 384
+template <int N>
+__host__ __device__ constexpr int tw3_off() {
+  return TW3_BASE + (N == 96 ? 0 : N == 192 ? 64 : 192);
+}
+// Row of spectrum index k in a natural-order buffer. For N = 3P a warp writes
+// register i to X = 3 index_P(lane, i) + k3, i.e. 3c + 48h + K (P = 128 and 32:
+// c < 4 or c = 0, h the lane's bit-reversed column, K < 48 the same for all lanes)
+// or 3c + 12h + K (P = 64, c < 2, K < 12); k + 4 floor(k / 48), resp. k + floor(k / 12),
+// puts the 32 lanes on 16 distinct 8-byte bank pairs, two each (the minimum), and
+// keeps consecutive k on consecutive rows apart from one skip per block.
+template <int N>
+__host__ __device__ constexpr int xf_row(int k) {
+  if constexpr (N == 192) return k + k / 12;
+  else if constexpr (N % 3 == 0) return k + 4 * (k / 48);
+  else return prow<N>(k);
+}
+template <int N>
+__host__ __device__ constexpr int xf_rows() {
+  if constexpr (N % 3 == 0) return xf_row<N>(N - 1) + 1;
+  else return Fft<N>::PEXT;
+}
+__host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
+template <int N>
+__host__ __device__ constexpr int xf_sw() {  // per-warp scratch (float2): sub-transforms, natural-order rows, N values
+  if constexpr (N % 3 == 0) return cmax(cmax(Fft<N / 3>::SW, xf_rows<N>()), N);
+  else return Fft<N>::SW;
+}
+
+// spectrum index held in register i after xf_fwd
+template <int N>
+__device__ __forceinline__ int xf_index(int lane, int i) {
+  if constexpr (N % 3 == 0) {
+    constexpr int MP = N / 96;
+    return 3 * out_index<N / 3>(lane, i % MP) + i / MP;
+  } else {
+    return out_index<N>(lane, i);
+  }
+}
+
+// 3-point DFT of (a, b, c) with kernel exp(-D 2 pi i jk / 3)
+template <int D>
+__device__ __forceinline__ void radix3(float2 &a, float2 &b, float2 &c) {
+  constexpr float S3 = 0.86602540378443865f;  // sin(2 pi / 3)
+  const float2 t1 = cadd(b, c), t2 = csub(b, c);
+  const float2 mm = make_float2(a.x - 0.5f * t1.x, a.y - 0.5f * t1.y);
+  const float2 r = D > 0 ? make_float2(S3 * t2.y, -S3 * t2.x) : make_float2(-S3 * t2.y, S3 * t2.x);  // -i D s t2
+  a = cadd(a, t1);
+  b = cadd(mm, r);
+  c = csub(mm, r);
+}
+
+template <int N, int D>
+__device__ __forceinline__ void xf_fwd(float2 (&v)[N / 32], float2 *S, const float2 *__restrict__ tw, int lane) {
+  if constexpr (N % 3 == 0) {
+    constexpr int P = N / 3, MP = P / 32;
+    const float2 *t3 = tw + tw3_off<N>();
+#pragma unroll
+    for (int m = 0; m < MP; ++m) {
+      radix3<D>(v[m], v[m + MP], v[m + 2 * MP]);
+      const int n = lane + 32 * m;
+      v[m + MP] = cmul(v[m + MP], twd<D>(t3, n));
+      v[m + 2 * MP] = cmul(v[m + 2 * MP], twd<D>(t3, 2 * n));
+    }
+#pragma unroll
+    for (int k3 = 0; k3 < 3; ++k3) {
+      float2 u[MP];
+#pragma unroll
+      for (int i = 0; i < MP; ++i) u[i] = v[k3 * MP + i];
+      fft_n2p<P, D>(u, S, tw, lane);
+#pragma unroll
+      for (int i = 0; i < MP; ++i) v[k3 * MP + i] = u[i];
+    }
+  } else {
+    fft_n2p<N, D>(v, S, tw, lane);
+  }
+}
+
+// the adjoint of xf_fwd: register-order input, natural output; xf_inv<N, -1>
+// inverts xf_fwd<N, +1> up to the factor N
+template <int N, int D>
+__device__ __forceinline__ void xf_inv(float2 (&v)[N / 32], float2 *S, const float2 *__restrict__ tw, int lane) {
+  if constexpr (N % 3 == 0) {
+    constexpr int P = N / 3, MP = P / 32;
+    const float2 *t3 = tw + tw3_off<N>();
+#pragma unroll
+    for (int k3 = 0; k3 < 3; ++k3) {
+      float2 u[MP];
+#pragma unroll
+      for (int i = 0; i < MP; ++i) u[i] = v[k3 * MP + i];
+      fft_p2n<P, D>(u, S, tw, lane);
+#pragma unroll
+      for (int i = 0; i < MP; ++i) v[k3 * MP + i] = u[i];
+    }
+#pragma unroll
+    for (int m = 0; m < MP; ++m) {
+      const int n = lane + 32 * m;
+      v[m + MP] = cmul(v[m + MP], twd<D>(t3, n));
+      v[m + 2 * MP] = cmul(v[m + 2 * MP], twd<D>(t3, 2 * n));
+      radix3<D>(v[m], v[m + MP], v[m + 2 * MP]);
+    }
+  } else {
+    fft_p2n<N, D>(v, S, tw, lane);
+  }
+}
+
 // ---- pass 2: forward y, written transposed -----------------------------------
 // CTA: (c, kz) plane, 16 consecutive x lines; output rows of 16 x values per ky.
 template <int NY>
 __global__ void __launch_bounds__(FFT_THREADS) k_fft_y_fwd(const float2 *__restrict__ A, float2 *__restrict__ B,
                                                            int nx, const float2 *__restrict__ tw) {
-  constexpr int M = Fft<NY>::M, SW = Fft<NY>::SW;
+  constexpr int M = (NY / 32), SW = xf_sw<NY>();
   extern __shared__ float2 fft_smem[];
-  float2 *T = fft_smem;  // Fft<NY>::PEXT swizzled rows x FFT_TS
+  float2 *T = fft_smem;  // xf_rows<NY>() swizzled rows x FFT_TS
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float2 *S = fft_smem + Fft<NY>::PEXT * FFT_TS + warp * SW;
+  float2 *S = fft_smem + xf_rows<NY>() * FFT_TS + warp * SW;
   const int nxt = nx / FFT_TILE;
   const int xt = blockIdx.x % nxt;
   const size_t ckz = blockIdx.x / nxt;
@@ -298,15 +413,15 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_y_fwd(const float2 *__restr
     float2 v[M];
 #pragma unroll
     for (int m = 0; m < M; ++m) v[m] = __ldg(line + lane + 32 * m);
-    fft_n2p<NY, 1>(v, S, tw, lane);
+    xf_fwd<NY, 1>(v, S, tw, lane);
 #pragma unroll
-    for (int i = 0; i < M; ++i) T[prow<NY>(out_index<NY>(lane, i)) * FFT_TS + wx] = v[i];
+    for (int i = 0; i < M; ++i) T[xf_row<NY>(xf_index<NY>(lane, i)) * FFT_TS + wx] = v[i];
   }
   __syncthreads();
   float2 *out = B + ckz * NY * nx + (size_t)xt * FFT_TILE;
   for (int idx = threadIdx.x; idx < NY * FFT_TILE; idx += FFT_THREADS) {
     const int ky = idx / FFT_TILE, j = idx % FFT_TILE;
-    out[(size_t)ky * nx + j] = T[prow<NY>(ky) * FFT_TS + j];
+    out[(size_t)ky * nx + j] = T[xf_row<NY>(ky) * FFT_TS + j];
   }
 }
 
@@ -326,7 +441,7 @@ template <int NX>
 __global__ void __launch_bounds__(XP_THREADS) k_fft_x_project(float2 *__restrict__ B, int ny, int nzh,
                                                               size_t cstride, float ffx, float ffy, float ffz,
                                                               float inv_total, const float2 *__restrict__ tw) {
-  constexpr int M = Fft<NX>::M, SW = Fft<NX>::SW;
+  constexpr int M = (NX / 32), SW = xf_sw<NX>();
   __shared__ float2 Sall[3 * XP_PAIRS * SW];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int comp = warp % 3, pl = warp / 3;
@@ -339,7 +454,7 @@ __global__ void __launch_bounds__(XP_THREADS) k_fft_x_project(float2 *__restrict
   if (active) {
 #pragma unroll
     for (int m = 0; m < M; ++m) v[m] = line[lane + 32 * m];
-    fft_n2p<NX, 1>(v, S, tw, lane);
+    xf_fwd<NX, 1>(v, S, tw, lane);
 #pragma unroll
     for (int i = 0; i < M; ++i) S[lane + 32 * i] = v[i];
   }
@@ -349,7 +464,7 @@ __global__ void __launch_bounds__(XP_THREADS) k_fft_x_project(float2 *__restrict
     const float q2 = wavenumber_f(ky, ny, ffy), q3 = (float)kz * ffz;
 #pragma unroll
     for (int i = 0; i < M; ++i) {
-      const int kx = out_index<NX>(lane, i);
+      const int kx = xf_index<NX>(lane, i);
       const float q1 = wavenumber_f(kx, NX, ffx);
       const float qq = q2 * q2 + q1 * q1 + 1e-18f;
       const float norm = __fdividef(1.0f, qq + q3 * q3);
@@ -363,7 +478,7 @@ __global__ void __launch_bounds__(XP_THREADS) k_fft_x_project(float2 *__restrict
   }
   __syncthreads();
   if (active) {
-    fft_p2n<NX, -1>(v, S, tw, lane);
+    xf_inv<NX, -1>(v, S, tw, lane);
 #pragma unroll
     for (int m = 0; m < M; ++m) line[lane + 32 * m] = v[m];
   }
@@ -373,7 +488,7 @@ __global__ void __launch_bounds__(XP_THREADS) k_fft_x_project(float2 *__restrict
 template <int NY>
 __global__ void __launch_bounds__(FFT_THREADS) k_fft_y_inv(const float2 *__restrict__ B, float2 *__restrict__ A,
                                                            int nx, const float2 *__restrict__ tw) {
-  constexpr int M = Fft<NY>::M, SW = Fft<NY>::SW;
+  constexpr int M = (NY / 32), SW = xf_sw<NY>();
   extern __shared__ float2 fft_smem[];
   float2 *T = fft_smem;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -394,10 +509,19 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_y_inv(const float2 *__restr
     float2 v[M];
 #pragma unroll
     for (int m = 0; m < M; ++m) v[m] = T[(lane + 32 * m) * FFT_TS + wx];
-    fft_n2p<NY, -1>(v, S, tw, lane);
+    xf_fwd<NY, -1>(v, S, tw, lane);
     float2 *line = A + (ckz * nx + (size_t)xt * FFT_TILE + wx) * NY;
+    if constexpr (NY % 3 == 0) {  // register order scatters at stride 3: store in natural order
 #pragma unroll
-    for (int i = 0; i < M; ++i) line[out_index<NY>(lane, i)] = v[i];
+      for (int i = 0; i < M; ++i) S[xf_row<NY>(xf_index<NY>(lane, i))] = v[i];
+      __syncwarp();
+#pragma unroll
+      for (int m = 0; m < M; ++m) line[lane + 32 * m] = S[xf_row<NY>(lane + 32 * m)];
+      __syncwarp();
+    } else {
+#pragma unroll
+      for (int i = 0; i < M; ++i) line[xf_index<NY>(lane, i)] = v[i];
+    }
   }
 }
 
@@ -415,7 +539,7 @@ template <int NZ, int ZT>
 __global__ void __launch_bounds__(FFT_THREADS) k_fft_z_r2c(const float *__restrict__ f, float2 *__restrict__ A,
                                                             int nx, int ny, const float2 *__restrict__ tw) {
   static_assert(FFT_TILE == 2 * FFT_WARPS, "two lines per warp");
-  constexpr int H = NZ / 2, M = Fft<NZ>::M, SW = Fft<NZ>::SW;
+  constexpr int H = NZ / 2, M = (NZ / 32), SW = xf_sw<NZ>();
   extern __shared__ float2 fft_smem[];
   float2 *T = fft_smem;  // (H + 1) x FFT_TS
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -437,16 +561,16 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_z_r2c(const float *__restri
 #pragma unroll 1
   for (int t = 0; t < ZT; ++t) {
     const int yt = yg * ZT + t;
-    fft_n2p<NZ, 1>(v, S, tw, lane);
+    xf_fwd<NZ, 1>(v, S, tw, lane);
 #pragma unroll
-    for (int i = 0; i < M; ++i) S[prow<NZ>(out_index<NZ>(lane, i))] = v[i];
+    for (int i = 0; i < M; ++i) S[xf_row<NZ>(xf_index<NZ>(lane, i))] = v[i];
     if (t + 1 < ZT) load(yt + 1);
     __syncwarp();
 #pragma unroll
     for (int m = 0; m < (H + 32) / 32; ++m) {
       const int k = lane + 32 * m;
       if (k <= H) {
-        const float2 zk = S[prow<NZ>(k)], zr = S[prow<NZ>((NZ - k) & (NZ - 1))];
+        const float2 zk = S[xf_row<NZ>(k)], zr = S[xf_row<NZ>(k == 0 ? 0 : NZ - k)];
         T[k * FFT_TS + wa] = make_float2(0.5f * (zk.x + zr.x), 0.5f * (zk.y - zr.y));
         T[k * FFT_TS + wb] = make_float2(0.5f * (zk.y + zr.y), -0.5f * (zk.x - zr.x));
       }
@@ -465,7 +589,7 @@ template <int NZ>
 __global__ void __launch_bounds__(FFT_THREADS) k_fft_z_c2r(const float2 *__restrict__ A, float *__restrict__ u,
                                                             int nx, int ny, const float2 *__restrict__ tw) {
   static_assert(FFT_TILE == 2 * FFT_WARPS, "two lines per warp");
-  constexpr int H = NZ / 2, M = Fft<NZ>::M, SW = Fft<NZ>::SW;
+  constexpr int H = NZ / 2, M = (NZ / 32), SW = xf_sw<NZ>();
   extern __shared__ float2 fft_smem[];
   float2 *T = fft_smem;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -497,22 +621,34 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_z_c2r(const float2 *__restr
       v[m] = make_float2(a.x + b.y, b.x - a.y);
     }
   }
-  fft_n2p<NZ, -1>(v, S, tw, lane);
+  xf_fwd<NZ, -1>(v, S, tw, lane);
   float *oa = u + (((size_t)c * nx + x) * ny + (size_t)yt * FFT_TILE + wa) * NZ;
   float *ob = oa + (size_t)FFT_WARPS * NZ;
+  if constexpr (NZ % 3 == 0) {  // register order scatters at stride 3: store in natural order
 #pragma unroll
-  for (int i = 0; i < M; ++i) {
-    const int o = out_index<NZ>(lane, i);
-    oa[o] = v[i].x;
-    ob[o] = v[i].y;
+    for (int i = 0; i < M; ++i) S[xf_row<NZ>(xf_index<NZ>(lane, i))] = v[i];
+    __syncwarp();
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const float2 z = S[xf_row<NZ>(lane + 32 * m)];
+      oa[lane + 32 * m] = z.x;
+      ob[lane + 32 * m] = z.y;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const int o = xf_index<NZ>(lane, i);
+      oa[o] = v[i].x;
+      ob[o] = v[i].y;
+    }
   }
 }
 
 template <int NZ>
-constexpr size_t smem_z() { return sizeof(float2) * ((NZ / 2 + 1) * FFT_TS + FFT_WARPS * Fft<NZ>::SW); }
+constexpr size_t smem_z() { return sizeof(float2) * ((NZ / 2 + 1) * FFT_TS + FFT_WARPS * xf_sw<NZ>()); }
 
 template <int NY>
-constexpr size_t smem_y() { return sizeof(float2) * (Fft<NY>::PEXT * FFT_TS + FFT_WARPS * Fft<NY>::SW); }
+constexpr size_t smem_y() { return sizeof(float2) * (xf_rows<NY>() * FFT_TS + FFT_WARPS * xf_sw<NY>()); }
 
 bool pow2_in(int n, int lo, int hi) { return n >= lo && n <= hi && (n & (n - 1)) == 0; }
 
@@ -581,36 +717,38 @@ fs_status x_project(fs_ctx *c, float2 *B, const float2 *tw) {
   return FS_OK;
 }
 
-#define FS_FFT_SWITCH(n, fn, ...)                    \
-  switch (n) {                                       \
-    case 32: FS_TRY(fn<32>(__VA_ARGS__)); break;     \
-    case 64: FS_TRY(fn<64>(__VA_ARGS__)); break;     \
-    case 128: FS_TRY(fn<128>(__VA_ARGS__)); break;   \
-    case 256: FS_TRY(fn<256>(__VA_ARGS__)); break;   \
-    case 512: FS_TRY(fn<512>(__VA_ARGS__)); break;   \
-    default: return FS_ERR_INVALID_ARG;              \
-  }
 #define FS_FFT_SWITCH_Z(n, fn, ...)                  \
   switch (n) {                                       \
     case 64: FS_TRY(fn<64>(__VA_ARGS__)); break;     \
+    case 96: FS_TRY(fn<96>(__VA_ARGS__)); break;     \
     case 128: FS_TRY(fn<128>(__VA_ARGS__)); break;   \
+    case 192: FS_TRY(fn<192>(__VA_ARGS__)); break;   \
     case 256: FS_TRY(fn<256>(__VA_ARGS__)); break;   \
+    case 384: FS_TRY(fn<384>(__VA_ARGS__)); break;   \
     case 512: FS_TRY(fn<512>(__VA_ARGS__)); break;   \
     default: return FS_ERR_INVALID_ARG;              \
+  }
+#define FS_FFT_SWITCH(n, fn, ...)                    \
+  if (n == 32) {                                     \
+    FS_TRY(fn<32>(__VA_ARGS__));                     \
+  } else {                                           \
+    FS_FFT_SWITCH_Z(n, fn, __VA_ARGS__)              \
   }
 
 }  // namespace
 
-bool fft32_supported(const fs_ctx *c) {
-  return pow2_in(c->nx, 32, 512) && pow2_in(c->ny, 32, 512) && pow2_in(c->nz, 64, 512);
-}
+// line lengths of the warp transforms: 2^p in [lo, 512], or 96, 192, 384
+static bool fft_len(int n, int lo) { return n >= lo && (pow2_in(n, lo, 512) || n == 96 || n == 192 || n == 384); }
+
+bool fft32_supported(const fs_ctx *c) { return fft_len(c->nx, 32) && fft_len(c->ny, 32) && fft_len(c->nz, 64); }
 
 fs_status fft32_init(fs_ctx *c) {
   c->fft_tw = nullptr;
   if (!fft32_supported(c)) return FS_OK;
   // [0, 1024): exp(-2 pi i j / 1024); then per N in {32, ..., 512}, at 1024 + N - 32,
-  // the lane table [k2 * 32 + lane] = exp(-2 pi i lane k2 / N), k2 < N / 32.
-  const int ntw = TW_FULL + 512 - 32 + 512;
+  // the lane table [k2 * 32 + lane] = exp(-2 pi i lane k2 / N), k2 < N / 32; then per
+  // N in {96, 192, 384}, at tw3_off<N>, exp(-2 pi i j / N), j < 2N/3.
+  const int ntw = TW3_BASE + TW3_LEN;
   float2 *h = (float2 *)malloc(sizeof(float2) * ntw);
   if (!h) return FS_ERR_OOM;
   const double TwoPI = 2. * FS_PI;
@@ -621,6 +759,10 @@ fs_status fft32_init(fs_ctx *c) {
         const long long j = (long long)l * k2;
         h[TW_FULL + n - 32 + k2 * 32 + l] = make_float2((float)cos(TwoPI * j / n), (float)-sin(TwoPI * j / n));
       }
+  const int n3[3] = {96, 192, 384}, off3[3] = {tw3_off<96>(), tw3_off<192>(), tw3_off<384>()};
+  for (int q = 0; q < 3; ++q)
+    for (int j = 0; j < 2 * n3[q] / 3; ++j)
+      h[off3[q] + j] = make_float2((float)cos(TwoPI * j / n3[q]), (float)-sin(TwoPI * j / n3[q]));
   cudaError_t e = cudaMalloc(&c->fft_tw, sizeof(float2) * ntw);
   if (e == cudaSuccess) e = cudaMemcpy(c->fft_tw, h, sizeof(float2) * ntw, cudaMemcpyHostToDevice);
   free(h);

@@ -409,7 +409,7 @@ enum {
   FS_STAGE_K_FFT_Y_FWD = 16, /* FP32 transform: the forward pass over y lines */
   FS_STAGE_K_FFT_Y_INV = 17, /* FP32 transform: the inverse pass over y lines */
   FS_STAGE_K_FFT_Z_INV = 18, /* FP32 transform: the inverse pass over z lines */
-  FS_STAGE_K_INTERP = 19,   /* the interpolation kernel alone (FP32: the tile pass, not the per-bead sums) */
+  FS_STAGE_K_INTERP = 19,   /* the interpolation kernel alone */
   FS_STAGE_COUNT = 32
 };
 typedef struct fs_profile {

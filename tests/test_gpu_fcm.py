@@ -171,13 +171,22 @@ def flow_input(kind, dims, seed):
     raise ValueError(kind)
 
 
+def warp_fft_lengths_ok(dims):
+    """Line lengths of the FP32 warp transform: 2^p up to 512 (z from 64) or 96, 192, 384."""
+    ok = lambda n, lo: n >= lo and ((n & (n - 1)) == 0 and n <= 512 or n in (96, 192, 384))
+    return ok(dims[0], 32) and ok(dims[1], 32) and ok(dims[2], 64)
+
+
 @pytest.mark.parametrize("dims", [(64, 64, 64), (32, 128, 64), (128, 32, 256), (32, 32, 32),
-                                  (512, 32, 64), (256, 64, 128), (64, 512, 64), (32, 64, 512)])
+                                  (512, 32, 64), (256, 64, 128), (64, 512, 64), (32, 64, 512),
+                                  (96, 96, 96), (384, 32, 96), (32, 192, 384), (192, 96, 64), (64, 384, 192),
+                                  (48, 48, 48)])
 @pytest.mark.parametrize("kind", ["noise", "kz0", "kzN", "kxN"])
 def test_flow_solve_fp64_and_fp32_against_numpy(dims, kind):
-    """Power-of-two grids with nz >= 64 run the FP32 five-pass transform
-    (fs_fft.cu); 32^3 runs cuFFT. FP64 within 1e-12, FP32 within 1e-5 of the
-    largest velocity component."""
+    """Grids whose line lengths are 2^p (z from 64) or 3 * 2^p >= 96 run the FP32
+    five-pass transform (fs_fft.cu; its kernels show in the profile); 32^3 and 48^3
+    run cuFFT. FP64 within 1e-12, FP32 within 1e-5 of the largest velocity
+    component."""
     p = params_for(dims)
     f = flow_input(kind, dims, seed=sum(dims) + len(kind))
     ref = numpy_flow_solve(p, f)
@@ -185,10 +194,15 @@ def test_flow_solve_fp64_and_fp32_against_numpy(dims, kind):
     fcm = Fcm(ctx, 1)
     u64 = fcm.flow_solve(f).cpu().numpy()
     ctx.set_precision(abi.FS_PREC_FP32)
+    ctx.profile_enable()
     u32 = fcm.flow_solve(f).cpu().numpy()
+    prof = ctx.profile()
     ctx.close()
     assert rel_err(u64, ref) < 1e-12
     assert rel_err(u32, ref) < FP32_REL
+    warp = warp_fft_lengths_ok(dims)
+    for k in ("k_fft_z_fwd", "k_fft_y_fwd", "k_fft_y_inv", "k_fft_z_inv"):
+        assert (prof[k][1] > 0) == warp, (k, prof[k])
 
 
 def test_fp32_within_1e5_of_fp64(case64):
