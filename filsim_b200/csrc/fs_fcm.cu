@@ -291,12 +291,14 @@ __global__ void __launch_bounds__(FS_SPREAD_THREADS)
 // solve: stencil starts, F, T/2 and the weights (g, d, r, r d) per axis and
 // stencil index, with the FP32 arithmetic of k_spread<float> (gaussian_setup,
 // FCMfunctions.cpp:565-589: xx = xg dx - Y in double, then the float Gaussians).
-// k_spread32 then runs one CTA (8 warps) per 16^3 tile, which stages the tile's
-// candidate records once and covers its 16 columns of 4 x 16 x 4 points in two
-// passes: in pass p warp w owns x in [4(w&3), +4), z in [4cz, +4) with
-// cz = (w>>2) + 2p; lane l owns x = 4(w&3) + (l&3), the z pair 4cz + 2((l>>2)&1)
-// + {0, 1} and y = (l>>3) + 4k, k < 4: eight points held as four packed pairs per
-// component (two columns per warp even out the warps' bead counts). Per staged bead reaching the warp's column the lane forms the
+// k_spread32 then runs one CTA (8 warps) per 16^3 tile, which stages tables of
+// the tile's candidate beads (by tile coordinate, from their records) and covers
+// its 16 column blocks in two passes; with the default 4 x 16 x 4 blocks, in
+// pass p warp w owns x in [4(w&3), +4), z in [4cz, +4) with cz = (w>>2) + 2p;
+// lane l owns x = 4(w&3) + (l&3), the z pair 4cz + 2((l>>2)&1) + {0, 1} and
+// y = (l>>3) + 4k, k < 4: eight points held as four packed pairs per component
+// (two blocks per warp even out the warps' bead counts; the block shape is a
+// template knob). Per staged bead reaching the warp's column the lane forms the
 // x-z factors of its pair once, then each covered y row costs three packed
 // FMA chains and three packed Kahan updates:
 //   y = term + nc, t = s + y, nc = y - (t - s), s = t      (nc = -c of Kahan)
@@ -341,21 +343,22 @@ __global__ void k_spread_records32(const double *__restrict__ Y, const double *_
 }
 
 
-// the chunk's records (slot sl at sl RL, copied as they are) follow the tables
-// in dynamic shared memory: spread32_smem(ngd) bytes in all
+// the staged chunk: tables by tile coordinate, built straight from the records in
+// global memory (spread32_smem bytes of dynamic shared memory)
 template <int CH>
 struct SpreadStage32 {
   float4 xw[CH][FS_TILE];                    // (g, d, r, -) by tile-local x
   float zg[CH][FS_TILE], zd[CH][FS_TILE], zr[CH][FS_TILE];  // by tile-local z
   float4 yw[CH][FS_TILE];                    // (g, g, d, d) by tile-local y
   float2 yrd[CH][FS_TILE];                   // (r d, r d)
+  float4 fh[CH], hh[CH];                     // (F0, F1, F2, h0), (h1, h2, -, -): h = T / 2
   unsigned xzm[CH];                          // x coverage (16 bits) | z coverage (16 bits) << 16
   unsigned rows[CH];                         // y rows k with a covered y in [4k, 4k + 4)
 };
 
 template <int CH>
-__host__ __device__ constexpr size_t spread32_smem(int ngd) {
-  return (sizeof(SpreadStage32<CH>) + 15) / 16 * 16 + sizeof(float4) * CH * (size_t)spread_rec_len(ngd);
+__host__ __device__ constexpr size_t spread32_smem(int) {
+  return (sizeof(SpreadStage32<CH>) + 15) / 16 * 16;
 }
 
 // CX: the shape of a warp's column block, CX x 16 x (16 / CX) points (x, y, z),
@@ -368,7 +371,6 @@ __global__ void __launch_bounds__(FS_SPREAD32_THREADS, 3)
   constexpr int CZ = FS_TILE / CX, NCX = FS_TILE / CX;  // z width; columns across x
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SpreadStage32<CH> &st = *reinterpret_cast<SpreadStage32<CH> *>(smem_raw);
-  float4 *const raw = reinterpret_cast<float4 *>(smem_raw + (sizeof(SpreadStage32<CH>) + 15) / 16 * 16);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int tile = blockIdx.x;
   const int tz = tile % c.nbin[2], ty = (tile / c.nbin[2]) % c.nbin[1], tx = tile / (c.nbin[2] * c.nbin[1]);
@@ -398,28 +400,13 @@ __global__ void __launch_bounds__(FS_SPREAD32_THREADS, 3)
   int total = 0;
   for (int r = 0; r < nr; ++r) total += cand_len[r];
   const int ngd = c.ngd, RL = spread_rec_len(ngd);
-  // staging of candidates [base, base + nb): records to shared memory (slot sl at
-  // sl RL) with 16-byte asynchronous copies, one contiguous run per candidate bin,
-  // then tables by tile coordinate, eight threads per bead slot (thread j takes
-  // x, y and z in {j, j + 8})
+  // staging of candidates [base, base + nb): tables by tile coordinate, eight
+  // threads per bead slot (thread j takes x, y and z in {j, j + 8}), each reading
+  // its slot's record (candidate base + sl: bin range r, rank q in it) from global
+  // memory; not copying the records in first keeps a CTA at 55 KB of shared memory
+  // with 64 beads per pass (92.5 KB with the copies), so three CTAs fit on an SM
   auto stage = [&](int base, int nb) {
     __syncthreads();  // the previous tables are no longer read
-    {
-      int pre = 0;  // candidates before bin range r
-#pragma unroll 1
-      for (int r = 0; r < nr; ++r) {
-        const int lo = max(pre, base), hi = min(pre + cand_len[r], base + nb);
-        if (lo < hi) {
-          const float4 *src = rec + (size_t)(cand_rs[r] + lo - pre) * RL;
-          const unsigned dst = (unsigned)__cvta_generic_to_shared(&raw[(lo - base) * RL]);
-          for (int e = tid; e < (hi - lo) * RL; e += FS_SPREAD32_THREADS)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + 16 * e), "l"(src + e) : "memory");
-        }
-        pre += cand_len[r];
-      }
-    }
-    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
-    __syncthreads();
     const int j = tid & 7;
 #pragma unroll 1
     for (int s0 = 0; s0 < CH; s0 += FS_SPREAD32_THREADS / 8) {
@@ -427,8 +414,17 @@ __global__ void __launch_bounds__(FS_SPREAD32_THREADS, 3)
       const bool act = sl < nb;
       bool cov[6] = {false, false, false, false, false, false};
       if (act) {
-        const float4 *rw = raw + sl * RL;
-        const float4 hd = rw[0];
+        int q = base + sl, r = 0;
+        while (q >= cand_len[r]) {
+          q -= cand_len[r];
+          ++r;
+        }
+        const float4 *rw = rec + (size_t)(cand_rs[r] + q) * RL;
+        const float4 hd = __ldg(rw);
+        if (j == 0) {
+          st.fh[sl] = __ldg(rw + 1);
+          st.hh[sl] = __ldg(rw + 2);
+        }
         const int swv[3] = {__float_as_int(hd.x), __float_as_int(hd.y), __float_as_int(hd.z)};
         float4 w[6];
 #pragma unroll
@@ -436,7 +432,7 @@ __global__ void __launch_bounds__(FS_SPREAD32_THREADS, 3)
           const int a = it >> 1, l = j + 8 * (it & 1), Nn = c.N[a];
           const int i = wrap_near(l + wrap_near(X0[a] - swv[a], Nn), Nn);
           cov[it] = i < ngd;
-          w[it] = cov[it] ? rw[3 + a * ngd + i] : make_float4(0.f, 0.f, 0.f, 0.f);
+          w[it] = cov[it] ? __ldg(rw + 3 + a * ngd + i) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
         st.xw[sl][j] = w[0];
         st.xw[sl][j + 8] = w[1];
@@ -513,8 +509,8 @@ __global__ void __launch_bounds__(FS_SPREAD32_THREADS, 3)
           const float2 gz = *reinterpret_cast<const float2 *>(&st.zg[sl][zl]);
           const float2 dz = *reinterpret_cast<const float2 *>(&st.zd[sl][zl]);
           const float2 rz = *reinterpret_cast<const float2 *>(&st.zr[sl][zl]);
-          const float4 fh = raw[sl * RL + 1];  // F0, F1, F2, h0 (h = T / 2, GA_setup :536-547)
-          const float4 hh = raw[sl * RL + 2];  // h1, h2
+          const float4 fh = st.fh[sl];  // F0, F1, F2, h0 (h = T / 2, GA_setup :536-547)
+          const float4 hh = st.hh[sl];  // h1, h2
           // per z of the pair: f_a = F_a gx gz, the rotlet factors of k_spread (d = gdx gdz)
           const float gxz0 = wx.x * gz.x, gxz1 = wx.x * gz.y;
           const float dxz0 = wx.y * dz.x, dxz1 = wx.y * dz.y;
