@@ -25,7 +25,7 @@ value      mixed precision (FP32 spread/FFT/interpolation, FP64 Broyden and
            while the probes lose; steps with the reference's start run as captured
            step graphs; learned.gate reports how many timed steps took each); a
            learned step compares both starts only every 8th learned step and in
-           between judges each filament's learned start against the carried
+           between checks each filament's learned start against the carried
            plain-start residual (fs_warm_start_bound);
            inputs resident in HBM, device-timed with CUDA events on the
            context's stream, max over ranks; weak scaling (one independent

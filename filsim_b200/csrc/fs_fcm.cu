@@ -1001,7 +1001,7 @@ fs_status fcm_init(fs_ctx *c) {
     FS_CUDA(cudaFuncSetAttribute(k_interp<float, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap(16 * wf)));
   }
   c->tune_spread_chunk = 64;
-  c->tune_spread_cols = 4;
+  c->tune_spread_cols = 2;  // 2 x 16 x 8 blocks: fs_autotune's choice at 384^3 and 512^3
   c->tune_interp_wpb = 8;
   c->tune_fft32 = 0;
   return fft32_init(c);

@@ -49,7 +49,7 @@ struct fs_mlp {
   float *rP, *rL;                  // per filament residuals
   int *plain_next;                 // per filament: take the plain start until the next comparison step
   // carried bound (fs_warm_start_bound): between comparison steps the learned
-  // start alone is solved and judged against rP of the last comparison step
+  // start alone is solved and checked against rP of the last comparison step
   int bound_refresh;               // 0: compare with the plain start every step
   int bound_age;                   // learned steps since rP was measured
   bool bound_ok;                   // rP holds a comparison step's plain residuals
@@ -697,7 +697,7 @@ fs_status learn_warm_start(fs_ctx *c, int nt, fs_status (*solve)(fs_ctx *, int))
   }
   if (carried) {
     // one solve: the learned start (the plain guess for the flagged filaments),
-    // judged per filament against rP, the plain start's residual of the last
+    // checked per filament against rP, the plain start's residual of the last
     // comparison step; a filament found worse takes the plain start from the
     // next step on, and its residual stands for this step
     ++m->bound_age;

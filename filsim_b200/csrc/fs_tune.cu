@@ -35,9 +35,10 @@ fs_status fs_autotune(fs_ctx *c, int reps, int *choice_h, float *best_ms_h) {
   FS_CUDA(cudaEventCreate(&e1));
   const int ffts = (c->precision == FS_PREC_FP32 && c->fft_tw) ? 2 : 1;
   float best = 1e30f;
-  // the column shape only changes the FP32 spread
-  const int cx_lo = c->precision == FS_PREC_FP32 ? 2 : 4, cx_hi = c->precision == FS_PREC_FP32 ? 8 : 4;
-  int bch = 64, bwpb = 8, bfft = 0, bcx = 4;
+  // the column shape only changes the FP32 spread (FP64 keeps the current one)
+  const bool f32 = c->precision == FS_PREC_FP32;
+  const int cx_lo = f32 ? 2 : c->tune_spread_cols, cx_hi = f32 ? 8 : c->tune_spread_cols;
+  int bch = 64, bwpb = 8, bfft = 0, bcx = c->tune_spread_cols;
   fs_status st = FS_OK;
   for (int ch = 32; ch <= 64 && st == FS_OK; ch *= 2)
     for (int wpb = 4; wpb <= 16 && st == FS_OK; wpb *= 2)

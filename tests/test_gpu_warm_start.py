@@ -160,7 +160,7 @@ def test_trained_network_gain(gpu_lib):
     x0_rms = th[:, :3].pow(2).mean().sqrt().item()
     assert x0_err < 0.9 * x0_rms
     # the same six steps from the same state: plain start, then the learned start
-    # with its fallback judged against a carried plain residual (refreshed every 8
+    # with its fallback checked against a carried plain residual (refreshed every 8
     # learned steps), so that it costs one solve on all steps but the first
     nsteps = 6
     sim.upload(s0)
