@@ -158,7 +158,10 @@ fs_status step_implicit(fs_ctx *c, int nt, int *iters_out, bool commit = true, i
   if (learn_recording(c)) FS_TRY(learn_capture_targets(c, iter));
   if (learn_on) learn_gate_record(c, learned, c->diag.mobility_solves - solves0);
   FS_TRY(learn_end_step(c));
-  if (commit) FS_TRY(fil_step(c, nt));
+  if (commit) {
+    FS_TRY(hist_end_step(c));  // only a step that moves X to Xt shifts the history
+    FS_TRY(fil_step(c, nt));
+  }
   c->diag.last_nt = nt;
   c->diag.last_iters = iter;
   c->diag.total_iters += iter;
@@ -239,6 +242,7 @@ fs_status fs_create(const fs_params *p, int max_beads, int max_filaments, void *
   c->max_beads = max_beads;
   c->max_fil = max_filaments;
   c->precision = p->precision;
+  c->start_order = 1;
   c->L[0] = p->npts_x * p->dx;
   c->L[1] = p->npts_y * p->dx;
   c->L[2] = p->npts_z * p->dx;
@@ -292,6 +296,7 @@ fs_status fs_destroy(fs_ctx *c) {
     for (int i = 0; i < 2 * FS_PROF_SLOTS; ++i) cudaEventDestroy(c->prof.ev[i]);
   graph_free(c);
   mlp_free(c);
+  hist_free(c);
   cudaFree(c->gemm_err);
   fcm_free(c);
   slab_free(c);
@@ -461,6 +466,7 @@ fs_status fs_state_upload(fs_ctx *c, const fs_host_state *s) {
   const bool same_layout = c->have_state && c->fil_start_h && c->nfil == nf && c->np == np &&
                            memcmp(c->fil_start_h, s->fil_start, sizeof(int) * (nf + 1)) == 0;
   FS_TRY(learn_before_upload(c, same_layout));
+  FS_TRY(hist_before_upload(c, same_layout));
   if (!same_layout) {
     graph_invalidate(c);
     FS_CUDA(cudaStreamSynchronize(st));
@@ -487,7 +493,7 @@ fs_status fs_state_upload(fs_ctx *c, const fs_host_state *s) {
     if (lams_h[i]) FS_CUDA(cudaMemcpyAsync(lams[i], lams_h[i], nl3, cudaMemcpyHostToDevice, st));
     else FS_CUDA(cudaMemsetAsync(lams[i], 0, nl3, st));
   }
-  FS_TRY(learn_after_upload(c));
+  FS_TRY(hist_after_upload(c));
   if (s->kap) FS_CUDA(cudaMemcpyAsync(c->kap, s->kap, sizeof(double) * nf, cudaMemcpyHostToDevice, st));
   if (s->c) FS_CUDA(cudaMemcpyAsync(c->cc, s->c, sizeof(double) * nf, cudaMemcpyHostToDevice, st));
   if (!same_layout || !s->kap || !s->c) {
@@ -769,7 +775,13 @@ fs_status fs_state_update(fs_ctx *c, const double *update) {
   return fil_state_update(c, update);
 }
 
-fs_status fs_step(fs_ctx *c, int nt) { return c ? fil_step(c, nt) : FS_ERR_INVALID_ARG; }
+fs_status fs_step(fs_ctx *c, int nt) {
+  if (!c) return FS_ERR_INVALID_ARG;
+  if (!c->have_state) return FS_ERR_STATE;
+  FS_TRY(learn_end_step(c));
+  FS_TRY(hist_end_step(c));
+  return fil_step(c, nt);
+}
 
 static fs_status run_one(fs_ctx *c, int nt, int *iters_h, int choice = -1) {
   FS_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(int) * FLAG_COUNT, c->stream));
@@ -795,6 +807,7 @@ static bool use_gated_graph(const fs_ctx *c, int nt) {
 static fs_status run_one_gated(fs_ctx *c, int nt, int *iters_h) {
   if (learn_gate_choose(c)) return run_one(c, nt, iters_h, 1);
   FS_TRY(learn_end_step(c));  // the graph ends with Filament::step
+  FS_TRY(hist_end_step(c));
   FS_TRY(graph_launch_step(c, nt));
   int it = 0;
   fs_status s = graph_flush(c, &it);

@@ -1,7 +1,8 @@
 // fs_filament.cu -- filament mechanics, approximate Jacobian and Broyden
 // update of the implicit BDF2 step, FP64 on sm_100a.
 //
-//   k_initial_guess      Filament::initialGuess (Filament.hpp:227-237, Bead.hpp:202-217)
+//   k_initial_guess      Filament::initialGuess (Filament.hpp:227-237, Bead.hpp:202-217); with
+//                        start order 2 the first bead extrapolated to second order (fs_start.cu)
 //   k_unrobot_assign     Filament::unRobotArmify (Filament.hpp:489-505) +
 //                        Fcm::assign_filament_data's Y = fmod(Xs, L) (FCMfunctions.cpp:882-918)
 //   k_forces             setZeroForcesTorques, applyElasticTorques, applyConstraintForcesTorques,
@@ -191,14 +192,23 @@ __device__ void link_strain_twist(const FilConsts &k, int f, int nw, int i, doub
 }
 
 // ---- per-bead / per-filament kernels -----------------------------------------
+// order 2 with the history held (*hist_ok): the first bead from 3X - 3Xt + Xtt,
+// rounded as written (fs_start.cu); otherwise the reference's 2X - Xt
 __global__ void k_initial_guess(int np, const int *__restrict__ seg_id, const double *__restrict__ X,
                                 const double *__restrict__ Xt, const double *__restrict__ U,
                                 const double *__restrict__ Ut, const double *__restrict__ q, double *__restrict__ Xs,
-                                double *__restrict__ Us, double *__restrict__ qs) {
+                                double *__restrict__ Us, double *__restrict__ qs, int order,
+                                const double *__restrict__ Xtt, const int *__restrict__ hist_ok) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= np) return;
-  if (seg_id[b] == 0)
-    for (int d = 0; d < 3; ++d) Xs[3 * b + d] = 2. * X[3 * b + d] - Xt[3 * b + d];
+  if (seg_id[b] == 0) {
+    if (order == 2 && *hist_ok)
+      for (int d = 0; d < 3; ++d)
+        Xs[3 * b + d] =
+            __dadd_rn(__dsub_rn(__dmul_rn(3., X[3 * b + d]), __dmul_rn(3., Xt[3 * b + d])), Xtt[3 * b + d]);
+    else
+      for (int d = 0; d < 3; ++d) Xs[3 * b + d] = 2. * X[3 * b + d] - Xt[3 * b + d];
+  }
   double us[3];
   for (int d = 0; d < 3; ++d) us[d] = 2. * U[3 * b + d] - Ut[3 * b + d];
   for (int d = 0; d < 3; ++d) Us[3 * b + d] = us[d];
@@ -1237,8 +1247,9 @@ FilConsts make_fconsts(const fs_ctx *c) {
 fs_status fil_initial_guess(fs_ctx *c) {
   if (!c->have_state) return FS_ERR_STATE;
   ProfScope ps(c, FS_STAGE_UPDATE);
+  const int order = (c->start_order == 2 && c->hist_Xtt) ? 2 : 1;
   k_initial_guess<<<fs_blocks(c->np, 256), 256, 0, c->stream>>>(c->np, c->seg_id, c->X, c->Xt, c->U, c->Ut, c->q,
-                                                                 c->Xs, c->Us, c->qs);
+                                                                 c->Xs, c->Us, c->qs, order, c->hist_Xtt, c->hist_ok);
   FS_LAUNCH_CHECK();
   return FS_OK;
 }

@@ -125,6 +125,7 @@ fs_status capture_step(fs_ctx *c, int nt, fs_graph *g, cudaGraph_t *out) {
   FS_TRY(st2);
   FS_CUDA(e_end);
   FS_TRY(learn_end_step(c));
+  FS_TRY(hist_end_step(c));
   FS_TRY(fil_step(c, nt));
   k_step_done<<<1, 1, 0, c->stream>>>(g->dev, c->flags, GRAPH_STEP_SLOTS);
   FS_LAUNCH_CHECK();

@@ -122,6 +122,15 @@ struct fs_ctx {
   fs_diag diag;
   size_t bytes;
   struct fs_mlp *mlp;    // learned warm start (fs_mlp.cu); null until fs_mlp_create
+  // start of the implicit step (fs_set_start_order, fs_start.cu): 1 the reference's
+  // first-bead extrapolation 2X - Xt, 2 quadratic, 3X - 3Xt + Xtt
+  int start_order;
+  // positions two steps back (fs_start.cu), kept while the quadratic or the learned
+  // start is on (3 max_beads doubles each); hist_ok (device) is 1 while hist_Xtt
+  // holds them; hist_pX, hist_pXt: X, Xt before an upload
+  double *hist_Xtt, *hist_pX, *hist_pXt;
+  int *hist_ok;
+  bool hist_cmp_pending;
   struct fs_graph *graph;  // captured steady step (fs_graph.cu); null until first used
   int graph_mode;        // 1: steady steps run as CUDA graphs with the Broyden loop on the device
   int graph_gen;         // bumped whenever captured graphs of this context become stale
@@ -231,8 +240,13 @@ fs_status learn_warm_start(fs_ctx *c, int nt, fs_status (*solve)(fs_ctx *, int))
 fs_status learn_diag_apply(fs_ctx *c, const double *b, double *x);
 fs_status learn_capture_targets(fs_ctx *c, int iters);
 fs_status learn_end_step(fs_ctx *c);
+bool hist_wanted(const fs_ctx *c);
+fs_status hist_ensure(fs_ctx *c);
+void hist_free(fs_ctx *c);
+fs_status hist_end_step(fs_ctx *c);
+fs_status hist_before_upload(fs_ctx *c, bool same_layout);
+fs_status hist_after_upload(fs_ctx *c);
 fs_status learn_before_upload(fs_ctx *c, bool same_layout);
-fs_status learn_after_upload(fs_ctx *c);
 void mlp_free(fs_ctx *c);
 
 // ordered bit patterns for atomicMin/Max on non-negative doubles

@@ -56,9 +56,6 @@ struct fs_mlp {
   int *count;                      // [0] filaments put back to the plain start
   int *count_h;
   int nfil_alloc, np_alloc;
-  double *Xtt, *pX, *pXt;          // positions two steps back; X, Xt before an upload (3 Np)
-  int *xtt_ok;                     // Xtt holds the positions two steps back
-  bool cmp_pending;
   bool jdiag_on;                   // jdiag holds this step's diagonal
   bool have_targets;
   bool override_next;              // the next warm start uses pred as given (fs_learn_override)
@@ -329,15 +326,6 @@ __global__ void k_targets(int nfil, const int *__restrict__ fil_start, int nw_mo
   }
 }
 
-// the position history survives an upload only if X and Xt are unchanged
-__global__ void k_hist_check(size_t n, const double *__restrict__ X, const double *__restrict__ Xt,
-                             const double *__restrict__ pX, const double *__restrict__ pXt, int *__restrict__ ok) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n && (X[i] != pX[i] || Xt[i] != pXt[i])) *ok = 0;
-}
-
-__global__ void k_set_int(int *p, int v) { *p = v; }
-
 __global__ void k_diag_axpy(size_t n, const double *__restrict__ d, const double *__restrict__ b, double *__restrict__ x) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) x[i] += d[i] * b[i];
@@ -571,15 +559,8 @@ fs_status ensure_step_buffers(fs_ctx *c) {
   cudaFree(m->rP);
   cudaFree(m->rL);
   cudaFree(m->plain_next);
-  cudaFree(m->Xtt);
-  cudaFree(m->pX);
-  cudaFree(m->pXt);
   const size_t np = c->max_beads, nf = c->max_fil;
   size_t b = 0;
-  FS_TRY(dalloc(&m->Xtt, 3 * np, &b));
-  FS_TRY(dalloc(&m->pX, 3 * np, &b));
-  FS_TRY(dalloc(&m->pXt, 3 * np, &b));
-  FS_CUDA(cudaMemsetAsync(m->xtt_ok, 0, sizeof(int), c->stream));
   FS_TRY(dalloc(&m->gXs, 3 * np, &b));
   FS_TRY(dalloc(&m->gUs, 3 * np, &b));
   FS_TRY(dalloc(&m->gqs, 4 * np, &b));
@@ -666,7 +647,7 @@ fs_status learn_save_guess(fs_ctx *c) {
 fs_status learn_features(fs_ctx *c, float *out) {
   fs_mlp *m = c->mlp;
   FS_TRY(ensure_step_buffers(c));
-  k_features<<<fs_blocks(c->nfil, 8), 256, 0, c->stream>>>(c->nfil, c->fil_start, m->nw, c->X, c->Xt, m->Xtt, m->xtt_ok,
+  k_features<<<fs_blocks(c->nfil, 8), 256, 0, c->stream>>>(c->nfil, c->fil_start, m->nw, c->X, c->Xt, c->hist_Xtt, c->hist_ok,
                                                            c->q, c->U, c->Ut, c->lam, c->lam1, c->lam2, c->kap,
                                                            1.0 / c->p.dt, m->nfeat, out);
   FS_LAUNCH_CHECK();
@@ -792,43 +773,19 @@ fs_status learn_capture_targets(fs_ctx *c, int iters) {
   return FS_OK;
 }
 
-// before Filament::step moves X -> Xt: keep Xt as the positions two steps back
 // before Filament::step of every step (also before a captured plain-start step,
-// whose graph ends with it): Xtt <- Xt, the positions two steps back afterwards
+// whose graph ends with it); the position history is kept by hist_end_step
 fs_status learn_end_step(fs_ctx *c) {
   fs_mlp *m = c->mlp;
   if (!m) return FS_OK;
   m->jdiag_on = false;
-  FS_TRY(ensure_step_buffers(c));
-  FS_CUDA(cudaMemcpyAsync(m->Xtt, c->Xt, sizeof(double) * 3 * c->np, cudaMemcpyDeviceToDevice, c->stream));
-  k_set_int<<<1, 1, 0, c->stream>>>(m->xtt_ok, 1);
-  FS_LAUNCH_CHECK();
   return FS_OK;
 }
 
-// around fs_state_upload: the history stays valid when the upload repeats X and Xt
+// before fs_state_upload: carried residuals are per filament, so another layout drops them
 fs_status learn_before_upload(fs_ctx *c, bool same_layout) {
   fs_mlp *m = c->mlp;
-  if (!m) return FS_OK;
-  m->cmp_pending = false;
-  if (!same_layout || !m->Xtt || m->np_alloc < c->np) {
-    m->bound_ok = false;  // other filaments: the carried residuals no longer apply
-    if (m->xtt_ok) FS_CUDA(cudaMemsetAsync(m->xtt_ok, 0, sizeof(int), c->stream));
-    return FS_OK;
-  }
-  FS_CUDA(cudaMemcpyAsync(m->pX, c->X, sizeof(double) * 3 * c->np, cudaMemcpyDeviceToDevice, c->stream));
-  FS_CUDA(cudaMemcpyAsync(m->pXt, c->Xt, sizeof(double) * 3 * c->np, cudaMemcpyDeviceToDevice, c->stream));
-  m->cmp_pending = true;
-  return FS_OK;
-}
-
-fs_status learn_after_upload(fs_ctx *c) {
-  fs_mlp *m = c->mlp;
-  if (!m || !m->cmp_pending) return FS_OK;
-  m->cmp_pending = false;
-  const size_t n = (size_t)3 * c->np;
-  k_hist_check<<<fs_blocks((long long)n, 256), 256, 0, c->stream>>>(n, c->X, c->Xt, m->pX, m->pXt, m->xtt_ok);
-  FS_LAUNCH_CHECK();
+  if (m && !same_layout) m->bound_ok = false;
   return FS_OK;
 }
 
@@ -856,8 +813,7 @@ void mlp_free(fs_ctx *c) {
   }
   void *rest[] = {m->in_mu, m->in_sd, m->out_mu, m->out_sd, m->X,   m->XT,   m->Y,    m->T,     m->dY,
                   m->dYT,   m->outbuf, m->loss, m->err,    m->gXs, m->gUs,  m->gqs,  m->glam,  m->updl,
-                  m->jdiag, m->feat,  m->pred,  m->tgt,    m->rP,  m->rL,   m->count, m->Xtt, m->pX,
-                  m->pXt,   m->xtt_ok};
+                  m->jdiag, m->feat,  m->pred,  m->tgt,    m->rP,  m->rL,   m->count};
   for (void *p : rest) cudaFree(p);
   if (m->count_h) cudaFreeHost(m->count_h);
   delete m;
@@ -920,11 +876,11 @@ fs_status fs_mlp_create(fs_ctx *c, int nw, int hidden, int batch_capacity, unsig
   FS_TRY(dalloc(&m->loss, 1, &b));
   FS_TRY(dalloc(&m->err, 1, &b));
   FS_TRY(dalloc(&m->count, 1, &b));
-  FS_TRY(dalloc(&m->xtt_ok, 1, &b));
-  FS_CUDA(cudaMemsetAsync(m->xtt_ok, 0, sizeof(int), c->stream));
   FS_CUDA(cudaMallocHost(&m->count_h, sizeof(int)));
   FS_CUDA(cudaMemsetAsync(m->err, 0, sizeof(int), c->stream));
   c->bytes += b;
+  FS_TRY(hist_ensure(c));  // the features' acceleration needs the positions two steps back
+  graph_invalidate(c);     // captured steps must now keep that history
   // identity normalisation until the caller sets the data's
   std::vector<float> zeros(m->k_in > m->k_out ? m->k_in : m->k_out, 0.f), ones(zeros.size(), 1.f);
   FS_CUDA(cudaMemcpy(m->in_mu, zeros.data(), sizeof(float) * m->k_in, cudaMemcpyHostToDevice));

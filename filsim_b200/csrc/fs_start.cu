@@ -1,0 +1,120 @@
+// fs_start.cu -- the start of the implicit step's Broyden iteration beyond the
+// reference's, and the positions two steps back that it needs. No reference
+// counterpart.
+//
+// The reference starts every step from Xs = 2X - Xt for the first bead of each
+// filament and Us = 2U - Ut for every bead (Filament::initialGuess,
+// Filament.hpp:227-237, Bead.hpp:202-216). U is itself a per-step increment, so
+// the orientations are extrapolated to second order, but the first bead's
+// position to first order only, and the other beads follow it through the
+// robot-arm construction: its error moves the whole filament. With start order 2
+// the first bead starts from 3X - 3Xt + Xtt, Xtt the positions two steps back,
+// on every step for which the context holds that history (not the first step
+// after a layout change or an upload of other positions). The Broyden loop and
+// its convergence test are unchanged, so a step converges to the reference's
+// tolerance from either start.
+//
+// The history is also the learned start's acceleration feature (fs_mlp.cu). It
+// is kept while either needs it: before Filament::step moves X to Xt, Xtt <- Xt.
+#include "fs_internal.cuh"
+
+namespace {
+
+__global__ void k_set_flag(int *p, int v) { *p = v; }
+
+// the history survives an upload only if X and Xt are unchanged
+__global__ void k_hist_same(size_t n, const double *__restrict__ X, const double *__restrict__ Xt,
+                            const double *__restrict__ pX, const double *__restrict__ pXt, int *__restrict__ ok) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && (X[i] != pX[i] || Xt[i] != pXt[i])) *ok = 0;
+}
+
+}  // namespace
+
+bool hist_wanted(const fs_ctx *c) { return c->mlp != nullptr || c->start_order == 2; }
+
+fs_status hist_ensure(fs_ctx *c) {
+  if (c->hist_Xtt) return FS_OK;
+  const size_t n = (size_t)3 * (c->max_beads > 0 ? c->max_beads : 1);
+  double **arrs[3] = {&c->hist_Xtt, &c->hist_pX, &c->hist_pXt};
+  for (double **a : arrs) {
+    const cudaError_t e = cudaMalloc(a, sizeof(double) * n);
+    if (e != cudaSuccess) {
+      hist_free(c);
+      return e == cudaErrorMemoryAllocation ? FS_ERR_OOM : FS_ERR_CUDA;
+    }
+  }
+  const cudaError_t e = cudaMalloc(&c->hist_ok, sizeof(int));
+  if (e != cudaSuccess) {
+    hist_free(c);
+    return e == cudaErrorMemoryAllocation ? FS_ERR_OOM : FS_ERR_CUDA;
+  }
+  c->bytes += 3 * sizeof(double) * n + sizeof(int);
+  c->hist_cmp_pending = false;
+  FS_CUDA(cudaMemsetAsync(c->hist_ok, 0, sizeof(int), c->stream));
+  return FS_OK;
+}
+
+void hist_free(fs_ctx *c) {
+  if (c->hist_Xtt || c->hist_ok) {
+    const size_t n = (size_t)3 * (c->max_beads > 0 ? c->max_beads : 1);
+    c->bytes -= 3 * sizeof(double) * n + sizeof(int);
+  }
+  cudaFree(c->hist_Xtt);
+  cudaFree(c->hist_pX);
+  cudaFree(c->hist_pXt);
+  cudaFree(c->hist_ok);
+  c->hist_Xtt = c->hist_pX = c->hist_pXt = nullptr;
+  c->hist_ok = nullptr;
+  c->hist_cmp_pending = false;
+}
+
+// before Filament::step of every step (also in a captured step, whose graph ends
+// with it): Xtt <- Xt, the positions two steps back once X has moved to Xt
+fs_status hist_end_step(fs_ctx *c) {
+  if (!c->hist_Xtt || !hist_wanted(c)) return FS_OK;
+  FS_CUDA(cudaMemcpyAsync(c->hist_Xtt, c->Xt, sizeof(double) * 3 * (size_t)c->np, cudaMemcpyDeviceToDevice,
+                          c->stream));
+  k_set_flag<<<1, 1, 0, c->stream>>>(c->hist_ok, 1);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+// around fs_state_upload: the history stays valid when the upload repeats X and Xt
+fs_status hist_before_upload(fs_ctx *c, bool same_layout) {
+  c->hist_cmp_pending = false;
+  if (!c->hist_Xtt) return FS_OK;
+  if (!same_layout) {
+    FS_CUDA(cudaMemsetAsync(c->hist_ok, 0, sizeof(int), c->stream));
+    return FS_OK;
+  }
+  const size_t b = sizeof(double) * 3 * (size_t)c->np;
+  FS_CUDA(cudaMemcpyAsync(c->hist_pX, c->X, b, cudaMemcpyDeviceToDevice, c->stream));
+  FS_CUDA(cudaMemcpyAsync(c->hist_pXt, c->Xt, b, cudaMemcpyDeviceToDevice, c->stream));
+  c->hist_cmp_pending = true;
+  return FS_OK;
+}
+
+fs_status hist_after_upload(fs_ctx *c) {
+  if (!c->hist_cmp_pending) return FS_OK;
+  c->hist_cmp_pending = false;
+  const size_t n = (size_t)3 * c->np;
+  k_hist_same<<<fs_blocks((long long)n, 256), 256, 0, c->stream>>>(n, c->X, c->Xt, c->hist_pX, c->hist_pXt,
+                                                                  c->hist_ok);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+extern "C" {
+
+fs_status fs_set_start_order(fs_ctx *c, int order) {
+  if (!c || (order != 1 && order != 2)) return FS_ERR_INVALID_ARG;
+  if (order == 2) FS_TRY(hist_ensure(c));
+  c->start_order = order;
+  // a history no longer kept would go stale
+  if (!hist_wanted(c) && c->hist_ok) FS_CUDA(cudaMemsetAsync(c->hist_ok, 0, sizeof(int), c->stream));
+  graph_invalidate(c);  // captured steps bake the start
+  return FS_OK;
+}
+
+}  // extern "C"

@@ -75,6 +75,11 @@ class Context:
     def set_precision(self, prec):
         check(lib().fs_set_precision(self.h, prec), "fs_set_precision")
 
+    def set_start_order(self, order):
+        """1: the reference's start (first bead from 2X - Xt); 2: the first bead from
+        3X - 3Xt + Xtt once the context holds the positions two steps back."""
+        check(lib().fs_set_start_order(self.h, order), "fs_set_start_order")
+
     def device_bytes(self):
         n = ctypes.c_size_t()
         check(lib().fs_device_bytes(self.h, ctypes.byref(n)), "fs_device_bytes")

@@ -481,6 +481,19 @@ fs_status fs_learn_override(fs_ctx *ctx, const float *pred_d);
  * rows) from the learned start exceeds that of the plain start is put back to
  * the plain start. */
 fs_status fs_set_warm_start(fs_ctx *ctx, int mode);
+/* Start of each implicit step's Broyden iteration (no reference counterpart).
+ * order 1 (the default): Filament::initialGuess, the first bead of each filament
+ * from 2X - Xt (Filament.hpp:227-237, Bead.hpp:202-216). order 2: the first bead
+ * from 3X - 3Xt + Xtt, Xtt its position two steps back, which the context keeps
+ * from then on (order 1 on a step without that history: the first step, or the
+ * first after an upload that changes X or Xt); every other unknown starts as in
+ * order 1. The reference's start extrapolates the orientations (through
+ * Us = 2U - Ut, U a per-step increment) to second order but the first bead's
+ * position, which carries the whole filament, to first order only; order 2
+ * makes it second order too. The Broyden loop and its convergence test are
+ * unchanged: a step converges to the same tolerance from either start. A
+ * learned start (fs_set_warm_start) corrects whichever start is set. */
+fs_status fs_set_start_order(fs_ctx *ctx, int order);
 /* Cost gate of the learned start (no reference counterpart): with period > 0,
  * each step runs the start whose running mean of mobility solves per step is
  * lower (the learned one only when it is lower by at least the margin of

@@ -41,6 +41,8 @@ class Context {
   fs_ctx *get() const { return ctx_; }
   void synchronize() { check(fs_synchronize(ctx_), "fs_synchronize"); }
   void set_precision(int prec) { check(fs_set_precision(ctx_, prec), "fs_set_precision"); }
+  // 2: the first bead of each filament started from 3X - 3Xt + Xtt (1: the reference's 2X - Xt)
+  void set_start_order(int order) { check(fs_set_start_order(ctx_, order), "fs_set_start_order"); }
   // steady steps as CUDA graphs with the Broyden loop on the device
   void set_graph_mode(bool on) { check(fs_set_graph_mode(ctx_, on ? 1 : 0), "fs_set_graph_mode"); }
   // fastest launch variants for the uploaded suspension; returns ms per mobility solve

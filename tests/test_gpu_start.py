@@ -1,0 +1,114 @@
+"""Start order 2 (fs_start.cu, fs_set_start_order): the first bead of each
+filament starts from 3X - 3Xt + Xtt once the context holds the positions two
+steps back, and from the reference's 2X - Xt (Bead.hpp:202-216) without that
+history; steps converge to the reference start's solution within the
+tolerance, in fewer Broyden iterations; captured steps are bitwise the
+host-driven ones; an upload of other positions drops the history."""
+import numpy as np
+import pytest
+
+from filsim_b200 import abi
+from filsim_b200.configs import make_sediment_case, sediment_params
+from filsim_b200.fcm import Context, Simulation
+
+pytestmark = pytest.mark.gpu
+
+NFIL, NW = 24, 16
+
+
+def prepared(order, seed=5, prec=abi.FS_PREC_FP64, **kw):
+    p, s = make_sediment_case(64, NFIL, NW, seed, **kw)
+    ctx = Context(p, max_beads=s.np, max_filaments=s.nfil)
+    ctx.set_precision(prec)
+    ctx.set_start_order(order)
+    return ctx, Simulation(ctx, s)
+
+
+def first_beads(sim):
+    return sim.susp.fil_start[:-1]
+
+
+def test_start_formula_and_history(gpu_lib):
+    ctx, sim = prepared(2)
+    b0 = first_beads(sim)
+    # a fresh context has no history: the reference's start
+    a = sim.download()
+    sim.initial_guess()
+    g = sim.download()
+    assert np.array_equal(g["Xs"][b0], (2 * a["X"] - a["Xt"])[b0])
+    X = []
+    for nt in range(1, 7):
+        it, st = sim.step_implicit(nt)
+        assert st == abi.FS_OK
+        X.append(sim.download()["X"].copy())
+    sim.initial_guess()
+    g = sim.download()
+    assert np.array_equal(g["X"], X[-1])
+    assert np.array_equal(g["Xs"][b0], ((3 * X[-1] - 3 * X[-2]) + X[-3])[b0])
+    # an upload of the same X, Xt keeps the history; other positions drop it
+    s = sim.susp.copy()
+    sim.download_into(s)
+    sim.upload(s)
+    sim.initial_guess()
+    assert np.array_equal(sim.download()["Xs"][b0], ((3 * X[-1] - 3 * X[-2]) + X[-3])[b0])
+    s.arrays["X"][:] += 1e-3
+    sim.upload(s)
+    sim.initial_guess()
+    g = sim.download()
+    assert np.array_equal(g["Xs"][b0], (2 * g["X"] - g["Xt"])[b0])
+    # order 1 on the same context: the reference's start
+    sim.upload(s)
+    for nt in range(7, 10):
+        sim.step_implicit(nt)
+    ctx.set_start_order(1)
+    sim.initial_guess()
+    g = sim.download()
+    assert np.array_equal(g["Xs"][b0], (2 * g["X"] - g["Xt"])[b0])
+    ctx.close()
+
+
+def test_same_solution_fewer_iterations(gpu_lib):
+    """At TOL 1e-12 both starts converge to the same trajectory (positions within
+    1e-8 of dx after 16 steps); at TOL 1e-6 the quadratic start needs fewer
+    Broyden iterations over the steady steps."""
+    out = {}
+    for order in (1, 2):
+        ctx, sim = prepared(order, tol=1e-12)
+        its, st = sim.run_steps(1, 16)
+        assert st == abi.FS_OK
+        out[order] = (its, sim.download())
+        ctx.close()
+    dx = sediment_params(64).dx
+    assert np.abs(out[1][1]["X"] - out[2][1]["X"]).max() / dx < 1e-8
+    assert np.abs(out[1][1]["q"] - out[2][1]["q"]).max() < 1e-8
+    its = {}
+    for order in (1, 2):
+        ctx, sim = prepared(order)
+        i, st = sim.run_steps(1, 24)
+        assert st == abi.FS_OK
+        its[order] = i
+        ctx.close()
+    print("iterations, steps 13-24: reference start", its[1][12:].tolist(), "quadratic", its[2][12:].tolist())
+    assert its[2][12:].sum() < its[1][12:].sum()
+
+
+@pytest.mark.parametrize("prec", [abi.FS_PREC_FP64, abi.FS_PREC_FP32])
+def test_graph_steps_are_host_steps(gpu_lib, prec):
+    out = []
+    for graph in (0, 1):
+        ctx, sim = prepared(2, prec=prec)
+        ctx.call("fs_set_graph_mode", graph)
+        its, st = sim.run_steps(1, 20)
+        assert st == abi.FS_OK
+        out.append((its, sim.download()))
+        ctx.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    for k in ("X", "q", "lam", "U"):
+        assert np.array_equal(out[0][1][k], out[1][1][k]), k
+
+
+def test_invalid_order(gpu_lib):
+    ctx, sim = prepared(1)
+    for bad in (0, 3, -1):
+        assert abi.lib().fs_set_start_order(ctx.h, bad) == abi.FS_ERR_INVALID_ARG
+    ctx.close()
