@@ -15,23 +15,27 @@ in the steady BDF2 regime with the quadratic extrapolation, the regime of 188 of
 the 200 steps of the configured run. Every arm starts from that same state.
 
 value      mixed precision (FP32 spread/FFT/interpolation, FP64 Broyden and
-           filament mechanics) with the learned warm start (trained untimed
-           before the run by the library's own kernels on 20 seeded plain-solver
-           runs of this workload, K_B log-uniform in [0.1, 10]) under its cost
-           gate (fs_warm_start_gate, period 8: each step takes the start with the
-           lower running mean of mobility solves per step, the learned one only
-           when it saves a solve per step over at least two of its steps, and
-           probes the other one after 8 steps, an interval that doubles up to 128
-           while the probes lose; steps with the reference's start run as captured
-           step graphs; learned.gate reports how many timed steps took each); a
-           learned step compares both starts only every 8th learned step and in
-           between checks each filament's learned start against the carried
-           plain-start residual (fs_warm_start_bound);
-           inputs resident in HBM, device-timed with CUDA events on the
-           context's stream, max over ranks; weak scaling (one independent
-           replica per GPU).
+           filament mechanics); each step starts with the first bead of every
+           filament at 3X - 3Xt + Xtt (fs_set_start_order 2; the reference's start
+           takes 2X - Xt, a first-order extrapolation of the position that carries
+           the whole filament); on top of that start, the learned warm start
+           (trained untimed before the run by the library's own kernels on 20
+           seeded runs of this workload with the same start, K_B log-uniform in
+           [0.1, 10]) under its cost gate (fs_warm_start_gate, period 8: each step
+           takes the start with the lower running mean of mobility solves per
+           step, the learned one only when it saves at least 0.25 solves per step
+           over at least two of its steps, and probes the other one after 8 steps,
+           an interval that doubles up to 128 while the probes lose; steps without
+           the learned start run as captured step graphs; learned.gate reports how
+           many timed steps took each); a learned step compares both starts only
+           every 8th learned step and in between checks each filament's learned
+           start against the carried residual (fs_warm_start_bound). The Broyden
+           loop and its convergence test (max |Err| <= 1e-6) are the reference's.
+           Inputs resident in HBM, device-timed with CUDA events on the context's
+           stream, max over ranks; weak scaling (one independent replica per GPU).
 learned_every_step the same steps with the learned start on every step.
-fp32_plain_start   the same steps from the reference's extrapolated start.
+fp32_quadratic_start the same steps with the second-order start alone.
+fp32_plain_start   the same steps from the reference's start (2X - Xt).
 plain_fp64 the same steps with the FCM chain in FP64 and the reference's start.
 e2e        the value arm through the C-ABI with HOST state: every step uploads
            the suspension's state from pinned host memory (fs_state_upload), steps,
@@ -104,6 +108,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip training; time the reference's start only")
     ap.add_argument("--no-graph", action="store_true", help="host-driven steps only (no CUDA graphs)")
+    ap.add_argument("--start-order", type=int, default=2, choices=[1, 2],
+                    help="start of the value arm's steps (fs_set_start_order): 2 the first bead from "
+                         "3X - 3Xt + Xtt (default), 1 the reference's 2X - Xt; the plain arms always use 1")
     ap.add_argument("--train-seeds", type=int, default=20, help="plain-solver runs that generate training data")
     ap.add_argument("--workload", default="sediment_512",
                     choices=["sediment_512", "mobility_256", "ensemble_64", "mlp", "trajectory_200"],
@@ -277,6 +284,7 @@ def run_ours(args, rank, world):
             return make_sediment_case(WORKLOAD["npts"], WORKLOAD["nfil"], nw, seed=seed, kap=kb)
 
         seeds = [TRAIN_SEED0 + 100 * rank + i for i in range(args.train_seeds)]
+        ctx.set_start_order(args.start_order)  # targets: corrections to the value arm's start
         feats, tgts, its_tr = generate(make_case, seeds, PREP_STEPS + 1, 1, model=model)
         t1 = time.time()
         model.fit_normalization(feats, tgts)
@@ -303,8 +311,9 @@ def run_ours(args, rank, world):
                   "fs_warm_start_gate_stats")
         return steps, solves
 
-    def timed_steps(prec, mode, profile=False, gate=0):
+    def timed_steps(prec, mode, profile=False, gate=0, start=1):
         ctx.set_precision(prec)
+        ctx.set_start_order(start)
         if learned:
             set_warm_start(ctx, mode)
             abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate if mode else 0), "fs_warm_start_gate")
@@ -346,10 +355,12 @@ def run_ours(args, rank, world):
 
     mode = 1 if learned else 0
     gate = GATE_PERIOD if learned else 0
-    ms, its, st, _, clocks, launches, diag = timed_steps(abi.FS_PREC_FP32, mode, gate=gate)
+    start = args.start_order
+    ms, its, st, _, clocks, launches, diag = timed_steps(abi.FS_PREC_FP32, mode, gate=gate, start=start)
     # stage breakdown: the same steps again, host-driven with CUDA-event stage timing
     # (graph-captured steps carry no events); not part of the timed value
     abi.check(abi.lib().fs_set_graph_mode(ctx.h, 0), "fs_set_graph_mode")
+    ctx.set_start_order(start)
     if learned:
         set_warm_start(ctx, mode)
         abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate), "fs_warm_start_gate")
@@ -369,6 +380,8 @@ def run_ours(args, rank, world):
         "config": {"workload": WORKLOAD["name"], "grid": [WORKLOAD["npts"]] * 3, "filaments": WORKLOAD["nfil"],
                    "beads_per_filament": nw, "beads": npb, "dt": p.dt, "tol": p.tol,
                    "precision": "mixed", "learned_warm_start": bool(learned),
+                   "start": ("first bead from 3X - 3Xt + Xtt (fs_set_start_order 2)" if start == 2
+                             else "the reference's (first bead from 2X - Xt)"),
                    "timed_steps": [nt0 + W, nt0 + W + K - 1],
                    "start_up": "steps 1-%d (implicit Euler, constant/linear tension extrapolation) run untimed"
                                % PREP_STEPS,
@@ -436,20 +449,27 @@ def run_ours(args, rank, world):
     # the same steps from the reference's start (no learned iterate), FP32 chain,
     # and with the learned start on every step (no cost gate)
     if learned:
-        msa, itsa, sta, _, _, _, da = timed_steps(abi.FS_PREC_FP32, mode, gate=0)
+        msa, itsa, sta, _, _, _, da = timed_steps(abi.FS_PREC_FP32, mode, gate=0, start=start)
         nla = da.learned_filaments + da.fallback_filaments
         out["learned_every_step"] = {"value": world * npb * K / (msa / 1e3), "ms_per_step": msa / K,
                                      "iters_per_step": float(np.mean(itsa)),
                                      "status": abi.STATUS_NAMES.get(sta, sta),
                                      "mobility_solves_per_step": da.mobility_solves / K,
                                      "learned_fraction": da.learned_filaments / max(1, nla)}
-        ms0, its0, st0, _, _, _, d0 = timed_steps(abi.FS_PREC_FP32, 0)
+    if learned and start == 2:
+        msq, itsq, stq, _, _, _, dq = timed_steps(abi.FS_PREC_FP32, 0, start=2)
+        out["fp32_quadratic_start"] = {"value": world * npb * K / (msq / 1e3), "ms_per_step": msq / K,
+                                       "iters_per_step": float(np.mean(itsq)),
+                                       "status": abi.STATUS_NAMES.get(stq, stq),
+                                       "mobility_solves_per_step": dq.mobility_solves / K}
+    if learned or start == 2:
+        ms0, its0, st0, _, _, _, d0 = timed_steps(abi.FS_PREC_FP32, 0, start=1)
         out["fp32_plain_start"] = {"value": world * npb * K / (ms0 / 1e3), "ms_per_step": ms0 / K,
                                    "iters_per_step": float(np.mean(its0)), "status": abi.STATUS_NAMES.get(st0, st0),
                                    "mobility_solves_per_step": d0.mobility_solves / K}
     # plain FP64 FCM chain, reference start
     if not args.no_fp64:
-        ms64, its64, st64, _, _, _, d64 = timed_steps(abi.FS_PREC_FP64, 0)
+        ms64, its64, st64, _, _, _, d64 = timed_steps(abi.FS_PREC_FP64, 0, start=1)
         out["plain_fp64"] = {"value": world * npb * K / (ms64 / 1e3), "ms_per_step": ms64 / K,
                              "iters_per_step": float(np.mean(its64)), "status": abi.STATUS_NAMES.get(st64, st64)}
         out["speedup_vs_plain_fp64"] = out["value"] / out["plain_fp64"]["value"]
@@ -457,6 +477,7 @@ def run_ours(args, rank, world):
     # end to end through the C-ABI with pinned host state (same start and precision as value)
     if not args.no_e2e:
         ctx.set_precision(abi.FS_PREC_FP32)
+        ctx.set_start_order(start)
         if learned:
             set_warm_start(ctx, mode)
             abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate), "fs_warm_start_gate")
@@ -506,9 +527,11 @@ def run_trajectory(args, rank, world):
     """Workload trajectory_200: the configured run of sediment_512, steps 1-200
     from the placed suspension (start-up steps included), once with the mixed-
     precision chain (FP32 spread/FFT/interpolation, FP64 Broyden and mechanics)
-    and once in FP64, both from the reference's start with graph-captured steady
+    and once in FP64, both from the reference's start, and once more mixed with the
+    second-order start (fs_set_start_order 2), all with graph-captured steady
     steps. Records per-step Broyden iterations, the status, the final barrier
-    minimum squared distance and the wall time of each run."""
+    minimum squared distance, the wall time of each run and, for the second-order
+    start, how far its final positions are from the reference start's."""
     import numpy as np
     import torch
     from filsim_b200 import abi
@@ -524,8 +547,11 @@ def run_trajectory(args, rank, world):
     abi.check(abi.lib().fs_set_graph_mode(ctx.h, 1), "fs_set_graph_mode")
     out = {"workload": "trajectory_%d" % nsteps, "grid": [WORKLOAD["npts"]] * 3, "filaments": WORKLOAD["nfil"],
            "beads_per_filament": WORKLOAD["nw"], "beads": susp.np, "dt": p.dt, "tol": p.tol, "steps": nsteps}
-    for name, prec in (("mixed", abi.FS_PREC_FP32), ("fp64", abi.FS_PREC_FP64)):
+    finals = {}
+    for name, prec, start in (("mixed", abi.FS_PREC_FP32, 1), ("mixed_second_order_start", abi.FS_PREC_FP32, 2),
+                              ("fp64", abi.FS_PREC_FP64, 1)):
         ctx.set_precision(prec)
+        ctx.set_start_order(start)
         sim = Simulation(ctx, susp.copy())
         torch.cuda.synchronize()
         t0 = time.time()
@@ -540,6 +566,9 @@ def run_trajectory(args, rank, world):
                      "final_min_dist2": d.min_dist2, "final_max_abs_err": d.last_max_abs_err,
                      "wall_s": wall, "mobility_solves": int(d.mobility_solves), "clocks": clk.summary(),
                      "final_mean_z": float(X[:, 2].mean())}
+        finals[name] = X.copy()
+    out["mixed_second_order_start"]["final_max_dX_vs_mixed_over_dx"] = float(
+        np.abs(finals["mixed_second_order_start"] - finals["mixed"]).max() / p.dx)
     ctx.close()
     return out
 

@@ -806,8 +806,9 @@ static bool use_gated_graph(const fs_ctx *c, int nt) {
 
 static fs_status run_one_gated(fs_ctx *c, int nt, int *iters_h) {
   if (learn_gate_choose(c)) return run_one(c, nt, iters_h, 1);
-  FS_TRY(learn_end_step(c));  // the graph ends with Filament::step
-  FS_TRY(hist_end_step(c));
+  // the graph ends with hist_end_step and Filament::step (its start reads the
+  // history, so it must not shift before the launch)
+  FS_TRY(learn_end_step(c));
   FS_TRY(graph_launch_step(c, nt));
   int it = 0;
   fs_status s = graph_flush(c, &it);

@@ -224,13 +224,16 @@ def test_cost_gate(gpu_lib):
     ctx.close()
 
 
-def test_gated_plain_steps_run_as_graphs_bitwise(gpu_lib):
+@pytest.mark.parametrize("start_order", [1, 2])
+def test_gated_plain_steps_run_as_graphs_bitwise(gpu_lib, start_order):
     """Under the cost gate, the steps given the plain start run as captured step
     graphs when graph mode is on: the trajectory, the iteration counts and the
-    gate's choices are bitwise those of the host-driven run."""
+    gate's choices are bitwise those of the host-driven run, with the reference's
+    start and with the second-order start (whose history the graph keeps)."""
     out = []
     for graph in (0, 1):
         ctx, model, sim = prepared()
+        ctx.set_start_order(start_order)
         set_warm_start(ctx, 1)
         ctx.call("fs_warm_start_gate", 3)
         ctx.call("fs_set_graph_mode", graph)
