@@ -641,7 +641,7 @@ def run_ensemble(args, rank, world):
     torch.cuda.set_device(dev)
     K, W = args.steps, args.warmup
     boxes = make_boxes(ENSEMBLE_SEED + rank)
-    ens = Ensemble(boxes, precision=abi.FS_PREC_FP32)
+    ens = Ensemble(boxes, precision=abi.FS_PREC_FP32, start_order=args.start_order)
     t0 = time.time()
     ens.startup(PREP_STEPS)
     t_start = time.time() - t0
@@ -679,7 +679,9 @@ def run_ensemble(args, rank, world):
                       "grids": {str(g): grids.count(g) for g in sorted(set(grids))}, "beads": beads,
                       "filaments": int(sum(b[2].nfil for b in boxes)), "beads_per_filament": 16,
                       "timed_steps": [nt0 + W, nt0 + W + K - 1], "start_up_seconds": t_start,
-                      "l2": "no flush; most boxes fit in L2 (the workload's own sizes)"},
+                      "l2": "no flush; most boxes fit in L2 (the workload's own sizes)",
+                      "start": ("first bead from 3X - 3Xt + Xtt (fs_set_start_order 2)" if args.start_order == 2
+                                else "the reference's (first bead from 2X - Xt)")},
            "box_step_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99)),
                            "max": float(ms.max())},
            "iters_per_step": float(its.mean()), "status": abi.STATUS_NAMES.get(st, st),

@@ -192,8 +192,8 @@ __device__ void link_strain_twist(const FilConsts &k, int f, int nw, int i, doub
 }
 
 // ---- per-bead / per-filament kernels -----------------------------------------
-// order 2 with the history held (*hist_ok): the first bead from 3X - 3Xt + Xtt,
-// rounded as written (fs_start.cu); otherwise the reference's 2X - Xt
+// order 2 with a history of two steps (*hist_ok == 2): the first bead from
+// 3X - 3Xt + Xtt, rounded as written (fs_start.cu); otherwise the reference's 2X - Xt
 __global__ void k_initial_guess(int np, const int *__restrict__ seg_id, const double *__restrict__ X,
                                 const double *__restrict__ Xt, const double *__restrict__ U,
                                 const double *__restrict__ Ut, const double *__restrict__ q, double *__restrict__ Xs,
@@ -202,7 +202,7 @@ __global__ void k_initial_guess(int np, const int *__restrict__ seg_id, const do
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= np) return;
   if (seg_id[b] == 0) {
-    if (order == 2 && *hist_ok)
+    if (order == 2 && *hist_ok >= 2)
       for (int d = 0; d < 3; ++d)
         Xs[3 * b + d] =
             __dadd_rn(__dsub_rn(__dmul_rn(3., X[3 * b + d]), __dmul_rn(3., Xt[3 * b + d])), Xtt[3 * b + d]);

@@ -126,8 +126,9 @@ struct fs_ctx {
   // first-bead extrapolation 2X - Xt, 2 quadratic, 3X - 3Xt + Xtt
   int start_order;
   // positions two steps back (fs_start.cu), kept while the quadratic or the learned
-  // start is on (3 max_beads doubles each); hist_ok (device) is 1 while hist_Xtt
-  // holds them; hist_pX, hist_pXt: X, Xt before an upload
+  // start is on (3 max_beads doubles each); hist_ok (device): steps run since the
+  // history was reset, up to 2 (hist_Xtt holds positions two steps back once it is
+  // 1, all from this context's own steps at 2); hist_pX, hist_pXt: X, Xt before an upload
   double *hist_Xtt, *hist_pX, *hist_pXt;
   int *hist_ok;
   bool hist_cmp_pending;

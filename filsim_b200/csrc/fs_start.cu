@@ -9,8 +9,10 @@
 // position to first order only, and the other beads follow it through the
 // robot-arm construction: its error moves the whole filament. With start order 2
 // the first bead starts from 3X - 3Xt + Xtt, Xtt the positions two steps back,
-// on every step for which the context holds that history (not the first step
-// after a layout change or an upload of other positions). The Broyden loop and
+// once the context's history spans two steps it ran itself: not on the first two
+// steps after creation, a layout change or an upload of other positions (an
+// uploaded Xt need not be a step's: a suspension placed at rest has Xt = X, and
+// extrapolating through the impulsive start overshoots). The Broyden loop and
 // its convergence test are unchanged, so a step converges to the reference's
 // tolerance from either start.
 //
@@ -20,7 +22,10 @@
 
 namespace {
 
-__global__ void k_set_flag(int *p, int v) { *p = v; }
+// hist_ok counts the steps since the history was last reset, up to 2
+__global__ void k_hist_tick(int *ok) {
+  if (*ok < 2) ++*ok;
+}
 
 // the history survives an upload only if X and Xt are unchanged
 __global__ void k_hist_same(size_t n, const double *__restrict__ X, const double *__restrict__ Xt,
@@ -75,7 +80,7 @@ fs_status hist_end_step(fs_ctx *c) {
   if (!c->hist_Xtt || !hist_wanted(c)) return FS_OK;
   FS_CUDA(cudaMemcpyAsync(c->hist_Xtt, c->Xt, sizeof(double) * 3 * (size_t)c->np, cudaMemcpyDeviceToDevice,
                           c->stream));
-  k_set_flag<<<1, 1, 0, c->stream>>>(c->hist_ok, 1);
+  k_hist_tick<<<1, 1, 0, c->stream>>>(c->hist_ok);
   FS_LAUNCH_CHECK();
   return FS_OK;
 }

@@ -485,9 +485,10 @@ fs_status fs_set_warm_start(fs_ctx *ctx, int mode);
  * order 1 (the default): Filament::initialGuess, the first bead of each filament
  * from 2X - Xt (Filament.hpp:227-237, Bead.hpp:202-216). order 2: the first bead
  * from 3X - 3Xt + Xtt, Xtt its position two steps back, which the context keeps
- * from then on (order 1 on a step without that history: the first step, or the
- * first after an upload that changes X or Xt); every other unknown starts as in
- * order 1. The reference's start extrapolates the orientations (through
+ * from then on; order 1 until that history spans two steps the context ran
+ * itself (the first two steps, and the first two after an upload that changes X
+ * or Xt: an uploaded Xt need not come from a step); every other unknown starts
+ * as in order 1. The reference's start extrapolates the orientations (through
  * Us = 2U - Ut, U a per-step increment) to second order but the first bead's
  * position, which carries the whole filament, to first order only; order 2
  * makes it second order too. The Broyden loop and its convergence test are

@@ -31,11 +31,14 @@ def first_beads(sim):
 def test_start_formula_and_history(gpu_lib):
     ctx, sim = prepared(2)
     b0 = first_beads(sim)
-    # a fresh context has no history: the reference's start
+    # a fresh context has no history: the reference's start, also on its second step
     a = sim.download()
     sim.initial_guess()
     g = sim.download()
     assert np.array_equal(g["Xs"][b0], (2 * a["X"] - a["Xt"])[b0])
+    s1 = sim.susp.copy()
+    sim.download_into(s1)
+    sim.upload(s1)
     X = []
     for nt in range(1, 7):
         it, st = sim.step_implicit(nt)
@@ -56,10 +59,21 @@ def test_start_formula_and_history(gpu_lib):
     sim.initial_guess()
     g = sim.download()
     assert np.array_equal(g["Xs"][b0], (2 * g["X"] - g["Xt"])[b0])
-    # order 1 on the same context: the reference's start
+    # one step later the history holds the uploaded Xt, not a step's: still 2X - Xt
     sim.upload(s)
-    for nt in range(7, 10):
-        sim.step_implicit(nt)
+    sim.step_implicit(7)
+    sim.initial_guess()
+    g = sim.download()
+    assert np.array_equal(g["Xs"][b0], (2 * g["X"] - g["Xt"])[b0])
+    # two steps: second order again
+    x7 = g["X"].copy()
+    sim.step_implicit(8)
+    x8 = sim.download()["X"].copy()
+    sim.step_implicit(9)
+    sim.initial_guess()
+    g = sim.download()
+    assert np.array_equal(g["Xs"][b0], ((3 * g["X"] - 3 * x8) + x7)[b0])
+    # order 1 on the same context: the reference's start
     ctx.set_start_order(1)
     sim.initial_guess()
     g = sim.download()
