@@ -18,7 +18,10 @@ value      mixed precision (FP32 spread/FFT/interpolation, FP64 Broyden and
            filament mechanics); each step starts with the first bead of every
            filament at 3X - 3Xt + Xtt (fs_set_start_order 2; the reference's start
            takes 2X - Xt, a first-order extrapolation of the position that carries
-           the whole filament); on top of that start, the learned warm start
+           the whole filament) and the tensions at 2 lam - lam1
+           (fs_set_tension_extrapolation 1; the reference's quadratic
+           extrapolation amplifies the converged tensions' tolerance noise); on top
+           of that start, the learned warm start
            (trained untimed before the run by the library's own kernels on 20
            seeded runs of this workload with the same start, K_B log-uniform in
            [0.1, 10]) under its cost gate (fs_warm_start_gate, period 8: each step
@@ -34,7 +37,7 @@ value      mixed precision (FP32 spread/FFT/interpolation, FP64 Broyden and
            Inputs resident in HBM, device-timed with CUDA events on the context's
            stream, max over ranks; weak scaling (one independent replica per GPU).
 learned_every_step the same steps with the learned start on every step.
-fp32_quadratic_start the same steps with the second-order start alone.
+fp32_improved_start the same steps with that start alone (no learned start).
 fp32_plain_start   the same steps from the reference's start (2X - Xt).
 plain_fp64 the same steps with the FCM chain in FP64 and the reference's start.
 e2e        the value arm through the C-ABI with HOST state: every step uploads
@@ -91,6 +94,13 @@ NCU_TRAFFIC_PER_POINT = {
 NCU_TRAFFIC_SOURCE = "ncu capture of one timed step at 512^3 (13 launches per kernel), per grid point"
 
 
+def start_label(start, tension):
+    """The config's description of a step start (fs_set_start_order, fs_set_tension_extrapolation)."""
+    pos = "first bead from 3X - 3Xt + Xtt" if start == 2 else "first bead from 2X - Xt (the reference's)"
+    ten = "tensions 2 lam - lam1" if tension == 1 else "tensions 3 lam - 3 lam1 + lam2 (the reference's)"
+    return "%s; %s after lambda_extrap_step" % (pos, ten)
+
+
 def warp_fft_length(n):
     """Grid lengths the FP32 warp transform covers on every axis (fs_fft.cu): 2^p in
     [64, 512] or 96, 192, 384; other grids run cuFFT."""
@@ -111,6 +121,9 @@ def parse():
     ap.add_argument("--start-order", type=int, default=2, choices=[1, 2],
                     help="start of the value arm's steps (fs_set_start_order): 2 the first bead from "
                          "3X - 3Xt + Xtt (default), 1 the reference's 2X - Xt; the plain arms always use 1")
+    ap.add_argument("--tension-order", type=int, default=1, choices=[1, 2],
+                    help="tension start of the value arm's steps (fs_set_tension_extrapolation): 1 linear "
+                         "(default), 2 the reference's quadratic; the plain arms always use 2")
     ap.add_argument("--train-seeds", type=int, default=20, help="plain-solver runs that generate training data")
     ap.add_argument("--workload", default="sediment_512",
                     choices=["sediment_512", "mobility_256", "ensemble_64", "mlp", "trajectory_200"],
@@ -285,6 +298,7 @@ def run_ours(args, rank, world):
 
         seeds = [TRAIN_SEED0 + 100 * rank + i for i in range(args.train_seeds)]
         ctx.set_start_order(args.start_order)  # targets: corrections to the value arm's start
+        ctx.set_tension_extrapolation(args.tension_order)
         feats, tgts, its_tr = generate(make_case, seeds, PREP_STEPS + 1, 1, model=model)
         t1 = time.time()
         model.fit_normalization(feats, tgts)
@@ -311,9 +325,10 @@ def run_ours(args, rank, world):
                   "fs_warm_start_gate_stats")
         return steps, solves
 
-    def timed_steps(prec, mode, profile=False, gate=0, start=1):
+    def timed_steps(prec, mode, profile=False, gate=0, start=1, tension=2):
         ctx.set_precision(prec)
         ctx.set_start_order(start)
+        ctx.set_tension_extrapolation(tension)
         if learned:
             set_warm_start(ctx, mode)
             abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate if mode else 0), "fs_warm_start_gate")
@@ -355,12 +370,14 @@ def run_ours(args, rank, world):
 
     mode = 1 if learned else 0
     gate = GATE_PERIOD if learned else 0
-    start = args.start_order
-    ms, its, st, _, clocks, launches, diag = timed_steps(abi.FS_PREC_FP32, mode, gate=gate, start=start)
+    start, tension = args.start_order, args.tension_order
+    ms, its, st, _, clocks, launches, diag = timed_steps(abi.FS_PREC_FP32, mode, gate=gate, start=start,
+                                                         tension=tension)
     # stage breakdown: the same steps again, host-driven with CUDA-event stage timing
     # (graph-captured steps carry no events); not part of the timed value
     abi.check(abi.lib().fs_set_graph_mode(ctx.h, 0), "fs_set_graph_mode")
     ctx.set_start_order(start)
+    ctx.set_tension_extrapolation(tension)
     if learned:
         set_warm_start(ctx, mode)
         abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate), "fs_warm_start_gate")
@@ -380,8 +397,7 @@ def run_ours(args, rank, world):
         "config": {"workload": WORKLOAD["name"], "grid": [WORKLOAD["npts"]] * 3, "filaments": WORKLOAD["nfil"],
                    "beads_per_filament": nw, "beads": npb, "dt": p.dt, "tol": p.tol,
                    "precision": "mixed", "learned_warm_start": bool(learned),
-                   "start": ("first bead from 3X - 3Xt + Xtt (fs_set_start_order 2)" if start == 2
-                             else "the reference's (first bead from 2X - Xt)"),
+                   "start": start_label(start, tension),
                    "timed_steps": [nt0 + W, nt0 + W + K - 1],
                    "start_up": "steps 1-%d (implicit Euler, constant/linear tension extrapolation) run untimed"
                                % PREP_STEPS,
@@ -449,27 +465,27 @@ def run_ours(args, rank, world):
     # the same steps from the reference's start (no learned iterate), FP32 chain,
     # and with the learned start on every step (no cost gate)
     if learned:
-        msa, itsa, sta, _, _, _, da = timed_steps(abi.FS_PREC_FP32, mode, gate=0, start=start)
+        msa, itsa, sta, _, _, _, da = timed_steps(abi.FS_PREC_FP32, mode, gate=0, start=start, tension=tension)
         nla = da.learned_filaments + da.fallback_filaments
         out["learned_every_step"] = {"value": world * npb * K / (msa / 1e3), "ms_per_step": msa / K,
                                      "iters_per_step": float(np.mean(itsa)),
                                      "status": abi.STATUS_NAMES.get(sta, sta),
                                      "mobility_solves_per_step": da.mobility_solves / K,
                                      "learned_fraction": da.learned_filaments / max(1, nla)}
-    if learned and start == 2:
-        msq, itsq, stq, _, _, _, dq = timed_steps(abi.FS_PREC_FP32, 0, start=2)
-        out["fp32_quadratic_start"] = {"value": world * npb * K / (msq / 1e3), "ms_per_step": msq / K,
+    if learned and (start, tension) != (1, 2):
+        msq, itsq, stq, _, _, _, dq = timed_steps(abi.FS_PREC_FP32, 0, start=start, tension=tension)
+        out["fp32_improved_start"] = {"value": world * npb * K / (msq / 1e3), "ms_per_step": msq / K,
                                        "iters_per_step": float(np.mean(itsq)),
                                        "status": abi.STATUS_NAMES.get(stq, stq),
                                        "mobility_solves_per_step": dq.mobility_solves / K}
-    if learned or start == 2:
-        ms0, its0, st0, _, _, _, d0 = timed_steps(abi.FS_PREC_FP32, 0, start=1)
+    if learned or (start, tension) != (1, 2):
+        ms0, its0, st0, _, _, _, d0 = timed_steps(abi.FS_PREC_FP32, 0, start=1, tension=2)
         out["fp32_plain_start"] = {"value": world * npb * K / (ms0 / 1e3), "ms_per_step": ms0 / K,
                                    "iters_per_step": float(np.mean(its0)), "status": abi.STATUS_NAMES.get(st0, st0),
                                    "mobility_solves_per_step": d0.mobility_solves / K}
     # plain FP64 FCM chain, reference start
     if not args.no_fp64:
-        ms64, its64, st64, _, _, _, d64 = timed_steps(abi.FS_PREC_FP64, 0, start=1)
+        ms64, its64, st64, _, _, _, d64 = timed_steps(abi.FS_PREC_FP64, 0, start=1, tension=2)
         out["plain_fp64"] = {"value": world * npb * K / (ms64 / 1e3), "ms_per_step": ms64 / K,
                              "iters_per_step": float(np.mean(its64)), "status": abi.STATUS_NAMES.get(st64, st64)}
         out["speedup_vs_plain_fp64"] = out["value"] / out["plain_fp64"]["value"]
@@ -478,6 +494,7 @@ def run_ours(args, rank, world):
     if not args.no_e2e:
         ctx.set_precision(abi.FS_PREC_FP32)
         ctx.set_start_order(start)
+        ctx.set_tension_extrapolation(tension)
         if learned:
             set_warm_start(ctx, mode)
             abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate), "fs_warm_start_gate")
@@ -528,10 +545,11 @@ def run_trajectory(args, rank, world):
     from the placed suspension (start-up steps included), once with the mixed-
     precision chain (FP32 spread/FFT/interpolation, FP64 Broyden and mechanics)
     and once in FP64, both from the reference's start, and once more mixed with the
-    second-order start (fs_set_start_order 2), all with graph-captured steady
-    steps. Records per-step Broyden iterations, the status, the final barrier
-    minimum squared distance, the wall time of each run and, for the second-order
-    start, how far its final positions are from the reference start's."""
+    improved start (fs_set_start_order 2, fs_set_tension_extrapolation 1), all
+    with graph-captured steady steps. Records per-step Broyden iterations, the
+    status, the final barrier minimum squared distance, the wall time of each run
+    and, for the improved start, how far its final positions are from the
+    reference start's."""
     import numpy as np
     import torch
     from filsim_b200 import abi
@@ -548,10 +566,12 @@ def run_trajectory(args, rank, world):
     out = {"workload": "trajectory_%d" % nsteps, "grid": [WORKLOAD["npts"]] * 3, "filaments": WORKLOAD["nfil"],
            "beads_per_filament": WORKLOAD["nw"], "beads": susp.np, "dt": p.dt, "tol": p.tol, "steps": nsteps}
     finals = {}
-    for name, prec, start in (("mixed", abi.FS_PREC_FP32, 1), ("mixed_second_order_start", abi.FS_PREC_FP32, 2),
-                              ("fp64", abi.FS_PREC_FP64, 1)):
+    for name, prec, start, tension in (("mixed", abi.FS_PREC_FP32, 1, 2),
+                                       ("mixed_improved_start", abi.FS_PREC_FP32, 2, 1),
+                                       ("fp64", abi.FS_PREC_FP64, 1, 2)):
         ctx.set_precision(prec)
         ctx.set_start_order(start)
+        ctx.set_tension_extrapolation(tension)
         sim = Simulation(ctx, susp.copy())
         torch.cuda.synchronize()
         t0 = time.time()
@@ -567,8 +587,9 @@ def run_trajectory(args, rank, world):
                      "wall_s": wall, "mobility_solves": int(d.mobility_solves), "clocks": clk.summary(),
                      "final_mean_z": float(X[:, 2].mean())}
         finals[name] = X.copy()
-    out["mixed_second_order_start"]["final_max_dX_vs_mixed_over_dx"] = float(
-        np.abs(finals["mixed_second_order_start"] - finals["mixed"]).max() / p.dx)
+    out["mixed_improved_start"]["start"] = start_label(2, 1)
+    out["mixed_improved_start"]["final_max_dX_vs_mixed_over_dx"] = float(
+        np.abs(finals["mixed_improved_start"] - finals["mixed"]).max() / p.dx)
     ctx.close()
     return out
 
@@ -641,7 +662,8 @@ def run_ensemble(args, rank, world):
     torch.cuda.set_device(dev)
     K, W = args.steps, args.warmup
     boxes = make_boxes(ENSEMBLE_SEED + rank)
-    ens = Ensemble(boxes, precision=abi.FS_PREC_FP32, start_order=args.start_order)
+    ens = Ensemble(boxes, precision=abi.FS_PREC_FP32, start_order=args.start_order,
+                   tension_order=args.tension_order)
     t0 = time.time()
     ens.startup(PREP_STEPS)
     t_start = time.time() - t0
@@ -680,8 +702,7 @@ def run_ensemble(args, rank, world):
                       "filaments": int(sum(b[2].nfil for b in boxes)), "beads_per_filament": 16,
                       "timed_steps": [nt0 + W, nt0 + W + K - 1], "start_up_seconds": t_start,
                       "l2": "no flush; most boxes fit in L2 (the workload's own sizes)",
-                      "start": ("first bead from 3X - 3Xt + Xtt (fs_set_start_order 2)" if args.start_order == 2
-                                else "the reference's (first bead from 2X - Xt)")},
+                      "start": start_label(args.start_order, args.tension_order)},
            "box_step_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99)),
                            "max": float(ms.max())},
            "iters_per_step": float(its.mean()), "status": abi.STATUS_NAMES.get(st, st),

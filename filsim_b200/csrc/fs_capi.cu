@@ -243,6 +243,7 @@ fs_status fs_create(const fs_params *p, int max_beads, int max_filaments, void *
   c->max_fil = max_filaments;
   c->precision = p->precision;
   c->start_order = 1;
+  c->tension_order = 2;
   c->L[0] = p->npts_x * p->dx;
   c->L[1] = p->npts_y * p->dx;
   c->L[2] = p->npts_z * p->dx;

@@ -15,7 +15,8 @@
 //   k_schur_apply        filamentJsolver::solve (FilamentJacobianSolver.hpp:49-73): J0^-1 b from
 //                        the Schur inverse, then the bad-Broyden history corrections
 //   k_broyden_cols       history update of main.cpp:640-663
-//   k_update / k_step    Filament::update (Filament.hpp:425-452), Filament::step (:455-478)
+//   k_update / k_step    Filament::update (Filament.hpp:425-452), Filament::step (:455-478); with
+//                        tension order 1 the tensions extrapolated linearly after lambda_extrap_step
 #include <algorithm>
 #include "fs_internal.cuh"
 
@@ -1188,7 +1189,7 @@ __global__ void k_update(int np, const int *__restrict__ fil_id, const int *__re
 __global__ void k_step(int np, int nlink, double *__restrict__ X, double *__restrict__ Xs, double *__restrict__ Xt,
                        double *__restrict__ U, double *__restrict__ Us, double *__restrict__ Ut,
                        double *__restrict__ q, double *__restrict__ qt, double *__restrict__ lam,
-                       double *__restrict__ lam1, double *__restrict__ lam2, int nt, int ex) {
+                       double *__restrict__ lam1, double *__restrict__ lam2, int nt, int ex, int tension_order) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < np) {
     const int b = t;
@@ -1206,12 +1207,12 @@ __global__ void k_step(int np, int nlink, double *__restrict__ X, double *__rest
   }
   if (t < 3 * nlink) {
     const int kk = t;
-    if (nt > ex) {
+    if (nt > ex && tension_order == 2) {
       double lamtmp = 3 * lam[kk] - 3 * lam1[kk] + lam2[kk];
       lam2[kk] = lam1[kk];
       lam1[kk] = lam[kk];
       lam[kk] = lamtmp;
-    } else if (nt == ex) {
+    } else if (nt >= ex) {  // the reference: at nt == ex only; tension order 1 from then on
       double lamtmp = 2. * lam[kk] - lam1[kk];
       lam2[kk] = lam1[kk];
       lam1[kk] = lam[kk];
@@ -1383,7 +1384,8 @@ fs_status fil_step(fs_ctx *c, int nt) {
   ProfScope ps(c, FS_STAGE_UPDATE);
   int n = c->np > 3 * c->nlink ? c->np : 3 * c->nlink;
   k_step<<<fs_blocks(n, 256), 256, 0, c->stream>>>(c->np, c->nlink, c->X, c->Xs, c->Xt, c->U, c->Us, c->Ut, c->q,
-                                                    c->qt, c->lam, c->lam1, c->lam2, nt, c->p.lambda_extrap_step);
+                                                    c->qt, c->lam, c->lam1, c->lam2, nt, c->p.lambda_extrap_step,
+                                                    c->tension_order == 1 ? 1 : 2);
   FS_LAUNCH_CHECK();
   return FS_OK;
 }

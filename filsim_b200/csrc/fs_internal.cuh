@@ -125,6 +125,9 @@ struct fs_ctx {
   // start of the implicit step (fs_set_start_order, fs_start.cu): 1 the reference's
   // first-bead extrapolation 2X - Xt, 2 quadratic, 3X - 3Xt + Xtt
   int start_order;
+  // tension start of the next step (fs_set_tension_extrapolation, fs_start.cu): 2 the
+  // reference's quadratic extrapolation after lambda_extrap_step, 1 linear (0: 2)
+  int tension_order;
   // positions two steps back (fs_start.cu), kept while the quadratic or the learned
   // start is on (3 max_beads doubles each); hist_ok (device): steps run since the
   // history was reset, up to 2 (hist_Xtt holds positions two steps back once it is

@@ -18,6 +18,13 @@
 //
 // The history is also the learned start's acceleration feature (fs_mlp.cu). It
 // is kept while either needs it: before Filament::step moves X to Xt, Xtt <- Xt.
+//
+// Filament::step also starts the next step's tensions: constant before
+// lambda_extrap_step, linear at it and quadratic, 3 lam - 3 lam1 + lam2, after it
+// (main.cpp's lambda extrapolation). The converged tensions carry the Broyden
+// tolerance's noise, which the quadratic extrapolation multiplies by up to 7;
+// tension order 1 keeps the linear 2 lam - lam1 (noise up to 3) after
+// lambda_extrap_step too.
 #include "fs_internal.cuh"
 
 namespace {
@@ -119,6 +126,13 @@ fs_status fs_set_start_order(fs_ctx *c, int order) {
   // a history no longer kept would go stale
   if (!hist_wanted(c) && c->hist_ok) FS_CUDA(cudaMemsetAsync(c->hist_ok, 0, sizeof(int), c->stream));
   graph_invalidate(c);  // captured steps bake the start
+  return FS_OK;
+}
+
+fs_status fs_set_tension_extrapolation(fs_ctx *c, int order) {
+  if (!c || (order != 1 && order != 2)) return FS_ERR_INVALID_ARG;
+  c->tension_order = order;
+  graph_invalidate(c);  // captured steps bake Filament::step's extrapolation
   return FS_OK;
 }
 

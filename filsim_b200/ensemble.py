@@ -6,8 +6,8 @@ gravity (0,0,-1) per bead, dt = 0.05, BDF2. Filament counts are capped at a bead
 volume fraction of 5% (48^3: 12, 64^3: 30, 96^3: 102, 128^3: 243): the uncapped
 draw is not placeable (256 filaments of 16 beads fill 99.8% of a 48^3 box).
 
-Each box is its own context (grid, parameters, suspension, stream, start order:
-fs_set_start_order). After the start-up steps every ensemble step is one CUDA
+Each box is its own context (grid, parameters, suspension, stream, step start:
+fs_set_start_order, fs_set_tension_extrapolation). After the start-up steps every ensemble step is one CUDA
 graph launch holding every box's captured step, Broyden loops on the device
 (fs_graph.cu).
 """
@@ -51,13 +51,14 @@ def make_boxes(seed, nboxes=64, grids=GRIDS, nfil_range=(8, 256), nw=NW, kb_rang
 class Ensemble:
     """One context per box, all advanced by fs_batch_run."""
 
-    def __init__(self, boxes, precision=abi.FS_PREC_FP32, start_order=1):
+    def __init__(self, boxes, precision=abi.FS_PREC_FP32, start_order=1, tension_order=2):
         self.boxes = boxes
         self.ctxs, self.sims = [], []
         for npts, p, s, kb in boxes:
             c = Context(p, max_beads=s.np, max_filaments=s.nfil)
             c.set_precision(precision)
             c.set_start_order(start_order)
+            c.set_tension_extrapolation(tension_order)
             check(lib().fs_set_graph_mode(c.h, 1), "fs_set_graph_mode")
             self.ctxs.append(c)
             self.sims.append(Simulation(c, s))

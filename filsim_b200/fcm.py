@@ -80,6 +80,11 @@ class Context:
         3X - 3Xt + Xtt once the context holds the positions two steps back."""
         check(lib().fs_set_start_order(self.h, order), "fs_set_start_order")
 
+    def set_tension_extrapolation(self, order):
+        """2: the reference's quadratic tension extrapolation after lambda_extrap_step;
+        1: linear from lambda_extrap_step on."""
+        check(lib().fs_set_tension_extrapolation(self.h, order), "fs_set_tension_extrapolation")
+
     def device_bytes(self):
         n = ctypes.c_size_t()
         check(lib().fs_device_bytes(self.h, ctypes.byref(n)), "fs_device_bytes")

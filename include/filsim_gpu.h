@@ -495,6 +495,14 @@ fs_status fs_set_warm_start(fs_ctx *ctx, int mode);
  * unchanged: a step converges to the same tolerance from either start. A
  * learned start (fs_set_warm_start) corrects whichever start is set. */
 fs_status fs_set_start_order(fs_ctx *ctx, int order);
+/* Tension start of each step, set by Filament::step for the next one (no
+ * reference counterpart). order 2 (the default): the reference's constant
+ * extrapolation before lambda_extrap_step, linear at it, quadratic
+ * (3 lam - 3 lam1 + lam2) after it. order 1: linear (2 lam - lam1) from
+ * lambda_extrap_step on: the converged tensions carry the Broyden tolerance's
+ * noise, which the quadratic extrapolation amplifies up to 7x and the linear one
+ * up to 3x. The Broyden loop and its convergence test are unchanged. */
+fs_status fs_set_tension_extrapolation(fs_ctx *ctx, int order);
 /* Cost gate of the learned start (no reference counterpart): with period > 0,
  * each step runs the start whose running mean of mobility solves per step is
  * lower (the learned one only when it is lower by at least the margin of

@@ -43,6 +43,10 @@ class Context {
   void set_precision(int prec) { check(fs_set_precision(ctx_, prec), "fs_set_precision"); }
   // 2: the first bead of each filament started from 3X - 3Xt + Xtt (1: the reference's 2X - Xt)
   void set_start_order(int order) { check(fs_set_start_order(ctx_, order), "fs_set_start_order"); }
+  // 1: tensions extrapolated linearly after lambda_extrap_step (2: the reference's quadratic)
+  void set_tension_extrapolation(int order) {
+    check(fs_set_tension_extrapolation(ctx_, order), "fs_set_tension_extrapolation");
+  }
   // steady steps as CUDA graphs with the Broyden loop on the device
   void set_graph_mode(bool on) { check(fs_set_graph_mode(ctx_, on ? 1 : 0), "fs_set_graph_mode"); }
   // fastest launch variants for the uploaded suspension; returns ms per mobility solve
