@@ -652,16 +652,27 @@ def run_ensemble(args, rank, world):
     gravity, dt = 0.05), FP32 chain. After 12 untimed start-up steps per box, each
     ensemble step is one CUDA graph launch holding every box's step with its
     Broyden loop on the device. Beside it: the same boxes stepped one at a time by
-    the host-driven step."""
+    the host-driven step. With several ranks (one GPU each) the same 64 boxes are
+    split by estimated cost (partition_boxes): each rank runs its share as one
+    ensemble, the time is the slowest rank's, and the value is all boxes' bead-steps
+    over it (strong scaling; no collective on the data)."""
     import numpy as np
     import torch
     from filsim_b200 import abi
-    from filsim_b200.ensemble import Ensemble, make_boxes
+    from filsim_b200 import replicas
+    from filsim_b200.ensemble import Ensemble, make_boxes, partition_boxes
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", dev))
     K, W = args.steps, args.warmup
-    boxes = make_boxes(ENSEMBLE_SEED + rank)
+    all_boxes = make_boxes(ENSEMBLE_SEED)
+    mine = partition_boxes(all_boxes, world)[rank]
+    boxes = [all_boxes[i] for i in mine]
     ens = Ensemble(boxes, precision=abi.FS_PREC_FP32, start_order=args.start_order,
                    tension_order=args.tension_order)
     t0 = time.time()
@@ -671,12 +682,15 @@ def run_ensemble(args, rank, world):
     nt0 = PREP_STEPS + 1
     ens.run(nt0, W)                                    # captures the ensemble graph, warms up
     launches0 = abi.lib().fs_kernel_launches()
+    replicas.barrier(dist)
     with ClockSampler(dev) as clk:
         torch.cuda.nvtx.range_push("timed_steps")
         its, ms, total, st = ens.run(nt0 + W, K)
         torch.cuda.nvtx.range_pop()
+    replicas.barrier(dist)
     launches = abi.lib().fs_kernel_launches() - launches0
-    beads = int(ens.beads.sum())
+    total = replicas.max_over_ranks(total, dist, device="cuda")
+    beads = int(sum(b[2].np for b in all_boxes))
     value = beads * K / (total / 1e3)
     # the same boxes, one at a time, host-driven steps (no graphs, one sync per iteration)
     K2 = max(1, min(K, 4))
@@ -691,15 +705,17 @@ def run_ensemble(args, rank, world):
         sim.run_steps(nt0 + W + K, K2)
         c.synchronize()
         seq_ms += (time.perf_counter() - t1) * 1e3
+    seq_ms = replicas.max_over_ranks(seq_ms, dist, device="cuda")
     seq_value = beads * K2 / (seq_ms / 1e3)
-    grids = [b[0] for b in boxes]
+    grids = [b[0] for b in all_boxes]
     out = {"metric": "bead-steps/s (ensemble of 64 boxes, one graph launch per step)", "value": value,
-           "unit": "bead-steps/s", "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": total / K,
-           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 FCM chain + f64 Broyden",
+           "unit": "bead-steps/s", "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": total / K,
+           "higher_is_better": True, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+           "dtype": "f32 FCM chain + f64 Broyden",
            "data": "synthetic (seeded rejection-placed filaments)",
-           "config": {"workload": "ensemble_64", "boxes": len(boxes),
+           "config": {"workload": "ensemble_64", "boxes": len(all_boxes), "boxes_per_rank": len(boxes),
                       "grids": {str(g): grids.count(g) for g in sorted(set(grids))}, "beads": beads,
-                      "filaments": int(sum(b[2].nfil for b in boxes)), "beads_per_filament": 16,
+                      "filaments": int(sum(b[2].nfil for b in all_boxes)), "beads_per_filament": 16,
                       "timed_steps": [nt0 + W, nt0 + W + K - 1], "start_up_seconds": t_start,
                       "l2": "no flush; most boxes fit in L2 (the workload's own sizes)",
                       "start": start_label(args.start_order, args.tension_order)},
@@ -714,7 +730,10 @@ def run_ensemble(args, rank, world):
            "sequential_host_driven": {"value": seq_value, "ms_per_ensemble_step": seq_ms / K2, "steps": K2},
            "speedup_vs_sequential": value / seq_value}
     ens.close()
-    return out
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out if rank == 0 else None
 
 
 def run_mlp(args, rank, world):

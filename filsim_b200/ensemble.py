@@ -7,9 +7,11 @@ volume fraction of 5% (48^3: 12, 64^3: 30, 96^3: 102, 128^3: 243): the uncapped
 draw is not placeable (256 filaments of 16 beads fill 99.8% of a 48^3 box).
 
 Each box is its own context (grid, parameters, suspension, stream, step start:
-fs_set_start_order, fs_set_tension_extrapolation). After the start-up steps every ensemble step is one CUDA
-graph launch holding every box's captured step, Broyden loops on the device
-(fs_graph.cu).
+fs_set_start_order, fs_set_tension_extrapolation). After the start-up steps every
+ensemble step is one CUDA graph launch holding every box's captured step, Broyden
+loops on the device (fs_graph.cu). Over several GPUs the boxes are split by estimated cost
+(partition_boxes), one ensemble per rank; the boxes are independent, so no
+collective touches the data.
 """
 import ctypes
 import math
@@ -46,6 +48,29 @@ def make_boxes(seed, nboxes=64, grids=GRIDS, nfil_range=(8, 256), nw=NW, kb_rang
         s = random_suspension(p, nfil, nw, seed=seed * 1000 + i, kap=kb)
         boxes.append((npts, p, s, kb))
     return boxes
+
+
+def box_cost(npts, nbeads):
+    """Estimated cost of one box-step: its FCM solves stream the grid (npts^3
+    points) and spread/interpolate 12^3-point stencils per bead; iterations per
+    step are not known in advance and are taken as equal across boxes."""
+    return float(npts) ** 3 + 12.0 ** 3 * nbeads
+
+
+def partition_boxes(boxes, world):
+    """Boxes (the make_boxes tuples) split over `world` ranks by estimated cost:
+    the most expensive box first, each to the rank with the least cost so far
+    (ties to the lower rank). Returns, per rank, the indices of its boxes in
+    ascending order; every box goes to exactly one rank."""
+    cost = [box_cost(npts, s.np) for npts, _, s, _ in boxes]
+    order = sorted(range(len(boxes)), key=lambda i: (-cost[i], i))
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += cost[i]
+    return [sorted(p) for p in parts]
 
 
 class Ensemble:
