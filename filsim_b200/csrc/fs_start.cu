@@ -85,8 +85,9 @@ void hist_free(fs_ctx *c) {
 // with it): Xtt <- Xt, the positions two steps back once X has moved to Xt
 fs_status hist_end_step(fs_ctx *c) {
   if (!c->hist_Xtt || !hist_wanted(c)) return FS_OK;
-  FS_CUDA(cudaMemcpyAsync(c->hist_Xtt, c->Xt, sizeof(double) * 3 * (size_t)c->np, cudaMemcpyDeviceToDevice,
-                          c->stream));
+  if (c->np > 0)
+    FS_CUDA(cudaMemcpyAsync(c->hist_Xtt, c->Xt, sizeof(double) * 3 * (size_t)c->np, cudaMemcpyDeviceToDevice,
+                            c->stream));
   k_hist_tick<<<1, 1, 0, c->stream>>>(c->hist_ok);
   FS_LAUNCH_CHECK();
   return FS_OK;
@@ -95,7 +96,7 @@ fs_status hist_end_step(fs_ctx *c) {
 // around fs_state_upload: the history stays valid when the upload repeats X and Xt
 fs_status hist_before_upload(fs_ctx *c, bool same_layout) {
   c->hist_cmp_pending = false;
-  if (!c->hist_Xtt) return FS_OK;
+  if (!c->hist_Xtt || (same_layout && c->np == 0)) return FS_OK;  // no beads: nothing to compare
   if (!same_layout) {
     FS_CUDA(cudaMemsetAsync(c->hist_ok, 0, sizeof(int), c->stream));
     return FS_OK;
