@@ -58,7 +58,7 @@ class FsDiag(ctypes.Structure):
         ("last_nt", c_int), ("last_iters", c_int), ("total_iters", c_longlong), ("mobility_solves", c_longlong),
         ("not_converged_steps", c_int), ("nonfinite", c_int), ("explosion", c_int), ("reserved", c_int),
         ("min_dist2", c_double), ("last_max_abs_err", c_double),
-        ("learned_filaments", c_longlong), ("fallback_filaments", c_longlong),
+        ("learned_filaments", c_longlong), ("fallback_filaments", c_longlong), ("escalated_iters", c_longlong),
     ]
 
 
@@ -218,6 +218,7 @@ def _declare(L):
         "fs_warm_start_gate": (c_int, [c_void_p, c_int]),
         "fs_set_start_order": (c_int, [c_void_p, c_int]),
         "fs_set_tension_extrapolation": (c_int, [c_void_p, c_int]),
+        "fs_set_precision_escalation": (c_int, [c_void_p, c_int]),
         "fs_warm_start_gate_margin": (c_int, [c_void_p, c_double]),
         "fs_warm_start_bound": (c_int, [c_void_p, c_int]),
         "fs_set_slab": (c_int, [c_void_p, c_int, c_int]),

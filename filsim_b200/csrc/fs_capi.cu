@@ -143,7 +143,24 @@ fs_status step_implicit(fs_ctx *c, int nt, int *iters_out, bool commit = true, i
   if (c->flags_h[FLAG_PIVOT]) return FS_ERR_NONFINITE;
   int check = c->flags_h[FLAG_CHECK];
   int iter = 0;
+  // precision escalation: an FP32 step past escalate_after iterations finishes in FP64
+  struct Precision {
+    fs_ctx *c;
+    int prec;
+    ~Precision() {
+      if (c->precision != prec) {
+        c->precision = prec;
+        fcm_set_stream(c, c->stream);
+      }
+    }
+  } restore{c, c->precision};
+  const int esc = (c->precision == FS_PREC_FP32 && c->escalate_after > 0) ? c->escalate_after : 0;
   while (check && iter < c->p.broyden_maxiter) {
+    if (esc > 0 && iter == esc) {
+      c->precision = FS_PREC_FP64;
+      FS_TRY(fcm_set_stream(c, c->stream));
+    }
+    if (c->precision != restore.prec) c->diag.escalated_iters++;
     FS_TRY(fil_broyden_apply(c, c->err, c->upd, iter));
     FS_TRY(fil_state_update(c, c->upd));
     FS_TRY(fil_forces(c, nt));
@@ -828,6 +845,13 @@ fs_status fs_step_implicit(fs_ctx *c, int nt, int *iters_h) {
   }
   if (use_gated_graph(c, nt)) return run_one_gated(c, nt, iters_h);
   return run_one(c, nt, iters_h);
+}
+
+fs_status fs_set_precision_escalation(fs_ctx *c, int after_iters) {
+  if (!c || after_iters < 0) return FS_ERR_INVALID_ARG;
+  c->escalate_after = after_iters;
+  graph_invalidate(c);  // captured FP32 steps bake the second loop
+  return FS_OK;
 }
 
 fs_status fs_set_graph_mode(fs_ctx *c, int on) {

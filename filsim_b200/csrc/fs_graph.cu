@@ -8,7 +8,9 @@
 // forces, Jacobian, cell link, first barrier + mobility solve and residual), a
 // conditional WHILE node whose body is one Broyden iteration (apply, update,
 // forces, barrier + mobility, residual, history column, err <- newerr), and the
-// end of the step (Filament::step). The loop condition is the reference's
+// end of the step (Filament::step). With precision escalation an FP32 step has a
+// second WHILE node after the first, its body captured with the FP64 chain. The
+// loop condition is the reference's
 // `check` (any |Err| > TOL) and iter < broyden_maxiter, set on the device by
 // cudaGraphSetConditional; the iteration count lives in device memory and the
 // Broyden kernels read it there. A run of steps is a sequence of graph launches
@@ -19,7 +21,7 @@
 #include <vector>
 #include "fs_internal.cuh"
 
-enum { GD_ITER = 0, GD_STEPS, GD_NONFIN, GD_EXPLODE, GD_NOTCONV, GD_PIVOT, GD_CAPACITY, GD_HDR = 8 };
+enum { GD_ITER = 0, GD_STEPS, GD_NONFIN, GD_EXPLODE, GD_NOTCONV, GD_PIVOT, GD_CAPACITY, GD_ESC, GD_HDR = 8 };
 constexpr int GRAPH_STEP_SLOTS = 4096;
 
 struct fs_graph {
@@ -29,6 +31,7 @@ struct fs_graph {
   int *host = nullptr;  // pinned copy
   unsigned long long *ts = nullptr;  // per launched step: device clock (ns) at its start and end (batches)
   unsigned long long kpre = 0, kbody = 0;  // kernels per launch outside / inside the loop
+  unsigned long long kbody64 = 0;          // kernels per iteration of the escalated FP64 loop
   int precision = -1, np = -1, nfil = -1, pending = 0;
 };
 
@@ -44,12 +47,19 @@ __global__ void k_loop_head(int *__restrict__ gd, const int *__restrict__ flags,
 }
 
 __global__ void k_loop_tail(int *__restrict__ gd, const int *__restrict__ flags, int maxiter,
-                            cudaGraphConditionalHandle h) {
+                            cudaGraphConditionalHandle h, int escalated) {
   const int it = gd[GD_ITER] + 1;
   gd[GD_ITER] = it;
+  if (escalated) gd[GD_ESC] += 1;
   gd[GD_NONFIN] |= flags[FLAG_NONFINITE];
   gd[GD_EXPLODE] |= flags[FLAG_EXPLODE];
   cudaGraphSetConditional(h, (flags[FLAG_CHECK] && it < maxiter) ? 1u : 0u);
+}
+
+// between the FP32 loop and the escalated FP64 loop: go on while unconverged
+__global__ void k_loop_mid(const int *__restrict__ gd, const int *__restrict__ flags, int maxiter,
+                           cudaGraphConditionalHandle h) {
+  cudaGraphSetConditional(h, (flags[FLAG_CHECK] && gd[GD_ITER] < maxiter) ? 1u : 0u);
 }
 
 __global__ void k_step_done(int *__restrict__ gd, const int *__restrict__ flags, int slots) {
@@ -67,35 +77,11 @@ __global__ void k_stamp(const int *__restrict__ gd, unsigned long long *__restri
   if (k >= 0 && k < slots) ts[2 * k + which] = t;
 }
 
-// the start, loop and end of one step, captured on c->stream
-fs_status capture_step(fs_ctx *c, int nt, fs_graph *g, cudaGraph_t *out) {
-  const int maxiter = c->p.broyden_maxiter;
-  FS_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(int) * FLAG_COUNT, c->stream));
-  FS_TRY(fil_initial_guess(c));
-  FS_TRY(fil_forces(c, nt));
-  FS_TRY(fil_jacobian_build(c, nt));
-  FS_TRY(cells_link(c, c->Xs, c->np));
-  FS_TRY(step_barrier_mobility(c, nt));
-  FS_TRY(fil_error_check(c, c->V, c->W, c->err, nt));
-  cudaStreamCaptureStatus cs;
-  cudaGraph_t cg;
-  const cudaGraphNode_t *deps = nullptr;
-  size_t nd = 0;
-  FS_CUDA(cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &cg, &deps, &nd));
-  cudaGraphConditionalHandle h;
-  FS_CUDA(cudaGraphConditionalHandleCreate(&h, cg, 0, 0));
-  k_loop_head<<<1, 1, 0, c->stream>>>(g->dev, c->flags, maxiter, h);
-  FS_LAUNCH_CHECK();
-  FS_CUDA(cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &cg, &deps, &nd));
-  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
-  cp.conditional.handle = h;
-  cp.conditional.type = cudaGraphCondTypeWhile;
-  cp.conditional.size = 1;
-  cudaGraphNode_t cnode;
-  FS_CUDA(cudaGraphAddNode(&cnode, cg, deps, nd, &cp));
-  FS_CUDA(cudaStreamUpdateCaptureDependencies(c->stream, &cnode, 1, cudaStreamSetCaptureDependencies));
-  // one Broyden iteration (main.cpp:572-673), captured into the loop body
-  cudaGraph_t body = cp.conditional.phGraph_out[0];
+// one Broyden iteration (main.cpp:572-673) captured into the conditional node's
+// body graph on g->body_stream, ending with the loop condition (limit: the last
+// iteration count it may reach)
+fs_status capture_body(fs_ctx *c, int nt, fs_graph *g, cudaGraph_t body, cudaGraphConditionalHandle h, int limit,
+                       bool escalated, unsigned long long *kernels) {
   cudaStream_t main_stream = c->stream;
   const unsigned long long k0 = __atomic_load_n(&g_fs_kernel_launches, __ATOMIC_RELAXED);
   FS_CUDA(cudaStreamBeginCaptureToGraph(g->body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
@@ -112,7 +98,7 @@ fs_status capture_step(fs_ctx *c, int nt, fs_graph *g, cudaGraph_t *out) {
                                      c->stream) != cudaSuccess)
     st = FS_ERR_CUDA;
   if (st == FS_OK) {
-    k_loop_tail<<<1, 1, 0, c->stream>>>(g->dev, c->flags, maxiter, h);
+    k_loop_tail<<<1, 1, 0, c->stream>>>(g->dev, c->flags, limit, h, escalated ? 1 : 0);
     if (cudaGetLastError() != cudaSuccess) st = FS_ERR_CUDA;
     __atomic_fetch_add(&g_fs_kernel_launches, 1ull, __ATOMIC_RELAXED);
   }
@@ -120,10 +106,78 @@ fs_status capture_step(fs_ctx *c, int nt, fs_graph *g, cudaGraph_t *out) {
   const cudaError_t e_end = cudaStreamEndCapture(g->body_stream, &body_out);
   c->stream = main_stream;
   const fs_status st2 = fcm_set_stream(c, c->stream);
-  g->kbody = __atomic_load_n(&g_fs_kernel_launches, __ATOMIC_RELAXED) - k0;
+  *kernels = __atomic_load_n(&g_fs_kernel_launches, __ATOMIC_RELAXED) - k0;
   FS_TRY(st);
   FS_TRY(st2);
   FS_CUDA(e_end);
+  return FS_OK;
+}
+
+// a conditional handle of the graph being captured on c->stream
+fs_status new_cond_handle(fs_ctx *c, cudaGraphConditionalHandle *h) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cg;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  FS_CUDA(cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &cg, &deps, &nd));
+  FS_CUDA(cudaGraphConditionalHandleCreate(h, cg, 0, 0));
+  return FS_OK;
+}
+
+// a conditional WHILE node after the capture's current dependencies; its body graph
+fs_status add_while_node(fs_ctx *c, cudaGraphConditionalHandle h, cudaGraph_t *body) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cg;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  FS_CUDA(cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &cg, &deps, &nd));
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  FS_CUDA(cudaGraphAddNode(&cnode, cg, deps, nd, &cp));
+  FS_CUDA(cudaStreamUpdateCaptureDependencies(c->stream, &cnode, 1, cudaStreamSetCaptureDependencies));
+  *body = cp.conditional.phGraph_out[0];
+  return FS_OK;
+}
+
+// the start, loop(s) and end of one step, captured on c->stream. With precision
+// escalation (fs_set_precision_escalation) an FP32 step runs two loops: the FP32
+// iterations up to the escalation count, then, while unconverged, the rest with
+// the FP64 chain.
+fs_status capture_step(fs_ctx *c, int nt, fs_graph *g, cudaGraph_t *out) {
+  const int maxiter = c->p.broyden_maxiter;
+  const int esc = (c->precision == FS_PREC_FP32 && c->escalate_after > 0) ? c->escalate_after : 0;
+  const int limit1 = esc > 0 && esc < maxiter ? esc : maxiter;
+  FS_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(int) * FLAG_COUNT, c->stream));
+  FS_TRY(fil_initial_guess(c));
+  FS_TRY(fil_forces(c, nt));
+  FS_TRY(fil_jacobian_build(c, nt));
+  FS_TRY(cells_link(c, c->Xs, c->np));
+  FS_TRY(step_barrier_mobility(c, nt));
+  FS_TRY(fil_error_check(c, c->V, c->W, c->err, nt));
+  cudaGraphConditionalHandle h;
+  FS_TRY(new_cond_handle(c, &h));
+  k_loop_head<<<1, 1, 0, c->stream>>>(g->dev, c->flags, limit1, h);
+  FS_LAUNCH_CHECK();
+  cudaGraph_t body;
+  FS_TRY(add_while_node(c, h, &body));
+  FS_TRY(capture_body(c, nt, g, body, h, limit1, false, &g->kbody));
+  g->kbody64 = 0;
+  if (esc > 0 && limit1 < maxiter) {
+    cudaGraphConditionalHandle h2;
+    FS_TRY(new_cond_handle(c, &h2));
+    k_loop_mid<<<1, 1, 0, c->stream>>>(g->dev, c->flags, maxiter, h2);
+    FS_LAUNCH_CHECK();
+    cudaGraph_t body2;
+    FS_TRY(add_while_node(c, h2, &body2));
+    c->precision = FS_PREC_FP64;
+    const fs_status st = capture_body(c, nt, g, body2, h2, maxiter, true, &g->kbody64);
+    c->precision = FS_PREC_FP32;
+    FS_TRY(st);
+    FS_TRY(fcm_set_stream(c, c->stream));
+  }
   FS_TRY(learn_end_step(c));
   FS_TRY(hist_end_step(c));
   FS_TRY(fil_step(c, nt));
@@ -175,6 +229,13 @@ static fs_status graph_prepare(fs_ctx *c) {
     FS_CUDA(cudaMemsetAsync(g->dev, 0, sizeof(int) * GD_HDR, c->stream));
   }
   FS_TRY(fcm_set_stream(c, c->stream));
+  if (c->precision == FS_PREC_FP32 && c->escalate_after > 0) {
+    // the escalated loop's FP64 plans must exist before a capture
+    c->precision = FS_PREC_FP64;
+    const fs_status st = fcm_set_stream(c, c->stream);
+    c->precision = FS_PREC_FP32;
+    FS_TRY(st);
+  }
   return learn_prepare_capture(c);
 }
 
@@ -195,7 +256,7 @@ static fs_status graph_build(fs_ctx *c, int nt) {
   // captured kernels were counted once; launches are counted per graph launch instead
   const unsigned long long captured = __atomic_load_n(&g_fs_kernel_launches, __ATOMIC_RELAXED) - k0;
   __atomic_fetch_sub(&g_fs_kernel_launches, captured, __ATOMIC_RELAXED);
-  g->kpre = captured - g->kbody;
+  g->kpre = captured - g->kbody - g->kbody64;
   if (st != FS_OK) {
     if (graph) cudaGraphDestroy(graph);
     return st;
@@ -231,7 +292,11 @@ fs_status graph_flush(fs_ctx *c, int *iters_h) {
   c->diag.last_iters = g->host[GD_HDR + n - 1];
   c->diag.mobility_solves += n + its;
   c->diag.not_converged_steps += g->host[GD_NOTCONV];
-  __atomic_fetch_add(&g_fs_kernel_launches, (unsigned long long)n * g->kpre + (unsigned long long)its * g->kbody,
+  const long long esc_its = g->host[GD_ESC];  // iterations of the escalated FP64 loop
+  c->diag.escalated_iters += esc_its;
+  __atomic_fetch_add(&g_fs_kernel_launches,
+                     (unsigned long long)n * g->kpre + (unsigned long long)(its - esc_its) * g->kbody +
+                         (unsigned long long)esc_its * g->kbody64,
                      __ATOMIC_RELAXED);
   if (g->host[GD_NONFIN]) c->diag.nonfinite = 1;
   if (g->host[GD_EXPLODE]) c->diag.explosion = 1;
@@ -303,7 +368,7 @@ static fs_status batch_build(fs_batch *b, int nt) {
     __atomic_fetch_add(&g_fs_kernel_launches, 1ull, __ATOMIC_RELAXED);
     if (cudaGetLastError() != cudaSuccess || cudaEventRecord(b->join[i], c->stream) != cudaSuccess) st = FS_ERR_CUDA;
     const unsigned long long kb = __atomic_load_n(&g_fs_kernel_launches, __ATOMIC_RELAXED) - k0;
-    g->kpre = kb - g->kbody;
+    g->kpre = kb - g->kbody - g->kbody64;
     captured += kb;
   }
   for (int i = 0; i < b->n && st == FS_OK; ++i)

@@ -128,6 +128,9 @@ struct fs_ctx {
   // tension start of the next step (fs_set_tension_extrapolation, fs_start.cu): 2 the
   // reference's quadratic extrapolation after lambda_extrap_step, 1 linear (0: 2)
   int tension_order;
+  // FP32 steps go on in FP64 after this many Broyden iterations (0: never;
+  // fs_set_precision_escalation)
+  int escalate_after;
   // positions two steps back (fs_start.cu), kept while the quadratic or the learned
   // start is on (3 max_beads doubles each); hist_ok (device): steps run since the
   // history was reset, up to 2 (hist_Xtt holds positions two steps back once it is

@@ -85,6 +85,11 @@ class Context:
         1: linear from lambda_extrap_step on."""
         check(lib().fs_set_tension_extrapolation(self.h, order), "fs_set_tension_extrapolation")
 
+    def set_precision_escalation(self, after_iters):
+        """FP32 steps still not converged after after_iters Broyden iterations run the
+        rest of their iterations with the FP64 chain; 0 turns it off."""
+        check(lib().fs_set_precision_escalation(self.h, after_iters), "fs_set_precision_escalation")
+
     def device_bytes(self):
         n = ctypes.c_size_t()
         check(lib().fs_device_bytes(self.h, ctypes.byref(n)), "fs_device_bytes")

@@ -102,6 +102,7 @@ typedef struct fs_diag {
   double last_max_abs_err;      /* max |Err| at the end of the last step */
   long long learned_filaments;  /* filament-steps started from the learned iterate */
   long long fallback_filaments; /* filament-steps put back to the plain start (worse first residual) */
+  long long escalated_iters;    /* Broyden iterations FP32 steps ran in FP64 (fs_set_precision_escalation) */
 } fs_diag;
 
 /*
@@ -503,6 +504,14 @@ fs_status fs_set_start_order(fs_ctx *ctx, int order);
  * noise, which the quadratic extrapolation amplifies up to 7x and the linear one
  * up to 3x. The Broyden loop and its convergence test are unchanged. */
 fs_status fs_set_tension_extrapolation(fs_ctx *ctx, int order);
+/* Precision escalation of the mixed-precision chain (no reference counterpart):
+ * with after_iters > 0 and the context in FS_PREC_FP32, a step still not
+ * converged after after_iters Broyden iterations runs its remaining iterations
+ * with the FP64 chain (host-driven and captured steps alike), then the next
+ * step starts in FP32 again. The FP32 chain's error (~1e-6 of the velocities)
+ * can leave a step that starts close to the tolerance wandering near it; the
+ * FP64 iterations end that. 0 (the default) turns it off. */
+fs_status fs_set_precision_escalation(fs_ctx *ctx, int after_iters);
 /* Cost gate of the learned start (no reference counterpart): with period > 0,
  * each step runs the start whose running mean of mobility solves per step is
  * lower (the learned one only when it is lower by at least the margin of

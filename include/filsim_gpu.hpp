@@ -47,6 +47,10 @@ class Context {
   void set_tension_extrapolation(int order) {
     check(fs_set_tension_extrapolation(ctx_, order), "fs_set_tension_extrapolation");
   }
+  // FP32 steps not converged after after_iters Broyden iterations finish in FP64 (0: off)
+  void set_precision_escalation(int after_iters) {
+    check(fs_set_precision_escalation(ctx_, after_iters), "fs_set_precision_escalation");
+  }
   // steady steps as CUDA graphs with the Broyden loop on the device
   void set_graph_mode(bool on) { check(fs_set_graph_mode(ctx_, on ? 1 : 0), "fs_set_graph_mode"); }
   // fastest launch variants for the uploaded suspension; returns ms per mobility solve
