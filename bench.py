@@ -101,6 +101,22 @@ def start_label(start, tension):
     return "%s; %s after lambda_extrap_step" % (pos, ten)
 
 
+# Broyden memory across steps (fs_set_broyden_memory): keep J0 and up to 16 history
+# columns after a step of fewer than 8 iterations, carry the last 4 columns after a
+# longer one, restart a step on carried state at 30 iterations
+MEMORY_DEFAULT = (16, 4, 8, 30)
+MEMORY_OFF = (0, 0, 0, 0)
+
+
+def memory_label(mem):
+    """The config's description of the Broyden memory (fs_set_broyden_memory)."""
+    if tuple(mem) == MEMORY_OFF:
+        return "off (the reference's iteration: J0 rebuilt and the history emptied every step)"
+    k, c, t, r = mem
+    return ("J0 and up to %d history columns kept after a step of fewer than %d iterations; the last %d columns "
+            "carried beside a new J0 after a longer one; restart at %d iterations" % (k, t, c, r))
+
+
 def warp_fft_length(n):
     """Grid lengths the FP32 warp transform covers on every axis (fs_fft.cu): 2^p in
     [64, 512] or 96, 192, 384; other grids run cuFFT."""
@@ -124,6 +140,13 @@ def parse():
     ap.add_argument("--tension-order", type=int, default=1, choices=[1, 2],
                     help="tension start of the value arm's steps (fs_set_tension_extrapolation): 1 linear "
                          "(default), 2 the reference's quadratic; the plain arms always use 2")
+    ap.add_argument("--escalate", type=int, default=0,
+                    help="fs_set_precision_escalation for the value arm and the ensemble: FP32 steps still not "
+                         "converged after this many Broyden iterations finish in FP64 (0: off, the default; "
+                         "trajectory_200 runs it beside the plain runs, at 15 unless given)")
+    ap.add_argument("--broyden-memory", default=":".join(map(str, MEMORY_DEFAULT)),
+                    help="fs_set_broyden_memory for the value arm and the ensemble, KEEP:CARRY:THRESHOLD:RESTART "
+                         "(default %s); 0 turns it off (the reference's iteration)" % ":".join(map(str, MEMORY_DEFAULT)))
     ap.add_argument("--train-seeds", type=int, default=20, help="plain-solver runs that generate training data")
     ap.add_argument("--workload", default="sediment_512",
                     choices=["sediment_512", "mobility_256", "ensemble_64", "mlp", "trajectory_200"],
@@ -137,6 +160,9 @@ def parse():
                          "workload name in config says so)")
     ap.add_argument("--filaments", type=int, default=None, help="and another filament count")
     args = ap.parse_args()
+    args.memory = MEMORY_OFF if args.broyden_memory == "0" else tuple(int(v) for v in args.broyden_memory.split(":"))
+    if len(args.memory) != 4:
+        ap.error("--broyden-memory wants KEEP:CARRY:THRESHOLD:RESTART or 0")
     if args.grid or args.filaments:
         w = WORKLOAD if args.workload == "sediment_512" else None
         if args.workload == "mobility_256":
@@ -325,10 +351,12 @@ def run_ours(args, rank, world):
                   "fs_warm_start_gate_stats")
         return steps, solves
 
-    def timed_steps(prec, mode, profile=False, gate=0, start=1, tension=2):
+    def timed_steps(prec, mode, profile=False, gate=0, start=1, tension=2, esc=0, mem=MEMORY_OFF):
         ctx.set_precision(prec)
         ctx.set_start_order(start)
         ctx.set_tension_extrapolation(tension)
+        ctx.set_precision_escalation(esc)
+        ctx.set_broyden_memory(*mem)
         if learned:
             set_warm_start(ctx, mode)
             abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate if mode else 0), "fs_warm_start_gate")
@@ -372,12 +400,14 @@ def run_ours(args, rank, world):
     gate = GATE_PERIOD if learned else 0
     start, tension = args.start_order, args.tension_order
     ms, its, st, _, clocks, launches, diag = timed_steps(abi.FS_PREC_FP32, mode, gate=gate, start=start,
-                                                         tension=tension)
+                                                         tension=tension, esc=args.escalate, mem=args.memory)
     # stage breakdown: the same steps again, host-driven with CUDA-event stage timing
     # (graph-captured steps carry no events); not part of the timed value
     abi.check(abi.lib().fs_set_graph_mode(ctx.h, 0), "fs_set_graph_mode")
     ctx.set_start_order(start)
     ctx.set_tension_extrapolation(tension)
+    ctx.set_precision_escalation(args.escalate)
+    ctx.set_broyden_memory(*args.memory)
     if learned:
         set_warm_start(ctx, mode)
         abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate), "fs_warm_start_gate")
@@ -397,7 +427,8 @@ def run_ours(args, rank, world):
         "config": {"workload": WORKLOAD["name"], "grid": [WORKLOAD["npts"]] * 3, "filaments": WORKLOAD["nfil"],
                    "beads_per_filament": nw, "beads": npb, "dt": p.dt, "tol": p.tol,
                    "precision": "mixed", "learned_warm_start": bool(learned),
-                   "start": start_label(start, tension),
+                   "start": start_label(start, tension), "escalate_after_iters": args.escalate,
+                   "broyden_memory": memory_label(args.memory),
                    "timed_steps": [nt0 + W, nt0 + W + K - 1],
                    "start_up": "steps 1-%d (implicit Euler, constant/linear tension extrapolation) run untimed"
                                % PREP_STEPS,
@@ -465,7 +496,8 @@ def run_ours(args, rank, world):
     # the same steps from the reference's start (no learned iterate), FP32 chain,
     # and with the learned start on every step (no cost gate)
     if learned:
-        msa, itsa, sta, _, _, _, da = timed_steps(abi.FS_PREC_FP32, mode, gate=0, start=start, tension=tension)
+        msa, itsa, sta, _, _, _, da = timed_steps(abi.FS_PREC_FP32, mode, gate=0, start=start, tension=tension,
+                                                  mem=args.memory)
         nla = da.learned_filaments + da.fallback_filaments
         out["learned_every_step"] = {"value": world * npb * K / (msa / 1e3), "ms_per_step": msa / K,
                                      "iters_per_step": float(np.mean(itsa)),
@@ -473,11 +505,19 @@ def run_ours(args, rank, world):
                                      "mobility_solves_per_step": da.mobility_solves / K,
                                      "learned_fraction": da.learned_filaments / max(1, nla)}
     if learned and (start, tension) != (1, 2):
-        msq, itsq, stq, _, _, _, dq = timed_steps(abi.FS_PREC_FP32, 0, start=start, tension=tension)
+        msq, itsq, stq, _, _, _, dq = timed_steps(abi.FS_PREC_FP32, 0, start=start, tension=tension,
+                                                  mem=args.memory)
         out["fp32_improved_start"] = {"value": world * npb * K / (msq / 1e3), "ms_per_step": msq / K,
                                        "iters_per_step": float(np.mean(itsq)),
                                        "status": abi.STATUS_NAMES.get(stq, stq),
                                        "mobility_solves_per_step": dq.mobility_solves / K}
+    if args.memory != MEMORY_OFF:
+        msn, itsn, stn, _, _, _, dn = timed_steps(abi.FS_PREC_FP32, 0, start=start, tension=tension)
+        out["fp32_no_broyden_memory"] = {"value": world * npb * K / (msn / 1e3), "ms_per_step": msn / K,
+                                         "iters_per_step": float(np.mean(itsn)),
+                                         "status": abi.STATUS_NAMES.get(stn, stn),
+                                         "mobility_solves_per_step": dn.mobility_solves / K,
+                                         "start": start_label(start, tension)}
     if learned or (start, tension) != (1, 2):
         ms0, its0, st0, _, _, _, d0 = timed_steps(abi.FS_PREC_FP32, 0, start=1, tension=2)
         out["fp32_plain_start"] = {"value": world * npb * K / (ms0 / 1e3), "ms_per_step": ms0 / K,
@@ -495,6 +535,8 @@ def run_ours(args, rank, world):
         ctx.set_precision(abi.FS_PREC_FP32)
         ctx.set_start_order(start)
         ctx.set_tension_extrapolation(tension)
+        ctx.set_precision_escalation(args.escalate)
+        ctx.set_broyden_memory(*args.memory)
         if learned:
             set_warm_start(ctx, mode)
             abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate), "fs_warm_start_gate")
@@ -544,9 +586,10 @@ def run_trajectory(args, rank, world):
     """Workload trajectory_200: the configured run of sediment_512, steps 1-200
     from the placed suspension (start-up steps included), once with the mixed-
     precision chain (FP32 spread/FFT/interpolation, FP64 Broyden and mechanics)
-    and once in FP64, both from the reference's start, and once more mixed with the
-    improved start (fs_set_start_order 2, fs_set_tension_extrapolation 1), all
-    with graph-captured steady steps. Records per-step Broyden iterations, the
+    and once in FP64, both from the reference's start, and mixed with the improved
+    start (fs_set_start_order 2, fs_set_tension_extrapolation 1) three more times:
+    alone, with precision escalation (fs_set_precision_escalation) and with the
+    Broyden memory (fs_set_broyden_memory); all with graph-captured steady steps. Records per-step Broyden iterations, the
     status, the final barrier minimum squared distance, the wall time of each run
     and, for the improved start, how far its final positions are from the
     reference start's."""
@@ -566,12 +609,19 @@ def run_trajectory(args, rank, world):
     out = {"workload": "trajectory_%d" % nsteps, "grid": [WORKLOAD["npts"]] * 3, "filaments": WORKLOAD["nfil"],
            "beads_per_filament": WORKLOAD["nw"], "beads": susp.np, "dt": p.dt, "tol": p.tol, "steps": nsteps}
     finals = {}
-    for name, prec, start, tension in (("mixed", abi.FS_PREC_FP32, 1, 2),
-                                       ("mixed_improved_start", abi.FS_PREC_FP32, 2, 1),
-                                       ("fp64", abi.FS_PREC_FP64, 1, 2)):
+    esc = args.escalate if args.escalate > 0 else 15
+    mem = args.memory if args.memory != MEMORY_OFF else MEMORY_DEFAULT
+    runs = (("mixed", abi.FS_PREC_FP32, 1, 2, 0, MEMORY_OFF),
+            ("mixed_improved_start", abi.FS_PREC_FP32, 2, 1, 0, MEMORY_OFF),
+            ("mixed_improved_start_escalated", abi.FS_PREC_FP32, 2, 1, esc, MEMORY_OFF),
+            ("mixed_improved_start_broyden_memory", abi.FS_PREC_FP32, 2, 1, 0, mem),
+            ("fp64", abi.FS_PREC_FP64, 1, 2, 0, MEMORY_OFF))
+    for name, prec, start, tension, after, memory in runs:
         ctx.set_precision(prec)
         ctx.set_start_order(start)
         ctx.set_tension_extrapolation(tension)
+        ctx.set_precision_escalation(after)
+        ctx.set_broyden_memory(*memory)
         sim = Simulation(ctx, susp.copy())
         torch.cuda.synchronize()
         t0 = time.time()
@@ -585,11 +635,13 @@ def run_trajectory(args, rank, world):
                      "not_converged_steps": int(d.not_converged_steps), "nonfinite": int(d.nonfinite),
                      "final_min_dist2": d.min_dist2, "final_max_abs_err": d.last_max_abs_err,
                      "wall_s": wall, "mobility_solves": int(d.mobility_solves), "clocks": clk.summary(),
-                     "final_mean_z": float(X[:, 2].mean())}
+                     "final_mean_z": float(X[:, 2].mean()), "escalated_iters": int(d.escalated_iters)}
         finals[name] = X.copy()
-    out["mixed_improved_start"]["start"] = start_label(2, 1)
-    out["mixed_improved_start"]["final_max_dX_vs_mixed_over_dx"] = float(
-        np.abs(finals["mixed_improved_start"] - finals["mixed"]).max() / p.dx)
+    for name in ("mixed_improved_start", "mixed_improved_start_escalated", "mixed_improved_start_broyden_memory"):
+        out[name]["start"] = start_label(2, 1)
+        out[name]["final_max_dX_vs_mixed_over_dx"] = float(np.abs(finals[name] - finals["mixed"]).max() / p.dx)
+    out["mixed_improved_start_escalated"]["escalate_after_iters"] = esc
+    out["mixed_improved_start_broyden_memory"]["broyden_memory"] = memory_label(mem)
     ctx.close()
     return out
 
@@ -674,7 +726,7 @@ def run_ensemble(args, rank, world):
     mine = partition_boxes(all_boxes, world)[rank]
     boxes = [all_boxes[i] for i in mine]
     ens = Ensemble(boxes, precision=abi.FS_PREC_FP32, start_order=args.start_order,
-                   tension_order=args.tension_order)
+                   tension_order=args.tension_order, escalate=args.escalate, memory=args.memory)
     t0 = time.time()
     ens.startup(PREP_STEPS)
     t_start = time.time() - t0
@@ -718,7 +770,8 @@ def run_ensemble(args, rank, world):
                       "filaments": int(sum(b[2].nfil for b in all_boxes)), "beads_per_filament": 16,
                       "timed_steps": [nt0 + W, nt0 + W + K - 1], "start_up_seconds": t_start,
                       "l2": "no flush; most boxes fit in L2 (the workload's own sizes)",
-                      "start": start_label(args.start_order, args.tension_order)},
+                      "start": start_label(args.start_order, args.tension_order),
+                      "escalate_after_iters": args.escalate, "broyden_memory": memory_label(args.memory)},
            "box_step_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99)),
                            "max": float(ms.max())},
            "iters_per_step": float(its.mean()), "status": abi.STATUS_NAMES.get(st, st),

@@ -14,7 +14,8 @@ BUILD = os.path.join(PKG, "_build")
 LIBDIR = os.path.join(PKG, "_lib")
 OUT = os.path.join(LIBDIR, "libfilsim_gpu.so")
 SOURCES = ["fs_sort.cu", "fs_fcm.cu", "fs_cells.cu", "fs_filament.cu", "fs_capi.cu", "fs_suspension.cu",
-           "fs_noalloc.cu", "fs_fft.cu", "fs_mlp.cu", "fs_graph.cu", "fs_tune.cu", "fs_runfiles.cu", "fs_slab.cu", "fs_start.cu"]
+           "fs_noalloc.cu", "fs_fft.cu", "fs_mlp.cu", "fs_graph.cu", "fs_tune.cu", "fs_runfiles.cu", "fs_slab.cu",
+           "fs_start.cu", "fs_bmem.cu"]
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

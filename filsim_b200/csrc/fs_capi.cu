@@ -131,7 +131,7 @@ fs_status step_implicit(fs_ctx *c, int nt, int *iters_out, bool commit = true, i
   const long long solves0 = c->diag.mobility_solves;
   if (learned || learn_recording(c)) FS_TRY(learn_save_guess(c));
   FS_TRY(fil_forces(c, nt));
-  FS_TRY(fil_jacobian_build(c, nt));
+  FS_TRY(fil_jacobian_build(c, nt, bmem_keep(c)));
   FS_TRY(cells_link(c, c->Xs, c->np));
   if (learned) {
     FS_TRY(learn_warm_start(c, nt, barrier_and_mobility));
@@ -161,15 +161,21 @@ fs_status step_implicit(fs_ctx *c, int nt, int *iters_out, bool commit = true, i
       FS_TRY(fcm_set_stream(c, c->stream));
     }
     if (c->precision != restore.prec) c->diag.escalated_iters++;
-    FS_TRY(fil_broyden_apply(c, c->err, c->upd, iter));
+    // with the Broyden memory on the column count lives on the device
+    const int *off = bmem_off(c);
+    const int hit = off ? 0 : iter;
+    FS_TRY(bmem_iter_begin(c, nt, iter, nullptr));
+    FS_TRY(fil_broyden_apply(c, c->err, c->upd, hit, nullptr, off));
     FS_TRY(fil_state_update(c, c->upd));
     FS_TRY(fil_forces(c, nt));
     FS_TRY(barrier_and_mobility(c, nt));
     FS_TRY(fil_error_check(c, c->V, c->W, c->newerr, nt));
-    FS_TRY(fil_broyden_update(c, iter));
+    FS_TRY(fil_broyden_update(c, hit, nullptr, off));
+    FS_TRY(bmem_iter_end(c));
     std::swap(c->err, c->newerr);
     ++iter;
     FS_TRY(read_flags(c));
+    if (c->flags_h[FLAG_PIVOT]) return FS_ERR_NONFINITE;  // a J0 built at a memory restart
     check = c->flags_h[FLAG_CHECK];
   }
   if (learn_recording(c)) FS_TRY(learn_capture_targets(c, iter));
@@ -177,6 +183,7 @@ fs_status step_implicit(fs_ctx *c, int nt, int *iters_out, bool commit = true, i
   FS_TRY(learn_end_step(c));
   if (commit) {
     FS_TRY(hist_end_step(c));  // only a step that moves X to Xt shifts the history
+    FS_TRY(bmem_end_step(c, iter, nullptr));  // and carries Broyden columns
     FS_TRY(fil_step(c, nt));
   }
   c->diag.last_nt = nt;
@@ -315,6 +322,7 @@ fs_status fs_destroy(fs_ctx *c) {
   graph_free(c);
   mlp_free(c);
   hist_free(c);
+  bmem_free(c);
   cudaFree(c->gemm_err);
   fcm_free(c);
   slab_free(c);

@@ -550,8 +550,9 @@ __global__ void __launch_bounds__(256) k_jacobian_schur(
     const double *__restrict__ TAU, const double *__restrict__ lam, const double *__restrict__ kap,
     const double *__restrict__ cmod, const long long *__restrict__ soff, const long long *__restrict__ aoff,
     double *__restrict__ Sinv_all, double *__restrict__ aux_all, int nt, FilConsts k, double a, double ah,
-    int *__restrict__ flags) {
+    int *__restrict__ flags, const int *__restrict__ keep) {
   extern __shared__ double S[];  // 3nw x 3nw, row-major
+  if (keep && *keep) return;  // the previous step's J0 stays (fs_set_broyden_memory)
   const int f = blockIdx.x;
   const int b0 = fil_start[f], nw = fil_start[f + 1] - b0, l0 = b0 - f;
   if (nw < 2) return;  // J0 is the identity
@@ -646,13 +647,14 @@ __global__ void __launch_bounds__(256) k_jacobian_schur(
 // pivoting (the first maximum wins); one CTA per filament with S in shared memory.
 __global__ void __launch_bounds__(384) k_schur_gj(const int *__restrict__ fil_start,
                                                   const long long *__restrict__ soff, double *__restrict__ Sinv_all,
-                                                  int *__restrict__ flags) {
+                                                  int *__restrict__ flags, const int *__restrict__ keep) {
   extern __shared__ double S[];
   __shared__ int perm[3 * FS_MAX_NW];
   __shared__ double fcol[3 * FS_MAX_NW];
   __shared__ int colsrc[3 * FS_MAX_NW];
   __shared__ int s_piv;
   __shared__ double s_inv, s_diag;
+  if (keep && *keep) return;
   const int f = blockIdx.x;
   const int nw = fil_start[f + 1] - fil_start[f];
   if (nw < 2) return;
@@ -745,13 +747,15 @@ constexpr int GJ_CW = 24;        // columns per warp
 constexpr int GJ_MAX_M = 96;     // m handled by the register kernel
 __global__ void __launch_bounds__(384, 2) k_schur_gj_reg(const int *__restrict__ fil_start,
                                                       const long long *__restrict__ soff,
-                                                      double *__restrict__ Sinv_all, int *__restrict__ flags) {
+                                                      double *__restrict__ Sinv_all, int *__restrict__ flags,
+                                                      const int *__restrict__ keep) {
   constexpr int CW = GJ_CW;
   __shared__ double fcol[GJ_MAX_M], rowkc[GJ_MAX_M + CW];
   __shared__ __align__(16) double prow_s[GJ_MAX_M + CW];
   __shared__ double cand_v[3], cand_inv[3];
   __shared__ int cand_r[3];
   __shared__ int perm[GJ_MAX_M], colsrc[GJ_MAX_M], dstcol[GJ_MAX_M];
+  if (keep && *keep) return;
   const int f = blockIdx.x;
   const int nw = fil_start[f + 1] - fil_start[f], m = 3 * nw;
   if (nw < 2 || m > GJ_MAX_M) return;  // block-uniform
@@ -982,7 +986,8 @@ __global__ void __launch_bounds__(128) k_schur_apply(const int *__restrict__ fil
                                                      const double *__restrict__ aux_all, const double *__restrict__ b,
                                                      double *__restrict__ x, const double *__restrict__ C,
                                                      const double *__restrict__ dots, int iter,
-                                                     const int *__restrict__ iter_d, size_t n6, double dt,
+                                                     const int *__restrict__ iter_d,
+                                                     const int *__restrict__ off_d, size_t n6, double dt,
                                                      double fac) {
   __shared__ double bb[6 * FS_MAX_NW], xs[6 * FS_MAX_NW], y[3 * FS_MAX_NW], w[3 * FS_MAX_NW];
   __shared__ double auxs[20 * (FS_MAX_NW - 1) + 3 * FS_MAX_NW + 1];
@@ -997,7 +1002,7 @@ __global__ void __launch_bounds__(128) k_schur_apply(const int *__restrict__ fil
   } else {
     schur_apply_one(nw, Sinv_all + soff[f], aux_all + aoff[f], auxs, bb, xs, y, w, dt, fac);
   }
-  const int ncol = iter_d ? *iter_d : iter;
+  const int ncol = (iter_d ? *iter_d : iter) + (off_d ? *off_d : 0);
   for (int r = tid; r < n; r += nthr) {
     double v = xs[r];
 #pragma unroll 4
@@ -1070,19 +1075,20 @@ __global__ void k_error_check(int np, const int *__restrict__ fil_id, const int 
 #define RED_THREADS 256
 #define RED_BLOCKS 296
 
-// partial dot products D_i . b for i < iter (iter_d ? *iter_d : iter): each of the
+// partial dot products D_i . b for i < iter (iter_d ? *iter_d : iter), plus the
+// columns carried from earlier steps (off_d ? *off_d : 0, fs_start.cu): each of the
 // RED_BLOCKS blocks sums a fixed strided slice of every column, so the partials
 // (and the fixed-order final sums) do not depend on how many columns there are
 __global__ void __launch_bounds__(RED_THREADS) k_dots(const double *__restrict__ D, const double *__restrict__ b,
                                                        size_t n6, int iter, const int *__restrict__ iter_d,
-                                                       double *__restrict__ partial) {
+                                                       const int *__restrict__ off_d, double *__restrict__ partial) {
   // columns in groups of DOT_COLS: a thread reads b[k] once per group and keeps
   // the group's loads in flight together; each column's sum runs in the same
   // order as one column at a time (k ascending per thread, then the shuffle
   // tree, then the warps in order), so the partials are bitwise those
   constexpr int DOT_COLS = 16;
   __shared__ double sh[DOT_COLS][RED_THREADS / 32];
-  const int ncol = iter_d ? *iter_d : iter;
+  const int ncol = (iter_d ? *iter_d : iter) + (off_d ? *off_d : 0);
   for (int i0 = 0; i0 < ncol; i0 += DOT_COLS) {
     double acc[DOT_COLS];
 #pragma unroll
@@ -1112,10 +1118,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_dots(const double *__restrict__
 
 // fixed-order final sums: one warp per output
 __global__ void k_reduce_rows(const double *__restrict__ partial, int nparts, int nrows, double *__restrict__ out,
-                              int do_sqrt, const int *__restrict__ nrows_d) {
+                              int do_sqrt, const int *__restrict__ nrows_d, const int *__restrict__ off_d) {
   const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (row >= (nrows_d ? *nrows_d : nrows)) return;
+  if (row >= (nrows_d ? *nrows_d : nrows) + (off_d ? *off_d : 0)) return;
   double acc = 0.0;
   for (int p = lane; p < nparts; p += 32) acc += partial[(size_t)row * nparts + p];
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -1144,14 +1150,15 @@ __global__ void __launch_bounds__(RED_THREADS) k_diff_sq(const double *__restric
 }
 
 // C_iter = -tmp/|dE| - upd/|dE|, D_iter = dE/|dE| (main.cpp:657-661)
-// column iter (iter_d ? *iter_d : iter) of the history
+// column iter (iter_d ? *iter_d : iter) of the history, after the columns carried
+// from earlier steps (off_d ? *off_d : 0)
 __global__ void k_broyden_cols(const double *__restrict__ tmp, const double *__restrict__ upd,
                                const double *__restrict__ dE, const double *__restrict__ nrm, size_t n6,
                                double *__restrict__ Cmat, double *__restrict__ Dmat, int iter,
-                               const int *__restrict__ iter_d) {
+                               const int *__restrict__ iter_d, const int *__restrict__ off_d) {
   size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n6) return;
-  const size_t col = (size_t)(iter_d ? *iter_d : iter) * n6;
+  const size_t col = (size_t)((iter_d ? *iter_d : iter) + (off_d ? *off_d : 0)) * n6;
   double *__restrict__ Ccol = Cmat + col;
   double *__restrict__ Dcol = Dmat + col;
   const double n = nrm[0];
@@ -1274,7 +1281,8 @@ fs_status fil_forces(fs_ctx *c, int nt) {
   return FS_OK;
 }
 
-fs_status fil_jacobian_build(fs_ctx *c, int nt) {
+// keep (device, or null): nonzero leaves the previous J0 in place
+fs_status fil_jacobian_build(fs_ctx *c, int nt, const int *keep) {
   if (!c->have_state) return FS_ERR_STATE;
   ProfScope ps(c, FS_STAGE_JACOBIAN);
   FilConsts k = make_fconsts(c);
@@ -1284,15 +1292,15 @@ fs_status fil_jacobian_build(fs_ctx *c, int nt) {
   const int jthreads = std::min(256, 32 * ((3 * c->max_nw + 31) / 32));
   k_jacobian_schur<<<c->nfil, jthreads, smem, c->stream>>>(c->fil_start, c->qs, c->Us, c->TAU, c->lam, c->kap, c->cc,
                                                       c->soff, c->aoff, c->Sinv, c->aux, nt, k, c->p.a, c->p.ah,
-                                                      c->flags);
+                                                      c->flags, keep);
   FS_LAUNCH_CHECK();
   // all filaments of at most 32 beads: the register kernel; otherwise the
   // shared-memory kernel for every filament
   if (3 * c->max_nw <= GJ_MAX_M) {
     const int m = 3 * c->max_nw, warps = ((m + 31) / 32) * ((m + GJ_CW - 1) / GJ_CW);
-    k_schur_gj_reg<<<c->nfil, 32 * warps, 0, c->stream>>>(c->fil_start, c->soff, c->Sinv, c->flags);
+    k_schur_gj_reg<<<c->nfil, 32 * warps, 0, c->stream>>>(c->fil_start, c->soff, c->Sinv, c->flags, keep);
   } else {
-    k_schur_gj<<<c->nfil, 384, smem, c->stream>>>(c->fil_start, c->soff, c->Sinv, c->flags);
+    k_schur_gj<<<c->nfil, 384, smem, c->stream>>>(c->fil_start, c->soff, c->Sinv, c->flags, keep);
   }
   FS_LAUNCH_CHECK();
   return FS_OK;
@@ -1334,38 +1342,43 @@ fs_status fil_error_check(fs_ctx *c, const double *V, const double *W, double *e
   return FS_OK;
 }
 
-// iter_d (graph capture): the history length is read on the device
-fs_status fil_broyden_apply(fs_ctx *c, const double *b, double *x, int iter, const int *iter_d) {
+// iter_d (graph capture): the history length is read on the device; off_d: the
+// columns carried from earlier steps before it (fs_set_broyden_memory), or none
+fs_status fil_broyden_apply(fs_ctx *c, const double *b, double *x, int iter, const int *iter_d, const int *off_d) {
   if (!c->have_state) return FS_ERR_STATE;
   ProfScope ps(c, FS_STAGE_BROYDEN);
   const size_t n6 = (size_t)6 * c->np;
-  if (iter > 0 || iter_d) {
-    const int rows = iter_d ? c->p.broyden_maxiter : iter;
-    k_dots<<<RED_BLOCKS, RED_THREADS, 0, c->stream>>>(c->Dmat, b, n6, iter, iter_d, c->partials);
+  if (iter > 0 || iter_d || off_d) {
+    // rows launched: a bound on the device count (with the memory on, callers pass
+    // iter 0 and no iter_d: the count is the carried and current columns, off_d)
+    const int base = iter_d ? c->p.broyden_maxiter : iter;
+    const int rows = off_d ? c->p.broyden_maxiter + c->bmem_cols + base : base;
+    k_dots<<<RED_BLOCKS, RED_THREADS, 0, c->stream>>>(c->Dmat, b, n6, iter, iter_d, off_d, c->partials);
     FS_LAUNCH_CHECK();
-    k_reduce_rows<<<fs_blocks(rows, 8), 256, 0, c->stream>>>(c->partials, RED_BLOCKS, rows, c->dots, 0, iter_d);
+    k_reduce_rows<<<fs_blocks(rows, 8), 256, 0, c->stream>>>(c->partials, RED_BLOCKS, iter, c->dots, 0, iter_d,
+                                                             off_d);
     FS_LAUNCH_CHECK();
   }
   k_schur_apply<<<c->nfil, 128, 0, c->stream>>>(c->fil_start, c->soff, c->aoff, c->Sinv, c->aux, b, x, c->Cmat,
-                                                 c->dots, iter, iter_d, n6, c->p.dt, 0.5 * c->p.dl);
+                                                 c->dots, iter, iter_d, off_d, n6, c->p.dt, 0.5 * c->p.dl);
   FS_LAUNCH_CHECK();
   return learn_diag_apply(c, b, x);  // learned initial inverse-Jacobian diagonal, when on
 }
 
 // main.cpp:641-663 with the current err/newerr/upd: history column `iter`
-fs_status fil_broyden_update(fs_ctx *c, int iter, const int *iter_d) {
+fs_status fil_broyden_update(fs_ctx *c, int iter, const int *iter_d, const int *off_d) {
   const size_t n6 = (size_t)6 * c->np;
   {
     ProfScope ps(c, FS_STAGE_BROYDEN);
     k_diff_sq<<<RED_BLOCKS, RED_THREADS, 0, c->stream>>>(c->newerr, c->err, c->dE, n6, c->partials);
     FS_LAUNCH_CHECK();
-    k_reduce_rows<<<1, 32, 0, c->stream>>>(c->partials, RED_BLOCKS, 1, c->scalars, 1, nullptr);
+    k_reduce_rows<<<1, 32, 0, c->stream>>>(c->partials, RED_BLOCKS, 1, c->scalars, 1, nullptr, nullptr);
     FS_LAUNCH_CHECK();
   }
-  FS_TRY(fil_broyden_apply(c, c->dE, c->tmp, iter, iter_d));
+  FS_TRY(fil_broyden_apply(c, c->dE, c->tmp, iter, iter_d, off_d));
   ProfScope ps(c, FS_STAGE_BROYDEN);
   k_broyden_cols<<<fs_blocks((long long)n6, 256), 256, 0, c->stream>>>(c->tmp, c->upd, c->dE, c->scalars, n6,
-                                                                       c->Cmat, c->Dmat, iter, iter_d);
+                                                                       c->Cmat, c->Dmat, iter, iter_d, off_d);
   FS_LAUNCH_CHECK();
   return FS_OK;
 }

@@ -87,13 +87,17 @@ fs_status capture_body(fs_ctx *c, int nt, fs_graph *g, cudaGraph_t body, cudaGra
   FS_CUDA(cudaStreamBeginCaptureToGraph(g->body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   c->stream = g->body_stream;
   fs_status st = fcm_set_stream(c, c->stream);
-  const int *iter_d = g->dev + GD_ITER;
-  if (st == FS_OK) st = fil_broyden_apply(c, c->err, c->upd, 0, iter_d);
+  // with the Broyden memory on the column count lives on the device (fs_bmem.cu)
+  const int *off = bmem_off(c);
+  const int *iter_d = off ? nullptr : g->dev + GD_ITER;
+  if (st == FS_OK) st = bmem_iter_begin(c, nt, 0, g->dev + GD_ITER);
+  if (st == FS_OK) st = fil_broyden_apply(c, c->err, c->upd, 0, iter_d, off);
   if (st == FS_OK) st = fil_state_update(c, c->upd);
   if (st == FS_OK) st = fil_forces(c, nt);
   if (st == FS_OK) st = step_barrier_mobility(c, nt);
   if (st == FS_OK) st = fil_error_check(c, c->V, c->W, c->newerr, nt);
-  if (st == FS_OK) st = fil_broyden_update(c, 0, iter_d);
+  if (st == FS_OK) st = fil_broyden_update(c, 0, iter_d, off);
+  if (st == FS_OK) st = bmem_iter_end(c);
   if (st == FS_OK && cudaMemcpyAsync(c->err, c->newerr, sizeof(double) * 6 * (size_t)c->np, cudaMemcpyDeviceToDevice,
                                      c->stream) != cudaSuccess)
     st = FS_ERR_CUDA;
@@ -153,7 +157,7 @@ fs_status capture_step(fs_ctx *c, int nt, fs_graph *g, cudaGraph_t *out) {
   FS_CUDA(cudaMemsetAsync(c->flags, 0, sizeof(int) * FLAG_COUNT, c->stream));
   FS_TRY(fil_initial_guess(c));
   FS_TRY(fil_forces(c, nt));
-  FS_TRY(fil_jacobian_build(c, nt));
+  FS_TRY(fil_jacobian_build(c, nt, bmem_keep(c)));
   FS_TRY(cells_link(c, c->Xs, c->np));
   FS_TRY(step_barrier_mobility(c, nt));
   FS_TRY(fil_error_check(c, c->V, c->W, c->err, nt));
@@ -180,6 +184,7 @@ fs_status capture_step(fs_ctx *c, int nt, fs_graph *g, cudaGraph_t *out) {
   }
   FS_TRY(learn_end_step(c));
   FS_TRY(hist_end_step(c));
+  FS_TRY(bmem_end_step(c, 0, g->dev + GD_ITER));
   FS_TRY(fil_step(c, nt));
   k_step_done<<<1, 1, 0, c->stream>>>(g->dev, c->flags, GRAPH_STEP_SLOTS);
   FS_LAUNCH_CHECK();

@@ -131,6 +131,15 @@ struct fs_ctx {
   // FP32 steps go on in FP64 after this many Broyden iterations (0: never;
   // fs_set_precision_escalation)
   int escalate_after;
+  // Broyden memory across steps (fs_set_broyden_memory, fs_bmem.cu): J0 and up to
+  // bmem_keep history columns continue after a step of fewer than bmem_thr
+  // iterations; after a longer one its last bmem_carry columns start the next
+  // step beside a new J0; a step on carried state that reaches bmem_restart
+  // iterations drops it (0: never). bmem_cols = max(bmem_keep, bmem_carry), 0 when
+  // off; bmem_cap: history columns allocated beyond broyden_maxiter; bmem_d: the
+  // device state (BM_COUNT ints, fs_bmem.cu)
+  int bmem_keep, bmem_carry, bmem_thr, bmem_restart, bmem_cols, bmem_cap;
+  int *bmem_d;
   // positions two steps back (fs_start.cu), kept while the quadratic or the learned
   // start is on (3 max_beads doubles each); hist_ok (device): steps run since the
   // history was reset, up to 2 (hist_Xtt holds positions two steps back once it is
@@ -214,13 +223,14 @@ fs_status cells_barrier(fs_ctx *c, const double *Y, double *F, int np, int nt, c
 
 fs_status fil_initial_guess(fs_ctx *c);
 fs_status fil_forces(fs_ctx *c, int nt);
-fs_status fil_jacobian_build(fs_ctx *c, int nt);
+fs_status fil_jacobian_build(fs_ctx *c, int nt, const int *keep = nullptr);
 fs_status fil_jacobian_prepare(fs_ctx *c);  // after an upload: kernel attributes for the filament lengths
 int fil_aux_size(int nw);
 fs_status fil_jacobian_inverse(fs_ctx *c, int f, double *out_d);
 fs_status fil_error_check(fs_ctx *c, const double *V, const double *W, double *err, int nt);
-fs_status fil_broyden_apply(fs_ctx *c, const double *b, double *x, int iter, const int *iter_d = nullptr);
-fs_status fil_broyden_update(fs_ctx *c, int iter, const int *iter_d = nullptr);
+fs_status fil_broyden_apply(fs_ctx *c, const double *b, double *x, int iter, const int *iter_d = nullptr,
+                            const int *off_d = nullptr);
+fs_status fil_broyden_update(fs_ctx *c, int iter, const int *iter_d = nullptr, const int *off_d = nullptr);
 fs_status fil_state_update(fs_ctx *c, const double *upd);
 fs_status fil_step(fs_ctx *c, int nt);
 fs_status fil_max_abs_err(fs_ctx *c, const double *err, double *out_h);
@@ -253,6 +263,25 @@ void hist_free(fs_ctx *c);
 fs_status hist_end_step(fs_ctx *c);
 fs_status hist_before_upload(fs_ctx *c, bool same_layout);
 fs_status hist_after_upload(fs_ctx *c);
+// Broyden memory (fs_bmem.cu). Device state: BM_NCOL history columns in use
+// (carried and this step's); BM_MOVE, BM_SRC the last carry's moved columns and
+// first source; BM_KEEPJ nonzero: the step keeps the previous J0; BM_SKIPJ
+// nonzero: the Jacobian build inside the iteration skips (zero at a restart);
+// BM_CARRIED nonzero while the step runs on carried columns or a kept J0.
+enum { BM_NCOL = 0, BM_MOVE, BM_SRC, BM_KEEPJ, BM_SKIPJ, BM_CARRIED, BM_COUNT = 8 };
+// with the memory on the Broyden kernels take their column count from BM_NCOL
+inline const int *bmem_off(const fs_ctx *c) { return c->bmem_cols > 0 ? c->bmem_d + BM_NCOL : nullptr; }
+inline const int *bmem_keep(const fs_ctx *c) { return c->bmem_cols > 0 ? c->bmem_d + BM_KEEPJ : nullptr; }
+// per iteration: the restart check (and J0 build at a restart) before the apply;
+// the column count after the history update
+fs_status bmem_iter_begin(fs_ctx *c, int nt, int iter, const int *iter_d);
+fs_status bmem_iter_end(fs_ctx *c);
+// after a committed step of its (its_d: on the device) iterations: the carry
+fs_status bmem_end_step(fs_ctx *c, int its, const int *its_d);
+fs_status bmem_reset(fs_ctx *c);
+void bmem_free(fs_ctx *c);
+// an upload that changes X or Xt drops the carried state (device side, k_hist_same)
+__device__ inline void bmem_drop(int *m) { m[BM_NCOL] = m[BM_KEEPJ] = m[BM_CARRIED] = 0; }
 fs_status learn_before_upload(fs_ctx *c, bool same_layout);
 void mlp_free(fs_ctx *c);
 

@@ -302,7 +302,7 @@ __global__ void k_targets(int nfil, const int *__restrict__ fil_start, int nw_mo
                           const double *__restrict__ Xs, const double *__restrict__ Us, const double *__restrict__ lam,
                           const double *__restrict__ gXs, const double *__restrict__ gUs,
                           const double *__restrict__ glam, const double *__restrict__ C, const double *__restrict__ D,
-                          int iters, size_t n6, float *__restrict__ tgt) {
+                          int iters, const int *__restrict__ off, size_t n6, float *__restrict__ tgt) {
   const int f = blockIdx.x;
   const int b0 = fil_start[f], nw = fil_start[f + 1] - b0, l0 = b0 - f;
   for (int t = threadIdx.x; t < ntgt; t += blockDim.x) {
@@ -318,7 +318,8 @@ __global__ void k_targets(int nfil, const int *__restrict__ fil_start, int nw_mo
       } else if (t < 12 * nw) {
         const size_t r = 6 * (size_t)b0 + (t - 6 * nw);
         double s = 0.0;
-        for (int i = 0; i < iters; ++i) s += C[(size_t)i * n6 + r] * D[(size_t)i * n6 + r];
+        const int ncol = iters + (off ? *off : 0);  // off: the column count with the Broyden memory on
+        for (int i = 0; i < ncol; ++i) s += C[(size_t)i * n6 + r] * D[(size_t)i * n6 + r];
         v = (float)s;
       }
     }
@@ -767,7 +768,8 @@ fs_status learn_diag_apply(fs_ctx *c, const double *b, double *x) {
 fs_status learn_capture_targets(fs_ctx *c, int iters) {
   fs_mlp *m = c->mlp;
   k_targets<<<c->nfil, 128, 0, c->stream>>>(c->nfil, c->fil_start, m->nw, m->ntgt, c->Xs, c->Us, c->lam, m->gXs,
-                                            m->gUs, m->glam, c->Cmat, c->Dmat, iters, (size_t)6 * c->np, m->tgt);
+                                            m->gUs, m->glam, c->Cmat, c->Dmat, bmem_off(c) ? 0 : iters, bmem_off(c),
+                                            (size_t)6 * c->np, m->tgt);
   FS_LAUNCH_CHECK();
   m->have_targets = true;
   return FS_OK;

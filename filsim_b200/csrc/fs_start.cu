@@ -25,6 +25,7 @@
 // tolerance's noise, which the quadratic extrapolation multiplies by up to 7;
 // tension order 1 keeps the linear 2 lam - lam1 (noise up to 3) after
 // lambda_extrap_step too.
+
 #include "fs_internal.cuh"
 
 namespace {
@@ -34,11 +35,16 @@ __global__ void k_hist_tick(int *ok) {
   if (*ok < 2) ++*ok;
 }
 
-// the history survives an upload only if X and Xt are unchanged
+// the history and the carried Broyden columns survive an upload only if X and Xt
+// are unchanged
 __global__ void k_hist_same(size_t n, const double *__restrict__ X, const double *__restrict__ Xt,
-                            const double *__restrict__ pX, const double *__restrict__ pXt, int *__restrict__ ok) {
+                            const double *__restrict__ pX, const double *__restrict__ pXt, int *__restrict__ ok,
+                            int *__restrict__ carried) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n && (X[i] != pX[i] || Xt[i] != pXt[i])) *ok = 0;
+  if (i < n && (X[i] != pX[i] || Xt[i] != pXt[i])) {
+    *ok = 0;
+    if (carried) bmem_drop(carried);
+  }
 }
 
 }  // namespace
@@ -93,13 +99,14 @@ fs_status hist_end_step(fs_ctx *c) {
   return FS_OK;
 }
 
-// around fs_state_upload: the history stays valid when the upload repeats X and Xt
+// around fs_state_upload: the history (and the carried Broyden columns) stay valid
+// when the upload repeats X and Xt
 fs_status hist_before_upload(fs_ctx *c, bool same_layout) {
   c->hist_cmp_pending = false;
   if (!c->hist_Xtt || (same_layout && c->np == 0)) return FS_OK;  // no beads: nothing to compare
   if (!same_layout) {
     FS_CUDA(cudaMemsetAsync(c->hist_ok, 0, sizeof(int), c->stream));
-    return FS_OK;
+    return bmem_reset(c);
   }
   const size_t b = sizeof(double) * 3 * (size_t)c->np;
   FS_CUDA(cudaMemcpyAsync(c->hist_pX, c->X, b, cudaMemcpyDeviceToDevice, c->stream));
@@ -113,7 +120,7 @@ fs_status hist_after_upload(fs_ctx *c) {
   c->hist_cmp_pending = false;
   const size_t n = (size_t)3 * c->np;
   k_hist_same<<<fs_blocks((long long)n, 256), 256, 0, c->stream>>>(n, c->X, c->Xt, c->hist_pX, c->hist_pXt,
-                                                                  c->hist_ok);
+                                                                  c->hist_ok, c->bmem_d);
   FS_LAUNCH_CHECK();
   return FS_OK;
 }

@@ -76,7 +76,8 @@ def partition_boxes(boxes, world):
 class Ensemble:
     """One context per box, all advanced by fs_batch_run."""
 
-    def __init__(self, boxes, precision=abi.FS_PREC_FP32, start_order=1, tension_order=2):
+    def __init__(self, boxes, precision=abi.FS_PREC_FP32, start_order=1, tension_order=2, escalate=0,
+                 memory=None):
         self.boxes = boxes
         self.ctxs, self.sims = [], []
         for npts, p, s, kb in boxes:
@@ -84,6 +85,9 @@ class Ensemble:
             c.set_precision(precision)
             c.set_start_order(start_order)
             c.set_tension_extrapolation(tension_order)
+            c.set_precision_escalation(escalate)
+            if memory is not None:
+                c.set_broyden_memory(*memory)  # (keep, carry, threshold, restart): fs_set_broyden_memory
             check(lib().fs_set_graph_mode(c.h, 1), "fs_set_graph_mode")
             self.ctxs.append(c)
             self.sims.append(Simulation(c, s))

@@ -85,6 +85,15 @@ class Context:
         1: linear from lambda_extrap_step on."""
         check(lib().fs_set_tension_extrapolation(self.h, order), "fs_set_tension_extrapolation")
 
+    def set_broyden_memory(self, keep_columns, carry_columns=0, threshold=0, restart_after=0):
+        """Broyden memory across steps: after a step of fewer than `threshold`
+        iterations J0 and up to keep_columns history columns continue into the next
+        step; after a longer one its last carry_columns columns start the next step
+        beside a new J0; a step on carried state reaching restart_after iterations
+        starts afresh (0: never). keep_columns = carry_columns = 0 turns it off."""
+        check(lib().fs_set_broyden_memory(self.h, keep_columns, carry_columns, threshold, restart_after),
+              "fs_set_broyden_memory")
+
     def set_precision_escalation(self, after_iters):
         """FP32 steps still not converged after after_iters Broyden iterations run the
         rest of their iterations with the FP64 chain; 0 turns it off."""

@@ -504,6 +504,25 @@ fs_status fs_set_start_order(fs_ctx *ctx, int order);
  * noise, which the quadratic extrapolation amplifies up to 7x and the linear one
  * up to 3x. The Broyden loop and its convergence test are unchanged. */
 fs_status fs_set_tension_extrapolation(fs_ctx *ctx, int order);
+/* Broyden memory across steps (no reference counterpart). The reference starts
+ * each step's iteration from J0^-1, the approximate inverse Jacobian of the
+ * filaments without their hydrodynamic coupling, adds one rank-one "bad Broyden"
+ * term per iteration (main.cpp:640-663) and drops them at the end of the step.
+ * With the memory on:
+ *  - after a converged step of fewer than `threshold` iterations whose history
+ *    holds at most keep_columns columns, the next step keeps that J0 (no rebuild)
+ *    and all the columns;
+ *  - after a converged step of `threshold` or more iterations, its last
+ *    carry_columns columns start the next step beside a new J0;
+ *  - otherwise the next step starts as the reference's does;
+ *  - a step running on carried state that reaches restart_after iterations
+ *    (0: never) rebuilds J0 at its current iterate and empties the history.
+ * An upload that changes X, Xt or the layout drops the carried state. The
+ * convergence test is unchanged. The history grows to broyden_maxiter +
+ * max(keep_columns, carry_columns) columns of 12 Np doubles. keep_columns =
+ * carry_columns = 0 (the default) turns it off; each at most FS_BROYDEN_MEMORY_MAX. */
+#define FS_BROYDEN_MEMORY_MAX 64
+fs_status fs_set_broyden_memory(fs_ctx *ctx, int keep_columns, int carry_columns, int threshold, int restart_after);
 /* Precision escalation of the mixed-precision chain (no reference counterpart):
  * with after_iters > 0 and the context in FS_PREC_FP32, a step still not
  * converged after after_iters Broyden iterations runs its remaining iterations

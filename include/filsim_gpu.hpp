@@ -47,6 +47,11 @@ class Context {
   void set_tension_extrapolation(int order) {
     check(fs_set_tension_extrapolation(ctx_, order), "fs_set_tension_extrapolation");
   }
+  // Broyden memory across steps (fs_set_broyden_memory; all zero: off)
+  void set_broyden_memory(int keep_columns, int carry_columns, int threshold, int restart_after) {
+    check(fs_set_broyden_memory(ctx_, keep_columns, carry_columns, threshold, restart_after),
+          "fs_set_broyden_memory");
+  }
   // FP32 steps not converged after after_iters Broyden iterations finish in FP64 (0: off)
   void set_precision_escalation(int after_iters) {
     check(fs_set_precision_escalation(ctx_, after_iters), "fs_set_precision_escalation");

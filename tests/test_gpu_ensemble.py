@@ -21,10 +21,12 @@ def small_boxes():
     return out
 
 
-@pytest.mark.parametrize("prec", [abi.FS_PREC_FP32, abi.FS_PREC_FP64])
-def test_batch_matches_boxes_alone(gpu_lib, prec):
+@pytest.mark.parametrize("prec,esc", [(abi.FS_PREC_FP32, 0), (abi.FS_PREC_FP64, 0), (abi.FS_PREC_FP32, 2)])
+def test_batch_matches_boxes_alone(gpu_lib, prec, esc):
+    """esc 2: each box's captured step escalates to FP64 after two iterations
+    (fs_set_precision_escalation), inside the ensemble graph as alone."""
     boxes = small_boxes()
-    ens = Ensemble(boxes, precision=prec)
+    ens = Ensemble(boxes, precision=prec, escalate=esc)
     ens.startup(13)
     its, ms, total, st = ens.run(14, 4)
     outs = [sim.download() for sim in ens.sims]
@@ -34,6 +36,7 @@ def test_batch_matches_boxes_alone(gpu_lib, prec):
     for b, (npts, p, s, kb) in enumerate(boxes):
         ctx = Context(p, max_beads=s.np, max_filaments=s.nfil)
         ctx.set_precision(prec)
+        ctx.set_precision_escalation(esc)
         sim = Simulation(ctx, s)
         ref_its, _ = sim.run_steps(1, 17)
         ref = sim.download()
