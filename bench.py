@@ -155,14 +155,22 @@ def parse():
                          "boxes advanced by one graph launch per step; trajectory_200: the configured run "
                          "of sediment_512, steps 1-200 from the placed suspension, mixed precision and FP64, "
                          "with per-step iterations (a record, not a throughput benchmark)")
-    ap.add_argument("--grid", type=int, default=None,
-                    help="sediment_512 / mobility_256 on another cubic grid (profiling cases; the "
-                         "workload name in config says so)")
+    ap.add_argument("--grid", default=None,
+                    help="sediment_512 / mobility_256 on another cubic grid N, or mobility_256 on NX,NY,NZ "
+                         "(profiling cases; the workload name in config says so)")
     ap.add_argument("--filaments", type=int, default=None, help="and another filament count")
     args = ap.parse_args()
     args.memory = MEMORY_OFF if args.broyden_memory == "0" else tuple(int(v) for v in args.broyden_memory.split(":"))
     if len(args.memory) != 4:
         ap.error("--broyden-memory wants KEEP:CARRY:THRESHOLD:RESTART or 0")
+    if args.grid:
+        g = tuple(int(v) for v in args.grid.split(","))
+        if len(g) == 3 and args.workload == "mobility_256":
+            args.grid = g  # a profiling case with lines of different lengths per axis
+        elif len(g) == 1:
+            args.grid = g[0]
+        else:
+            ap.error("--grid wants N, or NX,NY,NZ with --workload mobility_256")
     if args.grid or args.filaments:
         w = WORKLOAD if args.workload == "sediment_512" else None
         if args.workload == "mobility_256":
@@ -172,7 +180,8 @@ def parse():
             w["npts"] = args.grid or w["npts"]
             w["nfil"] = args.filaments or w["nfil"]
             base = "sediment" if args.workload == "sediment_512" else "mobility"
-            w["name"] = "%s_%d_%dx%d" % (base, w["npts"], w["nfil"], w["nw"])
+            gname = "x".join(map(str, w["npts"])) if isinstance(w["npts"], tuple) else "%d" % w["npts"]
+            w["name"] = "%s_%s_%dx%d" % (base, gname, w["nfil"], w["nw"])
     return args
 
 
@@ -690,7 +699,9 @@ def run_mobility(args, rank, world):
             "unit": "bead-solves/s", "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded rejection-placed filaments, F, T ~ N(0,1))",
-            "config": {"workload": w.get("name", "mobility_256"), "grid": [w["npts"]] * 3, "filaments": w["nfil"],
+            "config": {"workload": w.get("name", "mobility_256"),
+                       "grid": list(w["npts"]) if isinstance(w["npts"], tuple) else [w["npts"]] * 3,
+                       "filaments": w["nfil"],
                        "beads_per_filament": w["nw"], "beads": s.np, "l2": "grids (~0.4 GB) larger than L2"},
             "fp64": {"value": s.np * K / (res["fp64"]["ms"] / 1e3), "ms_per_step": res["fp64"]["ms"] / K},
             "fp32_error_vs_fp64": {"U": relerr(res["fp32"]["V"], res["fp64"]["V"]),
