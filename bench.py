@@ -106,6 +106,9 @@ def start_label(start, tension):
 # longer one, restart a step on carried state at 30 iterations
 MEMORY_DEFAULT = (16, 4, 8, 30)
 MEMORY_OFF = (0, 0, 0, 0)
+# velocity predictor (fs_set_velocity_predictor): half the update predicted from
+# the extrapolated velocities
+PREDICTOR_DEFAULT = 0.5
 
 
 def memory_label(mem):
@@ -147,6 +150,10 @@ def parse():
     ap.add_argument("--broyden-memory", default=":".join(map(str, MEMORY_DEFAULT)),
                     help="fs_set_broyden_memory for the value arm and the ensemble, KEEP:CARRY:THRESHOLD:RESTART "
                          "(default %s); 0 turns it off (the reference's iteration)" % ":".join(map(str, MEMORY_DEFAULT)))
+    ap.add_argument("--velocity-predictor", type=float, default=PREDICTOR_DEFAULT,
+                    help="fs_set_velocity_predictor weight for the value arm and the ensemble: one Broyden update "
+                         "of this weight from the residual with extrapolated velocities before each step's first "
+                         "residual (default %g; 0 turns it off)" % PREDICTOR_DEFAULT)
     ap.add_argument("--train-seeds", type=int, default=20, help="plain-solver runs that generate training data")
     ap.add_argument("--workload", default="sediment_512",
                     choices=["sediment_512", "mobility_256", "ensemble_64", "mlp", "trajectory_200"],
@@ -360,12 +367,13 @@ def run_ours(args, rank, world):
                   "fs_warm_start_gate_stats")
         return steps, solves
 
-    def timed_steps(prec, mode, profile=False, gate=0, start=1, tension=2, esc=0, mem=MEMORY_OFF):
+    def timed_steps(prec, mode, profile=False, gate=0, start=1, tension=2, esc=0, mem=MEMORY_OFF, pred=0.0):
         ctx.set_precision(prec)
         ctx.set_start_order(start)
         ctx.set_tension_extrapolation(tension)
         ctx.set_precision_escalation(esc)
         ctx.set_broyden_memory(*mem)
+        ctx.set_velocity_predictor(pred)
         if learned:
             set_warm_start(ctx, mode)
             abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate if mode else 0), "fs_warm_start_gate")
@@ -409,7 +417,8 @@ def run_ours(args, rank, world):
     gate = GATE_PERIOD if learned else 0
     start, tension = args.start_order, args.tension_order
     ms, its, st, _, clocks, launches, diag = timed_steps(abi.FS_PREC_FP32, mode, gate=gate, start=start,
-                                                         tension=tension, esc=args.escalate, mem=args.memory)
+                                                         tension=tension, esc=args.escalate, mem=args.memory,
+                                                         pred=args.velocity_predictor)
     # stage breakdown: the same steps again, host-driven with CUDA-event stage timing
     # (graph-captured steps carry no events); not part of the timed value
     abi.check(abi.lib().fs_set_graph_mode(ctx.h, 0), "fs_set_graph_mode")
@@ -417,6 +426,7 @@ def run_ours(args, rank, world):
     ctx.set_tension_extrapolation(tension)
     ctx.set_precision_escalation(args.escalate)
     ctx.set_broyden_memory(*args.memory)
+    ctx.set_velocity_predictor(args.velocity_predictor)
     if learned:
         set_warm_start(ctx, mode)
         abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate), "fs_warm_start_gate")
@@ -437,7 +447,7 @@ def run_ours(args, rank, world):
                    "beads_per_filament": nw, "beads": npb, "dt": p.dt, "tol": p.tol,
                    "precision": "mixed", "learned_warm_start": bool(learned),
                    "start": start_label(start, tension), "escalate_after_iters": args.escalate,
-                   "broyden_memory": memory_label(args.memory),
+                   "broyden_memory": memory_label(args.memory), "velocity_predictor": args.velocity_predictor,
                    "timed_steps": [nt0 + W, nt0 + W + K - 1],
                    "start_up": "steps 1-%d (implicit Euler, constant/linear tension extrapolation) run untimed"
                                % PREP_STEPS,
@@ -506,7 +516,7 @@ def run_ours(args, rank, world):
     # and with the learned start on every step (no cost gate)
     if learned:
         msa, itsa, sta, _, _, _, da = timed_steps(abi.FS_PREC_FP32, mode, gate=0, start=start, tension=tension,
-                                                  mem=args.memory)
+                                                  mem=args.memory, pred=args.velocity_predictor)
         nla = da.learned_filaments + da.fallback_filaments
         out["learned_every_step"] = {"value": world * npb * K / (msa / 1e3), "ms_per_step": msa / K,
                                      "iters_per_step": float(np.mean(itsa)),
@@ -515,14 +525,14 @@ def run_ours(args, rank, world):
                                      "learned_fraction": da.learned_filaments / max(1, nla)}
     if learned and (start, tension) != (1, 2):
         msq, itsq, stq, _, _, _, dq = timed_steps(abi.FS_PREC_FP32, 0, start=start, tension=tension,
-                                                  mem=args.memory)
+                                                  mem=args.memory, pred=args.velocity_predictor)
         out["fp32_improved_start"] = {"value": world * npb * K / (msq / 1e3), "ms_per_step": msq / K,
                                        "iters_per_step": float(np.mean(itsq)),
                                        "status": abi.STATUS_NAMES.get(stq, stq),
                                        "mobility_solves_per_step": dq.mobility_solves / K}
-    if args.memory != MEMORY_OFF:
+    if args.memory != MEMORY_OFF or args.velocity_predictor > 0:
         msn, itsn, stn, _, _, _, dn = timed_steps(abi.FS_PREC_FP32, 0, start=start, tension=tension)
-        out["fp32_no_broyden_memory"] = {"value": world * npb * K / (msn / 1e3), "ms_per_step": msn / K,
+        out["fp32_start_only"] = {"value": world * npb * K / (msn / 1e3), "ms_per_step": msn / K,
                                          "iters_per_step": float(np.mean(itsn)),
                                          "status": abi.STATUS_NAMES.get(stn, stn),
                                          "mobility_solves_per_step": dn.mobility_solves / K,
@@ -546,6 +556,7 @@ def run_ours(args, rank, world):
         ctx.set_tension_extrapolation(tension)
         ctx.set_precision_escalation(args.escalate)
         ctx.set_broyden_memory(*args.memory)
+        ctx.set_velocity_predictor(args.velocity_predictor)
         if learned:
             set_warm_start(ctx, mode)
             abi.check(abi.lib().fs_warm_start_gate(ctx.h, gate), "fs_warm_start_gate")
@@ -596,12 +607,13 @@ def run_trajectory(args, rank, world):
     from the placed suspension (start-up steps included), once with the mixed-
     precision chain (FP32 spread/FFT/interpolation, FP64 Broyden and mechanics)
     and once in FP64, both from the reference's start, and mixed with the improved
-    start (fs_set_start_order 2, fs_set_tension_extrapolation 1) three more times:
-    alone, with precision escalation (fs_set_precision_escalation) and with the
-    Broyden memory (fs_set_broyden_memory); all with graph-captured steady steps. Records per-step Broyden iterations, the
-    status, the final barrier minimum squared distance, the wall time of each run
-    and, for the improved start, how far its final positions are from the
-    reference start's."""
+    start (fs_set_start_order 2, fs_set_tension_extrapolation 1) four more times:
+    alone, with precision escalation (fs_set_precision_escalation), with the
+    Broyden memory (fs_set_broyden_memory), and with the memory and the velocity
+    predictor (fs_set_velocity_predictor); all with graph-captured steady steps.
+    Records per-step Broyden iterations, the status, the final barrier minimum
+    squared distance, the wall time of each run and, for the improved start, how
+    far its final positions are from the reference start's."""
     import numpy as np
     import torch
     from filsim_b200 import abi
@@ -620,17 +632,20 @@ def run_trajectory(args, rank, world):
     finals = {}
     esc = args.escalate if args.escalate > 0 else 15
     mem = args.memory if args.memory != MEMORY_OFF else MEMORY_DEFAULT
-    runs = (("mixed", abi.FS_PREC_FP32, 1, 2, 0, MEMORY_OFF),
-            ("mixed_improved_start", abi.FS_PREC_FP32, 2, 1, 0, MEMORY_OFF),
-            ("mixed_improved_start_escalated", abi.FS_PREC_FP32, 2, 1, esc, MEMORY_OFF),
-            ("mixed_improved_start_broyden_memory", abi.FS_PREC_FP32, 2, 1, 0, mem),
-            ("fp64", abi.FS_PREC_FP64, 1, 2, 0, MEMORY_OFF))
-    for name, prec, start, tension, after, memory in runs:
+    pw = args.velocity_predictor if args.velocity_predictor > 0 else PREDICTOR_DEFAULT
+    runs = (("mixed", abi.FS_PREC_FP32, 1, 2, 0, MEMORY_OFF, 0.0),
+            ("mixed_improved_start", abi.FS_PREC_FP32, 2, 1, 0, MEMORY_OFF, 0.0),
+            ("mixed_improved_start_escalated", abi.FS_PREC_FP32, 2, 1, esc, MEMORY_OFF, 0.0),
+            ("mixed_improved_start_broyden_memory", abi.FS_PREC_FP32, 2, 1, 0, mem, 0.0),
+            ("mixed_improved_start_memory_predictor", abi.FS_PREC_FP32, 2, 1, 0, mem, pw),
+            ("fp64", abi.FS_PREC_FP64, 1, 2, 0, MEMORY_OFF, 0.0))
+    for name, prec, start, tension, after, memory, weight in runs:
         ctx.set_precision(prec)
         ctx.set_start_order(start)
         ctx.set_tension_extrapolation(tension)
         ctx.set_precision_escalation(after)
         ctx.set_broyden_memory(*memory)
+        ctx.set_velocity_predictor(weight)
         sim = Simulation(ctx, susp.copy())
         torch.cuda.synchronize()
         t0 = time.time()
@@ -646,11 +661,14 @@ def run_trajectory(args, rank, world):
                      "wall_s": wall, "mobility_solves": int(d.mobility_solves), "clocks": clk.summary(),
                      "final_mean_z": float(X[:, 2].mean()), "escalated_iters": int(d.escalated_iters)}
         finals[name] = X.copy()
-    for name in ("mixed_improved_start", "mixed_improved_start_escalated", "mixed_improved_start_broyden_memory"):
+    for name in ("mixed_improved_start", "mixed_improved_start_escalated", "mixed_improved_start_broyden_memory",
+                 "mixed_improved_start_memory_predictor"):
         out[name]["start"] = start_label(2, 1)
         out[name]["final_max_dX_vs_mixed_over_dx"] = float(np.abs(finals[name] - finals["mixed"]).max() / p.dx)
     out["mixed_improved_start_escalated"]["escalate_after_iters"] = esc
     out["mixed_improved_start_broyden_memory"]["broyden_memory"] = memory_label(mem)
+    out["mixed_improved_start_memory_predictor"]["broyden_memory"] = memory_label(mem)
+    out["mixed_improved_start_memory_predictor"]["velocity_predictor"] = pw
     ctx.close()
     return out
 
@@ -737,7 +755,8 @@ def run_ensemble(args, rank, world):
     mine = partition_boxes(all_boxes, world)[rank]
     boxes = [all_boxes[i] for i in mine]
     ens = Ensemble(boxes, precision=abi.FS_PREC_FP32, start_order=args.start_order,
-                   tension_order=args.tension_order, escalate=args.escalate, memory=args.memory)
+                   tension_order=args.tension_order, escalate=args.escalate, memory=args.memory,
+                   predictor=args.velocity_predictor)
     t0 = time.time()
     ens.startup(PREP_STEPS)
     t_start = time.time() - t0
@@ -782,7 +801,8 @@ def run_ensemble(args, rank, world):
                       "timed_steps": [nt0 + W, nt0 + W + K - 1], "start_up_seconds": t_start,
                       "l2": "no flush; most boxes fit in L2 (the workload's own sizes)",
                       "start": start_label(args.start_order, args.tension_order),
-                      "escalate_after_iters": args.escalate, "broyden_memory": memory_label(args.memory)},
+                      "escalate_after_iters": args.escalate, "broyden_memory": memory_label(args.memory),
+                      "velocity_predictor": args.velocity_predictor},
            "box_step_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99)),
                            "max": float(ms.max())},
            "iters_per_step": float(its.mean()), "status": abi.STATUS_NAMES.get(st, st),

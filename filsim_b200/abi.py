@@ -220,6 +220,7 @@ def _declare(L):
         "fs_set_tension_extrapolation": (c_int, [c_void_p, c_int]),
         "fs_set_precision_escalation": (c_int, [c_void_p, c_int]),
         "fs_set_broyden_memory": (c_int, [c_void_p, c_int, c_int, c_int, c_int]),
+        "fs_set_velocity_predictor": (c_int, [c_void_p, c_double]),
         "fs_warm_start_gate_margin": (c_int, [c_void_p, c_double]),
         "fs_warm_start_bound": (c_int, [c_void_p, c_int]),
         "fs_set_slab": (c_int, [c_void_p, c_int, c_int]),

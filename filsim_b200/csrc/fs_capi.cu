@@ -133,6 +133,7 @@ fs_status step_implicit(fs_ctx *c, int nt, int *iters_out, bool commit = true, i
   FS_TRY(fil_forces(c, nt));
   FS_TRY(fil_jacobian_build(c, nt, bmem_keep(c)));
   FS_TRY(cells_link(c, c->Xs, c->np));
+  if (!learned) FS_TRY(vpred_step(c, nt));
   if (learned) {
     FS_TRY(learn_warm_start(c, nt, barrier_and_mobility));
   } else {
@@ -184,6 +185,7 @@ fs_status step_implicit(fs_ctx *c, int nt, int *iters_out, bool commit = true, i
   if (commit) {
     FS_TRY(hist_end_step(c));  // only a step that moves X to Xt shifts the history
     FS_TRY(bmem_end_step(c, iter, nullptr));  // and carries Broyden columns
+    FS_TRY(vpred_end_step(c));
     FS_TRY(fil_step(c, nt));
   }
   c->diag.last_nt = nt;
@@ -323,6 +325,7 @@ fs_status fs_destroy(fs_ctx *c) {
   mlp_free(c);
   hist_free(c);
   bmem_free(c);
+  vpred_free(c);
   cudaFree(c->gemm_err);
   fcm_free(c);
   slab_free(c);
@@ -806,6 +809,7 @@ fs_status fs_step(fs_ctx *c, int nt) {
   if (!c->have_state) return FS_ERR_STATE;
   FS_TRY(learn_end_step(c));
   FS_TRY(hist_end_step(c));
+  FS_TRY(vpred_end_step(c));
   return fil_step(c, nt);
 }
 

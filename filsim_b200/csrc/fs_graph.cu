@@ -159,6 +159,7 @@ fs_status capture_step(fs_ctx *c, int nt, fs_graph *g, cudaGraph_t *out) {
   FS_TRY(fil_forces(c, nt));
   FS_TRY(fil_jacobian_build(c, nt, bmem_keep(c)));
   FS_TRY(cells_link(c, c->Xs, c->np));
+  FS_TRY(vpred_step(c, nt));
   FS_TRY(step_barrier_mobility(c, nt));
   FS_TRY(fil_error_check(c, c->V, c->W, c->err, nt));
   cudaGraphConditionalHandle h;
@@ -185,6 +186,7 @@ fs_status capture_step(fs_ctx *c, int nt, fs_graph *g, cudaGraph_t *out) {
   FS_TRY(learn_end_step(c));
   FS_TRY(hist_end_step(c));
   FS_TRY(bmem_end_step(c, 0, g->dev + GD_ITER));
+  FS_TRY(vpred_end_step(c));
   FS_TRY(fil_step(c, nt));
   k_step_done<<<1, 1, 0, c->stream>>>(g->dev, c->flags, GRAPH_STEP_SLOTS);
   FS_LAUNCH_CHECK();

@@ -140,6 +140,13 @@ struct fs_ctx {
   // device state (BM_COUNT ints, fs_bmem.cu)
   int bmem_keep, bmem_carry, bmem_thr, bmem_restart, bmem_cols, bmem_cap;
   int *bmem_d;
+  // velocity predictor (fs_set_velocity_predictor, fs_start.cu): the weight of its
+  // update (0: off), V, W of the last two converged states (vp_V1, vp_W1 the
+  // latest), the extrapolated V, W, and vp_ok (device): converged states recorded
+  // since the last reset, up to 2
+  double vpred_weight;
+  double *vp_V1, *vp_W1, *vp_V2, *vp_W2, *vp_Vs, *vp_Ws;
+  int *vp_ok;
   // positions two steps back (fs_start.cu), kept while the quadratic or the learned
   // start is on (3 max_beads doubles each); hist_ok (device): steps run since the
   // history was reset, up to 2 (hist_Xtt holds positions two steps back once it is
@@ -257,6 +264,11 @@ fs_status learn_warm_start(fs_ctx *c, int nt, fs_status (*solve)(fs_ctx *, int))
 fs_status learn_diag_apply(fs_ctx *c, const double *b, double *x);
 fs_status learn_capture_targets(fs_ctx *c, int iters);
 fs_status learn_end_step(fs_ctx *c);
+// velocity predictor (fs_start.cu): the predicted update before a step's first
+// residual; the shift of the velocity history after a committed step
+fs_status vpred_step(fs_ctx *c, int nt);
+fs_status vpred_end_step(fs_ctx *c);
+void vpred_free(fs_ctx *c);
 bool hist_wanted(const fs_ctx *c);
 fs_status hist_ensure(fs_ctx *c);
 void hist_free(fs_ctx *c);

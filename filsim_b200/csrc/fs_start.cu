@@ -35,19 +35,84 @@ __global__ void k_hist_tick(int *ok) {
   if (*ok < 2) ++*ok;
 }
 
-// the history and the carried Broyden columns survive an upload only if X and Xt
-// are unchanged
+// the history, the carried Broyden columns and the velocity history survive an
+// upload only if X and Xt are unchanged
 __global__ void k_hist_same(size_t n, const double *__restrict__ X, const double *__restrict__ Xt,
                             const double *__restrict__ pX, const double *__restrict__ pXt, int *__restrict__ ok,
-                            int *__restrict__ carried) {
+                            int *__restrict__ carried, int *__restrict__ vp_ok) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n && (X[i] != pX[i] || Xt[i] != pXt[i])) {
     *ok = 0;
     if (carried) bmem_drop(carried);
+    if (vp_ok) *vp_ok = 0;
   }
 }
 
+// V*, W* = 2 V1 - V2, 2 W1 - W2 (rounded as written)
+__global__ void k_vpred_extrap(size_t n, const double *__restrict__ V1, const double *__restrict__ V2,
+                               const double *__restrict__ W1, const double *__restrict__ W2, double *__restrict__ Vs,
+                               double *__restrict__ Ws) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Vs[i] = __dsub_rn(__dmul_rn(2.0, V1[i]), V2[i]);
+  Ws[i] = __dsub_rn(__dmul_rn(2.0, W1[i]), W2[i]);
+}
+
+// the predicted residual times the weight; without two recorded states zero, so
+// that the update is zero and leaves the state bitwise as it was
+__global__ void k_vpred_gate(size_t n, const int *__restrict__ ok, double weight, double *__restrict__ err) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) err[i] = *ok < 2 ? 0.0 : weight * err[i];
+}
+
 }  // namespace
+
+// ---- velocity predictor ------------------------------------------------------------
+// The step's first residual needs a mobility solve at the initial guess. With the
+// predictor on, the step first takes one Broyden update from the residual with the
+// velocities extrapolated from the last two converged states, V* = 2 V1 - V2
+// (W alike), no solve: x <- x - w H E(x; V*, W*), w the weight, H the iteration's
+// current inverse Jacobian (J0^-1 and any carried Broyden columns), then the forces
+// at the new iterate; the iteration proper starts there. The update adds no history
+// column and counts as no iteration; the convergence test is unchanged.
+fs_status vpred_step(fs_ctx *c, int nt) {
+  if (c->vpred_weight == 0.0) return FS_OK;
+  const size_t n3 = (size_t)3 * c->np, n6 = 2 * n3;
+  if (n3 == 0) return FS_OK;
+  k_vpred_extrap<<<fs_blocks((long long)n3, 256), 256, 0, c->stream>>>(n3, c->vp_V1, c->vp_V2, c->vp_W1, c->vp_W2,
+                                                                      c->vp_Vs, c->vp_Ws);
+  FS_LAUNCH_CHECK();
+  FS_TRY(fil_error_check(c, c->vp_Vs, c->vp_Ws, c->err, nt));
+  k_vpred_gate<<<fs_blocks((long long)n6, 256), 256, 0, c->stream>>>(n6, c->vp_ok, c->vpred_weight, c->err);
+  FS_LAUNCH_CHECK();
+  FS_TRY(fil_broyden_apply(c, c->err, c->upd, 0, nullptr, bmem_off(c)));
+  FS_TRY(fil_state_update(c, c->upd));
+  return fil_forces(c, nt);
+}
+
+// after a committed step (host-driven and captured): the converged state's V, W
+fs_status vpred_end_step(fs_ctx *c) {
+  if (c->vpred_weight == 0.0 || c->np == 0) return FS_OK;
+  const size_t b = sizeof(double) * 3 * (size_t)c->np;
+  FS_CUDA(cudaMemcpyAsync(c->vp_V2, c->vp_V1, b, cudaMemcpyDeviceToDevice, c->stream));
+  FS_CUDA(cudaMemcpyAsync(c->vp_W2, c->vp_W1, b, cudaMemcpyDeviceToDevice, c->stream));
+  FS_CUDA(cudaMemcpyAsync(c->vp_V1, c->V, b, cudaMemcpyDeviceToDevice, c->stream));
+  FS_CUDA(cudaMemcpyAsync(c->vp_W1, c->W, b, cudaMemcpyDeviceToDevice, c->stream));
+  k_hist_tick<<<1, 1, 0, c->stream>>>(c->vp_ok);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+void vpred_free(fs_ctx *c) {
+  double **arrs[6] = {&c->vp_V1, &c->vp_W1, &c->vp_V2, &c->vp_W2, &c->vp_Vs, &c->vp_Ws};
+  if (c->vp_V1) c->bytes -= 6 * sizeof(double) * 3 * (size_t)(c->max_beads > 0 ? c->max_beads : 1) + sizeof(int);
+  for (double **a : arrs) {
+    cudaFree(*a);
+    *a = nullptr;
+  }
+  cudaFree(c->vp_ok);
+  c->vp_ok = nullptr;
+}
 
 bool hist_wanted(const fs_ctx *c) { return c->mlp != nullptr || c->start_order == 2; }
 
@@ -106,6 +171,7 @@ fs_status hist_before_upload(fs_ctx *c, bool same_layout) {
   if (!c->hist_Xtt || (same_layout && c->np == 0)) return FS_OK;  // no beads: nothing to compare
   if (!same_layout) {
     FS_CUDA(cudaMemsetAsync(c->hist_ok, 0, sizeof(int), c->stream));
+    if (c->vp_ok) FS_CUDA(cudaMemsetAsync(c->vp_ok, 0, sizeof(int), c->stream));
     return bmem_reset(c);
   }
   const size_t b = sizeof(double) * 3 * (size_t)c->np;
@@ -120,7 +186,7 @@ fs_status hist_after_upload(fs_ctx *c) {
   c->hist_cmp_pending = false;
   const size_t n = (size_t)3 * c->np;
   k_hist_same<<<fs_blocks((long long)n, 256), 256, 0, c->stream>>>(n, c->X, c->Xt, c->hist_pX, c->hist_pXt,
-                                                                  c->hist_ok, c->bmem_d);
+                                                                  c->hist_ok, c->bmem_d, c->vp_ok);
   FS_LAUNCH_CHECK();
   return FS_OK;
 }
@@ -134,6 +200,35 @@ fs_status fs_set_start_order(fs_ctx *c, int order) {
   // a history no longer kept would go stale
   if (!hist_wanted(c) && c->hist_ok) FS_CUDA(cudaMemsetAsync(c->hist_ok, 0, sizeof(int), c->stream));
   graph_invalidate(c);  // captured steps bake the start
+  return FS_OK;
+}
+
+fs_status fs_set_velocity_predictor(fs_ctx *c, double weight) {
+  if (!c || !(weight >= 0.0 && weight <= 2.0)) return FS_ERR_INVALID_ARG;
+  const bool on = weight > 0.0;
+  if (on && !c->vp_V1) {
+    const size_t n = (size_t)3 * (c->max_beads > 0 ? c->max_beads : 1);
+    double **arrs[6] = {&c->vp_V1, &c->vp_W1, &c->vp_V2, &c->vp_W2, &c->vp_Vs, &c->vp_Ws};
+    cudaError_t e = cudaSuccess;
+    for (double **a : arrs)
+      if (e == cudaSuccess) e = cudaMalloc(a, sizeof(double) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&c->vp_ok, sizeof(int));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      for (double **a : arrs) {
+        cudaFree(*a);
+        *a = nullptr;
+      }
+      cudaFree(c->vp_ok);
+      c->vp_ok = nullptr;
+      return e == cudaErrorMemoryAllocation ? FS_ERR_OOM : FS_ERR_CUDA;
+    }
+    c->bytes += 6 * sizeof(double) * n + sizeof(int);
+    FS_TRY(hist_ensure(c));  // an upload compares X and Xt
+  }
+  if (c->vp_ok) FS_CUDA(cudaMemsetAsync(c->vp_ok, 0, sizeof(int), c->stream));
+  c->vpred_weight = weight;
+  graph_invalidate(c);  // captured steps bake the predictor
   return FS_OK;
 }
 

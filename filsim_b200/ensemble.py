@@ -77,7 +77,7 @@ class Ensemble:
     """One context per box, all advanced by fs_batch_run."""
 
     def __init__(self, boxes, precision=abi.FS_PREC_FP32, start_order=1, tension_order=2, escalate=0,
-                 memory=None):
+                 memory=None, predictor=0.0):
         self.boxes = boxes
         self.ctxs, self.sims = [], []
         for npts, p, s, kb in boxes:
@@ -88,6 +88,7 @@ class Ensemble:
             c.set_precision_escalation(escalate)
             if memory is not None:
                 c.set_broyden_memory(*memory)  # (keep, carry, threshold, restart): fs_set_broyden_memory
+            c.set_velocity_predictor(predictor)
             check(lib().fs_set_graph_mode(c.h, 1), "fs_set_graph_mode")
             self.ctxs.append(c)
             self.sims.append(Simulation(c, s))

@@ -94,6 +94,12 @@ class Context:
         check(lib().fs_set_broyden_memory(self.h, keep_columns, carry_columns, threshold, restart_after),
               "fs_set_broyden_memory")
 
+    def set_velocity_predictor(self, weight):
+        """Before each step's first residual, one Broyden update of the given weight
+        from the residual with V, W extrapolated from the last two converged states
+        (no solve); 0 turns it off."""
+        check(lib().fs_set_velocity_predictor(self.h, float(weight)), "fs_set_velocity_predictor")
+
     def set_precision_escalation(self, after_iters):
         """FP32 steps still not converged after after_iters Broyden iterations run the
         rest of their iterations with the FP64 chain; 0 turns it off."""

@@ -504,6 +504,17 @@ fs_status fs_set_start_order(fs_ctx *ctx, int order);
  * noise, which the quadratic extrapolation amplifies up to 7x and the linear one
  * up to 3x. The Broyden loop and its convergence test are unchanged. */
 fs_status fs_set_tension_extrapolation(fs_ctx *ctx, int order);
+/* Velocity predictor (no reference counterpart): with weight w > 0 each implicit
+ * step, before its first residual (which needs a mobility solve), takes one
+ * Broyden update x <- x - w H E(x; V*, W*) from the residual evaluated with the
+ * velocities extrapolated from the last two converged states, V* = 2 V1 - V2 and
+ * W* = 2 W1 - W2: no solve. H is the iteration's inverse Jacobian at that point
+ * (J0^-1 and any Broyden columns the memory carried). The iteration proper starts
+ * at the updated iterate; the update adds no history column and counts as no
+ * iteration, and the convergence test is unchanged. Without two converged states
+ * since creation, a layout change or an upload that changes X or Xt the update is
+ * zero. w in [0, 2]; 0 (the default) turns it off. */
+fs_status fs_set_velocity_predictor(fs_ctx *ctx, double weight);
 /* Broyden memory across steps (no reference counterpart). The reference starts
  * each step's iteration from J0^-1, the approximate inverse Jacobian of the
  * filaments without their hydrodynamic coupling, adds one rank-one "bad Broyden"

@@ -47,6 +47,10 @@ class Context {
   void set_tension_extrapolation(int order) {
     check(fs_set_tension_extrapolation(ctx_, order), "fs_set_tension_extrapolation");
   }
+  // one predicted Broyden update of this weight before each step's first residual (0: off)
+  void set_velocity_predictor(double weight) {
+    check(fs_set_velocity_predictor(ctx_, weight), "fs_set_velocity_predictor");
+  }
   // Broyden memory across steps (fs_set_broyden_memory; all zero: off)
   void set_broyden_memory(int keep_columns, int carry_columns, int threshold, int restart_after) {
     check(fs_set_broyden_memory(ctx_, keep_columns, carry_columns, threshold, restart_after),
