@@ -306,6 +306,27 @@ def test_reference_default_stencil_ngd20(oracle, gpu_lib, shape, nfil, nw, seed)
     assert rel_err(W32, W) < FP32_REL
 
 
+@pytest.mark.parametrize("ngd", [11, 13])
+def test_odd_stencil_widths(oracle, gpu_lib, ngd):
+    """Odd ngd (the stencil starts ngd/2 - 1 points below the bead's cell, as in
+    gaussian_setup): FP64 within 1e-10 of the oracle and FP32 within 1e-5 of FP64,
+    with several interpolation warps per CTA (each warp's tables keep their
+    alignment for odd ngd^2)."""
+    from filsim_b200.abi import make_params
+    from filsim_b200.suspension import random_forces, random_suspension, fcm_positions
+    p = make_params((32, 32, 48), ngd=ngd)
+    s = random_suspension(p, 6, 3, 51, min_sep=1.5)
+    F, T = random_forces(s.np, 52)
+    Y = fcm_positions(p, s.X)
+    V0, W0 = oracle.fcm_mobility(p, Y, F, T)
+    V, W = gpu_mobility(p, Y, F, T)
+    assert rel_err(V, V0) < FP64_REL
+    assert rel_err(W, W0) < FP64_REL
+    V32, W32 = gpu_mobility(p, Y, F, T, abi.FS_PREC_FP32)
+    assert rel_err(V32, V) < FP32_REL
+    assert rel_err(W32, W) < FP32_REL
+
+
 def test_stencil_limits_are_checked(gpu_lib):
     """ngd above 20, or above a grid dimension, is rejected at context creation."""
     from filsim_b200.abi import FsError, make_params
