@@ -778,6 +778,151 @@ __global__ void __launch_bounds__(32 * WPB) k_interp(const R *__restrict__ u, co
 }
 
 
+// FP32 interpolation with float4 gathers along z. The stencil's z run of ngd
+// points starting at zs lies in nq = ceil(((zs & 3) + ngd) / 4) aligned quads of
+// four points (a quad's first index is a multiple of 4; with Nz a multiple of 4 and
+// Nz >= ngd + 6 the quads of one run are distinct modulo Nz). A lane takes (ij,
+// quad) slots: one 16-byte load per component instead of four 4-byte ones, z weights
+// per quad position (zero off the run), the quad's four products summed in FP32
+// and the sum added in FP64. The products are k_interp<float>'s.
+constexpr int IQ_MAX = (FS_NGD_MAX + 6) / 4;  // quads a z run of ngd points can touch
+struct InterpQuad {
+  float4 wg[IQ_MAX], wd[IQ_MAX], wr[IQ_MAX];  // g, gd, r of the quad's four points (0 off the run)
+  int zq[IQ_MAX];                              // the quad's first z index
+};
+__host__ __device__ constexpr size_t interp_q_quad_offset() { return (sizeof(InterpWarp<float>) + 15) / 16 * 16; }
+__host__ __device__ constexpr size_t interp_q_xy_offset() {
+  return (interp_q_quad_offset() + sizeof(InterpQuad) + 15) / 16 * 16;
+}
+__host__ __device__ constexpr size_t interp_q_warp_bytes(int ngd) {
+  return (interp_q_xy_offset() + (size_t)ngd * ngd * (sizeof(XY4<float>) + sizeof(long long)) + 31) / 32 * 32;
+}
+inline bool interp_q_ok(const fs_ctx *c) { return c->nz % 4 == 0 && c->nz >= c->p.ngd + 6; }
+
+template <int WPB>
+__global__ void __launch_bounds__(32 * WPB) k_interp_q(const float *__restrict__ u, const double *__restrict__ Y,
+                                                       const int *__restrict__ order, const int *__restrict__ bead_sw,
+                                                       int np, FcmConsts c, double *__restrict__ V,
+                                                       double *__restrict__ W) {
+  extern __shared__ __align__(32) unsigned char interp_smem[];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int wid = blockIdx.x * WPB + wl;
+  if (wid >= np) return;
+  const int b = order[wid];
+  const int ngd = c.ngd, n2 = ngd * ngd, Nz = c.N[2];
+  unsigned char *base = interp_smem + (size_t)wl * interp_q_warp_bytes(ngd);
+  InterpWarp<float> &s = *reinterpret_cast<InterpWarp<float> *>(base);
+  InterpQuad &q = *reinterpret_cast<InterpQuad *>(base + interp_q_quad_offset());
+  XY4<float> *xy = reinterpret_cast<XY4<float> *>(base + interp_q_xy_offset());
+  long long *off = reinterpret_cast<long long *>(xy + n2);
+  for (int a = 0; a < 3; ++a) {  // lane i < ngd takes stencil index i of each axis (as k_interp)
+    const int i = lane;
+    if (i >= ngd) continue;
+    const double Yv = Y[3 * b + a];
+    const int xc = (int)(Yv / c.dx);
+    const int xg = xc - c.ngdh + (i + 1);
+    const int ix = bead_sw[3 * b + a] + i;
+    s.ind[a][i] = ix >= c.N[a] ? ix - c.N[a] : ix;
+    const double xx = ((double)xg) * c.dx - Yv;
+    const float xf = (float)xx;
+    s.g[a][i] = (float)c.anorm * fs_exp<float>(-xf * xf / (float)c.anorm2);
+    s.gd[a][i] = (float)c.anormdip * fs_exp<float>(-xf * xf / (float)c.anormdip2);
+    s.r[a][i] = -xf / (float)c.sigmadipsq;
+  }
+  __syncwarp();
+  const int zs = s.ind[2][0];
+  const int nq = ((zs & 3) + ngd + 3) >> 2;
+  if (lane < nq) {
+    int z0 = (zs & ~3) + 4 * lane;
+    if (z0 >= Nz) z0 -= Nz;
+    float w[3][4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      int k = z0 + t - zs;
+      if (k < 0) k += Nz;
+      const bool on = k < ngd;
+      const int kk = on ? k : 0;  // the tables are read only inside the run
+      w[0][t] = on ? s.g[2][kk] : 0.f;
+      w[1][t] = on ? s.gd[2][kk] : 0.f;
+      w[2][t] = on ? s.r[2][kk] : 0.f;
+    }
+    q.wg[lane] = make_float4(w[0][0], w[0][1], w[0][2], w[0][3]);
+    q.wd[lane] = make_float4(w[1][0], w[1][1], w[1][2], w[1][3]);
+    q.wr[lane] = make_float4(w[2][0], w[2][1], w[2][2], w[2][3]);
+    q.zq[lane] = z0;
+  }
+  for (int ij = lane; ij < n2; ij += 32) {
+    const int i = ij / ngd, j = ij - i * ngd;
+    XY4<float> e;
+    e.gg = s.g[0][i] * s.g[1][j];
+    e.dd = s.gd[0][i] * s.gd[1][j];
+    e.rx = s.r[0][i];
+    e.ry = s.r[1][j];
+    xy[ij] = e;
+    off[ij] = ((long long)s.ind[0][i] * c.N[1] + s.ind[1][j]) * Nz;
+  }
+  __syncwarp();
+  const size_t N = (size_t)c.N[0] * c.N[1] * Nz;
+  const float *ux = u, *uy = u + N, *uz = u + 2 * N;
+  double v0 = 0, v1 = 0, v2 = 0, w0 = 0, w1 = 0, w2 = 0;
+  // slot sl = ij * nq + qi; a step of 32 slots advances (ij, qi) by (32 / nq, 32 % nq)
+  const int nslot = n2 * nq, dij = 32 / nq, dq = 32 - dij * nq;
+  int ij = lane / nq, qi = lane - ij * nq;
+  for (int sl = lane; sl < nslot; sl += 32) {
+    const XY4<float> e = xy[ij];
+    const long long m = off[ij] + q.zq[qi];
+    const float4 a0 = __ldg(reinterpret_cast<const float4 *>(ux + m));
+    const float4 a1 = __ldg(reinterpret_cast<const float4 *>(uy + m));
+    const float4 a2 = __ldg(reinterpret_cast<const float4 *>(uz + m));
+    const float4 g = q.wg[qi], gd = q.wd[qi], r = q.wr[qi];
+    float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f, p4 = 0.f, p5 = 0.f;
+    auto acc = [&](float x0, float x1, float x2, float gz, float gdz, float zz) {
+      const float temp = e.gg * gz;  // (gx gy) gz, the reference's order
+      const float tempd = e.dd * gdz;
+      p0 += x0 * temp;
+      p1 += x1 * temp;
+      p2 += x2 * temp;
+      p3 += (x2 * e.ry - x1 * zz) * tempd;
+      p4 += (x0 * zz - x2 * e.rx) * tempd;
+      p5 += (x1 * e.rx - x0 * e.ry) * tempd;
+    };
+    acc(a0.x, a1.x, a2.x, g.x, gd.x, r.x);
+    acc(a0.y, a1.y, a2.y, g.y, gd.y, r.y);
+    acc(a0.z, a1.z, a2.z, g.z, gd.z, r.z);
+    acc(a0.w, a1.w, a2.w, g.w, gd.w, r.w);
+    v0 += (double)p0;
+    v1 += (double)p1;
+    v2 += (double)p2;
+    w0 += (double)p3;
+    w1 += (double)p4;
+    w2 += (double)p5;
+    qi += dq;
+    ij += dij;
+    if (qi >= nq) {
+      qi -= nq;
+      ++ij;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+    v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+    v2 += __shfl_xor_sync(0xffffffffu, v2, o);
+    w0 += __shfl_xor_sync(0xffffffffu, w0, o);
+    w1 += __shfl_xor_sync(0xffffffffu, w1, o);
+    w2 += __shfl_xor_sync(0xffffffffu, w2, o);
+  }
+  if (lane == 0) {
+    const double norm = c.dx * c.dx * c.dx;
+    V[3 * b + 0] = v0 * norm;
+    V[3 * b + 1] = v1 * norm;
+    V[3 * b + 2] = v2 * norm;
+    W[3 * b + 0] = -0.5 * w0 * norm;
+    W[3 * b + 1] = -0.5 * w1 * norm;
+    W[3 * b + 2] = -0.5 * w2 * norm;
+  }
+}
+
 template <typename A, typename B>
 __global__ void k_convert(const A *__restrict__ in, B *__restrict__ out, size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -922,6 +1067,20 @@ fs_status interp_t(fs_ctx *c, const FcmConsts &k, const double *Y, double *V, do
   ProfScope ps(c, FS_STAGE_INTERP);
   ProfScope pk(c, FS_STAGE_K_INTERP);
   const R *ug = (const R *)c->grid_real;
+  if constexpr (sizeof(R) == 4) {
+    if (interp_q_ok(c)) {  // float4 gathers along z
+      const size_t wq = interp_q_warp_bytes(c->p.ngd);
+      const int wpb = (c->tune_interp_wpb == 16 && 16 * wq > FS_SMEM_MAX) ? 8 : c->tune_interp_wpb;
+      if (wpb == 4)
+        k_interp_q<4><<<fs_blocks(np, 4), 128, 4 * wq, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V, W);
+      else if (wpb == 16)
+        k_interp_q<16><<<fs_blocks(np, 16), 512, 16 * wq, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V, W);
+      else
+        k_interp_q<8><<<fs_blocks(np, 8), 256, 8 * wq, c->stream>>>(ug, Y, c->bins.sorted, c->bead_sw, np, k, V, W);
+      FS_LAUNCH_CHECK();
+      return FS_OK;
+    }
+  }
   const size_t wb = interp_warp_bytes<R>(c->p.ngd);
   const int wpb = (c->tune_interp_wpb == 16 && 16 * wb > FS_SMEM_MAX) ? 8 : c->tune_interp_wpb;
   if (wpb == 4)
@@ -1002,6 +1161,10 @@ fs_status fcm_init(fs_ctx *c) {
     FS_CUDA(cudaFuncSetAttribute(k_interp<float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap(4 * wf)));
     FS_CUDA(cudaFuncSetAttribute(k_interp<float, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap(8 * wf)));
     FS_CUDA(cudaFuncSetAttribute(k_interp<float, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap(16 * wf)));
+    const size_t wq = interp_q_warp_bytes(FS_NGD_MAX);
+    FS_CUDA(cudaFuncSetAttribute(k_interp_q<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap(4 * wq)));
+    FS_CUDA(cudaFuncSetAttribute(k_interp_q<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap(8 * wq)));
+    FS_CUDA(cudaFuncSetAttribute(k_interp_q<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap(16 * wq)));
   }
   c->tune_spread_chunk = 64;
   c->tune_spread_cols = 2;  // 2 x 16 x 8 blocks: fs_autotune's choice at 384^3 and 512^3
