@@ -44,6 +44,7 @@ struct GemmArgs {
 namespace fsg {
 
 constexpr int BM = 128, BK = 64, STAGES = 3, THREADS = 128;
+constexpr int GEMM_GROUP_M = 32;  // rows of tiles per group of the tile order
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -141,7 +142,15 @@ __global__ void __launch_bounds__(THREADS)
   __shared__ int s_fail, s_issued;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t base = (smem_u32(gemm_smem_raw) + 1023u) & ~1023u;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  // tiles in groups of GEMM_GROUP_M rows of tiles, walked column by column inside a
+  // group: the CTAs resident at one time share a few A panels and a band of B
+  // panels, which stay in L2 (block x fastest would sweep every A panel per column)
+  const int ntm = gridDim.x, ntn = gridDim.y;
+  const int lin = blockIdx.x + blockIdx.y * ntm;
+  const int per_group = GEMM_GROUP_M * ntn, grp = lin / per_group;
+  const int first_m = grp * GEMM_GROUP_M, gsize = min(ntm - first_m, GEMM_GROUP_M);
+  const int in_grp = lin - grp * per_group;
+  const int m0 = (first_m + in_grp % gsize) * BM, n0 = (in_grp / gsize) * BN;
   if (tid == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(smem_u32(&full[s]), 1);
