@@ -80,18 +80,18 @@ GATE_PERIOD = 8  # the learned start's cost gate: first probe of the other start
 BOUND_REFRESH = 8  # learned steps between comparisons with the plain start (fs_warm_start_bound)
 ENSEMBLE_SEED = 3000
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the FCM
-# kernels, per grid point: the mean over the 13 launches of each in one timed step
-# of the 512^3 workload under ncu (a one-pass metric set), FP32 chain, plain start.
+# kernels, per grid point: the mean over the launches of each in one timed step of
+# each FP32 arm of the 512^3 workload under ncu (a one-pass metric set).
 NCU_TRAFFIC_PER_POINT = {
-    "k_spread": (163.39e6 + 1600.56e6) / 512 ** 3,
-    "k_fft_z_fwd": (1610.73e6 + 1566.82e6) / 512 ** 3,
-    "k_fft_y_fwd": (1616.95e6 + 1565.75e6) / 512 ** 3,
-    "project": (1617.04e6 + 1553.08e6) / 512 ** 3,
-    "k_fft_y_inv": (1617.00e6 + 1565.84e6) / 512 ** 3,
-    "k_fft_z_inv": (1616.98e6 + 1562.83e6) / 512 ** 3,
-    "k_interp": (1553.40e6 + 6.13e6) / 512 ** 3,
+    "k_spread": (93.28e6 + 1553.20e6) / 512 ** 3,
+    "k_fft_z_fwd": (1610.70e6 + 1564.94e6) / 512 ** 3,
+    "k_fft_y_fwd": (1616.96e6 + 1565.83e6) / 512 ** 3,
+    "project": (1617.05e6 + 1553.13e6) / 512 ** 3,
+    "k_fft_y_inv": (1617.06e6 + 1565.69e6) / 512 ** 3,
+    "k_fft_z_inv": (1617.00e6 + 1562.84e6) / 512 ** 3,
+    "k_interp": (1557.31e6 + 6.21e6) / 512 ** 3,
 }
-NCU_TRAFFIC_SOURCE = "ncu capture of one timed step at 512^3 (13 launches per kernel), per grid point"
+NCU_TRAFFIC_SOURCE = "ncu capture of one timed step of each FP32 arm at 512^3 (17 launches per kernel), per grid point"
 
 
 def start_label(start, tension):
